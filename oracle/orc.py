@@ -1,0 +1,295 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY: ctypes access to the CPU checkers.
+
+  Oracle  -- the C restatement (oracle/_build/liboracle.so, qb_oracle.c),
+             run-time grid size N.
+  Ref     -- the unmodified upstream C sources compiled with the project's CPU
+             FFTW-API shim (oracle/_ref/libqbref_n32.so, N = 32), present
+             only where the upstream checkout existed at build time.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  Arrays are numpy: complex grids complex128 of shape (..., N, N)
+(element (l, k) = [l, k], the upstream index k + N*l), real grids float64.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libqbref_n32.so")
+
+_dp = C.POINTER(C.c_double)
+
+
+def build():
+    """Compile the checkers with oracle/Makefile (restatement always, upstream
+    sources when their checkout exists)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _ptr(a):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _c(a):
+    """complex128 C-contiguous copy/view"""
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _r(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class _Quad(C.Structure):
+    _fields_ = [("N", C.c_int), ("J", C.c_int), ("M", C.c_int), ("L", C.c_double), ("R", C.c_double),
+                ("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int), ("n4", C.c_int)] + \
+               [(n, _dp) for n in ("i1r1", "i1r2", "i2r1", "i2r2", "i3r1", "i3r2", "i4r1", "i4r2")]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_quad_create.restype = C.POINTER(_Quad)
+        L.orc_quad_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.orc_flux_right.restype = C.c_double
+        L.orc_flux_left.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """Quadrature tables for (N, J, M, L, R) plus the restated operators."""
+
+    def __init__(self, N, J, M, L, R):
+        self.N, self.J, self.M, self.L, self.R = N, J, M, L, R
+        self.q = lib().orc_quad_create(N, J, M, L, R)
+
+    def __del__(self):
+        if getattr(self, "q", None) is not None and _lib is not None:
+            _lib.orc_quad_free(self.q)
+            self.q = None
+
+    # tables as numpy views (copied)
+    def tables(self):
+        N, P, q = self.N, 2 * self.N, self.q.contents
+        def arr(p, n, shape, dt=np.float64):
+            a = np.ctypeslib.as_array(p, shape=(n,)).copy()
+            return a.view(dt).reshape(shape) if dt is not np.float64 else a.reshape(shape)
+        return {
+            "i1r1": arr(q.i1r1, q.n1 * P * P, (q.n1, P, P)), "i1r2": arr(q.i1r2, q.n1 * N * N, (q.n1, N, N)),
+            "i2r1": arr(q.i2r1, q.n2 * N * N, (q.n2, N, N)), "i2r2": arr(q.i2r2, q.n2 * N * N, (q.n2, N, N)),
+            "i3r1": np.ctypeslib.as_array(q.i3r1, shape=(q.n3 * 2 * N * N,)).copy().view(np.complex128).reshape(q.n3, N, N),
+            "i3r2": arr(q.i3r2, q.n3 * P * P, (q.n3, P, P)),
+            "i4r1": arr(q.i4r1, q.n4 * P * P, (q.n4, P, P)), "i4r2": arr(q.i4r2, q.n4 * N * N, (q.n4, N, N)),
+        }
+
+    def _int(self, fn, f, g, h, num, r1, r2):
+        out = np.zeros((self.N, self.N), np.complex128)
+        f, g, h = _c(f), _c(g), _c(h)
+        fn(self.N, _ptr(f), _ptr(g), _ptr(h), num, r1, r2, _ptr(out))
+        return out
+
+    def i1(self, f, g, h):
+        q = self.q.contents
+        return self._int(lib().orc_i1, f, g, h, q.n1, q.i1r1, q.i1r2)
+
+    def i4(self, f, g, h):
+        q = self.q.contents
+        return self._int(lib().orc_i1, f, g, h, q.n4, q.i4r1, q.i4r2)
+
+    def i2(self, f, g, h):
+        q = self.q.contents
+        return self._int(lib().orc_i2, f, g, h, q.n2, q.i2r1, q.i2r2)
+
+    def i3(self, f, g, h):
+        q = self.q.contents
+        return self._int(lib().orc_i3, f, g, h, q.n3, q.i3r1, q.i3r2)
+
+    def cc(self, W):
+        W = _c(W); out = np.zeros_like(W)
+        lib().orc_cc(self.q, _ptr(W), _ptr(out)); return out
+
+    def cd(self, W):
+        W = _c(W); out = np.zeros_like(W)
+        lib().orc_cd(self.q, _ptr(W), _ptr(out)); return out
+
+    def collision_step(self, W, dt, B=(0.0, 0.0, 0.0), rk4=False):
+        W = _c(W); out = np.zeros_like(W); Bv = _r(B)
+        fn = lib().orc_collision_step_rk4 if rk4 else lib().orc_collision_step
+        fn(self.q, _ptr(W), C.c_double(dt), _ptr(Bv), _ptr(out)); return out
+
+    def inhom_step(self, W, h, dt, Bext=None, bc="periodic"):
+        W = _r(W); n = W.shape[0]; out = np.zeros_like(W)
+        Bext = _r(np.zeros((n, 3)) if Bext is None else Bext)
+        lib().orc_inhom_step(self.q, 0 if bc == "periodic" else 1, n, _ptr(W), C.c_double(h), C.c_double(dt), _ptr(Bext), _ptr(out))
+        return out
+
+    def inhom_step_maxwell(self, W, h, dt, lam, WL, WR, Bext=None):
+        W = _r(W); n = W.shape[0]; out = np.zeros_like(W)
+        Bext = _r(np.zeros((n, 3)) if Bext is None else Bext)
+        WL, WR = _r(WL), _r(WR)
+        lib().orc_inhom_step_maxwell(self.q, n, _ptr(W), C.c_double(h), C.c_double(dt), C.c_double(lam),
+                                     _ptr(WL), _ptr(WR), _ptr(Bext), _ptr(out))
+        return out
+
+    def simulation_homogeneous(self, W0, dt, numsteps, B=(0.0, 0.0, 0.0)):
+        W0 = _r(W0); out = np.zeros((numsteps,) + W0.shape); Bv = _r(B)
+        lib().orc_simulation_homogeneous(self.q, _ptr(W0), C.c_double(dt), numsteps, _ptr(Bv), _ptr(out))
+        return out
+
+
+def i2_raw(N, f, g, h, psiR1, psiR2):
+    """I2 with caller-supplied tables (as test/I2_test.c builds them)."""
+    f, g, h, r1, r2 = _c(f), _c(g), _c(h), _r(psiR1), _r(psiR2)
+    out = np.zeros((N, N), np.complex128)
+    lib().orc_i2(N, _ptr(f), _ptr(g), _ptr(h), r1.shape[0], _ptr(r1), _ptr(r2), _ptr(out))
+    return out
+
+
+def lgwt(M, a, b):
+    x = np.zeros(M); w = np.zeros(M)
+    lib().orc_lgwt(M, C.c_double(a), C.c_double(b), _ptr(x), _ptr(w))
+    return x, w
+
+
+def to_fourier(Wv):
+    Wv = _r(Wv); N = Wv.shape[-1]; cells = Wv.size // (4 * N * N)
+    out = np.zeros(Wv.shape, np.complex128)
+    lib().orc_to_fourier(N, cells, _ptr(Wv), _ptr(out)); return out
+
+
+def from_fourier(Wf):
+    Wf = _c(Wf); N = Wf.shape[-1]; cells = Wf.size // (4 * N * N)
+    out = np.zeros(Wf.shape, np.float64)
+    lib().orc_from_fourier(N, cells, _ptr(Wf), _ptr(out)); return out
+
+
+def slope_periodic(h, dt, A, Un):
+    Un = _r(Un); out = np.zeros_like(Un)
+    lib().orc_slope_periodic(C.c_double(h), C.c_double(dt), C.c_double(A), len(Un), _ptr(Un), _ptr(out)); return out
+
+
+def slope_dirichlet(h, dt, A, Un):
+    Un = _r(Un); out = np.zeros_like(Un)
+    lib().orc_slope_dirichlet(C.c_double(h), C.c_double(dt), C.c_double(A), len(Un), _ptr(Un), _ptr(out)); return out
+
+
+def slope_maxwell(h, dt, A, lam, fluxL, fluxR, UL, UR, Un):
+    """Un: (N, m) cell-major, i.e. the upstream m x N matrix Un[i + m*j]."""
+    A, UL, UR, Un = _r(A), _r(UL), _r(UR), _r(Un)
+    out = np.zeros_like(Un)
+    lib().orc_slope_maxwell(C.c_double(h), C.c_double(dt), len(A), _ptr(A), Un.shape[0], C.c_double(lam),
+                            C.c_double(fluxL), C.c_double(fluxR), _ptr(UL), _ptr(UR), _ptr(Un), _ptr(out))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The upstream sources themselves (N = 32), when built.
+
+_ref = None
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            return None
+        L = C.CDLL(REF_SO)
+        L.ref_ctx_create.restype = C.c_void_p
+        L.ref_ctx_create.argtypes = [C.c_uint, C.c_uint, C.c_double, C.c_double]
+        for n in ("ref_ctx_free", "ref_table_num", "ref_table_copy", "ref_i1", "ref_i2", "ref_i3", "ref_cc", "ref_cd",
+                  "ref_collision_step", "ref_inhom_step", "ref_inhom_step_maxwell", "ref_sim_hom"):
+            getattr(L, n).argtypes = None
+        L.ref_table_num.restype = C.c_uint
+        L.CalculateRightwardFlux.restype = C.c_double
+        L.CalculateLeftwardFlux.restype = C.c_double
+        _ref = L
+    return _ref
+
+
+class Ref:
+    """The upstream C functions at N = 32 with tables from the upstream builders."""
+    N = 32
+
+    def __init__(self, J, M, L, R):
+        self.J, self.M, self.L, self.R = J, M, L, R
+        self.h = C.c_void_p(ref_lib().ref_ctx_create(J, M, L, R))
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _ref is not None:
+            _ref.ref_ctx_free(self.h)
+            self.h = None
+
+    def table(self, which, part):
+        N, P = self.N, 2 * self.N
+        num = ref_lib().ref_table_num(self.h, which)
+        shapes = {(1, 1): (num, P, P), (1, 2): (num, N, N), (2, 1): (num, N, N), (2, 2): (num, N, N),
+                  (3, 1): (num, N, N, 2), (3, 2): (num, P, P), (4, 1): (num, P, P), (4, 2): (num, N, N)}
+        a = np.zeros(shapes[(which, part)])
+        ref_lib().ref_table_copy(self.h, which, part, _ptr(a))
+        return a.view(np.complex128)[..., 0] if which == 3 and part == 1 else a
+
+    def _int(self, fn, *args):
+        args = [_c(a) for a in args]
+        out = np.zeros((self.N, self.N), np.complex128)
+        fn(self.h, *[_ptr(a) for a in args], _ptr(out))
+        return out
+
+    def i1(self, f, g, h):
+        return self._int(lambda hh, *p: ref_lib().ref_i1(hh, 1, *p), f, g, h)
+
+    def i4(self, f, g, h):
+        return self._int(lambda hh, *p: ref_lib().ref_i1(hh, 4, *p), f, g, h)
+
+    def i2(self, f, g, h):
+        return self._int(ref_lib().ref_i2, f, g, h)
+
+    def i3(self, f, g, h):
+        return self._int(ref_lib().ref_i3, f, g, h)
+
+    def cc(self, W):
+        W = _c(W); out = np.zeros_like(W); ref_lib().ref_cc(self.h, _ptr(W), _ptr(out)); return out
+
+    def cd(self, W):
+        W = _c(W); out = np.zeros_like(W); ref_lib().ref_cd(self.h, _ptr(W), _ptr(out)); return out
+
+    def collision_step(self, W, dt, B=(0.0, 0.0, 0.0)):
+        W = _c(W); out = np.zeros_like(W); Bv = _r(B)
+        ref_lib().ref_collision_step(self.h, _ptr(W), C.c_double(dt), _ptr(Bv), _ptr(out)); return out
+
+    def inhom_step(self, W, h, dt, Bext=None, bc="periodic"):
+        W = _r(W); n = W.shape[0]; out = np.zeros_like(W)
+        Bext = _r(np.zeros((n, 3)) if Bext is None else Bext)
+        ref_lib().ref_inhom_step(self.h, 0 if bc == "periodic" else 1, C.c_uint(n), C.c_double(self.L), _ptr(W),
+                                 C.c_double(h), C.c_double(dt), _ptr(Bext), _ptr(out))
+        return out
+
+    def inhom_step_maxwell(self, W, h, dt, lam, WL, WR, Bext=None):
+        W = _r(W); n = W.shape[0]; out = np.zeros_like(W)
+        Bext = _r(np.zeros((n, 3)) if Bext is None else Bext)
+        WL, WR = _r(WL), _r(WR)
+        ref_lib().ref_inhom_step_maxwell(self.h, C.c_uint(n), C.c_double(self.L), _ptr(W), C.c_double(h), C.c_double(dt),
+                                         C.c_double(lam), _ptr(WL), _ptr(WR), _ptr(Bext), _ptr(out))
+        return out
+
+    def simulation_homogeneous(self, W0, dt, numsteps, B=(0.0, 0.0, 0.0)):
+        W0 = _r(W0); out = np.zeros((numsteps,) + W0.shape); Bv = _r(B)
+        ref_lib().ref_sim_hom(self.h, _ptr(W0), C.c_double(dt), C.c_uint(numsteps), _ptr(Bv), _ptr(out)); return out
+
+
+def ref_to_fourier(Wv):
+    Wv = _r(Wv); out = np.zeros(Wv.shape, np.complex128)
+    ref_lib().ref_to_fourier(_ptr(Wv), _ptr(out)); return out

@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the collision + transport time step on B200.
+
+Workload (the metric's configuration): spatially inhomogeneous periodic run,
+64 x-cells on [0,1) per GPU, N = 32 velocity grid on [-6,6)^2 (L = 6,
+R = 3.75), J = 16 angles, M = 16 Gauss-Legendre radial nodes, h = 1/64,
+dt = 0.4 h / L (CFL 0.4), Bext = 0, FP64, seeded Gaussian-mixture initial
+state.  One step = one Strang step (1/2 transport, midpoint collision on
+every cell, 1/2 transport) = 2 cell-collision evaluations per cell.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched by torchrun) every rank owns 64 cells of a 64N-cell
+periodic domain (weak scaling) and exchanges 2-cell halos with its ring
+neighbours over NCCL before each half step of transport.
+
+value  : cell-collision evals/s, whole job, state resident in HBM, device-timed
+         (CUDA events per step, L2 flushed before each step, max over ranks)
+e2e    : same metric through the upstream C API (InhomStepPeriodic on host
+         buffers, H2D + D2H inside every step) at N = 1; through the sharded
+         step with host staging at N > 1
+--impl reference : the upstream C sources (compiled here with the project's
+         CPU FFTW-API shim) on the host cores, bounded sample per step.
+"""
+import argparse
+import importlib.util
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "inhom-quantum-boltzmann-fourier-c_b200")
+METRIC = "cell-collision evals/s & sim steps/s vs plain FP64 GPU at <=1e-5 rel err"
+UNIT = "cell-collision evals/s"
+
+
+def _import(name, path):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(args):
+    return dict(N=args.grid, J=args.J, M=args.M, L=6.0, R=3.75, cells=args.cells,
+                h=1.0 / args.cells, dt=0.4 * (1.0 / args.cells) / 6.0, seed=1)
+
+
+def config_json(wl, world, flush):
+    return {"workload": f"inhomogeneous periodic Strang step, {wl['cells']} x-cells per GPU, N={wl['N']} "
+                        f"(padded {2 * wl['N']}), J={wl['J']} angles, M={wl['M']} Gauss-Legendre nodes, "
+                        f"L={wl['L']}, R={wl['R']}, h=1/{wl['cells']}, dt=0.4h/L, midpoint collision, FP64",
+            "cells_per_gpu": wl["cells"], "cells_total": wl["cells"] * world, "N": wl["N"], "J": wl["J"], "M": wl["M"],
+            "parallelism": f"x-cells sharded over {world} GPU(s), 2-cell halo exchange" if world > 1 else "1 GPU",
+            "l2": flush}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the upstream C code (oracle/_ref) on the host cores
+
+def _ref_eval_worker(args):
+    """one cell-collision evaluation (CcInt + CdInt) of the upstream code"""
+    J, M, L, R, Wv = args
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import orc
+    r = orc.Ref(J, M, L, R)
+    WF = orc.ref_to_fourier(Wv)
+    t = time.perf_counter()
+    r.cc(WF)
+    r.cd(WF)
+    return time.perf_counter() - t
+
+
+def cpu_sample(wl, procs, seed_offset=0):
+    """bounded sample: `procs` processes each evaluate C[W] of one cell"""
+    qbgpu = _import("qbgpu", os.path.join(PKG, "qbgpu.py"))
+    W = qbgpu.gaussian_mixture_state(wl["N"], wl["L"], seed=wl["seed"], ncells=wl["cells"])
+    jobs = [(wl["J"], wl["M"], wl["L"], wl["R"], W[(i + seed_offset) % wl["cells"]]) for i in range(procs)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        pool.map(_ref_eval_worker, jobs)
+    wall = time.perf_counter() - t0
+    return procs / wall, wall
+
+
+def ref_kind():
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import orc
+    return "reference" if orc.ref_available() else None
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.p = None
+        self.path = os.path.join("/tmp", f"qb_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.p is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+
+def i3_flops_per_term(N):
+    """algorithmic FP64 flops of the I3 kernel per (cell, quadrature term):
+    4 padded spectra (0.75 of a full 2N x 2N FFT each: half the rows are zero)
+    + 16 (i, j) pairs x (IFFT2 + FFT2) at 5 n log2 n per transform, plus the
+    pointwise products (19 flops per padded point per pair, 6 per N-point
+    per source)."""
+    P = 2 * N
+    F = 5.0 * P * P * math.log2(P * P)
+    return 4 * 0.75 * F + 32 * F + 16 * 19 * P * P + 4 * 6 * N * N
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    qbgpu = _import("qbgpu", os.path.join(PKG, "qbgpu.py"))
+    qd = _import("qb_dist", os.path.join(PKG, "qb_dist.py"))
+    L = qbgpu.lib()
+    wl = workload(args)
+    N, cells = wl["N"], wl["cells"]
+
+    Wall = qbgpu.gaussian_mixture_state(N, wl["L"], seed=wl["seed"], ncells=cells * world)
+    W0 = torch.from_numpy(Wall[rank * cells:(rank + 1) * cells].copy()).cuda()
+    q, ws = qbgpu.Quad(N, wl["J"], wl["M"], wl["L"], wl["R"]), qbgpu.Workspace(N)
+    B = torch.zeros((cells, 3), dtype=torch.float64, device="cuda")
+    bufs = [W0.clone(), torch.empty_like(W0)]
+
+    if world == 1:
+        def step(Win, Wout):
+            qbgpu.inhom_step(ws, q, Win, wl["h"], wl["dt"], B, out=Wout)
+    else:
+        stream = qbgpu._stream
+
+        def transport(ext):
+            out = torch.empty_like(ext)
+            qbgpu._check(L.qb_transport(N, wl["L"], ext.shape[0], qbgpu._ptr(ext), qbgpu._ptr(out), wl["h"], 0.5 * wl["dt"], 0, stream()), "qb_transport")
+            return out
+
+        def collision(Wt):
+            qbgpu._check(L.qb_fourier_collision(ws.h, q.h, Wt.shape[0], qbgpu._ptr(Wt), qbgpu._ptr(B), wl["dt"], stream()), "qb_fourier_collision")
+            return Wt
+
+        def step(Win, Wout):
+            Wout.copy_(qd.sharded_strang_step(Win, transport, collision))
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MB > 126 MB L2
+    for i in range(args.warmup):
+        step(bufs[i % 2], bufs[(i + 1) % 2])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    L.qb_profile_reset()
+    L.qb_profile_enable(1)
+    launches0 = L.qb_launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    cur = args.warmup % 2
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record()
+            step(bufs[cur], bufs[1 - cur])
+            evs[k][1].record()
+            cur = 1 - cur
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    L.qb_profile_enable(0)
+    launches = L.qb_launch_count() - launches0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * 2 * args.steps / (ms * 1e-3)
+    steps_per_s = args.steps / (ms * 1e-3)
+
+    # dominant kernel: the I3 cluster kernel
+    import ctypes
+    kms, kn = ctypes.c_double(), ctypes.c_long()
+    L.qb_profile_read(b"i3_cluster", ctypes.byref(kms), ctypes.byref(kn))
+    tot_ms, tot_n = ctypes.c_double(), ctypes.c_long()
+    L.qb_profile_read(b"", ctypes.byref(tot_ms), ctypes.byref(tot_n))
+    L.qb_fp64_peak_tflops.restype = ctypes.c_double
+    peak = L.qb_fp64_peak_tflops()
+    per_launch_ms = kms.value / max(1, kn.value)
+    flops_launch = cells * wl["J"] * wl["M"] * i3_flops_per_term(N)
+    achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "kernel": "k_i3 (I3 quadrature sums, 4-CTA cluster)", "achieved": round(achieved, 3),
+                "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak > 0 else None,
+                "peak_source": "measured live: DFMA loop on every SM (qb_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
+                "flops_per_launch": flops_launch, "launch_ms": round(per_launch_ms, 4), "launches": kn.value,
+                "share_of_step": round(kms.value / max(1e-9, tot_ms.value), 4), "traffic": None}
+    state_bytes = cells * 4 * N * N * 8
+    hbm = {"bound": "hbm", "note": "whole step: transport reads+writes the state twice, collision reads W^ and writes C (FP64)",
+           "bytes_per_step": 4 * state_bytes + 2 * cells * 3 * 4 * N * N * 16,
+           "achieved": round((4 * state_bytes + 2 * cells * 3 * 4 * N * N * 16) * steps_per_s / 1e9, 3), "unit": "GB/s"}
+
+    # end to end through the public API with host buffers
+    e2e = run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall)
+
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture)",
+            "config": config_json(wl, world, "flushed: 256 MB written before every timed step"),
+            "sim_steps_per_s": round(steps_per_s, 4), "roofline": roofline, "hbm_view": hbm, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind = ref_kind()
+        procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
+        if kind is not None:
+            rate, wall = cpu_sample(wl, procs)
+            line["cpu_baseline"] = {"value": round(rate, 5), "unit": UNIT, "cores": procs, "kind": kind,
+                                    "sample": f"{procs} processes x 1 cell-collision evaluation (CcInt + CdInt) of the upstream C code, "
+                                              f"{wall:.1f} s wall; FFTs through the project's CPU FFTW-API shim (FFTW absent)"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall):
+    import torch
+    N, cells = wl["N"], wl["cells"]
+    steps = max(1, min(args.steps, 5))
+    nbytes = cells * 4 * N * N * 8
+    if world == 1 and N == qbgpu.N_GRID:
+        up = qbgpu.Upstream()
+        quads = [up.fourier(1, wl["J"], wl["L"], wl["R"]), up.fourier(2, wl["J"], wl["L"], wl["R"]),
+                 up.fourier(3, wl["J"], wl["L"], wl["R"], wl["M"]), up.fourier(4, wl["J"], wl["L"], wl["R"])]
+        it = up.inhom_interm(cells, wl["L"])
+        hin = torch.from_numpy(Wall[:cells].copy()).pin_memory().numpy()
+        hout = torch.empty(hin.shape, dtype=torch.float64).pin_memory().numpy()
+        hB = torch.zeros((cells, 3), dtype=torch.float64).pin_memory().numpy()
+        up.inhom_step(hin, quads, wl["h"], wl["dt"], hB, L=wl["L"], interm=it)      # warm-up
+        t0 = time.perf_counter()
+        a, b = hin, hout
+        for _ in range(steps):
+            out = up.inhom_step(a, quads, wl["h"], wl["dt"], hB, L=wl["L"], interm=it)
+            b[...] = out
+            a, b = b, a
+        wall = time.perf_counter() - t0
+        up.L.InhomStepInterm_Delete(qbgpu.C.byref(it))
+        for w, qq in zip((1, 2, 3, 4), quads):
+            up.quad_delete(w, qq)
+        return {"value": round(cells * 2 * steps / wall, 3), "unit": UNIT, "h2d_bytes_per_step": nbytes + cells * 3 * 8,
+                "d2h_bytes_per_step": nbytes, "api": "InhomStepPeriodic (upstream C API, host buffers, pinned)", "steps": steps}
+    # sharded path with host staging per step
+    hin = torch.from_numpy(Wall[rank * cells:(rank + 1) * cells].copy()).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    L = qbgpu.lib()
+
+    def transport(ext):
+        out = torch.empty_like(ext)
+        qbgpu._check(L.qb_transport(N, wl["L"], ext.shape[0], qbgpu._ptr(ext), qbgpu._ptr(out), wl["h"], 0.5 * wl["dt"], 0, qbgpu._stream()), "qb_transport")
+        return out
+
+    def collision(Wt):
+        qbgpu._check(L.qb_fourier_collision(ws.h, q.h, Wt.shape[0], qbgpu._ptr(Wt), qbgpu._ptr(B), wl["dt"], qbgpu._stream()), "qb_fourier_collision")
+        return Wt
+
+    import torch.distributed as dist
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        Wd = hin.cuda(non_blocking=True)
+        if world > 1:
+            Wn = qd.sharded_strang_step(Wd, transport, collision)
+        else:
+            Wn = qbgpu.inhom_step(ws, q, Wd, wl["h"], wl["dt"], B)
+        hout.copy_(Wn, non_blocking=True)
+        torch.cuda.synchronize()
+        hin, hout = hout, hin
+    wall = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t.item())
+    return {"value": round(world * cells * 2 * steps / wall, 3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "api": "sharded Strang step (qbgpu batched API + NCCL halos), host staging", "steps": steps}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = workload(args)
+    kind = ref_kind()
+    if kind is None:
+        print(json.dumps({"impl": "reference", "unavailable": "upstream sources were not compiled into oracle/_ref (no checkout at build time)"}))
+        return
+    procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
+    for i in range(args.warmup):
+        cpu_sample(wl, procs, seed_offset=i)
+    rates, walls = [], []
+    for k in range(args.steps):
+        r, w = cpu_sample(wl, procs, seed_offset=args.warmup + k)
+        rates.append(r)
+        walls.append(w)
+    total = sum(walls)
+    value = procs * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture)",
+            "config": config_json(wl, 1, "n/a (CPU)"),
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": procs, "kind": kind,
+                             "sample": f"per step {procs} processes x 1 cell-collision evaluation (CcInt + CdInt) of the upstream C "
+                                       f"sources; FFTs through the project's CPU FFTW-API shim (FFTW absent)"},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cells", type=int, default=64)
+    ap.add_argument("--grid", type=int, default=32)
+    ap.add_argument("--J", type=int, default=16)
+    ap.add_argument("--M", type=int, default=16)
+    ap.add_argument("--cpu-procs", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,102 @@
+/* qbgpu.h — batched, device-resident extension API of libqbgpu.
+ *
+ * The upstream API (collision.h, integrals.h, simulation.h, ...) works on one
+ * host state per call with a compile-time N_GRID.  These entry points take
+ * the grid size at run time, operate on many cells per call, and take DEVICE
+ * pointers plus a CUDA stream (NULL = the workspace's own stream), so a caller
+ * that keeps the state resident in HBM pays no host transfers per step.
+ * Layouts are the upstream ones laid end to end: a velocity-space cell is
+ * wignerV_t (4 real N x N grids), a Fourier-space cell is wignerF_t (4 complex
+ * N x N grids, interleaved re/im), cells are consecutive.
+ *
+ * Every function returns 0 on success.  On failure it records a message for
+ * qb_last_error() and, unless the environment sets QB_ABORT_ON_ERROR=0,
+ * aborts the process; with QB_ABORT_ON_ERROR=0 it returns -1.
+ * None of these has an upstream counterpart; each names the upstream function
+ * whose arithmetic it batches.
+ */
+#ifndef QBGPU_H
+#define QBGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qb_quad qb_quad;              /* device quadrature tables for (N, J, M, L, R) */
+typedef struct qb_workspace qb_workspace;    /* device scratch + stream for one grid size */
+
+const char *qb_last_error(void);
+int qb_n_grid(void);                          /* N_GRID this library's upstream API was built for */
+int qb_supported_n(int N);                    /* 1 if kernels for grid size N are compiled */
+
+/* FourierI1..I4 (upstream src/quadrature.c:150-527) built on the GPU */
+qb_quad *qb_quad_create(int N, int J, int M, double L, double R);
+void qb_quad_free(qb_quad *q);
+
+qb_workspace *qb_workspace_create(int N);
+void qb_workspace_free(qb_workspace *ws);
+
+/* Cc and/or Cd (CcInt / CdInt, upstream src/collision.c:74-254) of ncells
+ * Fourier states; parts: 1 = Cc, 2 = Cd, 3 = both; cc / cd may be NULL. */
+int qb_collision_operators(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, int parts,
+                           void *cc, void *cd, void *stream);
+
+/* CollisionStep (midpoint, upstream src/simulation.c:105-136) of ncells
+ * Fourier states, B = 3 doubles per cell; rk4 != 0 uses classical RK4 on the
+ * same right-hand side instead.  Wnext must not alias W. */
+int qb_collision_step(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, const double *B,
+                      double dt, void *Wnext, int rk4, void *stream);
+
+/* one Strang step of InhomStepPeriodic (bc = 0) / InhomStepDirichlet (bc = 1)
+ * (upstream src/simulation.c:307-830) over ncells velocity-space cells with
+ * box half-width L; Bext = 3 doubles per cell.  Wnext must not alias W. */
+int qb_inhom_step(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
+                  double h, double dt, const double *Bext, int bc, void *stream);
+
+/* InhomStepMaxwell (upstream src/simulation.c:879-1165); WL / WR one
+ * velocity-space state each. */
+int qb_inhom_step_maxwell(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
+                          double h, double dt, double lambda, const double *WL, const double *WR,
+                          const double *Bext, void *stream);
+
+/* velocity space <-> Fourier space for ngrids N x N components
+ * (upstream src/simulation.c:224-283) */
+int qb_to_fourier(int N, int ngrids, const double *Wv, void *Wf, void *stream);
+int qb_from_fourier(int N, int ngrids, const void *Wf, double *Wv, void *stream);
+
+/* single I1 / I2 / I3 / I4 integral (which = 1..4) of Fourier grids f, g, h
+ * with the quad's tables (upstream src/integrals.c:90-382) */
+int qb_integral(qb_workspace *ws, const qb_quad *q, int which, const void *f, const void *g, const void *h,
+                void *out, void *stream);
+
+/* one half-step of transport (SlopeLimiterStepPeriodic / Dirichlet over every
+ * x-line, upstream src/simulation.c:426-448) for ncells velocity-space cells
+ * of grid size N in a box of half-width L: out = limiter(in) with step dt. */
+int qb_transport(int N, double L, int ncells, const double *in, double *out, double h, double dt, int bc, void *stream);
+
+/* the collision part of a Strang step on ncells velocity-space cells, in
+ * place: to Fourier space, CollisionStep, back (InternalFourierCollisionStep,
+ * upstream src/simulation.c:214-284) */
+int qb_fourier_collision(qb_workspace *ws, const qb_quad *q, int ncells, double *W, const double *Bext, double dt, void *stream);
+
+/* launch accounting: every engine kernel launch is counted; while profiling
+ * is on, launches are bracketed by CUDA events on their stream.
+ * qb_profile_read sums device milliseconds and launches of kernels whose
+ * name starts with `prefix` ("i3_cluster", "i1_terms", "i2_terms",
+ * "pad_fft", "fft_full", "assemble", "to_fourier", "from_fourier",
+ * "transport"; "" = all). */
+int qb_profile_enable(int on);
+int qb_profile_reset(void);
+int qb_profile_read(const char *prefix, double *ms, long *launches);
+long qb_launch_count(void);
+
+/* measured FP64 FMA throughput of the current device in TFLOP/s (a dependent-
+ * free DFMA loop on every SM, ~tens of ms) -- the denominator of the FP64
+ * roofline of the collision kernels. */
+double qb_fp64_peak_tflops(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QBGPU_H */

@@ -1,0 +1,714 @@
+// qb_engine.cu — launch wrappers and step orchestration of the GPU engine.
+#include "qb_engine.h"
+#include "qb_kernels.cuh"
+#include "qb_transport.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+namespace qb {
+
+// ---------------------------------------------------------------------------
+// errors
+static std::mutex g_err_mu;
+static std::string g_last_error;
+
+void fail(const char *file, int line, const std::string &msg) {
+	std::string m = std::string("qbgpu: ") + msg + " (" + file + ":" + std::to_string(line) + ")";
+	{
+		std::lock_guard<std::mutex> lk(g_err_mu);
+		g_last_error = m;
+	}
+	const char *e = getenv("QB_ABORT_ON_ERROR");
+	if (e == nullptr || strcmp(e, "0") != 0) {
+		fprintf(stderr, "%s\n", m.c_str());
+		abort();
+	}
+	throw std::runtime_error(m);
+}
+
+std::string last_error() {
+	std::lock_guard<std::mutex> lk(g_err_mu);
+	return g_last_error;
+}
+
+bool supported_n(int N) { return N == 8 || N == 16 || N == 32; }
+
+// ---------------------------------------------------------------------------
+// launch accounting
+namespace {
+struct ProfRec { std::string name; cudaEvent_t e0, e1; };
+std::mutex g_prof_mu;
+std::vector<ProfRec> g_prof;
+std::atomic<bool> g_prof_on{false};
+std::atomic<long> g_launches{0};
+}  // namespace
+
+void prof_enable(bool on) { g_prof_on = on; }
+long launch_count() { return g_launches.load(); }
+
+void prof_reset() {
+	std::lock_guard<std::mutex> lk(g_prof_mu);
+	for (auto &r : g_prof) { cudaEventDestroy(r.e0); cudaEventDestroy(r.e1); }
+	g_prof.clear();
+}
+
+void prof_read(const char *prefix, double *ms, long *launches) {
+	std::lock_guard<std::mutex> lk(g_prof_mu);
+	double t = 0;
+	long n = 0;
+	const size_t lp = strlen(prefix);
+	for (auto &r : g_prof) {
+		if (r.name.compare(0, lp, prefix) != 0) continue;
+		QB_CUDA(cudaEventSynchronize(r.e1));
+		float e = 0;
+		QB_CUDA(cudaEventElapsedTime(&e, r.e0, r.e1));
+		t += e;
+		n++;
+	}
+	*ms = t;
+	*launches = n;
+}
+
+ProfScope::ProfScope(const char *n, cudaStream_t st) : name(n), s(st) {
+	g_launches++;
+	if (g_prof_on) {
+		QB_CUDA(cudaEventCreate(&e0));
+		QB_CUDA(cudaEventCreate(&e1));
+		QB_CUDA(cudaEventRecord(e0, s));
+	}
+}
+
+ProfScope::~ProfScope() {
+	if (e0 != nullptr) {
+		cudaEventRecord(e1, s);
+		std::lock_guard<std::mutex> lk(g_prof_mu);
+		g_prof.push_back({ name, e0, e1 });
+	}
+}
+
+// ---------------------------------------------------------------------------
+// buffers
+void DevBuf::ensure(size_t n) {
+	if (n <= bytes && p != nullptr) return;
+	release();
+	QB_CUDA(cudaGetDevice(&device));
+	QB_CUDA(cudaMalloc(&p, n));
+	bytes = n;
+}
+
+void DevBuf::release() {
+	if (p != nullptr) {
+		int cur = -1;
+		cudaGetDevice(&cur);
+		if (device >= 0 && cur != device) cudaSetDevice(device);
+		cudaFree(p);
+		if (device >= 0 && cur != device) cudaSetDevice(cur);
+	}
+	p = nullptr;
+	bytes = 0;
+}
+
+Workspace::Workspace(int n) : N(n) {
+	if (!supported_n(N)) QB_FAIL("grid size N=" + std::to_string(N) + " has no compiled kernels");
+	QB_CUDA(cudaGetDevice(&device));
+	QB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+}
+
+Workspace::~Workspace() {
+	if (stream) cudaStreamDestroy(stream);
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers (templated on the padded size P)
+namespace {
+
+int num_sms() {
+	static int sms = 0;
+	if (sms == 0) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		if (sms <= 0) sms = 148;
+	}
+	return sms;
+}
+
+template <class K> void set_smem(K kernel, size_t bytes) {
+	QB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+template <int P> constexpr size_t smem_grids(int ngrids) { return sizeof(double2) * ((size_t)ngrids * Geo<P>::GRID + P); }
+
+// active clusters of the I3 kernel (occupancy query, cached per P)
+template <int P> int active_i3_clusters() {
+	static int cached = -1;
+	if (cached < 0) {
+		auto kern = k_i3<P, 4>;
+		set_smem(kern, smem_grids<P>(2));
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(4);
+		cfg.blockDim = dim3(Geo<P>::NT);
+		cfg.dynamicSmemBytes = smem_grids<P>(2);
+		cudaLaunchAttribute attr;
+		attr.id = cudaLaunchAttributeClusterDimension;
+		attr.val.clusterDim.x = 4; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+		cfg.attrs = &attr;
+		cfg.numAttrs = 1;
+		int n = 0;
+		if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
+			cudaGetLastError();
+			n = std::max(1, num_sms() / 4);
+		}
+		cached = n;
+	}
+	return cached;
+}
+
+// number of chunks minimising (waves x terms per chunk) for `units` independent
+// work units that each split their `nterms` terms into chunks
+int best_chunks(long units, int nterms, int slots, int max_chunks) {
+	int best = 1;
+	double best_cost = 1e300;
+	for (int c = 1; c <= std::min(nterms, max_chunks); c++) {
+		const long waves = (units * c + slots - 1) / slots;
+		const double cost = (double)waves * ((nterms + c - 1) / c) + 0.02 * c;   // small cost per partial grid
+		if (cost < best_cost - 1e-9) { best_cost = cost; best = c; }
+	}
+	return best;
+}
+
+template <int P> void launch_pad_fft(int ngrids, const double2 *src, double2 *out, cudaStream_t s) {
+	static bool init = false;
+	if (!init) { set_smem(k_pad_fft<P>, smem_grids<P>(1)); init = true; }
+	ProfScope ps("pad_fft", s);
+	k_pad_fft<P><<<ngrids, Geo<P>::NT, smem_grids<P>(1), s>>>(src, out);
+	QB_CUDA(cudaGetLastError());
+}
+
+template <int P> void launch_i1(const I1Params &p, long nblocks, cudaStream_t s) {
+	static bool init = false;
+	if (!init) { set_smem(k_i1_terms<P>, smem_grids<P>(2)); init = true; }
+	ProfScope ps("i1_terms", s);
+	k_i1_terms<P><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P>(2), s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+template <int P> void launch_i2(const I2Params &p, long nblocks, cudaStream_t s) {
+	static bool init = false;
+	if (!init) { set_smem(k_i2_terms<P>, smem_grids<P>(2)); init = true; }
+	ProfScope ps("i2_terms", s);
+	k_i2_terms<P><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P>(2), s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+template <int P, int CS> void launch_i3(const I3Params &p, long nclusters, cudaStream_t s) {
+	static bool init = false;
+	auto kern = k_i3<P, CS>;
+	if (!init) { set_smem(kern, smem_grids<P>(2)); init = true; }
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)(nclusters * CS));
+	cfg.blockDim = dim3(Geo<P>::NT);
+	cfg.dynamicSmemBytes = smem_grids<P>(2);
+	cfg.stream = s;
+	cudaLaunchAttribute attr;
+	attr.id = cudaLaunchAttributeClusterDimension;
+	attr.val.clusterDim.x = CS; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+	cfg.attrs = &attr;
+	cfg.numAttrs = 1;
+	ProfScope ps("i3_cluster", s);
+	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p));
+}
+
+template <int P> void launch_fft_full(const FullParams &p, long ngrids, cudaStream_t s) {
+	static bool init = false;
+	if (!init) { set_smem(k_fft_full<P>, smem_grids<P>(1)); init = true; }
+	ProfScope ps("fft_full", s);
+	k_fft_full<P><<<(unsigned)ngrids, Geo<P>::NT, smem_grids<P>(1), s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+template <int P> void launch_assemble(const AsmParams &p, long ncells, cudaStream_t s) {
+	static bool init = false;
+	if (!init) { set_smem(k_assemble<P>, smem_grids<P>(1)); init = true; }
+	ProfScope ps("assemble", s);
+	k_assemble<P><<<(unsigned)(ncells * 4), Geo<P>::NT, smem_grids<P>(1), s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// the factored right-hand side for one padded size
+template <int P> struct Rhs {
+	static constexpr int N = P / 2;
+	static constexpr long NN = (long)N * N, PP = (long)P * P;
+
+	// spectra of the four components
+	static void spectra(Workspace &ws, int ncells, const double2 *W, cudaStream_t s) {
+		ws.What.ensure(sizeof(double2) * 4 * ncells * PP);
+		launch_pad_fft<P>(4 * ncells, W, ws.What.as<double2>(), s);
+	}
+
+	// S sums for Cc (tasks g = W_1..W_3, F = -4 W^_0 + 2) or I4 (g = W_0..W_3, F = 2 W^_0 - 1)
+	static void i1_sums(Workspace &ws, const DevI1 &t, int ncells, const double2 *W, bool cc, DevBuf &part, DevBuf &fs, int nchunk, cudaStream_t s) {
+		const int ntask = cc ? 3 : 4;
+		part.ensure(sizeof(double2) * ncells * ntask * nchunk * PP);
+		I1Params p{};
+		p.ntask = ntask; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.g = W; p.g_cell = 4 * NN;
+		for (int k = 0; k < 4; k++) p.g_comp[k] = cc ? std::min(k + 1, 3) : k;
+		p.What = ws.What.as<double2>(); p.w_cell = 4 * PP; p.f_comp = 0;
+		p.fa = cc ? -4.0 : 2.0; p.fb = cc ? 2.0 : -1.0;
+		p.psi2 = t.psi2.as<double>(); p.phi = t.phi.as<double>();
+		p.out = part.as<double2>();
+		launch_i1<P>(p, (long)ncells * ntask * nchunk, s);
+		fs.ensure(sizeof(double2) * ncells * ntask * PP);
+		FullParams f{};
+		f.in = part.as<double2>(); f.grid_stride = nchunk * PP; f.part_stride = PP; f.nparts = nchunk;
+		f.out = fs.as<double2>();
+		launch_fft_full<P>(f, (long)ncells * ntask, s);
+	}
+
+	static void i2_sums(Workspace &ws, const DevI2 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
+		ws.i2p.ensure(sizeof(double2) * ncells * 4 * nchunk * PP);
+		I2Params p{};
+		p.ntask = 4; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = W; p.cell_stride = 4 * NN;
+		for (int k = 0; k < 4; k++) { p.f_comp[k] = k; p.g_comp[k] = k; }
+		p.psi1 = t.psi1.as<double>(); p.psi2 = t.psi2.as<double>();
+		p.out = ws.i2p.as<double2>();
+		launch_i2<P>(p, (long)ncells * 4 * nchunk, s);
+	}
+
+	static void i3_sums(Workspace &ws, const DevI3 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
+		ws.i3p.ensure(sizeof(double2) * ncells * nchunk * 4 * PP);
+		I3Params p{};
+		p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = W; p.src_cell = 4 * NN;
+		for (int r = 0; r < 4; r++) p.src_comp[r] = r;
+		p.Ghat = ws.What.as<double2>(); p.g_cell = 4 * PP;
+		const double eta[4] = { 1, -1, -1, -1 };
+		for (int r = 0; r < 4; r++) {           // CTA j: X_j = sum_i eta_i P_i . FFT2(psi2 . IFFT2(W^_i . P_j))
+			p.ncombo[r] = 4;
+			for (int i = 0; i < 4; i++) { p.ca[r][i] = i; p.cgi[r][i] = i; p.ccoef[r][i] = eta[i]; }
+		}
+		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
+		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
+		p.out = ws.i3p.as<double2>();
+		launch_i3<P, 4>(p, (long)ncells * nchunk, s);
+	}
+
+	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
+		ch = pick_chunks(N, ncells, q);
+		spectra(ws, ncells, W, s);
+		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
+		if (parts & RHS_CD) {
+			i1_sums(ws, *q.i4, ncells, W, false, ws.i1i4, ws.fs4, ch.i1, s);
+			i2_sums(ws, *q.i2, ncells, W, ch.i2, s);
+			i3_sums(ws, *q.i3, ncells, W, ch.i3, s);
+		}
+	}
+
+	static AsmParams asm_params(Workspace &ws, int parts, const Chunks &ch) {
+		AsmParams a{};
+		a.What = ws.What.as<double2>();
+		a.FS = (parts & RHS_CC) ? ws.fs.as<double2>() : nullptr;
+		a.FS4 = (parts & RHS_CD) ? ws.fs4.as<double2>() : nullptr;
+		a.Qp = (parts & RHS_CD) ? ws.i2p.as<double2>() : nullptr; a.nq = ch.i2;
+		a.Xp = (parts & RHS_CD) ? ws.i3p.as<double2>() : nullptr; a.nx = ch.i3;
+		a.s2 = 1.0 / (double)PP;
+		a.s1 = a.s2 * a.s2;
+		return a;
+	}
+
+	static void operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
+		Chunks ch;
+		prepare(ws, q, ncells, W, parts, ch, s);
+		AsmParams a = asm_params(ws, parts, ch);
+		a.mode = 0; a.out_cc = cc; a.out_cd = cd;
+		launch_assemble<P>(a, ncells, s);
+	}
+
+	static void update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
+		Chunks ch;
+		prepare(ws, q, ncells, wcur, RHS_ALL, ch, s);
+		AsmParams a = asm_params(ws, RHS_ALL, ch);
+		a.mode = 1; a.base = base; a.wcur = wcur; a.B = B; a.dtc = dtc; a.out = out;
+		launch_assemble<P>(a, ncells, s);
+	}
+};
+
+template <template <int> class F, class... A> void by_n(int N, A &&...args) {
+	switch (N) {
+	case 8: F<16>::run(args...); break;
+	case 16: F<32>::run(args...); break;
+	case 32: F<64>::run(args...); break;
+	default: QB_FAIL("grid size N=" + std::to_string(N) + " has no compiled kernels");
+	}
+}
+
+template <int P> struct OpsRun {
+	static void run(Workspace &ws, const QuadSet &q, int n, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
+		Rhs<P>::operators(ws, q, n, W, parts, cc, cd, s);
+	}
+};
+template <int P> struct UpdRun {
+	static void run(Workspace &ws, const QuadSet &q, int n, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
+		Rhs<P>::update(ws, q, n, base, wcur, B, dtc, out, s);
+	}
+};
+
+__global__ void k_axpy(long n, const double2 *__restrict__ base, double a, const double2 *__restrict__ k, double2 *__restrict__ out) {
+	const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = make_double2(base[i].x + a * k[i].x, base[i].y + a * k[i].y);
+}
+
+__global__ void k_rk4(long n, const double2 *__restrict__ W, double c, const double2 *k1, const double2 *k2, const double2 *k3, const double2 *k4, double2 *out) {
+	const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) {
+		out[i].x = W[i].x + c * (k1[i].x + 2 * k2[i].x + 2 * k3[i].x + k4[i].x);
+		out[i].y = W[i].y + c * (k1[i].y + 2 * k2[i].y + 2 * k3[i].y + k4[i].y);
+	}
+}
+
+}  // namespace
+
+Chunks pick_chunks(int N, int ncells, const QuadSet &q) {
+	Chunks c;
+	const int sms = num_sms();
+	if (q.i1) c.i1 = best_chunks((long)ncells * 7, std::max(1, q.i1->nterms), sms, 64);
+	if (q.i2) c.i2 = best_chunks((long)ncells * 4, std::max(1, q.i2->nterms), sms, 64);
+	if (q.i3) {
+		int act = 0;
+		switch (N) {
+		case 8: act = active_i3_clusters<16>(); break;
+		case 16: act = active_i3_clusters<32>(); break;
+		default: act = active_i3_clusters<64>(); break;
+		}
+		c.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), act, 256);
+	}
+	return c;
+}
+
+void collision_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *out_cc, double2 *out_cd, cudaStream_t s) {
+	by_n<OpsRun>(ws.N, ws, q, ncells, W, parts, out_cc, out_cd, s);
+}
+
+void collision_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
+	by_n<UpdRun>(ws.N, ws, q, ncells, base, wcur, B, dtc, out, s);
+}
+
+void collision_step(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, const double *B, double dt, double2 *Wnext, cudaStream_t s) {
+	const size_t bytes = sizeof(double2) * 4 * (size_t)ncells * ws.N * ws.N;
+	ws.wmid.ensure(bytes);
+	collision_update(ws, q, ncells, W, W, B, 0.5 * dt, ws.wmid.as<double2>(), s);
+	collision_update(ws, q, ncells, W, ws.wmid.as<double2>(), B, dt, Wnext, s);
+}
+
+void collision_step_rk4(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, const double *B, double dt, double2 *Wnext, cudaStream_t s) {
+	const long n = 4L * ncells * ws.N * ws.N;
+	ws.aux.ensure(sizeof(double2) * 5 * n);
+	double2 *k1 = ws.aux.as<double2>(), *k2 = k1 + n, *k3 = k2 + n, *k4 = k3 + n, *Ws = k4 + n;
+	const unsigned nb = (unsigned)((n + 255) / 256);
+	collision_update(ws, q, ncells, nullptr, W, B, 1.0, k1, s);
+	k_axpy<<<nb, 256, 0, s>>>(n, W, 0.5 * dt, k1, Ws);
+	collision_update(ws, q, ncells, nullptr, Ws, B, 1.0, k2, s);
+	k_axpy<<<nb, 256, 0, s>>>(n, W, 0.5 * dt, k2, Ws);
+	collision_update(ws, q, ncells, nullptr, Ws, B, 1.0, k3, s);
+	k_axpy<<<nb, 256, 0, s>>>(n, W, dt, k3, Ws);
+	collision_update(ws, q, ncells, nullptr, Ws, B, 1.0, k4, s);
+	k_rk4<<<nb, 256, 0, s>>>(n, W, dt / 6.0, k1, k2, k3, k4, Wnext);
+	QB_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// single-triple integrals (upstream I1integral / I2integral / I3integral)
+
+// out = scale * Extract(IFFT2(Z)) for one padded grid
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT) k_extract_ifft(const double2 *__restrict__ Z, double scale, double2 *__restrict__ out) {
+	using G = Geo<P>;
+	constexpr int N = G::N;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + G::GRID;
+	init_twiddles<P>(tw);
+	for (int i = threadIdx.x; i < P * P; i += G::NT) S[(i / P) * G::LDP + (i % P)] = Z[i];
+	__syncthreads();
+	fft2_smem<P, +1>(S, tw);
+	for (int q = threadIdx.x; q < N * N; q += G::NT) {
+		const double2 v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+		out[q] = make_double2(scale * v.x, scale * v.y);
+	}
+}
+
+// out[i] = a[i] * sum_k b[k*stride + i]   (a may be null: plain sum)
+__global__ void k_mul_sum(long n, const double2 *__restrict__ a, const double2 *__restrict__ b, int nparts, long stride, double2 *__restrict__ out) {
+	const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	double2 s = b[i];
+	for (int k = 1; k < nparts; k++) s = cadd(s, b[k * stride + i]);
+	out[i] = a ? cmul(a[i], s) : s;
+}
+
+namespace {
+void mul_sum(long n, const double2 *a, const double2 *b, int nparts, long stride, double2 *out, cudaStream_t s) {
+	k_mul_sum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, a, b, nparts, stride, out);
+	QB_CUDA(cudaGetLastError());
+}
+
+template <int P> void extract_ifft(const double2 *Z, double scale, double2 *out, cudaStream_t s) {
+	static bool init = false;
+	if (!init) { set_smem(k_extract_ifft<P>, smem_grids<P>(1)); init = true; }
+	k_extract_ifft<P><<<1, Geo<P>::NT, smem_grids<P>(1), s>>>(Z, scale, out);
+	QB_CUDA(cudaGetLastError());
+}
+
+// I1 = s^2 Extract(IFFT2(h^ . FFT2(sum_t phi_t . IFFT2(f^ . FFT2(Pad(psi2_t g))))))
+template <int P> struct I1S {
+	static void run(Workspace &ws, const DevI1 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+		constexpr long NN = (long)(P / 2) * (P / 2), PP = (long)P * P;
+		ws.aux.ensure(sizeof(double2) * 2 * NN);
+		double2 *fh = ws.aux.as<double2>();
+		QB_CUDA(cudaMemcpyAsync(fh, f, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(fh + NN, h, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		ws.What.ensure(sizeof(double2) * 2 * PP);
+		launch_pad_fft<P>(2, fh, ws.What.as<double2>(), s);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), num_sms(), 128);
+		ws.i1cc.ensure(sizeof(double2) * nchunk * PP);
+		I1Params p{};
+		p.ntask = 1; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.g = g; p.g_cell = 0; p.g_comp[0] = 0;
+		p.What = ws.What.as<double2>(); p.w_cell = 0; p.f_comp = 0; p.fa = 1.0; p.fb = 0.0;
+		p.psi2 = t.psi2.as<double>(); p.phi = t.phi.as<double>();
+		p.out = ws.i1cc.as<double2>();
+		launch_i1<P>(p, nchunk, s);
+		ws.fs.ensure(sizeof(double2) * 2 * PP);
+		FullParams fp{};
+		fp.in = ws.i1cc.as<double2>(); fp.grid_stride = 0; fp.part_stride = PP; fp.nparts = nchunk;
+		fp.out = ws.fs.as<double2>();
+		launch_fft_full<P>(fp, 1, s);
+		mul_sum(PP, ws.What.as<double2>() + PP, ws.fs.as<double2>(), 1, 0, ws.fs.as<double2>() + PP, s);
+		const double s2 = 1.0 / (double)PP;
+		extract_ifft<P>(ws.fs.as<double2>() + PP, s2 * s2, out, s);
+	}
+};
+
+// I2 = s Extract(IFFT2(h^ . sum_t FFT2(Pad(psi1_t f)) . FFT2(Pad(psi2_t g))))
+template <int P> struct I2S {
+	static void run(Workspace &ws, const DevI2 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+		constexpr long NN = (long)(P / 2) * (P / 2), PP = (long)P * P;
+		ws.aux.ensure(sizeof(double2) * 3 * NN);
+		double2 *fgh = ws.aux.as<double2>();
+		QB_CUDA(cudaMemcpyAsync(fgh, f, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(fgh + NN, g, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(fgh + 2 * NN, h, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		ws.What.ensure(sizeof(double2) * PP);
+		launch_pad_fft<P>(1, fgh + 2 * NN, ws.What.as<double2>(), s);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), num_sms(), 128);
+		ws.i2p.ensure(sizeof(double2) * nchunk * PP);
+		I2Params p{};
+		p.ntask = 1; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = fgh; p.cell_stride = 0; p.f_comp[0] = 0; p.g_comp[0] = 1;
+		p.psi1 = t.psi1.as<double>(); p.psi2 = t.psi2.as<double>();
+		p.out = ws.i2p.as<double2>();
+		launch_i2<P>(p, nchunk, s);
+		ws.fs.ensure(sizeof(double2) * PP);
+		mul_sum(PP, ws.What.as<double2>(), ws.i2p.as<double2>(), nchunk, PP, ws.fs.as<double2>(), s);
+		extract_ifft<P>(ws.fs.as<double2>(), 1.0 / (double)PP, out, s);
+	}
+};
+
+// I3 = s^2 Extract(IFFT2(sum_t FFT2(Pad(psi1_t f)) . FFT2(psi2_t . IFFT2(g^ . FFT2(Pad(psi1_t h))))))
+// on a 2-CTA cluster: rank 0 owns h (convolved with g^), rank 1 owns f.
+template <int P> struct I3S {
+	static void run(Workspace &ws, const DevI3 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+		constexpr long NN = (long)(P / 2) * (P / 2), PP = (long)P * P;
+		ws.aux.ensure(sizeof(double2) * 3 * NN);
+		double2 *src = ws.aux.as<double2>();
+		QB_CUDA(cudaMemcpyAsync(src, h, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(src + NN, f, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(src + 2 * NN, g, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		ws.What.ensure(sizeof(double2) * PP);
+		launch_pad_fft<P>(1, src + 2 * NN, ws.What.as<double2>(), s);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), std::max(1, num_sms() / 2), 256);
+		ws.i3p.ensure(sizeof(double2) * nchunk * 2 * PP);
+		I3Params p{};
+		p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = src; p.src_cell = 0; p.src_comp[0] = 0; p.src_comp[1] = 1;
+		p.Ghat = ws.What.as<double2>(); p.g_cell = 0;
+		p.ncombo[0] = 1; p.ca[0][0] = 1; p.cgi[0][0] = 0; p.ccoef[0][0] = 1.0;
+		p.ncombo[1] = 0;
+		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
+		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
+		p.out = ws.i3p.as<double2>();
+		launch_i3<P, 2>(p, nchunk, s);
+		ws.fs.ensure(sizeof(double2) * PP);
+		mul_sum(PP, nullptr, ws.i3p.as<double2>(), nchunk, 2 * PP, ws.fs.as<double2>(), s);   // rank-0 partials
+		const double s2 = 1.0 / (double)PP;
+		extract_ifft<P>(ws.fs.as<double2>(), s2 * s2, out, s);
+	}
+};
+}  // namespace
+
+void integral_i1(Workspace &ws, const DevI1 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+	by_n<I1S>(ws.N, ws, t, f, g, h, out, s);
+}
+void integral_i2(Workspace &ws, const DevI2 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+	by_n<I2S>(ws.N, ws, t, f, g, h, out, s);
+}
+void integral_i3(Workspace &ws, const DevI3 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+	by_n<I3S>(ws.N, ws, t, f, g, h, out, s);
+}
+
+// ---------------------------------------------------------------------------
+// Fourier representation, transport, Strang step
+namespace {
+template <int N> void launch_to_fourier(int ngrids, const double *Wv, double2 *Wf, cudaStream_t s) {
+	const size_t sm = sizeof(double2) * (N * (N + 1) + N);
+	ProfScope ps("to_fourier", s);
+	k_to_fourier<N><<<ngrids, Len<N>::T * N, sm, s>>>(Wv, Wf);
+	QB_CUDA(cudaGetLastError());
+}
+template <int N> void launch_from_fourier(int ngrids, const double2 *Wf, double *Wv, cudaStream_t s) {
+	const size_t sm = sizeof(double2) * (N * (N + 1) + N);
+	ProfScope ps("from_fourier", s);
+	k_from_fourier<N><<<ngrids, Len<N>::T * N, sm, s>>>(Wf, Wv);
+	QB_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s) {
+	if (ngrids <= 0) return;
+	switch (N) {
+	case 8: launch_to_fourier<8>(ngrids, Wv, Wf, s); break;
+	case 16: launch_to_fourier<16>(ngrids, Wv, Wf, s); break;
+	case 32: launch_to_fourier<32>(ngrids, Wv, Wf, s); break;
+	default: QB_FAIL("to_fourier: unsupported N");
+	}
+}
+
+void from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t s) {
+	if (ngrids <= 0) return;
+	switch (N) {
+	case 8: launch_from_fourier<8>(ngrids, Wf, Wv, s); break;
+	case 16: launch_from_fourier<16>(ngrids, Wf, Wv, s); break;
+	case 32: launch_from_fourier<32>(ngrids, Wf, Wv, s); break;
+	default: QB_FAIL("from_fourier: unsupported N");
+	}
+}
+
+void transport(int npts, int ncells, const double *in, double *out, const double *A_dev, double h, double dt, int bc, cudaStream_t s) {
+	if (ncells <= 0 || npts <= 0) return;
+	TransportParams p{};
+	p.ncells = ncells; p.npts = npts; p.in = in; p.out = out; p.A = A_dev; p.h = h; p.dt = dt; p.bc = bc;
+	const long n = (long)npts * ncells;
+	ProfScope ps("transport", s);
+	k_transport<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+void transport_maxwell_lines(int m, int ncells, const double *in, double *out, const double *A_dev, double h, double dt,
+                             double lambda, const double *flux_dev, const double *UL, const double *UR, cudaStream_t s) {
+	if (ncells <= 0 || m <= 0) return;
+	MaxwellParams p{};
+	p.ncells = ncells; p.m = m; p.remapN = 0; p.ncomp = 1;
+	p.in = in; p.out = out; p.A = A_dev; p.h = h; p.dt = dt; p.lambda = lambda;
+	p.flux = flux_dev; p.UL = UL; p.UR = UR;
+	const long n = (long)m * ncells;
+	k_transport_maxwell<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+void flux_pair(int m, const double *A_dev, const double *U_dev, double *out_dev, cudaStream_t s) {
+	k_flux_pair<<<1, 32, 0, s>>>(m, 0, A_dev, U_dev, out_dev);
+	QB_CUDA(cudaGetLastError());
+}
+
+namespace {
+void fourier_collision(Workspace &ws, const QuadSet &q, int nc, double *V, const double *B, double dt, cudaStream_t s) {
+	const int N = ws.N;
+	const long cs = 4L * N * N;
+	if (nc <= 0) return;
+	ws.fa.ensure(sizeof(double2) * cs * nc);
+	ws.fb.ensure(sizeof(double2) * cs * nc);
+	to_fourier(N, 4 * nc, V, ws.fa.as<double2>(), s);
+	collision_step(ws, q, nc, ws.fa.as<double2>(), B, dt, ws.fb.as<double2>(), s);
+	from_fourier(N, 4 * nc, ws.fb.as<double2>(), V, s);
+}
+}  // namespace
+
+void inhom_step(Workspace &ws, const QuadSet &q, int ncells, const double *W, double *Wnext, const double *A_dev,
+                double h, double dt, const double *Bext, int bc, cudaStream_t s) {
+	const int N = ws.N;
+	const long cs = 4L * N * N;
+	ws.va.ensure(sizeof(double) * cs * ncells);
+	double *Vt = ws.va.as<double>();
+	transport((int)cs, ncells, W, Vt, A_dev, h, 0.5 * dt, bc, s);
+	const int i0 = (bc == 1) ? 1 : 0, i1 = (bc == 1) ? ncells - 1 : ncells;
+	fourier_collision(ws, q, i1 - i0, Vt + i0 * cs, Bext + 3 * i0, dt, s);
+	transport((int)cs, ncells, Vt, Wnext, A_dev, h, 0.5 * dt, bc, s);
+}
+
+void inhom_step_maxwell(Workspace &ws, const QuadSet &q, int ncells, const double *W, double *Wnext, const double *vx_dev,
+                        double h, double dt, double lambda, const double *WL, const double *WR, const double *Bext, cudaStream_t s) {
+	const int N = ws.N, m = N * N;
+	const long cs = 4L * m;
+	ws.va.ensure(sizeof(double) * cs * ncells);
+	ws.aux2.ensure(sizeof(double) * (8 + 8L * m));
+	double *bnd = ws.aux2.as<double>(), *UL = bnd + 8, *UR = UL + 4L * m;
+	double *Vt = ws.va.as<double>();
+	k_maxwell_setup<<<1, 256, 0, s>>>(N, vx_dev, WL, WR, W, W + (ncells - 1) * cs, bnd, UL, UR);
+	QB_CUDA(cudaGetLastError());
+	MaxwellParams p{};
+	p.ncells = ncells; p.m = m; p.remapN = N; p.ncomp = 4;
+	p.A = vx_dev; p.h = h; p.dt = 0.5 * dt; p.lambda = lambda; p.flux = bnd + 2; p.UL = UL; p.UR = UR;
+	const unsigned nb = (unsigned)((cs * ncells + 255) / 256);
+	p.in = W; p.out = Vt;
+	k_transport_maxwell<<<nb, 256, 0, s>>>(p);
+	QB_CUDA(cudaGetLastError());
+	fourier_collision(ws, q, ncells, Vt, Bext, dt, s);
+	k_maxwell_flux<<<1, 32, 0, s>>>(N, vx_dev, Vt, Vt + (ncells - 1) * cs, bnd);
+	p.in = Vt; p.out = Wnext;
+	k_transport_maxwell<<<nb, 256, 0, s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// FFTW-API plans
+bool fft2_generic_supported(int n0, int n1) {
+	return n0 == n1 && (n0 == 8 || n0 == 16 || n0 == 32 || n0 == 64);
+}
+
+namespace {
+template <int L, int DIR> void launch_generic(bool r2c, const void *in, double2 *out, cudaStream_t s) {
+	const size_t sm = sizeof(double2) * (L * (L + 1) + L);
+	static bool init = false;
+	if (!init) { set_smem(k_fft2_generic<L, DIR>, sm); init = true; }
+	k_fft2_generic<L, DIR><<<1, Len<L>::T * L, sm, s>>>(in, out, r2c ? 1 : 0);
+	QB_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void fft2_generic(int L, int dir, bool r2c, const void *in_dev, double2 *out_dev, cudaStream_t s) {
+	if (dir < 0) {
+		switch (L) {
+		case 8: launch_generic<8, -1>(r2c, in_dev, out_dev, s); break;
+		case 16: launch_generic<16, -1>(r2c, in_dev, out_dev, s); break;
+		case 32: launch_generic<32, -1>(r2c, in_dev, out_dev, s); break;
+		case 64: launch_generic<64, -1>(r2c, in_dev, out_dev, s); break;
+		default: QB_FAIL("fft2: unsupported size");
+		}
+	} else {
+		switch (L) {
+		case 8: launch_generic<8, 1>(r2c, in_dev, out_dev, s); break;
+		case 16: launch_generic<16, 1>(r2c, in_dev, out_dev, s); break;
+		case 32: launch_generic<32, 1>(r2c, in_dev, out_dev, s); break;
+		case 64: launch_generic<64, 1>(r2c, in_dev, out_dev, s); break;
+		default: QB_FAIL("fft2: unsupported size");
+		}
+	}
+}
+
+}  // namespace qb

@@ -1,0 +1,232 @@
+// qb_ext.cu — batched device-pointer extension API (include/qbgpu.h).
+#include "qb_engine.h"
+
+extern "C" {
+#include "qbgpu.h"
+}
+
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+
+namespace {
+
+// run `f`; with QB_ABORT_ON_ERROR=0 a failure becomes a -1 return
+template <class F> int guarded(F &&f) {
+	try {
+		f();
+		return 0;
+	} catch (const std::exception &) {
+		return -1;
+	}
+}
+
+cudaStream_t pick(const qb_workspace *ws, void *stream) { return stream ? (cudaStream_t)stream : ws->stream; }
+
+void check(const qb_workspace *ws, const qb_quad *q) {
+	if (ws == nullptr || q == nullptr) QB_FAIL("null workspace or quadrature handle");
+	if (ws->N != q->q->N) QB_FAIL("workspace and quadrature tables are for different grid sizes");
+}
+
+// per-workspace per-point velocity tables for (N, L), kept in ws->vgrid
+const double *velocity_tables(qb_workspace *ws, double L, cudaStream_t s) {
+	const int N = ws->N;
+	const long NN = (long)N * N;
+	const double scale = (2 * L) / N;
+	std::vector<double> A(5 * NN + 1);
+	for (long j = 0; j < 4 * NN; j++) {
+		const int l = (int)((j % NN) / N);
+		A[j] = l < N / 2 ? scale * l : scale * (l - N);                                 // simulation.c:151-154
+	}
+	for (long q = 0; q < NN; q++) {
+		const int l = (int)(q / N);
+		A[4 * NN + q] = l < N / 2 ? scale * (l + 1) : scale * (l - N);                  // simulation.c:156-162
+	}
+	A[5 * NN] = L;
+	ws->vgrid.ensure(sizeof(double) * (5 * NN + 1));
+	QB_CUDA(cudaMemcpyAsync(ws->vgrid.p, A.data(), sizeof(double) * (5 * NN + 1), cudaMemcpyHostToDevice, s));
+	return ws->vgrid.as<double>();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *qb_last_error(void) {
+	thread_local std::string copy;
+	copy = qb::last_error();
+	return copy.c_str();
+}
+
+int qb_n_grid(void) { return N_GRID; }
+int qb_supported_n(int N) { return qb::supported_n(N) ? 1 : 0; }
+
+qb_quad *qb_quad_create(int N, int J, int M, double L, double R) {
+	qb_quad *q = nullptr;
+	guarded([&] {
+		if (!qb::supported_n(N)) QB_FAIL("grid size N=" + std::to_string(N) + " has no compiled kernels");
+		cudaStream_t s;
+		QB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+		auto base = qb::make_quad(N, J, M, L, R, s);
+		cudaStreamDestroy(s);
+		q = new qb_quad();
+		q->q = std::move(base);
+	});
+	return q;
+}
+
+void qb_quad_free(qb_quad *q) { delete q; }
+
+qb_workspace *qb_workspace_create(int N) {
+	qb_workspace *w = nullptr;
+	guarded([&] { w = new qb_workspace(N); });
+	return w;
+}
+
+void qb_workspace_free(qb_workspace *ws) { delete ws; }
+
+int qb_collision_operators(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, int parts, void *cc, void *cd, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		if (parts < 1 || parts > 3) QB_FAIL("parts must be 1 (Cc), 2 (Cd) or 3");
+		qb::collision_operators(*ws, q->q->set(), ncells, (const double2 *)W, parts, (double2 *)cc, (double2 *)cd, pick(ws, stream));
+	});
+}
+
+int qb_collision_step(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, const double *B, double dt, void *Wnext, int rk4, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		if (W == Wnext) QB_FAIL("qb_collision_step: Wnext must not alias W");
+		if (rk4) qb::collision_step_rk4(*ws, q->q->set(), ncells, (const double2 *)W, B, dt, (double2 *)Wnext, pick(ws, stream));
+		else qb::collision_step(*ws, q->q->set(), ncells, (const double2 *)W, B, dt, (double2 *)Wnext, pick(ws, stream));
+	});
+}
+
+int qb_inhom_step(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext, double h, double dt, const double *Bext, int bc, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		if (W == Wnext) QB_FAIL("qb_inhom_step: Wnext must not alias W");
+		if (bc != 0 && bc != 1) QB_FAIL("qb_inhom_step: bc must be 0 (periodic) or 1 (Dirichlet)");
+		cudaStream_t s = pick(ws, stream);
+		const double *A = velocity_tables(ws, q->q->L, s);
+		qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, s);
+	});
+}
+
+int qb_inhom_step_maxwell(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext, double h, double dt, double lambda,
+                          const double *WL, const double *WR, const double *Bext, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		if (W == Wnext) QB_FAIL("qb_inhom_step_maxwell: Wnext must not alias W");
+		cudaStream_t s = pick(ws, stream);
+		const double *A = velocity_tables(ws, q->q->L, s);
+		const long NN = (long)ws->N * ws->N;
+		qb::inhom_step_maxwell(*ws, q->q->set(), ncells, W, Wnext, A + 4 * NN, h, dt, lambda, WL, WR, Bext, s);
+	});
+}
+
+int qb_to_fourier(int N, int ngrids, const double *Wv, void *Wf, void *stream) {
+	return guarded([&] { qb::to_fourier(N, ngrids, Wv, (double2 *)Wf, (cudaStream_t)stream); });
+}
+
+int qb_from_fourier(int N, int ngrids, const void *Wf, double *Wv, void *stream) {
+	return guarded([&] { qb::from_fourier(N, ngrids, (const double2 *)Wf, Wv, (cudaStream_t)stream); });
+}
+
+int qb_integral(qb_workspace *ws, const qb_quad *q, int which, const void *f, const void *g, const void *h, void *out, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		cudaStream_t s = pick(ws, stream);
+		const double2 *F = (const double2 *)f, *G = (const double2 *)g, *H = (const double2 *)h;
+		switch (which) {
+		case 1: qb::integral_i1(*ws, q->q->i1, F, G, H, (double2 *)out, s); break;
+		case 2: qb::integral_i2(*ws, q->q->i2, F, G, H, (double2 *)out, s); break;
+		case 3: qb::integral_i3(*ws, q->q->i3, F, G, H, (double2 *)out, s); break;
+		case 4: qb::integral_i1(*ws, q->q->i4, F, G, H, (double2 *)out, s); break;
+		default: QB_FAIL("qb_integral: which must be 1..4");
+		}
+	});
+}
+
+int qb_transport(int N, double L, int ncells, const double *in, double *out, double h, double dt, int bc, void *stream) {
+	return guarded([&] {
+		if (!qb::supported_n(N)) QB_FAIL("qb_transport: unsupported N");
+		if (bc != 0 && bc != 1) QB_FAIL("qb_transport: bc must be 0 or 1");
+		thread_local std::unique_ptr<qb_workspace> tws;
+		if (!tws || tws->N != N) tws = std::make_unique<qb_workspace>(N);
+		cudaStream_t s = stream ? (cudaStream_t)stream : tws->stream;
+		const double *A = velocity_tables(tws.get(), L, s);
+		qb::transport(4 * N * N, ncells, in, out, A, h, dt, bc, s);
+	});
+}
+
+int qb_fourier_collision(qb_workspace *ws, const qb_quad *q, int ncells, double *W, const double *Bext, double dt, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		cudaStream_t s = pick(ws, stream);
+		const int N = ws->N;
+		const long cs = 4L * N * N;
+		ws->fa.ensure(sizeof(double2) * cs * ncells);
+		ws->fb.ensure(sizeof(double2) * cs * ncells);
+		qb::to_fourier(N, 4 * ncells, W, ws->fa.as<double2>(), s);
+		qb::collision_step(*ws, q->q->set(), ncells, ws->fa.as<double2>(), Bext, dt, ws->fb.as<double2>(), s);
+		qb::from_fourier(N, 4 * ncells, ws->fb.as<double2>(), W, s);
+	});
+}
+
+int qb_profile_enable(int on) { qb::prof_enable(on != 0); return 0; }
+int qb_profile_reset(void) { return guarded([&] { qb::prof_reset(); }); }
+int qb_profile_read(const char *prefix, double *ms, long *launches) {
+	return guarded([&] { qb::prof_read(prefix ? prefix : "", ms, launches); });
+}
+long qb_launch_count(void) { return qb::launch_count(); }
+
+}  // extern "C"
+
+// FP64 throughput probe: 8 independent FMA chains per thread
+__global__ void k_dfma_probe(int iters, double seed, double *sink) {
+	double a[8];
+#pragma unroll
+	for (int i = 0; i < 8; i++) a[i] = seed + threadIdx.x * 1e-9 + i;
+	const double b = 0.9999999, c = 1e-7;
+	for (int k = 0; k < iters; k++) {
+#pragma unroll
+		for (int i = 0; i < 8; i++) a[i] = fma(a[i], b, c);
+	}
+	double s = 0;
+#pragma unroll
+	for (int i = 0; i < 8; i++) s += a[i];
+	if (s == 123.456) sink[0] = s;   // keeps the loop alive; never true in practice
+}
+
+extern "C" double qb_fp64_peak_tflops(void) {
+	double result = -1;
+	guarded([&] {
+		int dev = 0, sms = 0;
+		QB_CUDA(cudaGetDevice(&dev));
+		QB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+		qb::DevBuf sink;
+		sink.ensure(sizeof(double));
+		const int threads = 256, blocks = sms * 8, iters = 20000;
+		cudaEvent_t e0, e1;
+		QB_CUDA(cudaEventCreate(&e0));
+		QB_CUDA(cudaEventCreate(&e1));
+		k_dfma_probe<<<blocks, threads>>>(100, 1.0, sink.as<double>());   // warm-up
+		double best = 0;
+		for (int rep = 0; rep < 3; rep++) {
+			QB_CUDA(cudaEventRecord(e0));
+			k_dfma_probe<<<blocks, threads>>>(iters, 1.0 + rep, sink.as<double>());
+			QB_CUDA(cudaEventRecord(e1));
+			QB_CUDA(cudaEventSynchronize(e1));
+			float ms = 0;
+			QB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+			const double flops = 2.0 * 8 * (double)iters * threads * blocks;
+			best = std::max(best, flops / (ms * 1e-3) / 1e12);
+		}
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		result = best;
+	});
+	return result;
+}

@@ -1,0 +1,148 @@
+// qb_fft.cuh — register/shared-memory FFT building blocks (FP64, sm_100a).
+//
+// A length-L transform (L = 8*T, T in {1,2,4,8}) is spread over T consecutive
+// lanes of one warp; every lane holds 8 complex values in registers:
+//   input : lane tau holds x[tau + T*r], r = 0..7
+//   step 1: radix-8 DFT over r in registers
+//   step 2: twiddle by w_L^(tau*q)
+//   step 3: transpose among the T lanes through an L-slot scratch (the row or
+//           column of the grid being transformed), XOR-swizzled so that a
+//           quarter-warp touches 8 distinct 16-byte bank groups
+//   step 4: R/T radix-T DFTs in registers
+//   output: lane tau' holds X[out_pos(tau', e)], e = 0..7
+// For T = 8 the output index set of a lane equals its input index set
+// (tau + 8e), which lets an inverse transform follow a forward one (or the
+// reverse) on the same column with no exchange in between.
+//
+// FFT sign convention as FFTW: DIR = -1 forward exp(-2 pi i jk/L),
+// DIR = +1 backward exp(+2 pi i jk/L), no normalisation.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace qb {
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {   // c + a*b
+	return make_double2(c.x + (a.x * b.x - a.y * b.y), c.y + (a.x * b.y + a.y * b.x));
+}
+__device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
+
+// a * (DIR * i)
+template <int DIR> __device__ __forceinline__ double2 mul_i(double2 a) {
+	return DIR < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+}
+// a * w8^1 with w8 = exp(DIR * 2 pi i / 8)
+template <int DIR> __device__ __forceinline__ double2 mul_w8(double2 a) {
+	const double s = 0.70710678118654752440;
+	return DIR < 0 ? make_double2(s * (a.x + a.y), s * (a.y - a.x)) : make_double2(s * (a.x - a.y), s * (a.x + a.y));
+}
+// a * w8^3
+template <int DIR> __device__ __forceinline__ double2 mul_w8_3(double2 a) {
+	const double s = 0.70710678118654752440;
+	return DIR < 0 ? make_double2(s * (a.y - a.x), -s * (a.x + a.y)) : make_double2(-s * (a.x + a.y), s * (a.x - a.y));
+}
+
+// in-place 8-point DFT, natural order in and out (radix-2 decimation in frequency)
+template <int DIR> __device__ __forceinline__ void dft8(double2 (&x)[8]) {
+	const double2 a0 = cadd(x[0], x[4]), a4 = csub(x[0], x[4]);
+	const double2 a1 = cadd(x[1], x[5]), a5 = mul_w8<DIR>(csub(x[1], x[5]));
+	const double2 a2 = cadd(x[2], x[6]), a6 = mul_i<DIR>(csub(x[2], x[6]));
+	const double2 a3 = cadd(x[3], x[7]), a7 = mul_w8_3<DIR>(csub(x[3], x[7]));
+	const double2 b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_i<DIR>(csub(a1, a3));
+	const double2 b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_i<DIR>(csub(a5, a7));
+	x[0] = cadd(b0, b1); x[4] = csub(b0, b1);
+	x[2] = cadd(b2, b3); x[6] = csub(b2, b3);
+	x[1] = cadd(b4, b5); x[5] = csub(b4, b5);
+	x[3] = cadd(b6, b7); x[7] = csub(b6, b7);
+}
+
+template <int DIR> __device__ __forceinline__ void dft4(double2 &x0, double2 &x1, double2 &x2, double2 &x3) {
+	const double2 a0 = cadd(x0, x2), a2 = csub(x0, x2), a1 = cadd(x1, x3), a3 = mul_i<DIR>(csub(x1, x3));
+	x0 = cadd(a0, a1); x2 = csub(a0, a1); x1 = cadd(a2, a3); x3 = csub(a2, a3);
+}
+
+__device__ __forceinline__ void dft2(double2 &x0, double2 &x1) {
+	const double2 a = x0; x0 = cadd(a, x1); x1 = csub(a, x1);
+}
+
+// Geometry of a length-L transform spread over T = L/8 lanes.
+template <int L> struct Len {
+	static_assert(L == 8 || L == 16 || L == 32 || L == 64, "supported transform lengths: 8..64");
+	static constexpr int T = L / 8;          // lanes per transform
+	static constexpr int U = 8 / T;          // radix-T DFTs per lane in step 4
+	// position of output e of lane tau
+	__device__ __forceinline__ static int out_pos(int tau, int e) { return (T == 1) ? e : (tau * U + e / T) + 8 * (e % T); }
+	// scratch slot of value (q, s) in the step-3 transpose
+	__device__ __forceinline__ static int xpos(int q, int s) { return q * T + (s ^ (q & (T - 1))); }
+};
+
+// Length-L transform of the 8 values in x (see file comment).  `scratch` is
+// an L-slot region addressed scratch[pos * sstride]; its previous contents are
+// destroyed.  `tw` holds w_L^e = exp(-2 pi i e/L), e < L.  Must be called by
+// all 32 lanes of the warp (contains __syncwarp).
+template <int L, int DIR>
+__device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch, int sstride, const double2 *tw) {
+	using G = Len<L>;
+	dft8<DIR>(x);
+	if constexpr (G::T > 1) {
+#pragma unroll
+		for (int q = 1; q < 8; q++) {
+			double2 w = tw[tau * q];
+			if (DIR > 0) w.y = -w.y;
+			x[q] = cmul(x[q], w);
+		}
+		__syncwarp();
+#pragma unroll
+		for (int q = 0; q < 8; q++) scratch[G::xpos(q, tau) * sstride] = x[q];
+		__syncwarp();
+#pragma unroll
+		for (int u = 0; u < G::U; u++)
+#pragma unroll
+			for (int s = 0; s < G::T; s++) x[u * G::T + s] = scratch[G::xpos(tau * G::U + u, s) * sstride];
+		__syncwarp();
+#pragma unroll
+		for (int u = 0; u < G::U; u++) {
+			if constexpr (G::T == 2) dft2(x[2 * u], x[2 * u + 1]);
+			else if constexpr (G::T == 4) dft4<DIR>(x[4 * u], x[4 * u + 1], x[4 * u + 2], x[4 * u + 3]);
+			else {
+				double2 y[8];
+#pragma unroll
+				for (int s = 0; s < 8; s++) y[s] = x[s];
+				dft8<DIR>(y);
+#pragma unroll
+				for (int s = 0; s < 8; s++) x[s] = y[s];
+			}
+		}
+	}
+}
+
+// Reorder a lane's transform outputs (positions out_pos) into the input
+// layout (positions tau + T*r) through the scratch; a no-op when T is 1 or 8.
+template <int L>
+__device__ __forceinline__ void out_to_in(double2 (&x)[8], int tau, double2 *scratch, int sstride) {
+	using G = Len<L>;
+	if constexpr (G::T != 1 && G::T != 8) {
+		__syncwarp();
+#pragma unroll
+		for (int e = 0; e < 8; e++) scratch[G::out_pos(tau, e) * sstride] = x[e];
+		__syncwarp();
+#pragma unroll
+		for (int r = 0; r < 8; r++) x[r] = scratch[(tau + G::T * r) * sstride];
+		__syncwarp();
+	}
+}
+
+// fill tw[e] = exp(-2 pi i e/L) for e < L (all threads of the block call it)
+template <int L>
+__device__ __forceinline__ void init_twiddles(double2 *tw) {
+	for (int e = threadIdx.x; e < L; e += blockDim.x) {
+		double s, c;
+		sincospi(-2.0 * (double)e / (double)L, &s, &c);
+		tw[e] = make_double2(c, s);
+	}
+}
+
+}  // namespace qb

@@ -1,0 +1,593 @@
+// qb_kernels.cuh — FP64 collision / transport kernels for sm_100a.
+//
+// Notation: N = velocity grid size, P = 2N padded size, all Fourier-space
+// grids complex (double2), element (l, k) at index k + n*l.  A P x P grid in
+// shared memory uses the row pitch LDP = P + 1 so that both row passes (one
+// row per quarter-warp) and column passes (one column per quarter-warp) are
+// free of bank conflicts.  A CTA has P*T threads (T = P/8 lanes per line,
+// one line = one row or one column): thread tid works on line tid / T as
+// lane tau = tid % T.
+//
+// The collision right-hand side is evaluated in factored form (upstream
+// loops: src/integrals.c:90-379, src/collision.c:74-254):
+//   x^ = FFT2(Pad(x)) for the four Pauli components (k_pad_fft)
+//   I1/I4-type sums  S = sum_t phi_t . IFFT2(F . FFT2(Pad(psi2_t . g)))  (k_i1_terms)
+//   I2-type sums     Q = sum_t FFT2(Pad(psi1_t f)) . FFT2(Pad(psi2_t g))  (k_i2_terms)
+//   I3-type sums     X_r = sum_t sum_i coef_i P_{t,a_i} . FFT2(psi2_t . IFFT2(G_i . P_{t,r}))
+//                    with P_{t,c} = FFT2(Pad(psi1_t . W_c))               (k_i3)
+//   then outer FFT/IFFT, Extract and the Pauli combination (k_fft_full, k_assemble).
+// Moving the sums over quadrature terms inside the outer transforms is exact
+// in real arithmetic; results agree with the upstream loop order to rounding.
+#pragma once
+#include <cooperative_groups.h>
+#include "qb_fft.cuh"
+
+namespace qb {
+
+namespace cg = cooperative_groups;
+
+template <int P> struct Geo {
+	static constexpr int N = P / 2;
+	static constexpr int T = Len<P>::T;
+	static constexpr int LDP = P + 1;
+	static constexpr int NT = P * T;            // threads per CTA
+	static constexpr int GRID = P * LDP;        // smem slots of one padded grid
+	// padded index -> index in the N grid, or -1 inside the zero band
+	__device__ __forceinline__ static int src(int p) { return p < N / 2 ? p : (p >= 3 * N / 2 ? p - N : -1); }
+	// N-grid index -> padded index (GridZeroPad, upstream src/grid.c:171-188)
+	__device__ __forceinline__ static int pad(int k) { return k < N / 2 ? k : k + N; }
+};
+
+// ---------------------------------------------------------------------------
+// multipliers applied to the N-grid input before zero padding
+struct MulNone {
+	__device__ __forceinline__ double2 operator()(int, double2 v) const { return v; }
+};
+struct MulReal {           // psi (real N x N) .* v   (MultiplyPointwiseRC)
+	const double *psi;
+	__device__ __forceinline__ double2 operator()(int idx, double2 v) const { const double p = psi[idx]; return make_double2(p * v.x, p * v.y); }
+};
+struct MulCplx {           // psi (complex N x N) .* v   (MultiplyPointwiseCC)
+	const double2 *psi;
+	__device__ __forceinline__ double2 operator()(int idx, double2 v) const { return cmul(psi[idx], v); }
+};
+
+// lane's 8 inputs of padded row `prow` of Pad(mul . src)
+template <int P, class Mul>
+__device__ __forceinline__ void load_pad_row(double2 (&x)[8], int prow, int tau, const double2 *__restrict__ src, const Mul &mul) {
+	using G = Geo<P>;
+	const int l = G::src(prow);
+#pragma unroll
+	for (int r = 0; r < 8; r++) {
+		const int k = G::src(tau + G::T * r);
+		x[r] = (l >= 0 && k >= 0) ? mul(k + G::N * l, src[k + G::N * l]) : czero();
+	}
+}
+
+// FFT2 (direction DIR) of Pad(mul . src) into the smem grid S (in place, two passes)
+template <int P, int DIR, class Mul>
+__device__ __forceinline__ void fft2_pad(double2 *S, const double2 *tw, const double2 *__restrict__ src, const Mul &mul) {
+	using G = Geo<P>;
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	double2 x[8];
+	load_pad_row<P>(x, line, tau, src, mul);
+	fft1d<P, DIR>(x, tau, S + line * G::LDP, 1, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[line * G::LDP + Len<P>::out_pos(tau, e)] = x[e];
+	__syncthreads();
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = S[(tau + G::T * r) * G::LDP + line];
+	fft1d<P, DIR>(x, tau, S + line, G::LDP, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[Len<P>::out_pos(tau, e) * G::LDP + line] = x[e];
+	__syncthreads();
+}
+
+// FFT2 of a full grid already in smem S (natural layout), in place
+template <int P, int DIR>
+__device__ __forceinline__ void fft2_smem(double2 *S, const double2 *tw) {
+	using G = Geo<P>;
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	double2 x[8];
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = S[line * G::LDP + tau + G::T * r];
+	fft1d<P, DIR>(x, tau, S + line * G::LDP, 1, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[line * G::LDP + Len<P>::out_pos(tau, e)] = x[e];
+	__syncthreads();
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = S[(tau + G::T * r) * G::LDP + line];
+	fft1d<P, DIR>(x, tau, S + line, G::LDP, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[Len<P>::out_pos(tau, e) * G::LDP + line] = x[e];
+	__syncthreads();
+}
+
+// copy smem grid (pitch LDP) to a dense global P x P grid, coalesced
+template <int P>
+__device__ __forceinline__ void smem_to_global(double2 *__restrict__ out, const double2 *S) {
+	using G = Geo<P>;
+	for (int i = threadIdx.x; i < P * P; i += G::NT) out[i] = S[(i / P) * G::LDP + (i % P)];
+}
+
+// ---------------------------------------------------------------------------
+// K1: padded forward spectra  out[b] = FFT2(Pad(src[b]))   (one CTA per grid)
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT) k_pad_fft(const double2 *__restrict__ src, double2 *__restrict__ out) {
+	using G = Geo<P>;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + G::GRID;
+	init_twiddles<P>(tw);
+	__syncthreads();
+	const long b = blockIdx.x;
+	fft2_pad<P, -1>(S, tw, src + b * G::N * G::N, MulNone{});
+	smem_to_global<P>(out + b * P * P, S);
+}
+
+// ---------------------------------------------------------------------------
+// K2: I1/I4-type term sums
+//   S[cell][task][chunk] = sum_{t in chunk} phi_t . IFFT2(F . FFT2(Pad(psi2_t . g)))
+//   g = gsrc[cell][g_comp[task]],  F = fa * What[cell][f_comp] + fb
+struct I1Params {
+	int ntask, nchunk, nterms;
+	const double2 *g; long g_cell;          // N x N grids
+	int g_comp[4];
+	const double2 *What; long w_cell;       // P x P grids
+	int f_comp; double fa, fb;
+	const double *psi2;                     // nterms x N x N
+	const double *phi;                      // nterms x P x P
+	double2 *out;                           // [cell][task][chunk][P*P]
+};
+
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1Params p) {
+	using G = Geo<P>;
+	using Lp = Len<P>;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *F = smem + G::GRID, *tw = smem + 2 * G::GRID;
+	const int chunk = blockIdx.x % p.nchunk;
+	const int task = (blockIdx.x / p.nchunk) % p.ntask;
+	const long cell = blockIdx.x / (p.nchunk * p.ntask);
+	init_twiddles<P>(tw);
+	const double2 *W = p.What + cell * p.w_cell + (long)p.f_comp * P * P;
+	for (int i = threadIdx.x; i < P * P; i += G::NT) {
+		const double2 w = W[i];
+		F[(i / P) * G::LDP + (i % P)] = make_double2(p.fa * w.x + p.fb, p.fa * w.y);
+	}
+	__syncthreads();
+	const double2 *g = p.g + cell * p.g_cell + (long)p.g_comp[task] * G::N * G::N;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	double2 acc[8];
+#pragma unroll
+	for (int e = 0; e < 8; e++) acc[e] = czero();
+	for (int t = t0; t < t1; t++) {
+		double2 x[8];
+		// rows: FFT of Pad(psi2_t . g)
+		load_pad_row<P>(x, line, tau, g, MulReal{p.psi2 + (long)t * G::N * G::N});
+		fft1d<P, -1>(x, tau, S + line * G::LDP, 1, tw);
+#pragma unroll
+		for (int e = 0; e < 8; e++) S[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+		__syncthreads();
+		// columns: FFT, multiply by F (convolution with f), inverse FFT
+#pragma unroll
+		for (int r = 0; r < 8; r++) x[r] = S[(tau + G::T * r) * G::LDP + line];
+		fft1d<P, -1>(x, tau, S + line, G::LDP, tw);
+#pragma unroll
+		for (int e = 0; e < 8; e++) x[e] = cmul(F[Lp::out_pos(tau, e) * G::LDP + line], x[e]);
+		out_to_in<P>(x, tau, S + line, G::LDP);
+		fft1d<P, +1>(x, tau, S + line, G::LDP, tw);
+#pragma unroll
+		for (int e = 0; e < 8; e++) S[Lp::out_pos(tau, e) * G::LDP + line] = x[e];
+		__syncthreads();
+		// rows: inverse FFT, multiply by phi_t, accumulate
+#pragma unroll
+		for (int r = 0; r < 8; r++) x[r] = S[line * G::LDP + tau + G::T * r];
+		fft1d<P, +1>(x, tau, S + line * G::LDP, 1, tw);
+		const double *phi = p.phi + (long)t * P * P + line * P;
+#pragma unroll
+		for (int e = 0; e < 8; e++) {
+			const double f = phi[Lp::out_pos(tau, e)];
+			acc[e].x += f * x[e].x;
+			acc[e].y += f * x[e].y;
+		}
+		__syncthreads();
+	}
+	double2 *o = p.out + ((cell * p.ntask + task) * p.nchunk + chunk) * (long)P * P + line * P;
+#pragma unroll
+	for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
+}
+
+// ---------------------------------------------------------------------------
+// K3: I2-type term sums
+//   Q[cell][task][chunk] = sum_t FFT2(Pad(psi1_t . f)) . FFT2(Pad(psi2_t . g))
+struct I2Params {
+	int ntask, nchunk, nterms;
+	const double2 *src; long cell_stride;   // N x N grids
+	int f_comp[4], g_comp[4];
+	const double *psi1, *psi2;              // nterms x N x N each
+	double2 *out;                           // [cell][task][chunk][P*P]
+};
+
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2Params p) {
+	using G = Geo<P>;
+	using Lp = Len<P>;
+	extern __shared__ double2 smem[];
+	double2 *A = smem, *B = smem + G::GRID, *tw = smem + 2 * G::GRID;
+	const int chunk = blockIdx.x % p.nchunk;
+	const int task = (blockIdx.x / p.nchunk) % p.ntask;
+	const long cell = blockIdx.x / (p.nchunk * p.ntask);
+	init_twiddles<P>(tw);
+	__syncthreads();
+	const double2 *f = p.src + cell * p.cell_stride + (long)p.f_comp[task] * G::N * G::N;
+	const double2 *g = p.src + cell * p.cell_stride + (long)p.g_comp[task] * G::N * G::N;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	double2 acc[8];
+#pragma unroll
+	for (int e = 0; e < 8; e++) acc[e] = czero();
+	for (int t = t0; t < t1; t++) {
+		fft2_pad<P, -1>(A, tw, f, MulReal{p.psi1 + (long)t * G::N * G::N});
+		double2 x[8];
+		load_pad_row<P>(x, line, tau, g, MulReal{p.psi2 + (long)t * G::N * G::N});
+		fft1d<P, -1>(x, tau, B + line * G::LDP, 1, tw);
+#pragma unroll
+		for (int e = 0; e < 8; e++) B[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+		__syncthreads();
+#pragma unroll
+		for (int r = 0; r < 8; r++) x[r] = B[(tau + G::T * r) * G::LDP + line];
+		fft1d<P, -1>(x, tau, B + line, G::LDP, tw);
+#pragma unroll
+		for (int e = 0; e < 8; e++) acc[e] = cfma(A[Lp::out_pos(tau, e) * G::LDP + line], x[e], acc[e]);
+		__syncthreads();
+	}
+	// column-mapped accumulator -> smem -> coalesced store
+#pragma unroll
+	for (int e = 0; e < 8; e++) A[Lp::out_pos(tau, e) * G::LDP + line] = acc[e];
+	__syncthreads();
+	smem_to_global<P>(p.out + ((cell * p.ntask + task) * p.nchunk + chunk) * (long)P * P, A);
+}
+
+// ---------------------------------------------------------------------------
+// K4: I3-type sums on a cluster of CS CTAs (one per source component).
+// CTA r of the cluster for (cell, chunk) computes P_r = FFT2(Pad(psi1_t . src_r))
+// into its shared memory; the other CTAs read it through distributed shared
+// memory.  For each of its combos (a, g, coef) it accumulates
+//   X_r += coef * P_a . FFT2(psi2_t . IFFT2(G_g . P_r)).
+struct I3Params {
+	int nchunk, nterms;
+	const double2 *src; long src_cell; int src_comp[4];   // N x N grids
+	const double2 *Ghat; long g_cell;                     // P x P grids, G_g at Ghat + cell*g_cell + g*P*P
+	int ncombo[4]; int ca[4][4], cgi[4][4]; double ccoef[4][4];
+	const double2 *psi1;                                  // nterms x N x N (complex)
+	const double *psi2T;                                  // transposed P x P tables
+	const int *psi2_idx; const double *psi2_scale;        // per term
+	double2 *out;                                         // [cell][chunk][CS][P*P]
+};
+
+template <int P, int CS>
+__global__ void __launch_bounds__(Geo<P>::NT) k_i3(const I3Params p) {
+	using G = Geo<P>;
+	using Lp = Len<P>;
+	extern __shared__ double2 smem[];
+	double2 *Pr = smem, *Ug = smem + G::GRID, *tw = smem + 2 * G::GRID;
+	cg::cluster_group cluster = cg::this_cluster();
+	const int rank = (int)cluster.block_rank();
+	const long cid = blockIdx.x / CS;
+	const int chunk = (int)(cid % p.nchunk);
+	const long cell = cid / p.nchunk;
+	init_twiddles<P>(tw);
+	__syncthreads();
+	const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[rank] * G::N * G::N;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	double2 acc[8];
+#pragma unroll
+	for (int e = 0; e < 8; e++) acc[e] = czero();
+	const int nc = p.ncombo[rank];
+	for (int t = t0; t < t1; t++) {
+		fft2_pad<P, -1>(Pr, tw, src, MulCplx{p.psi1 + (long)t * G::N * G::N});
+		cluster.sync();
+		const double *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
+		const double sc = p.psi2_scale[t];
+		for (int c = 0; c < nc; c++) {
+			const double2 *Gg = p.Ghat + cell * p.g_cell + (long)p.cgi[rank][c] * P * P;
+			double2 x[8];
+			// rows: IFFT of G_g . P_r
+#pragma unroll
+			for (int r = 0; r < 8; r++) {
+				const int k = tau + G::T * r;
+				x[r] = cmul(Gg[line * P + k], Pr[line * G::LDP + k]);
+			}
+			fft1d<P, +1>(x, tau, Ug + line * G::LDP, 1, tw);
+#pragma unroll
+			for (int e = 0; e < 8; e++) Ug[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+			__syncthreads();
+			// columns: IFFT, multiply by psi2_t, FFT
+#pragma unroll
+			for (int r = 0; r < 8; r++) x[r] = Ug[(tau + G::T * r) * G::LDP + line];
+			fft1d<P, +1>(x, tau, Ug + line, G::LDP, tw);
+#pragma unroll
+			for (int e = 0; e < 8; e++) {
+				const double f = sc * psi2[line * P + Lp::out_pos(tau, e)];
+				x[e].x *= f;
+				x[e].y *= f;
+			}
+			out_to_in<P>(x, tau, Ug + line, G::LDP);
+			fft1d<P, -1>(x, tau, Ug + line, G::LDP, tw);
+#pragma unroll
+			for (int e = 0; e < 8; e++) Ug[Lp::out_pos(tau, e) * G::LDP + line] = x[e];
+			__syncthreads();
+			// rows: FFT, multiply by P_a (remote), accumulate
+#pragma unroll
+			for (int r = 0; r < 8; r++) x[r] = Ug[line * G::LDP + tau + G::T * r];
+			fft1d<P, -1>(x, tau, Ug + line * G::LDP, 1, tw);
+			const double2 *Pa = cluster.map_shared_rank(Pr, p.ca[rank][c]);
+			const double coef = p.ccoef[rank][c];
+#pragma unroll
+			for (int e = 0; e < 8; e++) {
+				const double2 v = cmul(Pa[line * G::LDP + Lp::out_pos(tau, e)], x[e]);
+				acc[e].x += coef * v.x;
+				acc[e].y += coef * v.y;
+			}
+			__syncthreads();
+		}
+		cluster.sync();
+	}
+	double2 *o = p.out + ((cell * p.nchunk + chunk) * CS + rank) * (long)P * P + line * P;
+#pragma unroll
+	for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
+}
+
+// ---------------------------------------------------------------------------
+// K5: out[b] = FFT2(sum_{k<nparts} in[b*grid_stride + k*part_stride]) (full grids)
+struct FullParams {
+	const double2 *in; long grid_stride, part_stride; int nparts;
+	double2 *out;   // [b][P*P]
+};
+
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT) k_fft_full(const FullParams p) {
+	using G = Geo<P>;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + G::GRID;
+	init_twiddles<P>(tw);
+	const long b = blockIdx.x;
+	const double2 *in = p.in + b * p.grid_stride;
+	for (int i = threadIdx.x; i < P * P; i += G::NT) {
+		double2 s = in[i];
+		for (int k = 1; k < p.nparts; k++) s = cadd(s, in[k * p.part_stride + i]);
+		S[(i / P) * G::LDP + (i % P)] = s;
+	}
+	__syncthreads();
+	fft2_smem<P, -1>(S, tw);
+	smem_to_global<P>(p.out + b * (long)P * P, S);
+}
+
+// ---------------------------------------------------------------------------
+// K6: assembly of Cc and Cd for one (cell, component j):
+//   Zcc_j = Wh_h . FS_g - Wh_g . FS_h          ((g,h) = (2,3),(3,1),(1,2); upstream collision.c:232-253)
+//   Zcd_j = s2 (-Wh_j + d_j0) . Q - eta2_j s1 X_j
+//         + s1 (eta2_j Wh_0 . FS4_j + 2 Wh_j . FS4_0) - d_j0 2 s1 sum_c Wh_c . FS4_c   (collision.c:95-167)
+//   Cc_j = s1 Extract(IFFT2(Zcc_j)), Cd_j = Extract(IFFT2(Zcd_j))
+// mode 0 writes Cc and Cd; mode 1 writes base + dtc (Cc + Cd + CB) with the
+// magnetic rotation CB of `wcur` (upstream simulation.c:75-135).
+struct AsmParams {
+	const double2 *What;              // [cell][4][P*P]
+	const double2 *FS;                // [cell][3][P*P]  FFT2 of the Cc sums S_1..S_3, or null
+	const double2 *FS4;               // [cell][4][P*P]  FFT2 of the I4 sums, or null
+	const double2 *Qp; int nq;        // [cell][4][nq][P*P] I2 partials, or null
+	const double2 *Xp; int nx;        // [cell][nx][4][P*P] I3 partials, or null
+	double s1, s2;
+	int mode;
+	double2 *out_cc, *out_cd;         // mode 0: [cell][4][N*N] (either may be null)
+	const double2 *base, *wcur;       // mode 1: [cell][4][N*N]
+	const double *B; double dtc;      // B: [cell][3]
+	double2 *out;                     // mode 1
+};
+
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
+	using G = Geo<P>;
+	constexpr int N = G::N, NN = N * N, PP = P * P;
+	constexpr int PER = (NN + G::NT - 1) / G::NT;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + G::GRID;
+	const int j = blockIdx.x & 3;
+	const long cell = blockIdx.x >> 2;
+	init_twiddles<P>(tw);
+	const double eta2[4] = { 2, -2, -2, -2 };
+	const double2 *Wh = p.What + cell * 4 * PP;
+	double2 cc[PER], cd[PER];
+#pragma unroll
+	for (int u = 0; u < PER; u++) { cc[u] = czero(); cd[u] = czero(); }
+
+	// --- Cc ---
+	if (p.FS != nullptr && j > 0) {
+		const int gi = (j % 3) + 1, hi = ((j + 1) % 3) + 1;    // j=1:(2,3) j=2:(3,1) j=3:(1,2)
+		const double2 *FS = p.FS + cell * 3 * PP;
+		for (int i = threadIdx.x; i < PP; i += G::NT) {
+			const double2 z = csub(cmul(Wh[hi * PP + i], FS[(gi - 1) * PP + i]), cmul(Wh[gi * PP + i], FS[(hi - 1) * PP + i]));
+			S[(i / P) * G::LDP + (i % P)] = z;
+		}
+		__syncthreads();
+		fft2_smem<P, +1>(S, tw);
+#pragma unroll
+		for (int u = 0; u < PER; u++) {
+			const int q = threadIdx.x + u * G::NT;
+			if (q < NN) {
+				const double2 v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+				cc[u] = make_double2(p.s1 * v.x, p.s1 * v.y);
+			}
+		}
+		__syncthreads();
+	}
+	// --- Cd ---
+	if (p.FS4 != nullptr || p.Qp != nullptr || p.Xp != nullptr) {
+		for (int i = threadIdx.x; i < PP; i += G::NT) {
+			double2 z = czero();
+			if (p.Qp != nullptr) {
+				double2 q = czero();
+				for (int ii = 0; ii < 4; ii++) {
+					const double2 *Q = p.Qp + ((cell * 4 + ii) * p.nq) * (long)PP + i;
+					double2 s = czero();
+					for (int k = 0; k < p.nq; k++) s = cadd(s, Q[(long)k * PP]);
+					q.x += eta2[ii] * s.x; q.y += eta2[ii] * s.y;
+				}
+				double2 h = make_double2(-Wh[j * PP + i].x, -Wh[j * PP + i].y);
+				if (j == 0) h.x += 1.0;
+				const double2 v = cmul(h, q);
+				z.x += p.s2 * v.x; z.y += p.s2 * v.y;
+			}
+			if (p.Xp != nullptr) {
+				double2 s = czero();
+				for (int k = 0; k < p.nx; k++) s = cadd(s, p.Xp[((cell * p.nx + k) * 4 + j) * (long)PP + i]);
+				z.x -= eta2[j] * p.s1 * s.x; z.y -= eta2[j] * p.s1 * s.y;
+			}
+			if (p.FS4 != nullptr) {
+				const double2 *F4 = p.FS4 + cell * 4 * PP;
+				double2 v = cadd(cscale(cmul(Wh[i], F4[j * PP + i]), eta2[j]), cscale(cmul(Wh[j * PP + i], F4[i]), 2.0));
+				if (j == 0) {
+					double2 s = czero();
+					for (int c = 0; c < 4; c++) s = cadd(s, cmul(Wh[c * PP + i], F4[c * PP + i]));
+					v = csub(v, cscale(s, 2.0));
+				}
+				z.x += p.s1 * v.x; z.y += p.s1 * v.y;
+			}
+			S[(i / P) * G::LDP + (i % P)] = z;
+		}
+		__syncthreads();
+		fft2_smem<P, +1>(S, tw);
+#pragma unroll
+		for (int u = 0; u < PER; u++) {
+			const int q = threadIdx.x + u * G::NT;
+			if (q < NN) cd[u] = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+		}
+	}
+	// --- outputs ---
+#pragma unroll
+	for (int u = 0; u < PER; u++) {
+		const int q = threadIdx.x + u * G::NT;
+		if (q >= NN) continue;
+		const long o = (cell * 4 + j) * NN + q;
+		if (p.mode == 0) {
+			if (p.out_cc) p.out_cc[o] = cc[u];
+			if (p.out_cd) p.out_cd[o] = cd[u];
+		} else {
+			const double *B = p.B + cell * 3;
+			const double2 *w = p.wcur + cell * 4 * NN + q;
+			double2 cb = czero();          // -i [B, W] = 2 (B x w) . sigma
+			if (j == 1) cb = make_double2(2 * (B[1] * w[3 * NN].x - B[2] * w[2 * NN].x), 2 * (B[1] * w[3 * NN].y - B[2] * w[2 * NN].y));
+			if (j == 2) cb = make_double2(2 * (B[2] * w[1 * NN].x - B[0] * w[3 * NN].x), 2 * (B[2] * w[1 * NN].y - B[0] * w[3 * NN].y));
+			if (j == 3) cb = make_double2(2 * (B[0] * w[2 * NN].x - B[1] * w[1 * NN].x), 2 * (B[0] * w[2 * NN].y - B[1] * w[1 * NN].y));
+			const double2 b = p.base[o];
+			p.out[o] = make_double2(b.x + p.dtc * ((cc[u].x + cd[u].x) + cb.x), b.y + p.dtc * ((cc[u].y + cd[u].y) + cb.y));
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------
+// K7: velocity space -> Fourier space, one CTA per real N x N component:
+//   FFT2 / N^2 with the Hermitian completion of upstream simulation.c:224-261
+template <int N>
+__global__ void __launch_bounds__(Len<N>::T * N) k_to_fourier(const double *__restrict__ Wv, double2 *__restrict__ Wf) {
+	constexpr int T = Len<N>::T, LD = N + 1;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + N * LD;
+	init_twiddles<N>(tw);
+	__syncthreads();
+	const long b = blockIdx.x;
+	const double *in = Wv + b * N * N;
+	const int line = threadIdx.x / T, tau = threadIdx.x % T;
+	double2 x[8];
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = make_double2(in[line * N + tau + T * r], 0.0);
+	fft1d<N, -1>(x, tau, S + line * LD, 1, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[line * LD + Len<N>::out_pos(tau, e)] = x[e];
+	__syncthreads();
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = S[(tau + T * r) * LD + line];
+	fft1d<N, -1>(x, tau, S + line, LD, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[Len<N>::out_pos(tau, e) * LD + line] = x[e];
+	__syncthreads();
+	const double scale = 1.0 / (N * N);
+	double2 *out = Wf + b * N * N;
+	for (int i = threadIdx.x; i < N * N; i += T * N) {
+		const int l = i / N, k = i % N;
+		if (k <= N / 2) {
+			const double2 v = S[l * LD + k];
+			out[i] = make_double2(v.x * scale, v.y * scale);
+		} else {
+			const int lc = (N - l) % N, kc = N - k;
+			const double2 v = S[lc * LD + kc];
+			out[i] = make_double2(v.x * scale, -(v.y * scale));
+		}
+	}
+}
+
+// K8: Fourier space -> velocity space: backward FFT2, real part (simulation.c:270-283)
+template <int N>
+__global__ void __launch_bounds__(Len<N>::T * N) k_from_fourier(const double2 *__restrict__ Wf, double *__restrict__ Wv) {
+	constexpr int T = Len<N>::T, LD = N + 1;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + N * LD;
+	init_twiddles<N>(tw);
+	__syncthreads();
+	const long b = blockIdx.x;
+	const double2 *in = Wf + b * N * N;
+	const int line = threadIdx.x / T, tau = threadIdx.x % T;
+	double2 x[8];
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = in[line * N + tau + T * r];
+	fft1d<N, +1>(x, tau, S + line * LD, 1, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[line * LD + Len<N>::out_pos(tau, e)] = x[e];
+	__syncthreads();
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = S[(tau + T * r) * LD + line];
+	fft1d<N, +1>(x, tau, S + line, LD, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[Len<N>::out_pos(tau, e) * LD + line] = x[e];
+	__syncthreads();
+	double *out = Wv + b * N * N;
+	for (int i = threadIdx.x; i < N * N; i += T * N) out[i] = S[(i / N) * LD + (i % N)].x;
+}
+
+// K9: generic 2-D transform of n0 x n1 = L x L complex grids (FFTW-API plans).
+// mode 0: c2c (in complex), mode 1: r2c (in real, out n0 x (L/2+1))
+template <int L, int DIR>
+__global__ void __launch_bounds__(Len<L>::T * L) k_fft2_generic(const void *__restrict__ in, double2 *__restrict__ out, int r2c) {
+	constexpr int T = Len<L>::T, LD = L + 1;
+	extern __shared__ double2 smem[];
+	double2 *S = smem, *tw = smem + L * LD;
+	init_twiddles<L>(tw);
+	__syncthreads();
+	const int line = threadIdx.x / T, tau = threadIdx.x % T;
+	double2 x[8];
+#pragma unroll
+	for (int r = 0; r < 8; r++) {
+		const int i = line * L + tau + T * r;
+		x[r] = r2c ? make_double2(((const double *)in)[i], 0.0) : ((const double2 *)in)[i];
+	}
+	fft1d<L, DIR>(x, tau, S + line * LD, 1, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[line * LD + Len<L>::out_pos(tau, e)] = x[e];
+	__syncthreads();
+#pragma unroll
+	for (int r = 0; r < 8; r++) x[r] = S[(tau + T * r) * LD + line];
+	fft1d<L, DIR>(x, tau, S + line, LD, tw);
+#pragma unroll
+	for (int e = 0; e < 8; e++) S[Len<L>::out_pos(tau, e) * LD + line] = x[e];
+	__syncthreads();
+	if (r2c) {
+		constexpr int H = L / 2 + 1;
+		for (int i = threadIdx.x; i < L * H; i += T * L) out[i] = S[(i / H) * LD + (i % H)];
+	} else {
+		for (int i = threadIdx.x; i < L * L; i += T * L) out[i] = S[(i / L) * LD + (i % L)];
+	}
+}
+
+}  // namespace qb

@@ -1,0 +1,463 @@
+"""Python binding of libqbgpu (ctypes) — used by the tests, the smoke check and bench.py.
+
+Two surfaces:
+  * ``Upstream`` — the upstream C API exactly as a C caller sees it (host
+    buffers, struct pointers; N_GRID = 32 in lib/libqbgpu.so).  This is the
+    drop-in boundary: the same entry points test/*_test.c and main_*.c call.
+  * ``Quad`` / ``Workspace`` + module functions — the batched extension API of
+    include/qbgpu.h on device tensors (torch CUDA tensors are used only as
+    device memory and for the stream handle).
+
+The module never computes anything on the CPU: every operator is a call into
+the CUDA library, and loading fails loudly when the library is missing.
+
+Layouts (upstream): velocity-space cell = 4 real N x N grids (float64),
+Fourier-space cell = 4 complex N x N grids (complex128), element (l, k) at
+[..., l, k] == upstream index k + N*l; cells consecutive.
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+N_GRID = 32
+
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+
+def library_path(n_grid=N_GRID):
+    name = "libqbgpu.so" if n_grid == 32 else f"libqbgpu_n{n_grid}.so"
+    return os.path.join(LIB_DIR, name)
+
+
+_libs = {}
+
+
+def lib(n_grid=N_GRID):
+    """Load libqbgpu (raises if it has not been built)."""
+    if n_grid in _libs:
+        return _libs[n_grid]
+    path = library_path(n_grid)
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python inhom-quantum-boltzmann-fourier-c_b200/build.py`")
+    L = C.CDLL(path)
+    L.qb_last_error.restype = C.c_char_p
+    L.qb_quad_create.restype = _vp
+    L.qb_quad_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
+    L.qb_quad_free.argtypes = [_vp]
+    L.qb_workspace_create.restype = _vp
+    L.qb_workspace_create.argtypes = [C.c_int]
+    L.qb_workspace_free.argtypes = [_vp]
+    L.qb_collision_operators.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp]
+    L.qb_collision_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, _vp, C.c_int, _vp]
+    L.qb_inhom_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, C.c_double, _vp, C.c_int, _vp]
+    L.qb_inhom_step_maxwell.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp, _vp]
+    L.qb_to_fourier.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
+    L.qb_from_fourier.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
+    L.qb_integral.argtypes = [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.CalculateRightwardFlux.restype = C.c_double
+    L.CalculateLeftwardFlux.restype = C.c_double
+    _libs[n_grid] = L
+    return L
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed: {lib().qb_last_error().decode()}")
+
+
+# ---------------------------------------------------------------------------
+# batched extension API on device tensors
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device is required")
+    return torch
+
+
+def _stream():
+    return _vp(_torch().cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    assert t.is_cuda and t.is_contiguous()
+    return _vp(t.data_ptr())
+
+
+class Quad:
+    """Device quadrature tables (FourierI1..I4) for grid size N."""
+
+    def __init__(self, N, J, M, L, R):
+        self.N, self.J, self.M, self.L, self.R = N, J, M, L, R
+        self.h = lib().qb_quad_create(N, J, M, L, R)
+        if not self.h:
+            raise RuntimeError(f"qb_quad_create failed: {lib().qb_last_error().decode()}")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().qb_quad_free(self.h)
+            self.h = None
+
+
+class Workspace:
+    """Device scratch for one grid size (grows on demand)."""
+
+    def __init__(self, N):
+        self.N = N
+        self.h = lib().qb_workspace_create(N)
+        if not self.h:
+            raise RuntimeError(f"qb_workspace_create failed: {lib().qb_last_error().decode()}")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().qb_workspace_free(self.h)
+            self.h = None
+
+
+def collision_operators(ws, q, W, parts=3):
+    """(Cc, Cd) of Fourier states W: complex128 CUDA tensor (ncells, 4, N, N)."""
+    torch = _torch()
+    n = W.shape[0]
+    cc = torch.empty_like(W) if parts & 1 else None
+    cd = torch.empty_like(W) if parts & 2 else None
+    _check(lib().qb_collision_operators(ws.h, q.h, n, _ptr(W), parts, _ptr(cc) if cc is not None else None,
+                                        _ptr(cd) if cd is not None else None, _stream()), "qb_collision_operators")
+    return cc, cd
+
+
+def collision_step(ws, q, W, dt, B=None, rk4=False, out=None):
+    torch = _torch()
+    n = W.shape[0]
+    if B is None:
+        B = torch.zeros((n, 3), dtype=torch.float64, device=W.device)
+    out = torch.empty_like(W) if out is None else out
+    _check(lib().qb_collision_step(ws.h, q.h, n, _ptr(W), _ptr(B), dt, _ptr(out), 1 if rk4 else 0, _stream()), "qb_collision_step")
+    return out
+
+
+def inhom_step(ws, q, W, h, dt, Bext=None, bc="periodic", out=None):
+    """One Strang step; W: float64 CUDA tensor (ncells, 4, N, N)."""
+    torch = _torch()
+    n = W.shape[0]
+    if Bext is None:
+        Bext = torch.zeros((n, 3), dtype=torch.float64, device=W.device)
+    out = torch.empty_like(W) if out is None else out
+    _check(lib().qb_inhom_step(ws.h, q.h, n, _ptr(W), _ptr(out), h, dt, _ptr(Bext), 0 if bc == "periodic" else 1, _stream()),
+           "qb_inhom_step")
+    return out
+
+
+def inhom_step_maxwell(ws, q, W, h, dt, lam, WL, WR, Bext=None, out=None):
+    torch = _torch()
+    n = W.shape[0]
+    if Bext is None:
+        Bext = torch.zeros((n, 3), dtype=torch.float64, device=W.device)
+    out = torch.empty_like(W) if out is None else out
+    _check(lib().qb_inhom_step_maxwell(ws.h, q.h, n, _ptr(W), _ptr(out), h, dt, lam, _ptr(WL), _ptr(WR), _ptr(Bext), _stream()),
+           "qb_inhom_step_maxwell")
+    return out
+
+
+def to_fourier(Wv):
+    torch = _torch()
+    N = Wv.shape[-1]
+    out = torch.empty(Wv.shape, dtype=torch.complex128, device=Wv.device)
+    _check(lib().qb_to_fourier(N, Wv.numel() // (N * N), _ptr(Wv), _ptr(out), _stream()), "qb_to_fourier")
+    return out
+
+
+def from_fourier(Wf):
+    torch = _torch()
+    N = Wf.shape[-1]
+    out = torch.empty(Wf.shape, dtype=torch.float64, device=Wf.device)
+    _check(lib().qb_from_fourier(N, Wf.numel() // (N * N), _ptr(Wf), _ptr(out), _stream()), "qb_from_fourier")
+    return out
+
+
+def integral(ws, q, which, f, g, h):
+    torch = _torch()
+    out = torch.empty_like(f)
+    _check(lib().qb_integral(ws.h, q.h, which, _ptr(f), _ptr(g), _ptr(h), _ptr(out), _stream()), "qb_integral")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# the upstream C API (host buffers), N_GRID = 32
+
+class quadI1_t(C.Structure):
+    _fields_ = [("num", C.c_uint), ("psiR1", _dp), ("psiR2", _dp)]
+
+
+quadI2_t = quadI1_t
+quadI3_t = quadI1_t          # same layout: num + two pointers
+
+
+class interm_t(C.Structure):   # I1/I2/I3/Cc/Cd/collision/simulationHom interm: one handle
+    _fields_ = [("ws", _vp)]
+
+
+def _inhom_interm_type(n):
+    class inhomStepInterm_t(C.Structure):
+        _fields_ = [("numVol", C.c_uint), ("vgrid", C.c_double * n), ("vxgridMaxw", C.c_double * (n * n)), ("ws", _vp)]
+    return inhomStepInterm_t
+
+
+def _np(a, dt):
+    a = np.ascontiguousarray(a, dtype=dt)
+    return a, a.ctypes.data_as(_dp)
+
+
+class Upstream:
+    """The upstream entry points of libqbgpu, called the way a C driver calls them."""
+
+    def __init__(self, n_grid=N_GRID):
+        self.N = n_grid
+        self.L = lib(n_grid)
+        self.inhom_t = _inhom_interm_type(n_grid)
+
+    # quadrature structs -------------------------------------------------------
+    def fourier(self, which, J, L, R, M=None):
+        q = quadI1_t()
+        fn = {1: self.L.FourierI1, 2: self.L.FourierI2, 3: self.L.FourierI3, 4: self.L.FourierI4}[which]
+        if which == 3:
+            fn(C.c_uint(J), C.c_double(L), C.c_double(R), C.c_uint(M), C.byref(q))
+        else:
+            fn(C.c_uint(J), C.c_double(L), C.c_double(R), C.byref(q))
+        return q
+
+    def quad_delete(self, which, q):
+        {1: self.L.QuadI1_Delete, 2: self.L.QuadI2_Delete, 3: self.L.QuadI3_Delete, 4: self.L.QuadI1_Delete}[which](C.byref(q))
+
+    def quad_arrays(self, which, q):
+        N, P = self.N, 2 * self.N
+        n = q.num
+        sh1 = {1: (n, P, P), 2: (n, N, N), 3: (n, N, N, 2), 4: (n, P, P)}[which]
+        sh2 = {1: (n, N, N), 2: (n, N, N), 3: (n, P, P), 4: (n, N, N)}[which]
+        a1 = np.ctypeslib.as_array(q.psiR1, shape=(int(np.prod(sh1)),)).reshape(sh1).copy()
+        a2 = np.ctypeslib.as_array(q.psiR2, shape=(int(np.prod(sh2)),)).reshape(sh2).copy()
+        return (a1.view(np.complex128)[..., 0] if which == 3 else a1), a2
+
+    def quad_from_arrays(self, which, psiR1, psiR2):
+        """A caller-filled quad struct (as test/I2_test.c builds one)."""
+        q = quadI1_t()
+        {1: self.L.QuadI1_Allocate, 2: self.L.QuadI2_Allocate, 3: self.L.QuadI3_Allocate}[which](C.c_uint(len(psiR1)), C.byref(q))
+        r1 = np.ascontiguousarray(psiR1.view(np.float64) if np.iscomplexobj(psiR1) else psiR1, dtype=np.float64).ravel()
+        r2 = np.ascontiguousarray(psiR2, dtype=np.float64).ravel()
+        C.memmove(q.psiR1, r1.ctypes.data, r1.nbytes)
+        C.memmove(q.psiR2, r2.ctypes.data, r2.nbytes)
+        return q
+
+    # interms -------------------------------------------------------------------
+    def _interm(self, kind):
+        it = interm_t()
+        getattr(self.L, f"{kind}_Create")(C.byref(it))
+        return it
+
+    def _interm_del(self, kind, it):
+        getattr(self.L, f"{kind}_Delete")(C.byref(it))
+
+    # operators -----------------------------------------------------------------
+    def integral(self, which, f, g, h, q):
+        kind = {1: "I1interm", 2: "I2interm", 3: "I3interm", 4: "I1interm"}[which]
+        fn = {1: self.L.I1integral, 2: self.L.I2integral, 3: self.L.I3integral, 4: self.L.I1integral}[which]
+        it = self._interm(kind)
+        f, pf = _np(f, np.complex128); g, pg = _np(g, np.complex128); h, ph = _np(h, np.complex128)
+        out = np.zeros((self.N, self.N), np.complex128)
+        fn(pf, pg, ph, C.byref(q), C.byref(it), out.ctypes.data_as(_dp))
+        self._interm_del(kind, it)
+        return out
+
+    def cc(self, W, q1):
+        it = self._interm("CcInterm")
+        W, pW = _np(W, np.complex128)
+        out = np.zeros_like(W)
+        self.L.CcInt(pW, C.byref(q1), C.byref(it), out.ctypes.data_as(_dp))
+        self._interm_del("CcInterm", it)
+        return out
+
+    def cd(self, W, q2, q3, q4):
+        it = self._interm("CdInterm")
+        W, pW = _np(W, np.complex128)
+        out = np.zeros_like(W)
+        self.L.CdInt(pW, C.byref(q2), C.byref(q3), C.byref(q4), C.byref(it), out.ctypes.data_as(_dp))
+        self._interm_del("CdInterm", it)
+        return out
+
+    def collision_step(self, W, quads, dt, B=(0.0, 0.0, 0.0)):
+        it = self._interm("CollisionInterm")
+        W, pW = _np(W, np.complex128)
+        Bv, pB = _np(B, np.float64)
+        out = np.zeros_like(W)
+        self.L.CollisionStep(pW, *[C.byref(q) for q in quads], C.c_double(dt), pB, C.byref(it), out.ctypes.data_as(_dp))
+        self._interm_del("CollisionInterm", it)
+        return out
+
+    def inhom_interm(self, numVol, L):
+        it = self.inhom_t()
+        self.L.InhomStepInterm_Create(C.c_uint(numVol), C.c_double(L), C.byref(it))
+        return it
+
+    def inhom_step(self, W, quads, h, dt, Bext=None, bc="periodic", L=12.0, interm=None):
+        n = W.shape[0]
+        it = interm or self.inhom_interm(n, L)
+        W, pW = _np(W, np.float64)
+        Bv, pB = _np(np.zeros((n, 3)) if Bext is None else Bext, np.float64)
+        out = np.zeros_like(W)
+        fn = {"periodic": self.L.InhomStepPeriodic, "dirichlet": self.L.InhomStepDirichlet}[bc]
+        fn(pW, *[C.byref(q) for q in quads], C.c_double(h), C.c_double(dt), pB, C.byref(it), out.ctypes.data_as(_dp))
+        if interm is None:
+            self.L.InhomStepInterm_Delete(C.byref(it))
+        return out
+
+    def inhom_step_maxwell(self, W, quads, h, dt, lam, WL, WR, Bext=None, L=12.0):
+        n = W.shape[0]
+        it = self.inhom_interm(n, L)
+        W, pW = _np(W, np.float64)
+        WL, pL = _np(WL, np.float64); WR, pR = _np(WR, np.float64)
+        Bv, pB = _np(np.zeros((n, 3)) if Bext is None else Bext, np.float64)
+        out = np.zeros_like(W)
+        self.L.InhomStepMaxwell(pW, *[C.byref(q) for q in quads], C.c_double(h), C.c_double(dt), C.c_double(lam), pL, pR, pB,
+                                C.byref(it), out.ctypes.data_as(_dp))
+        self.L.InhomStepInterm_Delete(C.byref(it))
+        return out
+
+    def simulation_inhom(self, W0, quads, h, dt, numsteps, Bext=None, bc="periodic", L=12.0):
+        n = W0.shape[0]
+        it = self.inhom_interm(n, L)
+        W0, pW = _np(W0, np.float64)
+        Bv, pB = _np(np.zeros((n, 3)) if Bext is None else Bext, np.float64)
+        out = np.zeros((numsteps,) + W0.shape)
+        fn = {"periodic": self.L.SimulationInhomogeneousPeriodic, "dirichlet": self.L.SimulationInhomogeneousDirichlet}[bc]
+        fn(pW, *[C.byref(q) for q in quads], C.c_double(h), C.c_double(dt), C.c_uint(numsteps), pB, C.byref(it), out.ctypes.data_as(_dp))
+        self.L.InhomStepInterm_Delete(C.byref(it))
+        return out
+
+    def simulation_hom(self, W0, quads, dt, numsteps, B=(0.0, 0.0, 0.0)):
+        it = self._interm("SimulationHomInterm")
+        W0, pW = _np(W0, np.float64)
+        Bv, pB = _np(B, np.float64)
+        out = np.zeros((numsteps,) + W0.shape)
+        self.L.SimulationHomogeneous(pW, *[C.byref(q) for q in quads], C.c_double(dt), C.c_uint(numsteps), pB, C.byref(it), out.ctypes.data_as(_dp))
+        self._interm_del("SimulationHomInterm", it)
+        return out
+
+    def to_fourier_r2c(self, Wv):
+        """The upstream drivers' own transform to Fourier space through the FFTW
+        API (test/Cc_test.c:99-136): r2c plan, 1/N^2, Hermitian completion."""
+        N = self.N
+        Wv = np.ascontiguousarray(Wv, dtype=np.float64).reshape(-1, N, N)
+        out = np.zeros(Wv.shape, np.complex128)
+        half = np.zeros((N, N // 2 + 1), np.complex128)
+        self.L.fftw_plan_dft_r2c_2d.restype = _vp
+        self.L.fftw_plan_dft_r2c_2d.argtypes = [C.c_int, C.c_int, _vp, _vp, C.c_uint]
+        self.L.fftw_execute.argtypes = [_vp]
+        self.L.fftw_destroy_plan.argtypes = [_vp]
+        for i in range(Wv.shape[0]):
+            src = np.ascontiguousarray(Wv[i])
+            plan = self.L.fftw_plan_dft_r2c_2d(N, N, src.ctypes.data, half.ctypes.data, 1 << 6)
+            self.L.fftw_execute(plan)
+            self.L.fftw_destroy_plan(plan)
+            h = half / (N * N)
+            for l in range(N):
+                lc = (N - l) % N
+                out[i, l, :N // 2 + 1] = h[l]
+                for k in range(N // 2 + 1, N):
+                    out[i, l, k] = np.conj(h[lc, N - k])
+        return out
+
+    def slope(self, bc, h, dt, A, Un):
+        Un, pU = _np(Un, np.float64)
+        out = np.zeros_like(Un)
+        fn = self.L.SlopeLimiterStepPeriodic if bc == "periodic" else self.L.SlopeLimiterStepDirichlet
+        fn(C.c_double(h), C.c_double(dt), C.c_double(A), C.c_uint(len(Un)), pU, out.ctypes.data_as(_dp))
+        return out
+
+    def slope_maxwell(self, h, dt, A, lam, fluxL, fluxR, UL, UR, Un):
+        A, pA = _np(A, np.float64); UL, pL = _np(UL, np.float64); UR, pR = _np(UR, np.float64)
+        Un, pU = _np(Un, np.float64)
+        out = np.zeros_like(Un)
+        self.L.SlopeLimiterStepMaxwell(C.c_double(h), C.c_double(dt), C.c_uint(len(A)), pA, C.c_uint(Un.shape[0]), C.c_double(lam),
+                                       C.c_double(fluxL), C.c_double(fluxR), pL, pR, pU, out.ctypes.data_as(_dp))
+        return out
+
+    def lgwt(self, M, a, b):
+        x = np.zeros(M); w = np.zeros(M)
+        self.L.LegendreGaussQuad(C.c_uint(M), C.c_double(a), C.c_double(b), x.ctypes.data_as(_dp), w.ctypes.data_as(_dp))
+        return x, w
+
+
+# ---------------------------------------------------------------------------
+# seeded synthetic initial states (velocity box [-L, L)^2)
+
+def _splitmix64(x):
+    x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return x, z ^ (z >> 31)
+
+
+class _Rng:
+    """counter-based uniform doubles (splitmix64), reproducible across platforms"""
+
+    def __init__(self, seed):
+        self.s = seed & 0xFFFFFFFFFFFFFFFF
+
+    def uniform(self, a=0.0, b=1.0):
+        self.s, z = _splitmix64(self.s)
+        return a + (b - a) * ((z >> 11) * (1.0 / 9007199254740992.0))
+
+
+def mixture_params(seed, max_tries=1000):
+    """Two-component Gaussian mixture parameters: a_k ~ U[0.3,0.6], u_k ~ U[-1,1]^2,
+    T_k ~ U[0.5,1.5], s_k uniform in the ball |s| <= 0.9, phi_k ~ U[0, 2 pi);
+    redrawn until sum_k 1.3 a_k (1 + |s_k|)/2 <= 1 so that 0 <= W <= 1 holds
+    pointwise even with the 30% spatial modulation.
+    Returns (params, redraws)."""
+    rng = _Rng(seed)
+    for tries in range(max_tries):
+        comps = []
+        for _ in range(2):
+            a = rng.uniform(0.3, 0.6)
+            u = (rng.uniform(-1, 1), rng.uniform(-1, 1))
+            T = rng.uniform(0.5, 1.5)
+            while True:
+                s = np.array([rng.uniform(-0.9, 0.9) for _ in range(3)])
+                if np.linalg.norm(s) <= 0.9:
+                    break
+            phi = rng.uniform(0, 2 * math.pi)
+            comps.append((a, u, T, s, phi))
+        # largest eigenvalue <= sum_k (1 + 0.3) a_k (1 + |s_k|) / 2 (spatial modulation included)
+        if sum(1.3 * c[0] * (1 + np.linalg.norm(c[3])) / 2 for c in comps) <= 1.0:
+            return comps, tries
+    raise RuntimeError("no admissible mixture found")
+
+
+def velocity_grid(N, L):
+    k = np.arange(N)
+    return np.where(k < N // 2, k, k - N) * (2.0 * L / N)
+
+
+def gaussian_mixture_state(N, L, seed, ncells=1, modulation=0.3):
+    """Velocity-space Wigner states (ncells, 4, N, N) in Pauli form:
+    w0 = sum_k a_k(x) g_k / 2, w_vec = sum_k a_k(x) g_k s_k / 2 with
+    g_k = exp(-|v-u_k|^2 / (2 T_k)) and a_k(x) = a_k (1 + modulation sin(2 pi x + phi_k))
+    at cell centres x_i = (i + 1/2)/ncells (no modulation for one cell)."""
+    comps, _ = mixture_params(seed)
+    v = velocity_grid(N, L)
+    vx, vy = np.meshgrid(v, v, indexing="ij")        # [l, k]: l is v_x (slow), k is v_y
+    W = np.zeros((ncells, 4, N, N))
+    for i in range(ncells):
+        x = (i + 0.5) / ncells
+        for (a, u, T, s, phi) in comps:
+            ax = a * (1 + modulation * math.sin(2 * math.pi * x + phi)) if ncells > 1 else a
+            g = np.exp(-((vx - u[0]) ** 2 + (vy - u[1]) ** 2) / (2 * T))
+            W[i, 0] += ax * g / 2
+            for c in range(3):
+                W[i, c + 1] += ax * g * s[c] / 2
+    return W

@@ -3,7 +3,8 @@
  * The upstream API (collision.h, integrals.h, simulation.h, ...) works on one
  * host state per call with a compile-time N_GRID.  These entry points take
  * the grid size at run time, operate on many cells per call, and take DEVICE
- * pointers plus a CUDA stream (NULL = the workspace's own stream), so a caller
+ * pointers plus a CUDA stream (cudaStream_t; NULL = the legacy default stream),
+ * so a caller
  * that keeps the state resident in HBM pays no host transfers per step.
  * Layouts are the upstream ones laid end to end: a velocity-space cell is
  * wignerV_t (4 real N x N grids), a Fourier-space cell is wignerF_t (4 complex

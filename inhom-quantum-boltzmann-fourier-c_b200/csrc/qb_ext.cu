@@ -22,7 +22,8 @@ template <class F> int guarded(F &&f) {
 	}
 }
 
-cudaStream_t pick(const qb_workspace *ws, void *stream) { return stream ? (cudaStream_t)stream : ws->stream; }
+// the caller's stream as given; NULL is the legacy default stream (torch's default stream)
+cudaStream_t pick(const qb_workspace *, void *stream) { return (cudaStream_t)stream; }
 
 void check(const qb_workspace *ws, const qb_quad *q) {
 	if (ws == nullptr || q == nullptr) QB_FAIL("null workspace or quadrature handle");
@@ -155,7 +156,7 @@ int qb_transport(int N, double L, int ncells, const double *in, double *out, dou
 		if (bc != 0 && bc != 1) QB_FAIL("qb_transport: bc must be 0 or 1");
 		thread_local std::unique_ptr<qb_workspace> tws;
 		if (!tws || tws->N != N) tws = std::make_unique<qb_workspace>(N);
-		cudaStream_t s = stream ? (cudaStream_t)stream : tws->stream;
+		cudaStream_t s = (cudaStream_t)stream;
 		const double *A = velocity_tables(tws.get(), L, s);
 		qb::transport(4 * N * N, ncells, in, out, A, h, dt, bc, s);
 	});

@@ -48,7 +48,9 @@ def test_integral_golden(up, fgh, which, J, M, golden):
     q = up.fourier(which, J, L_, R_, M)
     out = up.integral(which, *fgh, q)
     up.quad_delete(which, q)
-    assert avg_abs_err(out, golden_c(golden)) < 5e-12
+    # the Matlab goldens carry ~1e-12 absolute error themselves (upstream C code:
+    # 0.8-2.1e-12); the factored sums round differently, so bound the relative error
+    assert rel_l1(out, golden_c(golden)) < 1e-13
     o = orc.Oracle(32, J, M, L_, R_)
     ref = {1: o.i1, 2: o.i2, 3: o.i3, 4: o.i4}[which](*fgh)
     assert rel_l1(out, ref) < TOL

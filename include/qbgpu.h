@@ -91,6 +91,19 @@ int qb_profile_reset(void);
 int qb_profile_read(const char *prefix, double *ms, long *launches);
 long qb_launch_count(void);
 
+/* The I3 integral of qb_integral(q, 3, ...) for callers that cannot allocate
+ * device memory (a stream being captured into a CUDA graph, a host
+ * application that owns all device memory, a latency-critical loop).  It has
+ * no counterpart in the upstream code.  All scratch comes from one static
+ * device array of 4 MiB compiled into the library; every GPU that loads the
+ * library holds it until exit, and the call itself allocates nothing.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress)
+ * and must come before any stream capture on that device.  Calls share the
+ * array: calls that can overlap on the GPU race, so serialise them.  Grid
+ * sizes up to N = 32 fit; larger ones are rejected with an error. f, g, h,
+ * out: device N x N complex grids. */
+int qb_integral_i3_noalloc(const qb_quad *q, const void *f, const void *g, const void *h, void *out, void *stream);
+
 /* measured FP64 FMA throughput of the current device in TFLOP/s (a dependent-
  * free DFMA loop on every SM, ~tens of ms) -- the denominator of the FP64
  * roofline of the collision kernels. */

@@ -81,8 +81,10 @@ template <int L> struct Len {
 
 // Length-L transform of the 8 values in x (see file comment).  `scratch` is
 // an L-slot region addressed scratch[pos * sstride]; its previous contents are
-// destroyed.  `tw` holds w_L^e = exp(-2 pi i e/L), e < L.  Must be called by
-// all 32 lanes of the warp (contains __syncwarp).
+// destroyed.  `tw` is the step-2 twiddle table of init_twiddles: entry
+// q*T + tau holds w_L^(tau*q), so the T lanes of a transform read T
+// consecutive entries for every q (one conflict-free shared-memory wavefront).
+// Must be called by all 32 lanes of the warp (contains __syncwarp).
 template <int L, int DIR>
 __device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch, int sstride, const double2 *tw) {
 	using G = Len<L>;
@@ -90,7 +92,7 @@ __device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch
 	if constexpr (G::T > 1) {
 #pragma unroll
 		for (int q = 1; q < 8; q++) {
-			double2 w = tw[tau * q];
+			double2 w = tw[q * G::T + tau];
 			if (DIR > 0) w.y = -w.y;
 			x[q] = cmul(x[q], w);
 		}
@@ -135,12 +137,15 @@ __device__ __forceinline__ void out_to_in(double2 (&x)[8], int tau, double2 *scr
 	}
 }
 
-// fill tw[e] = exp(-2 pi i e/L) for e < L (all threads of the block call it)
+// fill the step-2 twiddle table of fft1d<L>: tw[q*T + tau] = exp(-2 pi i tau q / L)
+// for q < 8, tau < T (L entries; all threads of the block call it)
 template <int L>
 __device__ __forceinline__ void init_twiddles(double2 *tw) {
+	constexpr int T = Len<L>::T;
 	for (int e = threadIdx.x; e < L; e += blockDim.x) {
+		const int q = e / T, tau = e % T;
 		double s, c;
-		sincospi(-2.0 * (double)e / (double)L, &s, &c);
+		sincospi(-2.0 * (double)(tau * q) / (double)L, &s, &c);
 		tw[e] = make_double2(c, s);
 	}
 }

@@ -384,7 +384,7 @@ def main():
     ap.add_argument("--grid", type=int, default=32)
     ap.add_argument("--J", type=int, default=16)
     ap.add_argument("--M", type=int, default=16)
-    ap.add_argument("--cpu-procs", type=int, default=8)
+    ap.add_argument("--cpu-procs", type=int, default=min(32, os.cpu_count() or 1))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

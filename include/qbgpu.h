@@ -50,7 +50,9 @@ int qb_collision_step(qb_workspace *ws, const qb_quad *q, int ncells, const void
 
 /* one Strang step of InhomStepPeriodic (bc = 0) / InhomStepDirichlet (bc = 1)
  * (upstream src/simulation.c:307-830) over ncells velocity-space cells with
- * box half-width L; Bext = 3 doubles per cell.  Wnext must not alias W. */
+ * box half-width L; Bext = 3 doubles per cell.  Wnext must not alias W.
+ * A repeated call with identical arguments replays a captured CUDA graph of
+ * the step (QB_CUDA_GRAPHS=0 launches kernel by kernel instead). */
 int qb_inhom_step(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
                   double h, double dt, const double *Bext, int bc, void *stream);
 
@@ -79,6 +81,26 @@ int qb_transport(int N, double L, int ncells, const double *in, double *out, dou
  * place: to Fourier space, CollisionStep, back (InternalFourierCollisionStep,
  * upstream src/simulation.c:214-284) */
 int qb_fourier_collision(qb_workspace *ws, const qb_quad *q, int ncells, double *W, const double *Bext, double dt, void *stream);
+
+/* Strang steps of ncells cells (bc 0 periodic, 1 Dirichlet) from the HOST
+ * initial state W0, state resident on the device; frame 0 (= W0) and every
+ * record_every-th state are appended to `path` in the upstream trajectory
+ * format (raw wignerV_t frames, as SimulationInhomogeneous* + WriteData
+ * produce, upstream src/simulation.c:1288-1341, src/util.c:70-91), each frame
+ * written while the GPU computes the following steps.  With record_every = 1
+ * the file equals upstream's Wevolv file.  numsteps counts frames including
+ * the initial one, as upstream.  The final state goes to final_out (host) if
+ * non-null; path may be NULL (no recording).  Returns the number of frames
+ * written, or -1. */
+long qb_simulate_record(qb_workspace *ws, const qb_quad *q, int ncells, const double *W0, double h, double dt, unsigned numsteps,
+                        const double *Bext, int bc, unsigned record_every, const char *path, double *final_out);
+
+/* per-cell diagnostics of velocity-space states W (device): out (device) gets
+ * 10 doubles per cell: w_tr, w_x, w_y, w_z (integrals, dv^2 included), mean
+ * velocity u_x, u_y, energy per particle, smallest and largest eigenvalue of
+ * W(v) over the grid, and the Fermi-Dirac entropy (upstream
+ * visualization/wignerMoments.m:15-37, visualization/entropy.m). */
+int qb_diagnostics(int N, double L, int ncells, const double *W, double *out, void *stream);
 
 /* launch accounting: every engine kernel launch is counted; while profiling
  * is on, launches are bracketed by CUDA events on their stream.

@@ -75,7 +75,8 @@ void prof_read(const char *prefix, double *ms, long *launches) {
 
 ProfScope::ProfScope(const char *n, cudaStream_t st) : name(n), s(st) {
 	g_launches++;
-	if (g_prof_on) {
+	cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+	if (g_prof_on && cudaStreamIsCapturing(s, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
 		QB_CUDA(cudaEventCreate(&e0));
 		QB_CUDA(cudaEventCreate(&e1));
 		QB_CUDA(cudaEventRecord(e0, s));
@@ -119,6 +120,9 @@ Workspace::Workspace(int n) : N(n) {
 }
 
 Workspace::~Workspace() {
+	if (graph_exec) cudaGraphExecDestroy(graph_exec);
+	if (ev_in) cudaEventDestroy(ev_in);
+	if (ev_out) cudaEventDestroy(ev_out);
 	if (stream) cudaStreamDestroy(stream);
 }
 

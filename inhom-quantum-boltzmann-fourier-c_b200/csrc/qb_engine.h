@@ -80,6 +80,12 @@ struct Workspace {
 	DevBuf fa, fb, va, vb;                   // state scratch (Fourier / velocity)
 	DevBuf io_in, io_out, bext, vgrid;       // staging for host-pointer calls
 	DevBuf aux, aux2;
+	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
+	// replay of a repeated Strang step (batched API): the launch sequence of
+	// one (pointers, parameters) key is captured once and relaunched
+	std::vector<double> graph_key;
+	cudaGraphExec_t graph_exec = nullptr;
+	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 	explicit Workspace(int N);
 	~Workspace();
 };

@@ -6,6 +6,8 @@ extern "C" {
 }
 
 #include <cstring>
+#include <cstdint>
+#include <cstdio>
 #include <vector>
 #include <algorithm>
 
@@ -31,7 +33,9 @@ void check(const qb_workspace *ws, const qb_quad *q) {
 }
 
 // per-workspace per-point velocity tables for (N, L), kept in ws->vgrid
+// (rebuilt only when L changes, so that repeated steps issue no host copy)
 const double *velocity_tables(qb_workspace *ws, double L, cudaStream_t s) {
+	if (ws->tables_L == L && ws->vgrid.p != nullptr) return ws->vgrid.as<double>();
 	const int N = ws->N;
 	const long NN = (long)N * N;
 	const double scale = (2 * L) / N;
@@ -47,7 +51,48 @@ const double *velocity_tables(qb_workspace *ws, double L, cudaStream_t s) {
 	A[5 * NN] = L;
 	ws->vgrid.ensure(sizeof(double) * (5 * NN + 1));
 	QB_CUDA(cudaMemcpyAsync(ws->vgrid.p, A.data(), sizeof(double) * (5 * NN + 1), cudaMemcpyHostToDevice, s));
+	QB_CUDA(cudaStreamSynchronize(s));
+	ws->tables_L = L;
 	return ws->vgrid.as<double>();
+}
+
+bool graphs_enabled() {
+	const char *e = getenv("QB_CUDA_GRAPHS");
+	return e == nullptr || strcmp(e, "0") != 0;
+}
+
+// One Strang step through a CUDA graph: the first call with a new key runs
+// the launch sequence directly (sizing every buffer), the second captures it
+// on the workspace stream, later calls relaunch the instantiated graph.  The
+// caller's stream is ordered before and after through events.
+void inhom_step_graphed(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext, double h, double dt,
+                        const double *Bext, int bc, cudaStream_t caller) {
+	const double *A = velocity_tables(ws, q->q->L, caller);
+	const std::vector<double> key = { (double)ncells, (double)(uintptr_t)W, (double)(uintptr_t)Wnext, h, dt,
+	                                  (double)(uintptr_t)Bext, (double)bc, (double)(uintptr_t)q, q->q->L };
+	if (!graphs_enabled() || key != ws->graph_key) {
+		if (ws->graph_exec) { cudaGraphExecDestroy(ws->graph_exec); ws->graph_exec = nullptr; }
+		ws->graph_key = key;
+		qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, caller);
+		return;
+	}
+	if (ws->ev_in == nullptr) {
+		QB_CUDA(cudaEventCreateWithFlags(&ws->ev_in, cudaEventDisableTiming));
+		QB_CUDA(cudaEventCreateWithFlags(&ws->ev_out, cudaEventDisableTiming));
+	}
+	if (ws->graph_exec == nullptr) {
+		cudaGraph_t g = nullptr;
+		QB_CUDA(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal));
+		qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, ws->stream);
+		QB_CUDA(cudaStreamEndCapture(ws->stream, &g));
+		QB_CUDA(cudaGraphInstantiate(&ws->graph_exec, g, 0));
+		cudaGraphDestroy(g);
+	}
+	QB_CUDA(cudaEventRecord(ws->ev_in, caller));
+	QB_CUDA(cudaStreamWaitEvent(ws->stream, ws->ev_in, 0));
+	QB_CUDA(cudaGraphLaunch(ws->graph_exec, ws->stream));
+	QB_CUDA(cudaEventRecord(ws->ev_out, ws->stream));
+	QB_CUDA(cudaStreamWaitEvent(caller, ws->ev_out, 0));
 }
 
 }  // namespace
@@ -109,9 +154,7 @@ int qb_inhom_step(qb_workspace *ws, const qb_quad *q, int ncells, const double *
 		check(ws, q);
 		if (W == Wnext) QB_FAIL("qb_inhom_step: Wnext must not alias W");
 		if (bc != 0 && bc != 1) QB_FAIL("qb_inhom_step: bc must be 0 (periodic) or 1 (Dirichlet)");
-		cudaStream_t s = pick(ws, stream);
-		const double *A = velocity_tables(ws, q->q->L, s);
-		qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, s);
+		inhom_step_graphed(ws, q, ncells, W, Wnext, h, dt, Bext, bc, pick(ws, stream));
 	});
 }
 
@@ -174,6 +217,69 @@ int qb_fourier_collision(qb_workspace *ws, const qb_quad *q, int ncells, double 
 		qb::collision_step(*ws, q->q->set(), ncells, ws->fa.as<double2>(), Bext, dt, ws->fb.as<double2>(), s);
 		qb::from_fourier(N, 4 * ncells, ws->fb.as<double2>(), W, s);
 	});
+}
+
+long qb_simulate_record(qb_workspace *ws, const qb_quad *q, int ncells, const double *W0, double h, double dt, unsigned numsteps,
+                        const double *Bext, int bc, unsigned record_every, const char *path, double *final_out) {
+	long frames = 0;
+	const int rc = guarded([&] {
+		check(ws, q);
+		if (bc != 0 && bc != 1) QB_FAIL("qb_simulate_record: bc must be 0 (periodic) or 1 (Dirichlet)");
+		if (record_every == 0) QB_FAIL("qb_simulate_record: record_every must be positive");
+		if (numsteps == 0) return;
+		const size_t bytes = sizeof(double) * 4 * (size_t)ws->N * ws->N * ncells;
+		cudaStream_t s = ws->stream;
+		FILE *fd = nullptr;
+		if (path != nullptr) {
+			fd = fopen(path, "wb");
+			if (fd == nullptr) QB_FAIL(std::string("qb_simulate_record: cannot open ") + path);
+			if (fwrite(W0, 1, bytes, fd) != bytes) QB_FAIL("qb_simulate_record: write failed");
+			frames++;
+		}
+		qb::DevBuf a, b, B;
+		a.ensure(bytes); b.ensure(bytes); B.ensure(sizeof(double) * 3 * ncells);
+		QB_CUDA(cudaMemcpyAsync(a.p, W0, bytes, cudaMemcpyHostToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(B.p, Bext, sizeof(double) * 3 * ncells, cudaMemcpyHostToDevice, s));
+		// two pinned staging buffers: frame n is copied while frame n-1 is written to the file
+		void *stage[2] = { nullptr, nullptr };
+		cudaEvent_t ev[2];
+		bool pending[2] = { false, false };
+		if (fd) {
+			for (int k = 0; k < 2; k++) {
+				QB_CUDA(cudaHostAlloc(&stage[k], bytes, cudaHostAllocDefault));
+				QB_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+			}
+		}
+		auto flush = [&](int k) {
+			QB_CUDA(cudaEventSynchronize(ev[k]));
+			if (fwrite(stage[k], 1, bytes, fd) != bytes) QB_FAIL("qb_simulate_record: write failed");
+			frames++;
+			pending[k] = false;
+		};
+		double *cur = a.as<double>(), *nxt = b.as<double>();
+		int slot = 0;
+		for (unsigned it = 1; it < numsteps; it++) {
+			inhom_step_graphed(ws, q, ncells, cur, nxt, h, dt, B.as<double>(), bc, s);
+			std::swap(cur, nxt);
+			if (fd && it % record_every == 0) {
+				if (pending[slot]) flush(slot);
+				QB_CUDA(cudaMemcpyAsync(stage[slot], cur, bytes, cudaMemcpyDeviceToHost, s));
+				QB_CUDA(cudaEventRecord(ev[slot], s));
+				pending[slot] = true;
+				if (pending[slot ^ 1]) flush(slot ^ 1);     // the older frame, while the GPU runs ahead
+				slot ^= 1;
+			}
+		}
+		for (int k : { slot, slot ^ 1 })
+			if (fd && pending[k]) flush(k);
+		if (final_out) QB_CUDA(cudaMemcpyAsync(final_out, cur, bytes, cudaMemcpyDeviceToHost, s));
+		QB_CUDA(cudaStreamSynchronize(s));
+		if (fd) {
+			fclose(fd);
+			for (int k = 0; k < 2; k++) { cudaFreeHost(stage[k]); cudaEventDestroy(ev[k]); }
+		}
+	});
+	return rc == 0 ? frames : -1;
 }
 
 int qb_profile_enable(int on) { qb::prof_enable(on != 0); return 0; }

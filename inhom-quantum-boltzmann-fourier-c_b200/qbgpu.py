@@ -59,6 +59,9 @@ def lib(n_grid=N_GRID):
     L.qb_to_fourier.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
     L.qb_from_fourier.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
     L.qb_integral.argtypes = [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.qb_simulate_record.restype = C.c_long
+    L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
+    L.qb_diagnostics.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp]
     L.CalculateRightwardFlux.restype = C.c_double
     L.CalculateLeftwardFlux.restype = C.c_double
     _libs[n_grid] = L
@@ -161,6 +164,36 @@ def inhom_step_maxwell(ws, q, W, h, dt, lam, WL, WR, Bext=None, out=None):
     _check(lib().qb_inhom_step_maxwell(ws.h, q.h, n, _ptr(W), _ptr(out), h, dt, lam, _ptr(WL), _ptr(WR), _ptr(Bext), _stream()),
            "qb_inhom_step_maxwell")
     return out
+
+
+DIAGNOSTICS = ("w_tr", "w_x", "w_y", "w_z", "u_x", "u_y", "energy", "lam_min", "lam_max", "entropy")
+
+
+def diagnostics(W, L):
+    """per-cell moments, eigenvalue bounds and entropy of velocity-space states
+    W (float64 CUDA tensor (ncells, 4, N, N)); returns (ncells, 10) tensor with
+    columns DIAGNOSTICS"""
+    torch = _torch()
+    N, n = W.shape[-1], W.shape[0]
+    out = torch.empty((n, len(DIAGNOSTICS)), dtype=torch.float64, device=W.device)
+    _check(lib().qb_diagnostics(N, L, n, _ptr(W), _ptr(out), _stream()), "qb_diagnostics")
+    return out
+
+
+def simulate_record(ws, q, W0, h, dt, numsteps, Bext=None, bc="periodic", record_every=1, path=None):
+    """numsteps frames (initial included) from host state W0 (numpy (ncells,4,N,N));
+    frames 0, k, 2k, ... appended to `path` in the upstream trajectory format.
+    Returns (final state, frames written)."""
+    W0 = np.ascontiguousarray(W0, dtype=np.float64)
+    n = W0.shape[0]
+    Bv = np.ascontiguousarray(np.zeros((n, 3)) if Bext is None else Bext, dtype=np.float64)
+    final = np.zeros_like(W0)
+    frames = lib().qb_simulate_record(ws.h, q.h, n, W0.ctypes.data, h, dt, numsteps, Bv.ctypes.data,
+                                      0 if bc == "periodic" else 1, record_every, path.encode() if path else None,
+                                      final.ctypes.data)
+    if frames < 0:
+        raise RuntimeError(f"qb_simulate_record failed: {lib().qb_last_error().decode()}")
+    return final, frames
 
 
 def to_fourier(Wv):

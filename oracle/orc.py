@@ -293,3 +293,29 @@ class Ref:
 def ref_to_fourier(Wv):
     Wv = _r(Wv); out = np.zeros(Wv.shape, np.complex128)
     ref_lib().ref_to_fourier(_ptr(Wv), _ptr(out)); return out
+
+
+def diagnostics(W, L):
+    """Moments, eigenvalue bounds and Fermi-Dirac entropy per cell, restating
+    visualization/wignerMoments.m:15-37 and visualization/entropy.m in numpy
+    (float64).  W: (ncells, 4, N, N) velocity space; columns as qbgpu.DIAGNOSTICS."""
+    W = np.asarray(W, dtype=np.float64)
+    N = W.shape[-1]
+    dv = 2.0 * L / N
+    v = np.where(np.arange(N) < N // 2, np.arange(N), np.arange(N) - N) * dv
+    vx, vy = np.meshgrid(v, v, indexing="ij")        # [l, k]: l is v_x
+    out = np.zeros((W.shape[0], 10))
+    for i, w in enumerate(W):
+        t = w[0]
+        r = np.sqrt(w[1] ** 2 + w[2] ** 2 + w[3] ** 2)
+        ux, uy = (vx * t).sum() / t.sum(), (vy * t).sum() / t.sum()
+        e = (0.5 * ((vx - ux) ** 2 + (vy - uy) ** 2) * t).sum() / t.sum()
+
+        def S(p):
+            ok = (p > 0) & (p < 1)
+            q = p[ok]
+            return -(q * np.log(q) + (1 - q) * np.log1p(-q)).sum()
+        out[i] = [w[0].sum() * dv * dv, w[1].sum() * dv * dv, w[2].sum() * dv * dv, w[3].sum() * dv * dv,
+                  ux, uy, e, (t - r).min(), (t + r).max(), (S(t - r) + S(t + r)) * dv * dv]
+    return out
+

@@ -4,7 +4,7 @@
 // lanes of one warp; every lane holds 8 complex values in registers:
 //   input : lane tau holds x[tau + T*r], r = 0..7
 //   step 1: radix-8 DFT over r in registers
-//   step 2: twiddle by w_L^(tau*q)
+//   step 2: twiddle by w_L^(tau*q) (powers of the lane's base twiddle)
 //   step 3: transpose among the T lanes through an L-slot scratch (the row or
 //           column of the grid being transformed), XOR-swizzled so that a
 //           quarter-warp touches 8 distinct 16-byte bank groups
@@ -81,19 +81,24 @@ template <int L> struct Len {
 
 // Length-L transform of the 8 values in x (see file comment).  `scratch` is
 // an L-slot region addressed scratch[pos * sstride]; its previous contents are
-// destroyed.  `tw` is the step-2 twiddle table of init_twiddles: entry
-// q*T + tau holds w_L^(tau*q), so the T lanes of a transform read T
-// consecutive entries for every q (one conflict-free shared-memory wavefront).
+// destroyed.  `tw` is the table of init_twiddles (tw[e] = w_L^e); a lane
+// reads only its base twiddle w_L^tau (the T lanes read T consecutive
+// entries: one conflict-free wavefront) and forms w_L^(tau*q), q = 2..7, by
+// repeated multiplication in registers, trading six shared-memory loads for
+// six complex multiplies (relative error of the powers below 1e-15).
 // Must be called by all 32 lanes of the warp (contains __syncwarp).
 template <int L, int DIR>
 __device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch, int sstride, const double2 *tw) {
 	using G = Len<L>;
 	dft8<DIR>(x);
 	if constexpr (G::T > 1) {
+		double2 w1 = tw[tau];
+		if (DIR > 0) w1.y = -w1.y;
+		double2 w = w1;
+		x[1] = cmul(x[1], w);
 #pragma unroll
-		for (int q = 1; q < 8; q++) {
-			double2 w = tw[q * G::T + tau];
-			if (DIR > 0) w.y = -w.y;
+		for (int q = 2; q < 8; q++) {
+			w = cmul(w, w1);
 			x[q] = cmul(x[q], w);
 		}
 		__syncwarp();
@@ -137,15 +142,13 @@ __device__ __forceinline__ void out_to_in(double2 (&x)[8], int tau, double2 *scr
 	}
 }
 
-// fill the step-2 twiddle table of fft1d<L>: tw[q*T + tau] = exp(-2 pi i tau q / L)
-// for q < 8, tau < T (L entries; all threads of the block call it)
+// fill the twiddle table of fft1d<L>: tw[e] = exp(-2 pi i e / L), e < L
+// (all threads of the block call it)
 template <int L>
 __device__ __forceinline__ void init_twiddles(double2 *tw) {
-	constexpr int T = Len<L>::T;
 	for (int e = threadIdx.x; e < L; e += blockDim.x) {
-		const int q = e / T, tau = e % T;
 		double s, c;
-		sincospi(-2.0 * (double)(tau * q) / (double)L, &s, &c);
+		sincospi(-2.0 * (double)e / (double)L, &s, &c);
 		tw[e] = make_double2(c, s);
 	}
 }

@@ -145,18 +145,18 @@ template <class K> void set_smem(K kernel, size_t bytes) {
 	QB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
-template <int P> constexpr size_t smem_grids(int ngrids) { return sizeof(double2) * ((size_t)ngrids * Geo<P>::GRID + P); }
+template <int P, class C = double2> constexpr size_t smem_grids(int ngrids) { return sizeof(C) * ((size_t)ngrids * Geo<P>::GRID + P); }
 
-// active clusters of the I3 kernel (occupancy query, cached per P)
-template <int P> int active_i3_clusters() {
+// active clusters of the I3 kernel (occupancy query, cached per P and C)
+template <int P, class C> int active_i3_clusters() {
 	static int cached = -1;
 	if (cached < 0) {
-		auto kern = k_i3<P, 4>;
-		set_smem(kern, smem_grids<P>(2));
+		auto kern = k_i3<P, 4, C>;
+		set_smem(kern, smem_grids<P, C>(2));
 		cudaLaunchConfig_t cfg = {};
 		cfg.gridDim = dim3(4);
 		cfg.blockDim = dim3(Geo<P>::NT);
-		cfg.dynamicSmemBytes = smem_grids<P>(2);
+		cfg.dynamicSmemBytes = smem_grids<P, C>(2);
 		cudaLaunchAttribute attr;
 		attr.id = cudaLaunchAttributeClusterDimension;
 		attr.val.clusterDim.x = 4; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
@@ -185,38 +185,38 @@ int best_chunks(long units, int nterms, int slots, int max_chunks) {
 	return best;
 }
 
-template <int P> void launch_pad_fft(int ngrids, const double2 *src, double2 *out, cudaStream_t s) {
+template <int P, class C> void launch_pad_fft(int ngrids, const double2 *src, C *out, cudaStream_t s) {
 	static bool init = false;
-	if (!init) { set_smem(k_pad_fft<P>, smem_grids<P>(1)); init = true; }
+	if (!init) { set_smem(k_pad_fft<P, C>, smem_grids<P, C>(1)); init = true; }
 	ProfScope ps("pad_fft", s);
-	k_pad_fft<P><<<ngrids, Geo<P>::NT, smem_grids<P>(1), s>>>(src, out);
+	k_pad_fft<P, C><<<ngrids, Geo<P>::NT, smem_grids<P, C>(1), s>>>(src, out);
 	QB_CUDA(cudaGetLastError());
 }
 
-template <int P> void launch_i1(const I1Params &p, long nblocks, cudaStream_t s) {
+template <int P, class C> void launch_i1(const I1ParamsT<C> &p, long nblocks, cudaStream_t s) {
 	static bool init = false;
-	if (!init) { set_smem(k_i1_terms<P>, smem_grids<P>(2)); init = true; }
+	if (!init) { set_smem(k_i1_terms<P, C>, smem_grids<P, C>(2)); init = true; }
 	ProfScope ps("i1_terms", s);
-	k_i1_terms<P><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P>(2), s>>>(p);
+	k_i1_terms<P, C><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P, C>(2), s>>>(p);
 	QB_CUDA(cudaGetLastError());
 }
 
-template <int P> void launch_i2(const I2Params &p, long nblocks, cudaStream_t s) {
+template <int P, class C> void launch_i2(const I2ParamsT<C> &p, long nblocks, cudaStream_t s) {
 	static bool init = false;
-	if (!init) { set_smem(k_i2_terms<P>, smem_grids<P>(2)); init = true; }
+	if (!init) { set_smem(k_i2_terms<P, C>, smem_grids<P, C>(2)); init = true; }
 	ProfScope ps("i2_terms", s);
-	k_i2_terms<P><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P>(2), s>>>(p);
+	k_i2_terms<P, C><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P, C>(2), s>>>(p);
 	QB_CUDA(cudaGetLastError());
 }
 
-template <int P, int CS> void launch_i3(const I3Params &p, long nclusters, cudaStream_t s) {
+template <int P, int CS, class C> void launch_i3(const I3ParamsT<C> &p, long nclusters, cudaStream_t s) {
 	static bool init = false;
-	auto kern = k_i3<P, CS>;
-	if (!init) { set_smem(kern, smem_grids<P>(2)); init = true; }
+	auto kern = k_i3<P, CS, C>;
+	if (!init) { set_smem(kern, smem_grids<P, C>(2)); init = true; }
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3((unsigned)(nclusters * CS));
 	cfg.blockDim = dim3(Geo<P>::NT);
-	cfg.dynamicSmemBytes = smem_grids<P>(2);
+	cfg.dynamicSmemBytes = smem_grids<P, C>(2);
 	cfg.stream = s;
 	cudaLaunchAttribute attr;
 	attr.id = cudaLaunchAttributeClusterDimension;
@@ -227,85 +227,142 @@ template <int P, int CS> void launch_i3(const I3Params &p, long nclusters, cudaS
 	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p));
 }
 
-template <int P> void launch_fft_full(const FullParams &p, long ngrids, cudaStream_t s) {
+template <int P, class C> void launch_fft_full(const FullParamsT<C> &p, long ngrids, cudaStream_t s) {
 	static bool init = false;
-	if (!init) { set_smem(k_fft_full<P>, smem_grids<P>(1)); init = true; }
+	if (!init) { set_smem(k_fft_full<P, C>, smem_grids<P, C>(1)); init = true; }
 	ProfScope ps("fft_full", s);
-	k_fft_full<P><<<(unsigned)ngrids, Geo<P>::NT, smem_grids<P>(1), s>>>(p);
+	k_fft_full<P, C><<<(unsigned)ngrids, Geo<P>::NT, smem_grids<P, C>(1), s>>>(p);
 	QB_CUDA(cudaGetLastError());
 }
 
-template <int P> void launch_assemble(const AsmParams &p, long ncells, cudaStream_t s) {
+template <int P, class C> void launch_assemble(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
 	static bool init = false;
-	if (!init) { set_smem(k_assemble<P>, smem_grids<P>(1)); init = true; }
+	if (!init) { set_smem(k_assemble<P, C>, smem_grids<P, C>(1)); init = true; }
 	ProfScope ps("assemble", s);
-	k_assemble<P><<<(unsigned)(ncells * 4), Geo<P>::NT, smem_grids<P>(1), s>>>(p);
+	k_assemble<P, C><<<(unsigned)(ncells * 4), Geo<P>::NT, smem_grids<P, C>(1), s>>>(p);
 	QB_CUDA(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------------------
-// the factored right-hand side for one padded size
-template <int P> struct Rhs {
+// quadrature tables in the working precision: FP64 tables as built, FP32
+// copies made once, on first use, by rounding the FP64 tables
+__global__ void k_round_f32(long n, const double *__restrict__ in, float *__restrict__ out) {
+	const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = (float)in[i];
+}
+
+std::mutex g_f32_mu;
+
+void round_table(const DevBuf &d, DevBuf &f, cudaStream_t s) {
+	const long n = (long)(d.bytes / sizeof(double));
+	if (n == 0 || f.p != nullptr) return;
+	f.ensure(sizeof(float) * n);
+	k_round_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, d.as<double>(), f.as<float>());
+	QB_CUDA(cudaGetLastError());
+}
+
+template <class C> struct Tab;
+template <> struct Tab<double2> {
+	static void prepare(const QuadSet &, cudaStream_t) {}
+	static const double *i1_psi2(const DevI1 &t) { return t.psi2.as<double>(); }
+	static const double *i1_phi(const DevI1 &t) { return t.phi.as<double>(); }
+	static const double *i2_psi1(const DevI2 &t) { return t.psi1.as<double>(); }
+	static const double *i2_psi2(const DevI2 &t) { return t.psi2.as<double>(); }
+	static const double2 *i3_psi1(const DevI3 &t) { return t.psi1.as<double2>(); }
+	static const double *i3_psi2T(const DevI3 &t) { return t.psi2T.as<double>(); }
+};
+template <> struct Tab<float2> {
+	// the copies are made on the caller's stream, which is then synchronised
+	// so that any stream may read them afterwards; this needs a stream that is
+	// not being captured, i.e. a first FP32 evaluation outside graph capture
+	static void prepare(const QuadSet &q, cudaStream_t s) {
+		std::lock_guard<std::mutex> lk(g_f32_mu);
+		const DevI1 *i1s[2] = { q.i1, q.i4 };
+		bool fresh = false;
+		for (const DevI1 *t : i1s)
+			if (t && t->psi2f.p == nullptr) { round_table(t->psi2, t->psi2f, s); round_table(t->phi, t->phif, s); fresh = true; }
+		if (q.i2 && q.i2->psi1f.p == nullptr) { round_table(q.i2->psi1, q.i2->psi1f, s); round_table(q.i2->psi2, q.i2->psi2f, s); fresh = true; }
+		if (q.i3 && q.i3->psi1f.p == nullptr) { round_table(q.i3->psi1, q.i3->psi1f, s); round_table(q.i3->psi2T, q.i3->psi2Tf, s); fresh = true; }
+		if (fresh) {
+			cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+			QB_CUDA(cudaStreamIsCapturing(s, &cap));
+			if (cap != cudaStreamCaptureStatusNone) QB_FAIL("the first FP32 evaluation with a table set must not be captured");
+			QB_CUDA(cudaStreamSynchronize(s));
+		}
+	}
+	static const float *i1_psi2(const DevI1 &t) { return t.psi2f.as<float>(); }
+	static const float *i1_phi(const DevI1 &t) { return t.phif.as<float>(); }
+	static const float *i2_psi1(const DevI2 &t) { return t.psi1f.as<float>(); }
+	static const float *i2_psi2(const DevI2 &t) { return t.psi2f.as<float>(); }
+	static const float2 *i3_psi1(const DevI3 &t) { return t.psi1f.as<float2>(); }
+	static const float *i3_psi2T(const DevI3 &t) { return t.psi2Tf.as<float>(); }
+};
+
+// ---------------------------------------------------------------------------
+// the factored right-hand side for one padded size P and working complex type C
+template <int P, class C> struct Rhs {
 	static constexpr int N = P / 2;
 	static constexpr long NN = (long)N * N, PP = (long)P * P;
+	using T = Tab<C>;
 
 	// spectra of the four components
 	static void spectra(Workspace &ws, int ncells, const double2 *W, cudaStream_t s) {
-		ws.What.ensure(sizeof(double2) * 4 * ncells * PP);
-		launch_pad_fft<P>(4 * ncells, W, ws.What.as<double2>(), s);
+		ws.What.ensure(sizeof(C) * 4 * ncells * PP);
+		launch_pad_fft<P>(4 * ncells, W, ws.What.as<C>(), s);
 	}
 
 	// S sums for Cc (tasks g = W_1..W_3, F = -4 W^_0 + 2) or I4 (g = W_0..W_3, F = 2 W^_0 - 1)
 	static void i1_sums(Workspace &ws, const DevI1 &t, int ncells, const double2 *W, bool cc, DevBuf &part, DevBuf &fs, int nchunk, cudaStream_t s) {
 		const int ntask = cc ? 3 : 4;
-		part.ensure(sizeof(double2) * ncells * ntask * nchunk * PP);
-		I1Params p{};
+		part.ensure(sizeof(C) * ncells * ntask * nchunk * PP);
+		I1ParamsT<C> p{};
 		p.ntask = ntask; p.nchunk = nchunk; p.nterms = t.nterms;
 		p.g = W; p.g_cell = 4 * NN;
 		for (int k = 0; k < 4; k++) p.g_comp[k] = cc ? std::min(k + 1, 3) : k;
-		p.What = ws.What.as<double2>(); p.w_cell = 4 * PP; p.f_comp = 0;
+		p.What = ws.What.as<C>(); p.w_cell = 4 * PP; p.f_comp = 0;
 		p.fa = cc ? -4.0 : 2.0; p.fb = cc ? 2.0 : -1.0;
-		p.psi2 = t.psi2.as<double>(); p.phi = t.phi.as<double>();
-		p.out = part.as<double2>();
+		p.psi2 = T::i1_psi2(t); p.phi = T::i1_phi(t);
+		p.out = part.as<C>();
 		launch_i1<P>(p, (long)ncells * ntask * nchunk, s);
-		fs.ensure(sizeof(double2) * ncells * ntask * PP);
-		FullParams f{};
-		f.in = part.as<double2>(); f.grid_stride = nchunk * PP; f.part_stride = PP; f.nparts = nchunk;
-		f.out = fs.as<double2>();
+		fs.ensure(sizeof(C) * ncells * ntask * PP);
+		FullParamsT<C> f{};
+		f.in = part.as<C>(); f.grid_stride = nchunk * PP; f.part_stride = PP; f.nparts = nchunk;
+		f.out = fs.as<C>();
 		launch_fft_full<P>(f, (long)ncells * ntask, s);
 	}
 
 	static void i2_sums(Workspace &ws, const DevI2 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
-		ws.i2p.ensure(sizeof(double2) * ncells * 4 * nchunk * PP);
-		I2Params p{};
+		ws.i2p.ensure(sizeof(C) * ncells * 4 * nchunk * PP);
+		I2ParamsT<C> p{};
 		p.ntask = 4; p.nchunk = nchunk; p.nterms = t.nterms;
 		p.src = W; p.cell_stride = 4 * NN;
 		for (int k = 0; k < 4; k++) { p.f_comp[k] = k; p.g_comp[k] = k; }
-		p.psi1 = t.psi1.as<double>(); p.psi2 = t.psi2.as<double>();
-		p.out = ws.i2p.as<double2>();
+		p.psi1 = T::i2_psi1(t); p.psi2 = T::i2_psi2(t);
+		p.out = ws.i2p.as<C>();
 		launch_i2<P>(p, (long)ncells * 4 * nchunk, s);
 	}
 
 	static void i3_sums(Workspace &ws, const DevI3 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
-		ws.i3p.ensure(sizeof(double2) * ncells * nchunk * 4 * PP);
-		I3Params p{};
+		ws.i3p.ensure(sizeof(C) * ncells * nchunk * 4 * PP);
+		I3ParamsT<C> p{};
 		p.nchunk = nchunk; p.nterms = t.nterms;
 		p.src = W; p.src_cell = 4 * NN;
 		for (int r = 0; r < 4; r++) p.src_comp[r] = r;
-		p.Ghat = ws.What.as<double2>(); p.g_cell = 4 * PP;
+		p.Ghat = ws.What.as<C>(); p.g_cell = 4 * PP;
 		const double eta[4] = { 1, -1, -1, -1 };
 		for (int r = 0; r < 4; r++) {           // CTA j: X_j = sum_i eta_i P_i . FFT2(psi2 . IFFT2(W^_i . P_j))
 			p.ncombo[r] = 4;
 			for (int i = 0; i < 4; i++) { p.ca[r][i] = i; p.cgi[r][i] = i; p.ccoef[r][i] = eta[i]; }
 		}
-		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
+		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
-		p.out = ws.i3p.as<double2>();
+		p.out = ws.i3p.as<C>();
 		launch_i3<P, 4>(p, (long)ncells * nchunk, s);
 	}
 
 	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
-		ch = pick_chunks(N, ncells, q);
+		T::prepare(q, s);
+		ch = pick_chunks(N, ncells, q, (int)(8 * sizeof(typename CT<C>::R)));
 		spectra(ws, ncells, W, s);
 		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
 		if (parts & RHS_CD) {
@@ -315,13 +372,13 @@ template <int P> struct Rhs {
 		}
 	}
 
-	static AsmParams asm_params(Workspace &ws, int parts, const Chunks &ch) {
-		AsmParams a{};
-		a.What = ws.What.as<double2>();
-		a.FS = (parts & RHS_CC) ? ws.fs.as<double2>() : nullptr;
-		a.FS4 = (parts & RHS_CD) ? ws.fs4.as<double2>() : nullptr;
-		a.Qp = (parts & RHS_CD) ? ws.i2p.as<double2>() : nullptr; a.nq = ch.i2;
-		a.Xp = (parts & RHS_CD) ? ws.i3p.as<double2>() : nullptr; a.nx = ch.i3;
+	static AsmParamsT<C> asm_params(Workspace &ws, int parts, const Chunks &ch) {
+		AsmParamsT<C> a{};
+		a.What = ws.What.as<C>();
+		a.FS = (parts & RHS_CC) ? ws.fs.as<C>() : nullptr;
+		a.FS4 = (parts & RHS_CD) ? ws.fs4.as<C>() : nullptr;
+		a.Qp = (parts & RHS_CD) ? ws.i2p.as<C>() : nullptr; a.nq = ch.i2;
+		a.Xp = (parts & RHS_CD) ? ws.i3p.as<C>() : nullptr; a.nx = ch.i3;
 		a.s2 = 1.0 / (double)PP;
 		a.s1 = a.s2 * a.s2;
 		return a;
@@ -330,7 +387,7 @@ template <int P> struct Rhs {
 	static void operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
 		Chunks ch;
 		prepare(ws, q, ncells, W, parts, ch, s);
-		AsmParams a = asm_params(ws, parts, ch);
+		AsmParamsT<C> a = asm_params(ws, parts, ch);
 		a.mode = 0; a.out_cc = cc; a.out_cd = cd;
 		launch_assemble<P>(a, ncells, s);
 	}
@@ -338,7 +395,7 @@ template <int P> struct Rhs {
 	static void update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
 		Chunks ch;
 		prepare(ws, q, ncells, wcur, RHS_ALL, ch, s);
-		AsmParams a = asm_params(ws, RHS_ALL, ch);
+		AsmParamsT<C> a = asm_params(ws, RHS_ALL, ch);
 		a.mode = 1; a.base = base; a.wcur = wcur; a.B = B; a.dtc = dtc; a.out = out;
 		launch_assemble<P>(a, ncells, s);
 	}
@@ -353,15 +410,19 @@ template <template <int> class F, class... A> void by_n(int N, A &&...args) {
 	}
 }
 
-template <int P> struct OpsRun {
-	static void run(Workspace &ws, const QuadSet &q, int n, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
-		Rhs<P>::operators(ws, q, n, W, parts, cc, cd, s);
-	}
+template <class C> struct OpsRun {
+	template <int P> struct F {
+		static void run(Workspace &ws, const QuadSet &q, int n, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
+			Rhs<P, C>::operators(ws, q, n, W, parts, cc, cd, s);
+		}
+	};
 };
-template <int P> struct UpdRun {
-	static void run(Workspace &ws, const QuadSet &q, int n, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
-		Rhs<P>::update(ws, q, n, base, wcur, B, dtc, out, s);
-	}
+template <class C> struct UpdRun {
+	template <int P> struct F {
+		static void run(Workspace &ws, const QuadSet &q, int n, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
+			Rhs<P, C>::update(ws, q, n, base, wcur, B, dtc, out, s);
+		}
+	};
 };
 
 __global__ void k_axpy(long n, const double2 *__restrict__ base, double a, const double2 *__restrict__ k, double2 *__restrict__ out) {
@@ -379,17 +440,18 @@ __global__ void k_rk4(long n, const double2 *__restrict__ W, double c, const dou
 
 }  // namespace
 
-Chunks pick_chunks(int N, int ncells, const QuadSet &q) {
+Chunks pick_chunks(int N, int ncells, const QuadSet &q, int prec) {
 	Chunks c;
 	const int sms = num_sms();
 	if (q.i1) c.i1 = best_chunks((long)ncells * 7, std::max(1, q.i1->nterms), sms, 64);
 	if (q.i2) c.i2 = best_chunks((long)ncells * 4, std::max(1, q.i2->nterms), sms, 64);
 	if (q.i3) {
 		int act = 0;
+		const bool f32 = prec == 32;
 		switch (N) {
-		case 8: act = active_i3_clusters<16>(); break;
-		case 16: act = active_i3_clusters<32>(); break;
-		default: act = active_i3_clusters<64>(); break;
+		case 8: act = f32 ? active_i3_clusters<16, float2>() : active_i3_clusters<16, double2>(); break;
+		case 16: act = f32 ? active_i3_clusters<32, float2>() : active_i3_clusters<32, double2>(); break;
+		default: act = f32 ? active_i3_clusters<64, float2>() : active_i3_clusters<64, double2>(); break;
 		}
 		c.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), act, 256);
 	}
@@ -397,11 +459,13 @@ Chunks pick_chunks(int N, int ncells, const QuadSet &q) {
 }
 
 void collision_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *out_cc, double2 *out_cd, cudaStream_t s) {
-	by_n<OpsRun>(ws.N, ws, q, ncells, W, parts, out_cc, out_cd, s);
+	if (ws.prec == 32) by_n<OpsRun<float2>::F>(ws.N, ws, q, ncells, W, parts, out_cc, out_cd, s);
+	else by_n<OpsRun<double2>::F>(ws.N, ws, q, ncells, W, parts, out_cc, out_cd, s);
 }
 
 void collision_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
-	by_n<UpdRun>(ws.N, ws, q, ncells, base, wcur, B, dtc, out, s);
+	if (ws.prec == 32) by_n<UpdRun<float2>::F>(ws.N, ws, q, ncells, base, wcur, B, dtc, out, s);
+	else by_n<UpdRun<double2>::F>(ws.N, ws, q, ncells, base, wcur, B, dtc, out, s);
 }
 
 void collision_step(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, const double *B, double dt, double2 *Wnext, cudaStream_t s) {
@@ -435,8 +499,8 @@ template <int P>
 __global__ void __launch_bounds__(Geo<P>::NT) k_extract_ifft(const double2 *__restrict__ Z, double scale, double2 *__restrict__ out) {
 	using G = Geo<P>;
 	constexpr int N = G::N;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + G::GRID;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	double2 *S = reinterpret_cast<double2 *>(smem_raw), *tw = S + G::GRID;
 	init_twiddles<P>(tw);
 	for (int i = threadIdx.x; i < P * P; i += G::NT) S[(i / P) * G::LDP + (i % P)] = Z[i];
 	__syncthreads();
@@ -547,7 +611,7 @@ template <int P> struct I3S {
 		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<double2>();
-		launch_i3<P, 2>(p, nchunk, s);
+		launch_i3<P, 2, double2>(p, nchunk, s);
 		ws.fs.ensure(sizeof(double2) * PP);
 		mul_sum(PP, nullptr, ws.i3p.as<double2>(), nchunk, 2 * PP, ws.fs.as<double2>(), s);   // rank-0 partials
 		const double s2 = 1.0 / (double)PP;
@@ -631,17 +695,128 @@ void flux_pair(int m, const double *A_dev, const double *U_dev, double *out_dev,
 }
 
 namespace {
+// ---------------------------------------------------------------------------
+// collision invariants.  The continuous collision operator conserves the
+// mass, momentum and energy of the trace component w0 (Cc_0 = 0; Cd_0 and the
+// magnetic term move none of them); the discrete operator keeps them only to
+// its quadrature accuracy (and the FP32 form to its rounding).  With
+// conservation switched on, the velocity-space step restores them: with
+// phi = (1, v_x, v_y, |v|^2) (grid-index units; the span does not depend on
+// the scale) and m_a = sum_v phi_a w0, the post-collision w0 becomes
+// w0 + |w0| sum_a lambda_a phi_a with lambda solving G lambda = m_before - m_after,
+// G_ab = sum_v |w0| phi_a phi_b.  Every sum is a fixed-order FP64 tree.
+constexpr int kInvThreads = 256;
+
+__device__ __forceinline__ void inv_basis(int q, int N, double (&phi)[4]) {
+	const int l = q / N, k = q % N;                       // l: v_x (slow index), k: v_y
+	const double vx = l < N / 2 ? l : l - N, vy = k < N / 2 ? k : k - N;
+	phi[0] = 1.0; phi[1] = vx; phi[2] = vy; phi[3] = vx * vx + vy * vy;
+}
+
+template <int K>
+__device__ __forceinline__ void inv_block_sum(double (&v)[K], double *sh) {
+	for (int k = 0; k < K; k++) sh[k * kInvThreads + threadIdx.x] = v[k];
+	__syncthreads();
+	for (int st = kInvThreads / 2; st > 0; st >>= 1) {
+		if (threadIdx.x < st)
+			for (int k = 0; k < K; k++) sh[k * kInvThreads + threadIdx.x] += sh[k * kInvThreads + threadIdx.x + st];
+		__syncthreads();
+	}
+	for (int k = 0; k < K; k++) v[k] = sh[k * kInvThreads];
+	__syncthreads();
+}
+
+__global__ void __launch_bounds__(kInvThreads) k_invariants(int N, const double *__restrict__ V, double *__restrict__ inv) {
+	__shared__ double sh[4 * kInvThreads];
+	const int NN = N * N;
+	const double *w0 = V + (long)blockIdx.x * 4 * NN;
+	double m[4] = { 0, 0, 0, 0 };
+	for (int q = threadIdx.x; q < NN; q += kInvThreads) {
+		double phi[4];
+		inv_basis(q, N, phi);
+		for (int a = 0; a < 4; a++) m[a] += phi[a] * w0[q];
+	}
+	inv_block_sum<4>(m, sh);
+	if (threadIdx.x < 4) inv[blockIdx.x * 4 + threadIdx.x] = m[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kInvThreads) k_restore_invariants(int N, double *__restrict__ V, const double *__restrict__ inv) {
+	__shared__ double sh[14 * kInvThreads];
+	__shared__ double lam[4];
+	const int NN = N * N;
+	double *w0 = V + (long)blockIdx.x * 4 * NN;
+	double a[14];                                          // m[4], then G upper triangle (10)
+	for (int k = 0; k < 14; k++) a[k] = 0.0;
+	for (int q = threadIdx.x; q < NN; q += kInvThreads) {
+		double phi[4];
+		inv_basis(q, N, phi);
+		const double w = w0[q], aw = fabs(w);
+		for (int i = 0; i < 4; i++) a[i] += phi[i] * w;
+		int t = 4;
+		for (int i = 0; i < 4; i++)
+			for (int j = i; j < 4; j++) a[t++] += aw * phi[i] * phi[j];
+	}
+	inv_block_sum<14>(a, sh);
+	if (threadIdx.x == 0) {
+		double G[4][5];
+		int t = 4;
+		for (int i = 0; i < 4; i++)
+			for (int j = i; j < 4; j++) { G[i][j] = a[t]; G[j][i] = a[t]; t++; }
+		for (int i = 0; i < 4; i++) G[i][4] = inv[blockIdx.x * 4 + i] - a[i];
+		// Gaussian elimination with partial pivoting (G is symmetric positive semidefinite)
+		bool ok = true;
+		for (int c = 0; c < 4; c++) {
+			int piv = c;
+			for (int r = c + 1; r < 4; r++) if (fabs(G[r][c]) > fabs(G[piv][c])) piv = r;
+			if (!(fabs(G[piv][c]) > 0.0)) { ok = false; break; }
+			if (piv != c) for (int k = 0; k < 5; k++) { const double x = G[c][k]; G[c][k] = G[piv][k]; G[piv][k] = x; }
+			for (int r = c + 1; r < 4; r++) {
+				const double f = G[r][c] / G[c][c];
+				for (int k = c; k < 5; k++) G[r][k] -= f * G[c][k];
+			}
+		}
+		if (ok)
+			for (int i = 3; i >= 0; i--) {
+				double x = G[i][4];
+				for (int k = i + 1; k < 4; k++) x -= G[i][k] * lam[k];
+				lam[i] = x / G[i][i];
+			}
+		else
+			for (int i = 0; i < 4; i++) lam[i] = 0.0;       // degenerate cell (w0 = 0 almost everywhere): leave it
+	}
+	__syncthreads();
+	for (int q = threadIdx.x; q < NN; q += kInvThreads) {
+		double phi[4];
+		inv_basis(q, N, phi);
+		const double w = w0[q];
+		w0[q] = w + fabs(w) * (lam[0] * phi[0] + lam[1] * phi[1] + lam[2] * phi[2] + lam[3] * phi[3]);
+	}
+}
+
+}  // namespace
+
 void fourier_collision(Workspace &ws, const QuadSet &q, int nc, double *V, const double *B, double dt, cudaStream_t s) {
 	const int N = ws.N;
 	const long cs = 4L * N * N;
 	if (nc <= 0) return;
+	const bool restore = ws.conserve != 0;
+	if (restore) {
+		ws.inv.ensure(sizeof(double) * 4 * nc);
+		ProfScope ps("invariants", s);
+		k_invariants<<<nc, kInvThreads, 0, s>>>(N, V, ws.inv.as<double>());
+		QB_CUDA(cudaGetLastError());
+	}
 	ws.fa.ensure(sizeof(double2) * cs * nc);
 	ws.fb.ensure(sizeof(double2) * cs * nc);
 	to_fourier(N, 4 * nc, V, ws.fa.as<double2>(), s);
 	collision_step(ws, q, nc, ws.fa.as<double2>(), B, dt, ws.fb.as<double2>(), s);
 	from_fourier(N, 4 * nc, ws.fb.as<double2>(), V, s);
+	if (restore) {
+		ProfScope ps("invariants", s);
+		k_restore_invariants<<<nc, kInvThreads, 0, s>>>(N, V, ws.inv.as<double>());
+		QB_CUDA(cudaGetLastError());
+	}
 }
-}  // namespace
 
 void inhom_step(Workspace &ws, const QuadSet &q, int ncells, const double *W, double *Wnext, const double *A_dev,
                 double h, double dt, const double *Bext, int bc, cudaStream_t s) {

@@ -44,11 +44,13 @@ struct DevBuf {
 
 // ---- quadrature tables on the device -----------------------------------------
 // I1-type (I1 and I4):  S = sum_t phi_t . IFFT2(F . FFT2(Pad(psi2_t . g)))
-struct DevI1 { int N = 0, nterms = 0; DevBuf psi2, phi; };
+// Each table set also holds FP32 roundings of its tables (the *f buffers),
+// made on first use by the FP32 precision form.
+struct DevI1 { int N = 0, nterms = 0; DevBuf psi2, phi; mutable DevBuf psi2f, phif; };
 // I2-type: Q = sum_t FFT2(Pad(psi1_t f)) . FFT2(Pad(psi2_t g))
-struct DevI2 { int N = 0, nterms = 0; DevBuf psi1, psi2; };
+struct DevI2 { int N = 0, nterms = 0; DevBuf psi1, psi2; mutable DevBuf psi1f, psi2f; };
 // I3-type: psi1_t complex N x N; psi2_t = scale[t] * table[idx[t]] (tables stored transposed)
-struct DevI3 { int N = 0, nterms = 0; DevBuf psi1, psi2T, idx, scale; };
+struct DevI3 { int N = 0, nterms = 0; DevBuf psi1, psi2T, idx, scale; mutable DevBuf psi1f, psi2Tf; };
 
 struct QuadSet { const DevI1 *i1 = nullptr; const DevI2 *i2 = nullptr; const DevI3 *i3 = nullptr; const DevI1 *i4 = nullptr; };
 
@@ -75,11 +77,14 @@ std::unique_ptr<Quad> make_quad(int N, int J, int M, double L, double R, cudaStr
 // ---- workspace: scratch for one evaluation stream ------------------------------
 struct Workspace {
 	int N = 0, device = -1;
+	int prec = 64;                           // working precision of the collision operator: 64 (FP64) or 32 (FP32 form)
+	int conserve = 0;                        // restore the collision invariants after each velocity-space collision step
 	cudaStream_t stream = nullptr;           // own stream (upstream API calls)
 	DevBuf What, i1cc, i1i4, i2p, i3p, fs, fs4, wmid;      // collision scratch
 	DevBuf fa, fb, va, vb;                   // state scratch (Fourier / velocity)
 	DevBuf io_in, io_out, bext, vgrid;       // staging for host-pointer calls
 	DevBuf aux, aux2;
+	DevBuf inv;                              // per-cell collision invariants (conservation on)
 	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
 	// replay of a repeated Strang step (batched API): the launch sequence of
 	// one (pointers, parameters) key is captured once and relaunched
@@ -92,7 +97,7 @@ struct Workspace {
 
 // chunking of the quadrature-term sums over CTAs (picked per launch shape)
 struct Chunks { int i1 = 1, i2 = 1, i3 = 1; };
-Chunks pick_chunks(int N, int ncells, const QuadSet &q);
+Chunks pick_chunks(int N, int ncells, const QuadSet &q, int prec);
 
 // ---- operators (device pointers, stream-ordered) ------------------------------
 enum RhsParts { RHS_CC = 1, RHS_CD = 2, RHS_ALL = 3 };
@@ -129,6 +134,11 @@ void transport_maxwell_lines(int m, int ncells, const double *in, double *out, c
 // sequential upstream-order flux sums: out_dev[0] rightward, out_dev[1] leftward
 void flux_pair(int m, const double *A_dev, const double *U_dev, double *out_dev, cudaStream_t s);
 
+// collision part of a Strang step on ncells velocity-space cells, in place:
+// to Fourier space, CollisionStep, back (upstream InternalFourierCollisionStep);
+// with ws.conserve set it also restores the trace component's mass, momentum
+// and energy
+void fourier_collision(Workspace &ws, const QuadSet &q, int ncells, double *V, const double *B, double dt, cudaStream_t s);
 // one Strang step over ncells cells (V space): 1/2 transport, collision, 1/2 transport.
 // A_dev: per-point velocities of a cell ([4][N*N], v_x of the slow index).
 // bc 0 periodic (all cells collide), 1 Dirichlet (first and last cell skip the collision)

@@ -69,7 +69,7 @@ void inhom_step_graphed(qb_workspace *ws, const qb_quad *q, int ncells, const do
                         const double *Bext, int bc, cudaStream_t caller) {
 	const double *A = velocity_tables(ws, q->q->L, caller);
 	const std::vector<double> key = { (double)ncells, (double)(uintptr_t)W, (double)(uintptr_t)Wnext, h, dt,
-	                                  (double)(uintptr_t)Bext, (double)bc, (double)(uintptr_t)q, q->q->L };
+	                                  (double)(uintptr_t)Bext, (double)bc, (double)(uintptr_t)q, q->q->L, (double)ws->prec, (double)ws->conserve };
 	if (!graphs_enabled() || key != ws->graph_key) {
 		if (ws->graph_exec) { cudaGraphExecDestroy(ws->graph_exec); ws->graph_exec = nullptr; }
 		ws->graph_key = key;
@@ -131,6 +131,23 @@ qb_workspace *qb_workspace_create(int N) {
 }
 
 void qb_workspace_free(qb_workspace *ws) { delete ws; }
+
+int qb_workspace_set_precision(qb_workspace *ws, int bits) {
+	return guarded([&] {
+		if (ws == nullptr) QB_FAIL("null workspace");
+		if (bits != 64 && bits != 32) QB_FAIL("precision must be 64 or 32 bits");
+		ws->prec = bits;
+	});
+}
+
+int qb_workspace_precision(const qb_workspace *ws) { return ws ? ws->prec : -1; }
+
+int qb_workspace_set_conservation(qb_workspace *ws, int on) {
+	return guarded([&] {
+		if (ws == nullptr) QB_FAIL("null workspace");
+		ws->conserve = on ? 1 : 0;
+	});
+}
 
 int qb_collision_operators(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, int parts, void *cc, void *cd, void *stream) {
 	return guarded([&] {
@@ -208,14 +225,7 @@ int qb_transport(int N, double L, int ncells, const double *in, double *out, dou
 int qb_fourier_collision(qb_workspace *ws, const qb_quad *q, int ncells, double *W, const double *Bext, double dt, void *stream) {
 	return guarded([&] {
 		check(ws, q);
-		cudaStream_t s = pick(ws, stream);
-		const int N = ws->N;
-		const long cs = 4L * N * N;
-		ws->fa.ensure(sizeof(double2) * cs * ncells);
-		ws->fb.ensure(sizeof(double2) * cs * ncells);
-		qb::to_fourier(N, 4 * ncells, W, ws->fa.as<double2>(), s);
-		qb::collision_step(*ws, q->q->set(), ncells, ws->fa.as<double2>(), Bext, dt, ws->fb.as<double2>(), s);
-		qb::from_fourier(N, 4 * ncells, ws->fb.as<double2>(), W, s);
+		qb::fourier_collision(*ws, q->q->set(), ncells, W, Bext, dt, pick(ws, stream));
 	});
 }
 

@@ -1,4 +1,5 @@
-// qb_fft.cuh — register/shared-memory FFT building blocks (FP64, sm_100a).
+// qb_fft.cuh — register/shared-memory FFT building blocks (sm_100a), generic
+// over the complex type C = double2 (FP64) or float2 (FP32).
 //
 // A length-L transform (L = 8*T, T in {1,2,4,8}) is spread over T consecutive
 // lanes of one warp; every lane holds 8 complex values in registers:
@@ -21,51 +22,75 @@
 
 namespace qb {
 
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {   // c + a*b
-	return make_double2(c.x + (a.x * b.x - a.y * b.y), c.y + (a.x * b.y + a.y * b.x));
+// scalar type of a complex type
+template <class C> struct CT;
+template <> struct CT<double2> { using R = double; };
+template <> struct CT<float2> { using R = float; };
+
+template <class C> __device__ __forceinline__ C mk(double re, double im) {
+	using R = typename CT<C>::R;
+	C z; z.x = (R)re; z.y = (R)im; return z;
 }
-__device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
+template <class C> __device__ __forceinline__ C czero() { return mk<C>(0.0, 0.0); }
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { C z; z.x = a.x + b.x; z.y = a.y + b.y; return z; }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { C z; z.x = a.x - b.x; z.y = a.y - b.y; return z; }
+template <class C> __device__ __forceinline__ C cmul(C a, C b) { C z; z.x = a.x * b.x - a.y * b.y; z.y = a.x * b.y + a.y * b.x; return z; }
+template <class C> __device__ __forceinline__ C cscale(C a, typename CT<C>::R s) { C z; z.x = a.x * s; z.y = a.y * s; return z; }
+template <class C> __device__ __forceinline__ C cfma(C a, C b, C c) {   // c + a*b
+	C z; z.x = c.x + (a.x * b.x - a.y * b.y); z.y = c.y + (a.x * b.y + a.y * b.x); return z;
+}
+// FP64 shorthands used by code that is FP64 only
+__device__ __forceinline__ double2 czero() { return czero<double2>(); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return cadd<double2>(a, b); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return csub<double2>(a, b); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return cmul<double2>(a, b); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return cscale<double2>(a, s); }
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) { return cfma<double2>(a, b, c); }
 
 // a * (DIR * i)
-template <int DIR> __device__ __forceinline__ double2 mul_i(double2 a) {
-	return DIR < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+template <int DIR, class C> __device__ __forceinline__ C mul_i(C a) {
+	C z;
+	if (DIR < 0) { z.x = a.y; z.y = -a.x; } else { z.x = -a.y; z.y = a.x; }
+	return z;
 }
 // a * w8^1 with w8 = exp(DIR * 2 pi i / 8)
-template <int DIR> __device__ __forceinline__ double2 mul_w8(double2 a) {
-	const double s = 0.70710678118654752440;
-	return DIR < 0 ? make_double2(s * (a.x + a.y), s * (a.y - a.x)) : make_double2(s * (a.x - a.y), s * (a.x + a.y));
+template <int DIR, class C> __device__ __forceinline__ C mul_w8(C a) {
+	using R = typename CT<C>::R;
+	const R s = (R)0.70710678118654752440;
+	C z;
+	if (DIR < 0) { z.x = s * (a.x + a.y); z.y = s * (a.y - a.x); } else { z.x = s * (a.x - a.y); z.y = s * (a.x + a.y); }
+	return z;
 }
 // a * w8^3
-template <int DIR> __device__ __forceinline__ double2 mul_w8_3(double2 a) {
-	const double s = 0.70710678118654752440;
-	return DIR < 0 ? make_double2(s * (a.y - a.x), -s * (a.x + a.y)) : make_double2(-s * (a.x + a.y), s * (a.x - a.y));
+template <int DIR, class C> __device__ __forceinline__ C mul_w8_3(C a) {
+	using R = typename CT<C>::R;
+	const R s = (R)0.70710678118654752440;
+	C z;
+	if (DIR < 0) { z.x = s * (a.y - a.x); z.y = -s * (a.x + a.y); } else { z.x = -s * (a.x + a.y); z.y = s * (a.x - a.y); }
+	return z;
 }
 
 // in-place 8-point DFT, natural order in and out (radix-2 decimation in frequency)
-template <int DIR> __device__ __forceinline__ void dft8(double2 (&x)[8]) {
-	const double2 a0 = cadd(x[0], x[4]), a4 = csub(x[0], x[4]);
-	const double2 a1 = cadd(x[1], x[5]), a5 = mul_w8<DIR>(csub(x[1], x[5]));
-	const double2 a2 = cadd(x[2], x[6]), a6 = mul_i<DIR>(csub(x[2], x[6]));
-	const double2 a3 = cadd(x[3], x[7]), a7 = mul_w8_3<DIR>(csub(x[3], x[7]));
-	const double2 b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_i<DIR>(csub(a1, a3));
-	const double2 b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_i<DIR>(csub(a5, a7));
+template <int DIR, class C> __device__ __forceinline__ void dft8(C (&x)[8]) {
+	const C a0 = cadd(x[0], x[4]), a4 = csub(x[0], x[4]);
+	const C a1 = cadd(x[1], x[5]), a5 = mul_w8<DIR>(csub(x[1], x[5]));
+	const C a2 = cadd(x[2], x[6]), a6 = mul_i<DIR>(csub(x[2], x[6]));
+	const C a3 = cadd(x[3], x[7]), a7 = mul_w8_3<DIR>(csub(x[3], x[7]));
+	const C b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_i<DIR>(csub(a1, a3));
+	const C b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_i<DIR>(csub(a5, a7));
 	x[0] = cadd(b0, b1); x[4] = csub(b0, b1);
 	x[2] = cadd(b2, b3); x[6] = csub(b2, b3);
 	x[1] = cadd(b4, b5); x[5] = csub(b4, b5);
 	x[3] = cadd(b6, b7); x[7] = csub(b6, b7);
 }
 
-template <int DIR> __device__ __forceinline__ void dft4(double2 &x0, double2 &x1, double2 &x2, double2 &x3) {
-	const double2 a0 = cadd(x0, x2), a2 = csub(x0, x2), a1 = cadd(x1, x3), a3 = mul_i<DIR>(csub(x1, x3));
+template <int DIR, class C> __device__ __forceinline__ void dft4(C &x0, C &x1, C &x2, C &x3) {
+	const C a0 = cadd(x0, x2), a2 = csub(x0, x2), a1 = cadd(x1, x3), a3 = mul_i<DIR>(csub(x1, x3));
 	x0 = cadd(a0, a1); x2 = csub(a0, a1); x1 = cadd(a2, a3); x3 = csub(a2, a3);
 }
 
-__device__ __forceinline__ void dft2(double2 &x0, double2 &x1) {
-	const double2 a = x0; x0 = cadd(a, x1); x1 = csub(a, x1);
+template <class C> __device__ __forceinline__ void dft2(C &x0, C &x1) {
+	const C a = x0; x0 = cadd(a, x1); x1 = csub(a, x1);
 }
 
 // Geometry of a length-L transform spread over T = L/8 lanes.
@@ -87,14 +112,14 @@ template <int L> struct Len {
 // repeated multiplication in registers, trading six shared-memory loads for
 // six complex multiplies (relative error of the powers below 1e-15).
 // Must be called by all 32 lanes of the warp (contains __syncwarp).
-template <int L, int DIR>
-__device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch, int sstride, const double2 *tw) {
+template <int L, int DIR, class C>
+__device__ __forceinline__ void fft1d(C (&x)[8], int tau, C *scratch, int sstride, const C *tw) {
 	using G = Len<L>;
 	dft8<DIR>(x);
 	if constexpr (G::T > 1) {
-		double2 w1 = tw[tau];
+		C w1 = tw[tau];
 		if (DIR > 0) w1.y = -w1.y;
-		double2 w = w1;
+		C w = w1;
 		x[1] = cmul(x[1], w);
 #pragma unroll
 		for (int q = 2; q < 8; q++) {
@@ -115,7 +140,7 @@ __device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch
 			if constexpr (G::T == 2) dft2(x[2 * u], x[2 * u + 1]);
 			else if constexpr (G::T == 4) dft4<DIR>(x[4 * u], x[4 * u + 1], x[4 * u + 2], x[4 * u + 3]);
 			else {
-				double2 y[8];
+				C y[8];
 #pragma unroll
 				for (int s = 0; s < 8; s++) y[s] = x[s];
 				dft8<DIR>(y);
@@ -128,8 +153,8 @@ __device__ __forceinline__ void fft1d(double2 (&x)[8], int tau, double2 *scratch
 
 // Reorder a lane's transform outputs (positions out_pos) into the input
 // layout (positions tau + T*r) through the scratch; a no-op when T is 1 or 8.
-template <int L>
-__device__ __forceinline__ void out_to_in(double2 (&x)[8], int tau, double2 *scratch, int sstride) {
+template <int L, class C>
+__device__ __forceinline__ void out_to_in(C (&x)[8], int tau, C *scratch, int sstride) {
 	using G = Len<L>;
 	if constexpr (G::T != 1 && G::T != 8) {
 		__syncwarp();
@@ -142,14 +167,14 @@ __device__ __forceinline__ void out_to_in(double2 (&x)[8], int tau, double2 *scr
 	}
 }
 
-// fill the twiddle table of fft1d<L>: tw[e] = exp(-2 pi i e / L), e < L
-// (all threads of the block call it)
-template <int L>
-__device__ __forceinline__ void init_twiddles(double2 *tw) {
+// fill the twiddle table of fft1d<L>: tw[e] = exp(-2 pi i e / L), e < L,
+// evaluated in FP64 and rounded to C (all threads of the block call it)
+template <int L, class C>
+__device__ __forceinline__ void init_twiddles(C *tw) {
 	for (int e = threadIdx.x; e < L; e += blockDim.x) {
 		double s, c;
 		sincospi(-2.0 * (double)e / (double)L, &s, &c);
-		tw[e] = make_double2(c, s);
+		tw[e] = mk<C>(c, s);
 	}
 }
 

@@ -1,4 +1,6 @@
-// qb_kernels.cuh — FP64 collision / transport kernels for sm_100a.
+// qb_kernels.cuh — collision kernels for sm_100a, generic over the working
+// complex type C (double2: the plain FP64 path; float2: the FP32 precision
+// form); the Wigner state itself is always FP64.
 //
 // Notation: N = velocity grid size, P = 2N padded size, all Fourier-space
 // grids complex (double2), element (l, k) at index k + n*l.  A P x P grid in
@@ -38,38 +40,45 @@ template <int P> struct Geo {
 	__device__ __forceinline__ static int pad(int k) { return k < N / 2 ? k : k + N; }
 };
 
+// resident CTAs per SM the term kernels are compiled for: the FP64 kernels
+// need ~128 registers a thread (one 512-thread CTA per SM at P = 64); the
+// FP32 ones fit two CTAs
+template <class C> struct Occ { static constexpr int CTAS = 1; };
+template <> struct Occ<float2> { static constexpr int CTAS = 2; };
+
 // ---------------------------------------------------------------------------
-// multipliers applied to the N-grid input before zero padding
-struct MulNone {
-	__device__ __forceinline__ double2 operator()(int, double2 v) const { return v; }
+// multipliers applied to the FP64 N-grid state before zero padding; the
+// product is formed in the working precision C
+template <class C> struct MulNone {
+	__device__ __forceinline__ C operator()(int, double2 v) const { return mk<C>(v.x, v.y); }
 };
-struct MulReal {           // psi (real N x N) .* v   (MultiplyPointwiseRC)
-	const double *psi;
-	__device__ __forceinline__ double2 operator()(int idx, double2 v) const { const double p = psi[idx]; return make_double2(p * v.x, p * v.y); }
+template <class C> struct MulReal {           // psi (real N x N) .* v   (MultiplyPointwiseRC)
+	const typename CT<C>::R *psi;
+	__device__ __forceinline__ C operator()(int idx, double2 v) const { return cscale(mk<C>(v.x, v.y), psi[idx]); }
 };
-struct MulCplx {           // psi (complex N x N) .* v   (MultiplyPointwiseCC)
-	const double2 *psi;
-	__device__ __forceinline__ double2 operator()(int idx, double2 v) const { return cmul(psi[idx], v); }
+template <class C> struct MulCplx {           // psi (complex N x N) .* v   (MultiplyPointwiseCC)
+	const C *psi;
+	__device__ __forceinline__ C operator()(int idx, double2 v) const { return cmul(psi[idx], mk<C>(v.x, v.y)); }
 };
 
 // lane's 8 inputs of padded row `prow` of Pad(mul . src)
-template <int P, class Mul>
-__device__ __forceinline__ void load_pad_row(double2 (&x)[8], int prow, int tau, const double2 *__restrict__ src, const Mul &mul) {
+template <int P, class C, class Mul>
+__device__ __forceinline__ void load_pad_row(C (&x)[8], int prow, int tau, const double2 *__restrict__ src, const Mul &mul) {
 	using G = Geo<P>;
 	const int l = G::src(prow);
 #pragma unroll
 	for (int r = 0; r < 8; r++) {
 		const int k = G::src(tau + G::T * r);
-		x[r] = (l >= 0 && k >= 0) ? mul(k + G::N * l, src[k + G::N * l]) : czero();
+		x[r] = (l >= 0 && k >= 0) ? mul(k + G::N * l, src[k + G::N * l]) : czero<C>();
 	}
 }
 
 // FFT2 (direction DIR) of Pad(mul . src) into the smem grid S (in place, two passes)
-template <int P, int DIR, class Mul>
-__device__ __forceinline__ void fft2_pad(double2 *S, const double2 *tw, const double2 *__restrict__ src, const Mul &mul) {
+template <int P, int DIR, class C, class Mul>
+__device__ __forceinline__ void fft2_pad(C *S, const C *tw, const double2 *__restrict__ src, const Mul &mul) {
 	using G = Geo<P>;
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
-	double2 x[8];
+	C x[8];
 	load_pad_row<P>(x, line, tau, src, mul);
 	fft1d<P, DIR>(x, tau, S + line * G::LDP, 1, tw);
 #pragma unroll
@@ -84,11 +93,11 @@ __device__ __forceinline__ void fft2_pad(double2 *S, const double2 *tw, const do
 }
 
 // FFT2 of a full grid already in smem S (natural layout), in place
-template <int P, int DIR>
-__device__ __forceinline__ void fft2_smem(double2 *S, const double2 *tw) {
+template <int P, int DIR, class C>
+__device__ __forceinline__ void fft2_smem(C *S, const C *tw) {
 	using G = Geo<P>;
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
-	double2 x[8];
+	C x[8];
 #pragma unroll
 	for (int r = 0; r < 8; r++) x[r] = S[line * G::LDP + tau + G::T * r];
 	fft1d<P, DIR>(x, tau, S + line * G::LDP, 1, tw);
@@ -104,23 +113,23 @@ __device__ __forceinline__ void fft2_smem(double2 *S, const double2 *tw) {
 }
 
 // copy smem grid (pitch LDP) to a dense global P x P grid, coalesced
-template <int P>
-__device__ __forceinline__ void smem_to_global(double2 *__restrict__ out, const double2 *S) {
+template <int P, class C>
+__device__ __forceinline__ void smem_to_global(C *__restrict__ out, const C *S) {
 	using G = Geo<P>;
 	for (int i = threadIdx.x; i < P * P; i += G::NT) out[i] = S[(i / P) * G::LDP + (i % P)];
 }
 
 // ---------------------------------------------------------------------------
 // K1: padded forward spectra  out[b] = FFT2(Pad(src[b]))   (one CTA per grid)
-template <int P>
-__global__ void __launch_bounds__(Geo<P>::NT) k_pad_fft(const double2 *__restrict__ src, double2 *__restrict__ out) {
+template <int P, class C>
+__global__ void __launch_bounds__(Geo<P>::NT) k_pad_fft(const double2 *__restrict__ src, C *__restrict__ out) {
 	using G = Geo<P>;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + G::GRID;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *S = reinterpret_cast<C *>(smem_raw), *tw = S + G::GRID;
 	init_twiddles<P>(tw);
 	__syncthreads();
 	const long b = blockIdx.x;
-	fft2_pad<P, -1>(S, tw, src + b * G::N * G::N, MulNone{});
+	fft2_pad<P, -1>(S, tw, src + b * G::N * G::N, MulNone<C>{});
 	smem_to_global<P>(out + b * P * P, S);
 }
 
@@ -128,43 +137,48 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_pad_fft(const double2 *__restric
 // K2: I1/I4-type term sums
 //   S[cell][task][chunk] = sum_{t in chunk} phi_t . IFFT2(F . FFT2(Pad(psi2_t . g)))
 //   g = gsrc[cell][g_comp[task]],  F = fa * What[cell][f_comp] + fb
-struct I1Params {
+template <class C> struct I1ParamsT {
+	using R = typename CT<C>::R;
 	int ntask, nchunk, nterms;
-	const double2 *g; long g_cell;          // N x N grids
+	const double2 *g; long g_cell;          // N x N grids (FP64 state)
 	int g_comp[4];
-	const double2 *What; long w_cell;       // P x P grids
+	const C *What; long w_cell;             // P x P grids
 	int f_comp; double fa, fb;
-	const double *psi2;                     // nterms x N x N
-	const double *phi;                      // nterms x P x P
-	double2 *out;                           // [cell][task][chunk][P*P]
+	const R *psi2;                          // nterms x N x N
+	const R *phi;                           // nterms x P x P
+	C *out;                                 // [cell][task][chunk][P*P]
 };
+using I1Params = I1ParamsT<double2>;
 
-template <int P>
-__global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1Params p) {
+template <int P, class C>
+__global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1ParamsT<C> p) {
 	using G = Geo<P>;
 	using Lp = Len<P>;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *F = smem + G::GRID, *tw = smem + 2 * G::GRID;
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *S = reinterpret_cast<C *>(smem_raw), *F = S + G::GRID, *tw = S + 2 * G::GRID;
 	const int chunk = blockIdx.x % p.nchunk;
 	const int task = (blockIdx.x / p.nchunk) % p.ntask;
 	const long cell = blockIdx.x / (p.nchunk * p.ntask);
 	init_twiddles<P>(tw);
-	const double2 *W = p.What + cell * p.w_cell + (long)p.f_comp * P * P;
+	const C *W = p.What + cell * p.w_cell + (long)p.f_comp * P * P;
+	const R fa = (R)p.fa, fb = (R)p.fb;
 	for (int i = threadIdx.x; i < P * P; i += G::NT) {
-		const double2 w = W[i];
-		F[(i / P) * G::LDP + (i % P)] = make_double2(p.fa * w.x + p.fb, p.fa * w.y);
+		const C w = W[i];
+		C f; f.x = fa * w.x + fb; f.y = fa * w.y;
+		F[(i / P) * G::LDP + (i % P)] = f;
 	}
 	__syncthreads();
 	const double2 *g = p.g + cell * p.g_cell + (long)p.g_comp[task] * G::N * G::N;
 	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
-	double2 acc[8];
+	C acc[8];
 #pragma unroll
-	for (int e = 0; e < 8; e++) acc[e] = czero();
+	for (int e = 0; e < 8; e++) acc[e] = czero<C>();
 	for (int t = t0; t < t1; t++) {
-		double2 x[8];
+		C x[8];
 		// rows: FFT of Pad(psi2_t . g)
-		load_pad_row<P>(x, line, tau, g, MulReal{p.psi2 + (long)t * G::N * G::N});
+		load_pad_row<P>(x, line, tau, g, MulReal<C>{p.psi2 + (long)t * G::N * G::N});
 		fft1d<P, -1>(x, tau, S + line * G::LDP, 1, tw);
 #pragma unroll
 		for (int e = 0; e < 8; e++) S[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
@@ -184,16 +198,16 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1Params p) {
 #pragma unroll
 		for (int r = 0; r < 8; r++) x[r] = S[line * G::LDP + tau + G::T * r];
 		fft1d<P, +1>(x, tau, S + line * G::LDP, 1, tw);
-		const double *phi = p.phi + (long)t * P * P + line * P;
+		const R *phi = p.phi + (long)t * P * P + line * P;
 #pragma unroll
 		for (int e = 0; e < 8; e++) {
-			const double f = phi[Lp::out_pos(tau, e)];
+			const R f = phi[Lp::out_pos(tau, e)];
 			acc[e].x += f * x[e].x;
 			acc[e].y += f * x[e].y;
 		}
 		__syncthreads();
 	}
-	double2 *o = p.out + ((cell * p.ntask + task) * p.nchunk + chunk) * (long)P * P + line * P;
+	C *o = p.out + ((cell * p.ntask + task) * p.nchunk + chunk) * (long)P * P + line * P;
 #pragma unroll
 	for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
 }
@@ -201,20 +215,22 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1Params p) {
 // ---------------------------------------------------------------------------
 // K3: I2-type term sums
 //   Q[cell][task][chunk] = sum_t FFT2(Pad(psi1_t . f)) . FFT2(Pad(psi2_t . g))
-struct I2Params {
+template <class C> struct I2ParamsT {
+	using R = typename CT<C>::R;
 	int ntask, nchunk, nterms;
-	const double2 *src; long cell_stride;   // N x N grids
+	const double2 *src; long cell_stride;   // N x N grids (FP64 state)
 	int f_comp[4], g_comp[4];
-	const double *psi1, *psi2;              // nterms x N x N each
-	double2 *out;                           // [cell][task][chunk][P*P]
+	const R *psi1, *psi2;                   // nterms x N x N each
+	C *out;                                 // [cell][task][chunk][P*P]
 };
+using I2Params = I2ParamsT<double2>;
 
-template <int P>
-__global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2Params p) {
+template <int P, class C>
+__global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2ParamsT<C> p) {
 	using G = Geo<P>;
 	using Lp = Len<P>;
-	extern __shared__ double2 smem[];
-	double2 *A = smem, *B = smem + G::GRID, *tw = smem + 2 * G::GRID;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *A = reinterpret_cast<C *>(smem_raw), *B = A + G::GRID, *tw = A + 2 * G::GRID;
 	const int chunk = blockIdx.x % p.nchunk;
 	const int task = (blockIdx.x / p.nchunk) % p.ntask;
 	const long cell = blockIdx.x / (p.nchunk * p.ntask);
@@ -224,13 +240,13 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2Params p) {
 	const double2 *g = p.src + cell * p.cell_stride + (long)p.g_comp[task] * G::N * G::N;
 	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
-	double2 acc[8];
+	C acc[8];
 #pragma unroll
-	for (int e = 0; e < 8; e++) acc[e] = czero();
+	for (int e = 0; e < 8; e++) acc[e] = czero<C>();
 	for (int t = t0; t < t1; t++) {
-		fft2_pad<P, -1>(A, tw, f, MulReal{p.psi1 + (long)t * G::N * G::N});
-		double2 x[8];
-		load_pad_row<P>(x, line, tau, g, MulReal{p.psi2 + (long)t * G::N * G::N});
+		fft2_pad<P, -1>(A, tw, f, MulReal<C>{p.psi1 + (long)t * G::N * G::N});
+		C x[8];
+		load_pad_row<P>(x, line, tau, g, MulReal<C>{p.psi2 + (long)t * G::N * G::N});
 		fft1d<P, -1>(x, tau, B + line * G::LDP, 1, tw);
 #pragma unroll
 		for (int e = 0; e < 8; e++) B[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
@@ -255,23 +271,26 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2Params p) {
 // into its shared memory; the other CTAs read it through distributed shared
 // memory.  For each of its combos (a, g, coef) it accumulates
 //   X_r += coef * P_a . FFT2(psi2_t . IFFT2(G_g . P_r)).
-struct I3Params {
+template <class C> struct I3ParamsT {
+	using R = typename CT<C>::R;
 	int nchunk, nterms;
-	const double2 *src; long src_cell; int src_comp[4];   // N x N grids
-	const double2 *Ghat; long g_cell;                     // P x P grids, G_g at Ghat + cell*g_cell + g*P*P
+	const double2 *src; long src_cell; int src_comp[4];   // N x N grids (FP64 state)
+	const C *Ghat; long g_cell;                           // P x P grids, G_g at Ghat + cell*g_cell + g*P*P
 	int ncombo[4]; int ca[4][4], cgi[4][4]; double ccoef[4][4];
-	const double2 *psi1;                                  // nterms x N x N (complex)
-	const double *psi2T;                                  // transposed P x P tables
+	const C *psi1;                                        // nterms x N x N (complex)
+	const R *psi2T;                                       // transposed P x P tables
 	const int *psi2_idx; const double *psi2_scale;        // per term
-	double2 *out;                                         // [cell][chunk][CS][P*P]
+	C *out;                                               // [cell][chunk][CS][P*P]
 };
+using I3Params = I3ParamsT<double2>;
 
-template <int P, int CS>
-__global__ void __launch_bounds__(Geo<P>::NT) k_i3(const I3Params p) {
+template <int P, int CS, class C>
+__global__ void __launch_bounds__(Geo<P>::NT, Occ<C>::CTAS) k_i3(const I3ParamsT<C> p) {
 	using G = Geo<P>;
 	using Lp = Len<P>;
-	extern __shared__ double2 smem[];
-	double2 *Pr = smem, *Ug = smem + G::GRID, *tw = smem + 2 * G::GRID;
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *Pr = reinterpret_cast<C *>(smem_raw), *Ug = Pr + G::GRID, *tw = Pr + 2 * G::GRID;
 	cg::cluster_group cluster = cg::this_cluster();
 	const int rank = (int)cluster.block_rank();
 	const long cid = blockIdx.x / CS;
@@ -282,18 +301,18 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i3(const I3Params p) {
 	const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[rank] * G::N * G::N;
 	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
-	double2 acc[8];
+	C acc[8];
 #pragma unroll
-	for (int e = 0; e < 8; e++) acc[e] = czero();
+	for (int e = 0; e < 8; e++) acc[e] = czero<C>();
 	const int nc = p.ncombo[rank];
 	for (int t = t0; t < t1; t++) {
-		fft2_pad<P, -1>(Pr, tw, src, MulCplx{p.psi1 + (long)t * G::N * G::N});
+		fft2_pad<P, -1>(Pr, tw, src, MulCplx<C>{p.psi1 + (long)t * G::N * G::N});
 		cluster.sync();
-		const double *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
-		const double sc = p.psi2_scale[t];
+		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
+		const R sc = (R)p.psi2_scale[t];
 		for (int c = 0; c < nc; c++) {
-			const double2 *Gg = p.Ghat + cell * p.g_cell + (long)p.cgi[rank][c] * P * P;
-			double2 x[8];
+			const C *Gg = p.Ghat + cell * p.g_cell + (long)p.cgi[rank][c] * P * P;
+			C x[8];
 			// rows: IFFT of G_g . P_r
 #pragma unroll
 			for (int r = 0; r < 8; r++) {
@@ -310,7 +329,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i3(const I3Params p) {
 			fft1d<P, +1>(x, tau, Ug + line, G::LDP, tw);
 #pragma unroll
 			for (int e = 0; e < 8; e++) {
-				const double f = sc * psi2[line * P + Lp::out_pos(tau, e)];
+				const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
 				x[e].x *= f;
 				x[e].y *= f;
 			}
@@ -323,11 +342,11 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i3(const I3Params p) {
 #pragma unroll
 			for (int r = 0; r < 8; r++) x[r] = Ug[line * G::LDP + tau + G::T * r];
 			fft1d<P, -1>(x, tau, Ug + line * G::LDP, 1, tw);
-			const double2 *Pa = cluster.map_shared_rank(Pr, p.ca[rank][c]);
-			const double coef = p.ccoef[rank][c];
+			const C *Pa = cluster.map_shared_rank(Pr, p.ca[rank][c]);
+			const R coef = (R)p.ccoef[rank][c];
 #pragma unroll
 			for (int e = 0; e < 8; e++) {
-				const double2 v = cmul(Pa[line * G::LDP + Lp::out_pos(tau, e)], x[e]);
+				const C v = cmul(Pa[line * G::LDP + Lp::out_pos(tau, e)], x[e]);
 				acc[e].x += coef * v.x;
 				acc[e].y += coef * v.y;
 			}
@@ -335,28 +354,29 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i3(const I3Params p) {
 		}
 		cluster.sync();
 	}
-	double2 *o = p.out + ((cell * p.nchunk + chunk) * CS + rank) * (long)P * P + line * P;
+	C *o = p.out + ((cell * p.nchunk + chunk) * CS + rank) * (long)P * P + line * P;
 #pragma unroll
 	for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
 }
 
 // ---------------------------------------------------------------------------
 // K5: out[b] = FFT2(sum_{k<nparts} in[b*grid_stride + k*part_stride]) (full grids)
-struct FullParams {
-	const double2 *in; long grid_stride, part_stride; int nparts;
-	double2 *out;   // [b][P*P]
+template <class C> struct FullParamsT {
+	const C *in; long grid_stride, part_stride; int nparts;
+	C *out;   // [b][P*P]
 };
+using FullParams = FullParamsT<double2>;
 
-template <int P>
-__global__ void __launch_bounds__(Geo<P>::NT) k_fft_full(const FullParams p) {
+template <int P, class C>
+__global__ void __launch_bounds__(Geo<P>::NT) k_fft_full(const FullParamsT<C> p) {
 	using G = Geo<P>;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + G::GRID;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *S = reinterpret_cast<C *>(smem_raw), *tw = S + G::GRID;
 	init_twiddles<P>(tw);
 	const long b = blockIdx.x;
-	const double2 *in = p.in + b * p.grid_stride;
+	const C *in = p.in + b * p.grid_stride;
 	for (int i = threadIdx.x; i < P * P; i += G::NT) {
-		double2 s = in[i];
+		C s = in[i];
 		for (int k = 1; k < p.nparts; k++) s = cadd(s, in[k * p.part_stride + i]);
 		S[(i / P) * G::LDP + (i % P)] = s;
 	}
@@ -371,14 +391,16 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_fft_full(const FullParams p) {
 //   Zcd_j = s2 (-Wh_j + d_j0) . Q - eta2_j s1 X_j
 //         + s1 (eta2_j Wh_0 . FS4_j + 2 Wh_j . FS4_0) - d_j0 2 s1 sum_c Wh_c . FS4_c   (collision.c:95-167)
 //   Cc_j = s1 Extract(IFFT2(Zcc_j)), Cd_j = Extract(IFFT2(Zcd_j))
-// mode 0 writes Cc and Cd; mode 1 writes base + dtc (Cc + Cd + CB) with the
-// magnetic rotation CB of `wcur` (upstream simulation.c:75-135).
-struct AsmParams {
-	const double2 *What;              // [cell][4][P*P]
-	const double2 *FS;                // [cell][3][P*P]  FFT2 of the Cc sums S_1..S_3, or null
-	const double2 *FS4;               // [cell][4][P*P]  FFT2 of the I4 sums, or null
-	const double2 *Qp; int nq;        // [cell][4][nq][P*P] I2 partials, or null
-	const double2 *Xp; int nx;        // [cell][nx][4][P*P] I3 partials, or null
+// The spectra and transforms are in the working precision C; Cc and Cd are
+// widened to FP64 for the outputs.  mode 0 writes Cc and Cd; mode 1 writes
+// base + dtc (Cc + Cd + CB) in FP64 with the magnetic rotation CB of `wcur`
+// (upstream simulation.c:75-135).
+template <class C> struct AsmParamsT {
+	const C *What;                    // [cell][4][P*P]
+	const C *FS;                      // [cell][3][P*P]  FFT2 of the Cc sums S_1..S_3, or null
+	const C *FS4;                     // [cell][4][P*P]  FFT2 of the I4 sums, or null
+	const C *Qp; int nq;              // [cell][4][nq][P*P] I2 partials, or null
+	const C *Xp; int nx;              // [cell][nx][4][P*P] I3 partials, or null
 	double s1, s2;
 	int mode;
 	double2 *out_cc, *out_cd;         // mode 0: [cell][4][N*N] (either may be null)
@@ -386,19 +408,22 @@ struct AsmParams {
 	const double *B; double dtc;      // B: [cell][3]
 	double2 *out;                     // mode 1
 };
+using AsmParams = AsmParamsT<double2>;
 
-template <int P>
-__global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
+template <int P, class C>
+__global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) {
 	using G = Geo<P>;
+	using R = typename CT<C>::R;
 	constexpr int N = G::N, NN = N * N, PP = P * P;
 	constexpr int PER = (NN + G::NT - 1) / G::NT;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + G::GRID;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *S = reinterpret_cast<C *>(smem_raw), *tw = S + G::GRID;
 	const int j = blockIdx.x & 3;
 	const long cell = blockIdx.x >> 2;
 	init_twiddles<P>(tw);
-	const double eta2[4] = { 2, -2, -2, -2 };
-	const double2 *Wh = p.What + cell * 4 * PP;
+	const R eta2[4] = { 2, -2, -2, -2 };
+	const R s1 = (R)p.s1, s2 = (R)p.s2;
+	const C *Wh = p.What + cell * 4 * PP;
 	double2 cc[PER], cd[PER];
 #pragma unroll
 	for (int u = 0; u < PER; u++) { cc[u] = czero(); cd[u] = czero(); }
@@ -406,9 +431,9 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
 	// --- Cc ---
 	if (p.FS != nullptr && j > 0) {
 		const int gi = (j % 3) + 1, hi = ((j + 1) % 3) + 1;    // j=1:(2,3) j=2:(3,1) j=3:(1,2)
-		const double2 *FS = p.FS + cell * 3 * PP;
+		const C *FS = p.FS + cell * 3 * PP;
 		for (int i = threadIdx.x; i < PP; i += G::NT) {
-			const double2 z = csub(cmul(Wh[hi * PP + i], FS[(gi - 1) * PP + i]), cmul(Wh[gi * PP + i], FS[(hi - 1) * PP + i]));
+			const C z = csub(cmul(Wh[hi * PP + i], FS[(gi - 1) * PP + i]), cmul(Wh[gi * PP + i], FS[(hi - 1) * PP + i]));
 			S[(i / P) * G::LDP + (i % P)] = z;
 		}
 		__syncthreads();
@@ -417,8 +442,8 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
 		for (int u = 0; u < PER; u++) {
 			const int q = threadIdx.x + u * G::NT;
 			if (q < NN) {
-				const double2 v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
-				cc[u] = make_double2(p.s1 * v.x, p.s1 * v.y);
+				const C v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+				cc[u] = make_double2(p.s1 * (double)v.x, p.s1 * (double)v.y);
 			}
 		}
 		__syncthreads();
@@ -426,34 +451,34 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
 	// --- Cd ---
 	if (p.FS4 != nullptr || p.Qp != nullptr || p.Xp != nullptr) {
 		for (int i = threadIdx.x; i < PP; i += G::NT) {
-			double2 z = czero();
+			C z = czero<C>();
 			if (p.Qp != nullptr) {
-				double2 q = czero();
+				C q = czero<C>();
 				for (int ii = 0; ii < 4; ii++) {
-					const double2 *Q = p.Qp + ((cell * 4 + ii) * p.nq) * (long)PP + i;
-					double2 s = czero();
+					const C *Q = p.Qp + ((cell * 4 + ii) * p.nq) * (long)PP + i;
+					C s = czero<C>();
 					for (int k = 0; k < p.nq; k++) s = cadd(s, Q[(long)k * PP]);
 					q.x += eta2[ii] * s.x; q.y += eta2[ii] * s.y;
 				}
-				double2 h = make_double2(-Wh[j * PP + i].x, -Wh[j * PP + i].y);
-				if (j == 0) h.x += 1.0;
-				const double2 v = cmul(h, q);
-				z.x += p.s2 * v.x; z.y += p.s2 * v.y;
+				C h; h.x = -Wh[j * PP + i].x; h.y = -Wh[j * PP + i].y;
+				if (j == 0) h.x += (R)1.0;
+				const C v = cmul(h, q);
+				z.x += s2 * v.x; z.y += s2 * v.y;
 			}
 			if (p.Xp != nullptr) {
-				double2 s = czero();
+				C s = czero<C>();
 				for (int k = 0; k < p.nx; k++) s = cadd(s, p.Xp[((cell * p.nx + k) * 4 + j) * (long)PP + i]);
-				z.x -= eta2[j] * p.s1 * s.x; z.y -= eta2[j] * p.s1 * s.y;
+				z.x -= eta2[j] * s1 * s.x; z.y -= eta2[j] * s1 * s.y;
 			}
 			if (p.FS4 != nullptr) {
-				const double2 *F4 = p.FS4 + cell * 4 * PP;
-				double2 v = cadd(cscale(cmul(Wh[i], F4[j * PP + i]), eta2[j]), cscale(cmul(Wh[j * PP + i], F4[i]), 2.0));
+				const C *F4 = p.FS4 + cell * 4 * PP;
+				C v = cadd(cscale(cmul(Wh[i], F4[j * PP + i]), eta2[j]), cscale(cmul(Wh[j * PP + i], F4[i]), (R)2.0));
 				if (j == 0) {
-					double2 s = czero();
+					C s = czero<C>();
 					for (int c = 0; c < 4; c++) s = cadd(s, cmul(Wh[c * PP + i], F4[c * PP + i]));
-					v = csub(v, cscale(s, 2.0));
+					v = csub(v, cscale(s, (R)2.0));
 				}
-				z.x += p.s1 * v.x; z.y += p.s1 * v.y;
+				z.x += s1 * v.x; z.y += s1 * v.y;
 			}
 			S[(i / P) * G::LDP + (i % P)] = z;
 		}
@@ -462,10 +487,13 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
 #pragma unroll
 		for (int u = 0; u < PER; u++) {
 			const int q = threadIdx.x + u * G::NT;
-			if (q < NN) cd[u] = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+			if (q < NN) {
+				const C v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+				cd[u] = make_double2((double)v.x, (double)v.y);
+			}
 		}
 	}
-	// --- outputs ---
+	// --- outputs (FP64) ---
 #pragma unroll
 	for (int u = 0; u < PER; u++) {
 		const int q = threadIdx.x + u * G::NT;
@@ -493,8 +521,8 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParams p) {
 template <int N>
 __global__ void __launch_bounds__(Len<N>::T * N) k_to_fourier(const double *__restrict__ Wv, double2 *__restrict__ Wf) {
 	constexpr int T = Len<N>::T, LD = N + 1;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + N * LD;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	double2 *S = reinterpret_cast<double2 *>(smem_raw), *tw = S + N * LD;
 	init_twiddles<N>(tw);
 	__syncthreads();
 	const long b = blockIdx.x;
@@ -532,8 +560,8 @@ __global__ void __launch_bounds__(Len<N>::T * N) k_to_fourier(const double *__re
 template <int N>
 __global__ void __launch_bounds__(Len<N>::T * N) k_from_fourier(const double2 *__restrict__ Wf, double *__restrict__ Wv) {
 	constexpr int T = Len<N>::T, LD = N + 1;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + N * LD;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	double2 *S = reinterpret_cast<double2 *>(smem_raw), *tw = S + N * LD;
 	init_twiddles<N>(tw);
 	__syncthreads();
 	const long b = blockIdx.x;
@@ -561,8 +589,8 @@ __global__ void __launch_bounds__(Len<N>::T * N) k_from_fourier(const double2 *_
 template <int L, int DIR>
 __global__ void __launch_bounds__(Len<L>::T * L) k_fft2_generic(const void *__restrict__ in, double2 *__restrict__ out, int r2c) {
 	constexpr int T = Len<L>::T, LD = L + 1;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + L * LD;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	double2 *S = reinterpret_cast<double2 *>(smem_raw), *tw = S + L * LD;
 	init_twiddles<L>(tw);
 	__syncthreads();
 	const int line = threadIdx.x / T, tau = threadIdx.x % T;

@@ -63,8 +63,8 @@ __global__ void __launch_bounds__(qb::Geo<P>::NT) k_noalloc_finish(const double2
                                                                    double2 *__restrict__ out) {
 	using G = qb::Geo<P>;
 	constexpr int N = G::N;
-	extern __shared__ double2 smem[];
-	double2 *S = smem, *tw = smem + G::GRID;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	double2 *S = reinterpret_cast<double2 *>(smem_raw), *tw = S + G::GRID;
 	qb::init_twiddles<P>(tw);
 	for (int i = threadIdx.x; i < P * P; i += G::NT) {
 		double2 s = X[i];
@@ -102,8 +102,8 @@ void run(const qb::DevI3 &t, const double2 *f, const double2 *g, const double2 *
 	QB_CUDA(cudaMemcpyAsync(src + 2 * NN, g, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
 
 	const size_t sm1 = sizeof(double2) * (G::GRID + P), sm2 = sizeof(double2) * (2 * G::GRID + P);
-	QB_CUDA(cudaFuncSetAttribute(qb::k_pad_fft<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-	qb::k_pad_fft<P><<<1, G::NT, sm1, s>>>(src + 2 * NN, ghat);
+	QB_CUDA(cudaFuncSetAttribute(qb::k_pad_fft<P, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+	qb::k_pad_fft<P, double2><<<1, G::NT, sm1, s>>>(src + 2 * NN, ghat);
 	QB_CUDA(cudaGetLastError());
 
 	qb::I3Params p{};
@@ -115,7 +115,7 @@ void run(const qb::DevI3 &t, const double2 *f, const double2 *g, const double2 *
 	p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
 	p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 	p.out = parts;
-	auto kern = qb::k_i3<P, 2>;
+	auto kern = qb::k_i3<P, 2, double2>;
 	QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3((unsigned)(nchunk * 2));

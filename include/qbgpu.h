@@ -37,6 +37,26 @@ void qb_quad_free(qb_quad *q);
 qb_workspace *qb_workspace_create(int N);
 void qb_workspace_free(qb_workspace *ws);
 
+/* working precision of the collision operator evaluated through `ws`:
+ * 64 (default) is the plain FP64 path of the upstream code; 32 is the FP32
+ * precision form, which has no upstream counterpart: the Wigner state, the
+ * Pauli-blocking assembly, the magnetic term and the time update stay FP64,
+ * while the spectra, the quadrature tables (rounded once per table set) and
+ * every FFT of the factored integrals run in FP32.  Transport is unaffected.
+ * The first FP32 evaluation with a table set rounds its tables and
+ * synchronises the stream, so it must not be inside a stream capture. */
+int qb_workspace_set_precision(qb_workspace *ws, int bits);
+int qb_workspace_precision(const qb_workspace *ws);
+
+/* on != 0: the velocity-space steps through `ws` (qb_inhom_step,
+ * qb_inhom_step_maxwell, qb_fourier_collision, qb_simulate_record) restore,
+ * after each collision, the mass, momentum and energy of the trace component
+ * w0 -- the invariants of the continuous collision operator, which the
+ * discrete one keeps only to its quadrature accuracy -- by the least change
+ * w0 += |w0| (l0 + l1 v_x + l2 v_y + l3 |v|^2) that puts them back.  No
+ * upstream counterpart; off by default (the upstream step). */
+int qb_workspace_set_conservation(qb_workspace *ws, int on);
+
 /* Cc and/or Cd (CcInt / CdInt, upstream src/collision.c:74-254) of ncells
  * Fourier states; parts: 1 = Cc, 2 = Cd, 3 = both; cc / cd may be NULL. */
 int qb_collision_operators(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, int parts,
@@ -101,6 +121,26 @@ long qb_simulate_record(qb_workspace *ws, const qb_quad *q, int ncells, const do
  * W(v) over the grid, and the Fermi-Dirac entropy (upstream
  * visualization/wignerMoments.m:15-37, visualization/entropy.m). */
 int qb_diagnostics(int N, double L, int ncells, const double *W, double *out, void *stream);
+
+/* Fermi-Dirac equilibrium with the conserved moments (spin density matrix,
+ * mean velocity, energy) of each of ncells velocity-space states W (device),
+ * written to WFD (device, same layout) (upstream visualization/asymptoticFD.m,
+ * calculateFDparams.m, createFD.m; the moments as qb_diagnostics).  The
+ * inverse temperature and the two chemical potentials solve the 3 moment
+ * equations by Newton's method on the host from the upstream starting points
+ * (1, 1, 1), then (1, 1, 0.5).  params (host, may be NULL) gets 9 doubles per
+ * cell: beta, mu_1, mu_2 (smaller / larger density eigenvalue), u_x, u_y,
+ * the unit spin direction n_x, n_y, n_z of the larger eigenvalue, and the
+ * residual norm of the moment equations.  Synchronises `stream`; N <= 64. */
+int qb_fermi_dirac_equilibrium(int N, double L, int ncells, const double *W, double *WFD, double *params, void *stream);
+
+/* per cell 2 doubles into out (device): the quantum relative entropy of W(v)
+ * to WFD(v) (eigenvalues clamped to [eps, 1 - eps]) summed over the points
+ * with WFD_0(v) > 1e-6, times dv^2, and the distance sum_j ||W_j - WFD_j||_1 dv^2
+ * in the matrix 1-norm (largest sum over v_y at fixed v_x) (upstream
+ * visualization/relentropy.m, visualization/visualizeHomBoltzmann.m:116-148).
+ * N <= 64. */
+int qb_relative_entropy(int N, double L, int ncells, const double *W, const double *WFD, double *out, void *stream);
 
 /* launch accounting: every engine kernel launch is counted; while profiling
  * is on, launches are bracketed by CUDA events on their stream.

@@ -52,6 +52,9 @@ def lib(n_grid=N_GRID):
     L.qb_workspace_create.restype = _vp
     L.qb_workspace_create.argtypes = [C.c_int]
     L.qb_workspace_free.argtypes = [_vp]
+    L.qb_workspace_set_precision.argtypes = [_vp, C.c_int]
+    L.qb_workspace_precision.argtypes = [_vp]
+    L.qb_workspace_set_conservation.argtypes = [_vp, C.c_int]
     L.qb_collision_operators.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp]
     L.qb_collision_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, _vp, C.c_int, _vp]
     L.qb_inhom_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, C.c_double, _vp, C.c_int, _vp]
@@ -62,6 +65,8 @@ def lib(n_grid=N_GRID):
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
     L.qb_diagnostics.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp]
+    L.qb_fermi_dirac_equilibrium.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
+    L.qb_relative_entropy.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.CalculateRightwardFlux.restype = C.c_double
     L.CalculateLeftwardFlux.restype = C.c_double
     _libs[n_grid] = L
@@ -100,25 +105,45 @@ class Quad:
         self.h = lib().qb_quad_create(N, J, M, L, R)
         if not self.h:
             raise RuntimeError(f"qb_quad_create failed: {lib().qb_last_error().decode()}")
+        self._free = lib().qb_quad_free
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().qb_quad_free(self.h)
+        # the bound function is kept on the object: module globals may already
+        # be gone when this runs at interpreter exit
+        if getattr(self, "h", None) and getattr(self, "_free", None):
+            self._free(self.h)
             self.h = None
 
 
 class Workspace:
-    """Device scratch for one grid size (grows on demand)."""
+    """Device scratch for one grid size (grows on demand).
 
-    def __init__(self, N):
+    precision=64 evaluates the collision operator in FP64 (the upstream
+    arithmetic); precision=32 selects the FP32 form (FP64 state and update,
+    FP32 spectra, tables and FFTs).  conserve=True restores the trace
+    component's mass, momentum and energy after each velocity-space collision."""
+
+    def __init__(self, N, precision=64, conserve=False):
         self.N = N
         self.h = lib().qb_workspace_create(N)
         if not self.h:
             raise RuntimeError(f"qb_workspace_create failed: {lib().qb_last_error().decode()}")
+        self._free = lib().qb_workspace_free
+        if precision != 64:
+            self.set_precision(precision)
+        if conserve:
+            _check(lib().qb_workspace_set_conservation(self.h, 1), "qb_workspace_set_conservation")
+
+    def set_precision(self, bits):
+        _check(lib().qb_workspace_set_precision(self.h, bits), "qb_workspace_set_precision")
+
+    @property
+    def precision(self):
+        return lib().qb_workspace_precision(self.h)
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().qb_workspace_free(self.h)
+        if getattr(self, "h", None) and getattr(self, "_free", None):
+            self._free(self.h)
             self.h = None
 
 
@@ -177,6 +202,31 @@ def diagnostics(W, L):
     N, n = W.shape[-1], W.shape[0]
     out = torch.empty((n, len(DIAGNOSTICS)), dtype=torch.float64, device=W.device)
     _check(lib().qb_diagnostics(N, L, n, _ptr(W), _ptr(out), _stream()), "qb_diagnostics")
+    return out
+
+
+FD_PARAMS = ("beta", "mu_1", "mu_2", "u_x", "u_y", "n_x", "n_y", "n_z", "residual")
+
+
+def fermi_dirac_equilibrium(W, L):
+    """Fermi-Dirac states with the conserved moments of each cell of W
+    (float64 CUDA tensor (ncells, 4, N, N)); returns (WFD tensor, params numpy
+    array (ncells, 9) with columns FD_PARAMS)"""
+    torch = _torch()
+    N, n = W.shape[-1], W.shape[0]
+    WFD = torch.empty_like(W)
+    par = np.zeros((n, len(FD_PARAMS)))
+    _check(lib().qb_fermi_dirac_equilibrium(N, L, n, _ptr(W), _ptr(WFD), par.ctypes.data_as(_vp), _stream()),
+           "qb_fermi_dirac_equilibrium")
+    return WFD, par
+
+
+def relative_entropy(W, WFD, L):
+    """(ncells, 2) tensor: quantum relative entropy of W to WFD and the 1-norm distance"""
+    torch = _torch()
+    N, n = W.shape[-1], W.shape[0]
+    out = torch.empty((n, 2), dtype=torch.float64, device=W.device)
+    _check(lib().qb_relative_entropy(N, L, n, _ptr(W), _ptr(WFD), _ptr(out), _stream()), "qb_relative_entropy")
     return out
 
 

@@ -319,3 +319,123 @@ def diagnostics(W, L):
                   ux, uy, e, (t - r).min(), (t + r).max(), (S(t - r) + S(t + r)) * dv * dv]
     return out
 
+
+
+# ---------------------------------------------------------------------------
+# Fermi-Dirac equilibrium and quantum relative entropy (test oracle), restating
+# visualization/asymptoticFD.m, calculateFDparams.m, createFD.m and
+# relentropy.m, and the relative-entropy / distance loops of
+# visualization/visualizeHomBoltzmann.m:116-148, in numpy/scipy (float64).
+
+def _vgrid(N, L):
+    return np.where(np.arange(N) < N // 2, np.arange(N), np.arange(N) - N) * (2.0 * L / N)
+
+
+def fd_params(lam, en):
+    """calculateFDparams.m: (beta, mu) of the 2-D Fermi-Dirac distribution with
+    spin densities lam (2,) and normalised energy en, by nonlinear least
+    squares on (z_up, z_dn, beta) from (1, 1, 1), retried from beta = 0.5 when
+    the residual stays above 1e-4 (as the Matlab does); returns (beta, mu, residual)."""
+    from scipy.optimize import least_squares
+    from scipy.special import spence
+    lam = np.asarray(lam, dtype=np.float64)
+    en_t = en * lam.sum()
+
+    def li2(x):                       # Li_2(x) = spence(1 - x)
+        return spence(1.0 - x)
+
+    def F(x):
+        zu, zd, b = x
+        rho = lambda z: 2 * np.pi / b * np.log1p(z)
+        ene = lambda z: -2 * np.pi / b ** 2 * li2(-z)
+        return np.array([rho(zu) - lam[0], rho(zd) - lam[1], ene(zu) + ene(zd) - en_t])
+
+    def Jac(x):
+        zu, zd, b = x
+        rho = lambda z: 2 * np.pi / b * np.log1p(z)
+        ene = lambda z: -2 * np.pi / b ** 2 * li2(-z)
+        dr = lambda z: (2 * np.pi / (b * (1 + z)), -rho(z) / b)
+        de = lambda z: (rho(z) / (b * z), -2 * ene(z) / b)
+        return np.array([[dr(zu)[0], 0, dr(zu)[1]], [0, dr(zd)[0], dr(zd)[1]], [de(zu)[0], de(zd)[0], de(zu)[1] + de(zd)[1]]])
+
+    best = None
+    for b0 in (1.0, 0.5):
+        r = least_squares(F, [1.0, 1.0, b0], jac=Jac, bounds=([1e-300, 1e-300, 1e-300], [np.inf, np.inf, np.inf]),
+                          ftol=1e-15, xtol=1e-15, gtol=1e-15, max_nfev=2000)
+        md = float(np.linalg.norm(F(r.x)))
+        if best is None or md < best[2]:
+            best = (r.x, None, md)
+        if md <= 1e-4:
+            break
+    x, _, md = best
+    beta = x[2]
+    return beta, np.log(x[:2]) / beta, md
+
+
+def asymptotic_fd(W, L):
+    """asymptoticFD.m per cell: W (ncells, 4, N, N) -> (WFD of the same shape,
+    params (ncells, 9) = beta, mu_1, mu_2, u_x, u_y, n_x, n_y, n_z, residual)
+    with n the unit spin direction of the larger density eigenvalue."""
+    W = np.asarray(W, dtype=np.float64)
+    N = W.shape[-1]
+    d = diagnostics(W, L)
+    v = _vgrid(N, L)
+    vx, vy = np.meshgrid(v, v, indexing="ij")        # [l, k]: l is v_x
+    out = np.zeros_like(W)
+    par = np.zeros((W.shape[0], 9))
+    for i in range(W.shape[0]):
+        w = d[i, :4]
+        r = np.sqrt(w[1] ** 2 + w[2] ** 2 + w[3] ** 2)
+        lam = np.array([w[0] - r, w[0] + r])         # eig of pauliToMatrix(w), ascending
+        n = w[1:] / r if r > 0 else np.array([0.0, 0.0, -1.0])
+        beta, mu, md = fd_params(lam, d[i, 6])
+        ux, uy = d[i, 4], d[i, 5]
+        e = 0.5 * ((vx - ux) ** 2 + (vy - uy) ** 2)
+        f1 = 1.0 / (np.exp(beta * (e - mu[0])) + 1.0)
+        f2 = 1.0 / (np.exp(beta * (e - mu[1])) + 1.0)
+        out[i, 0] = 0.5 * (f1 + f2)
+        for c in range(3):
+            out[i, c + 1] = 0.5 * (f2 - f1) * n[c]
+        par[i] = [beta, mu[0], mu[1], ux, uy, n[0], n[1], n[2], md]
+    return out, par
+
+
+def relative_entropy(W, WFD, L):
+    """per cell (KL, distFD): the quantum relative entropy (relentropy.m) of
+    W(v) to WFD(v) summed over points with WFD_0(v) > 1e-6, times dv^2, and
+    sum_j ||W_j - WFD_j||_1 dv^2 with the Matlab matrix 1-norm (largest column
+    sum; a column is a fixed v_x)."""
+    W = np.asarray(W, dtype=np.float64)
+    WFD = np.asarray(WFD, dtype=np.float64)
+    N = W.shape[-1]
+    dv2 = (2.0 * L / N) ** 2
+    eps = np.finfo(np.float64).eps
+    sx = np.array([[0, 1], [1, 0]], complex)
+    sy = np.array([[0, -1j], [1j, 0]], complex)
+    sz = np.array([[1, 0], [0, -1]], complex)
+    out = np.zeros((W.shape[0], 2))
+    for i in range(W.shape[0]):
+        kl = 0.0
+        for l in range(N):
+            for k in range(N):
+                if not WFD[i, 0, l, k] > 1e-6:
+                    continue
+                a = W[i, :, l, k]
+                b = WFD[i, :, l, k]
+                rho = a[0] * np.eye(2) + a[1] * sx + a[2] * sy + a[3] * sz
+                tau = b[0] * np.eye(2) + b[1] * sx + b[2] * sy + b[3] * sz
+                mu, U = np.linalg.eigh(rho)
+                nu, V = np.linalg.eigh(tau)
+                mu = np.where(mu <= 0, eps, mu)
+                mu = np.where(mu >= 1, 1 - eps, mu)
+                nu = np.where(nu <= 0, eps, nu)
+                nu = np.where(nu >= 1, 1 - eps, nu)
+                Wm = U.conj().T @ V
+                log_tau = Wm @ np.diag(np.log(nu)) @ Wm.conj().T
+                log_1tau = Wm @ np.diag(np.log(1 - nu)) @ Wm.conj().T
+                r = np.diag(mu)
+                val = np.trace(r @ (np.diag(np.log(mu)) - log_tau)) + np.trace((np.eye(2) - r) @ (np.diag(np.log(1 - mu)) - log_1tau))
+                kl += val.real * dv2
+        dist = sum(np.abs(W[i, j] - WFD[i, j]).sum(axis=1).max() * dv2 for j in range(4))
+        out[i] = [kl, dist]
+    return out

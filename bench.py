@@ -162,6 +162,21 @@ def i3_flops_per_term(N):
     return 4 * 0.75 * F + 32 * F + 16 * 19 * P * P + 4 * 6 * N * N
 
 
+def captured_traffic(kernel, wl):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload from
+    the committed ncu capture (profiles/dram_traffic.json, written from
+    dram__bytes_read.sum + dram__bytes_write.sum of one launch), or None"""
+    path = os.path.join(REPO, "profiles", "dram_traffic.json")
+    try:
+        rows = json.load(open(path))
+    except (OSError, ValueError):
+        return None
+    for r in rows:
+        if r.get("kernel") == kernel and all(r.get(k) == wl[k] for k in ("N", "J", "M", "cells")):
+            return r["bytes_per_launch"]
+    return None
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -250,7 +265,8 @@ def run_ours(args):
                 "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak > 0 else None,
                 "peak_source": "measured live: DFMA loop on every SM (qb_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
                 "flops_per_launch": flops_launch, "launch_ms": round(per_launch_ms, 4), "launches": kn.value,
-                "share_of_step": round(kms.value / max(1e-9, tot_ms.value), 4), "traffic": None}
+                "share_of_step": round(kms.value / max(1e-9, tot_ms.value), 4),
+                "traffic": captured_traffic("k_i3", wl)}
     state_bytes = cells * 4 * N * N * 8
     hbm = {"bound": "hbm", "note": "whole step: transport reads+writes the state twice, collision reads W^ and writes C (FP64)",
            "bytes_per_step": 4 * state_bytes + 2 * cells * 3 * 4 * N * N * 16,
@@ -258,6 +274,9 @@ def run_ours(args):
 
     # end to end through the public API with host buffers
     e2e = run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall)
+    prec = None
+    if world == 1 and not args.no_precision_form:
+        prec = run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value)
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
@@ -265,6 +284,8 @@ def run_ours(args):
             "config": config_json(wl, world, "flushed: 256 MB written before every timed step"),
             "sim_steps_per_s": round(steps_per_s, 4), "roofline": roofline, "hbm_view": hbm, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary()}
+    if prec is not None:
+        line["precision_form"] = prec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind = ref_kind()
         procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
@@ -278,6 +299,54 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
+    """The FP32 form of the collision operator on the same workload and timing
+    protocol, with its error against the FP64 path: Cc and Cd of the initial
+    state (relative L2 and L1 over all cells) and the state after the timed
+    number of Strang steps (relative L1)."""
+    import torch
+    N, cells = wl["N"], wl["cells"]
+    ws32, ws64 = qbgpu.Workspace(N, precision=32), qbgpu.Workspace(N)
+    W0 = torch.from_numpy(Wall[:cells].copy()).cuda()
+    bufs = [W0.clone(), torch.empty_like(W0)]
+
+    def step(Win, Wout):
+        qbgpu.inhom_step(ws32, q, Win, wl["h"], wl["dt"], B, out=Wout)
+    for i in range(args.warmup):
+        step(bufs[i % 2], bufs[(i + 1) % 2])
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    cur = args.warmup % 2
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record()
+        step(bufs[cur], bufs[1 - cur])
+        evs[k][1].record()
+        cur = 1 - cur
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    value32 = cells * 2 * args.steps / (ms * 1e-3)
+
+    def rel(a, b, o):
+        a, b = a.cpu().numpy().ravel(), b.cpu().numpy().ravel()
+        return float(np.linalg.norm(a - b, o) / np.linalg.norm(b, o))
+    Wf = torch.empty((cells, 4, N, N), dtype=torch.complex128, device="cuda")
+    qbgpu._check(qbgpu.lib().qb_to_fourier(N, 4 * cells, qbgpu._ptr(W0), qbgpu._ptr(Wf), qbgpu._stream()), "qb_to_fourier")
+    cc64, cd64 = qbgpu.collision_operators(ws64, q, Wf)
+    cc32, cd32 = qbgpu.collision_operators(ws32, q, Wf)
+    a, b = W0.clone(), W0.clone()
+    for _ in range(args.steps):
+        a = qbgpu.inhom_step(ws64, q, a, wl["h"], wl["dt"], B)
+        b = qbgpu.inhom_step(ws32, q, b, wl["h"], wl["dt"], B)
+    torch.cuda.synchronize()
+    return {"dtype": "f32 (FFTs, spectra, tables); f64 state, assembly and update", "value": round(value32, 3), "unit": UNIT,
+            "ms_per_step": round(ms / args.steps, 4), "sim_steps_per_s": round(args.steps / (ms * 1e-3), 4),
+            "speedup_vs_fp64": round(value32 / value64, 4),
+            "rel_err_vs_fp64": {"Cc_l2": rel(cc32, cc64, 2), "Cd_l2": rel(cd32, cd64, 2), "Cc_l1": rel(cc32, cc64, 1),
+                                "Cd_l1": rel(cd32, cd64, 1), f"W_l1_after_{args.steps}_steps": rel(b, a, 1)},
+            "bound": 1e-5}
 
 
 def run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall):
@@ -385,6 +454,7 @@ def main():
     ap.add_argument("--J", type=int, default=16)
     ap.add_argument("--M", type=int, default=16)
     ap.add_argument("--cpu-procs", type=int, default=min(32, os.cpu_count() or 1))
+    ap.add_argument("--no-precision-form", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

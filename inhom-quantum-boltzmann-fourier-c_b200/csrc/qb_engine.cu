@@ -172,14 +172,16 @@ template <int P, class C> int active_i3_clusters() {
 	return cached;
 }
 
-// number of chunks minimising (waves x terms per chunk) for `units` independent
-// work units that each split their `nterms` terms into chunks
-int best_chunks(long units, int nterms, int slots, int max_chunks) {
+// number of chunks minimising (waves x terms per chunk) + penalty x chunks for
+// `units` independent work units that each split their `nterms` terms into
+// chunks; `penalty` is the cost of one more partial grid (written by the term
+// kernel, read back by the reduction) in units of one term's time
+int best_chunks(long units, int nterms, int slots, int max_chunks, double penalty = 0.02) {
 	int best = 1;
 	double best_cost = 1e300;
 	for (int c = 1; c <= std::min(nterms, max_chunks); c++) {
 		const long waves = (units * c + slots - 1) / slots;
-		const double cost = (double)waves * ((nterms + c - 1) / c) + 0.02 * c;   // small cost per partial grid
+		const double cost = (double)waves * ((nterms + c - 1) / c) + penalty * c;
 		if (cost < best_cost - 1e-9) { best_cost = cost; best = c; }
 	}
 	return best;
@@ -453,7 +455,9 @@ Chunks pick_chunks(int N, int ncells, const QuadSet &q, int prec) {
 		case 16: act = f32 ? active_i3_clusters<32, float2>() : active_i3_clusters<32, double2>(); break;
 		default: act = f32 ? active_i3_clusters<64, float2>() : active_i3_clusters<64, double2>(); break;
 		}
-		c.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), act, 256);
+		// an I3 partial is 4 padded grids per cluster (256 KB at N = 32) written
+		// and read back at HBM speed; one term takes a cluster ~36 us there: 0.15
+		c.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), act, 256, 0.15);
 	}
 	return c;
 }

@@ -1,10 +1,11 @@
 """Build libqbgpu for sm_100a (B200) in-tree.
 
-    python inhom-quantum-boltzmann-fourier-c_b200/build.py [--n-grid 32] [--jobs 8]
+    python inhom-quantum-boltzmann-fourier-c_b200/build.py [--n-grid 32 --n-grid 64] [--jobs 8]
 
 Outputs (git-ignored, shipped with the tree):
   lib/libqbgpu.so          upstream C API for N_GRID = 32 + batched extension API
-  lib/libqbgpu_nXX.so      the same built for other N_GRID values when requested
+  lib/libqbgpu_n64.so      the same with the upstream C API for N_GRID = 64
+  lib/libqbgpu_nXX.so      other N_GRID values when requested (8, 16, 32, 64)
 
 Every translation unit is compiled by nvcc with
   -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo
@@ -80,5 +81,5 @@ if __name__ == "__main__":
     ap.add_argument("--jobs", type=int, default=8)
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
-    for t in build(tuple(a.n_grid or [32]), a.jobs, a.verbose):
+    for t in build(tuple(a.n_grid or [32, 64]), a.jobs, a.verbose):
         print(t)

@@ -1,6 +1,7 @@
 // qb_engine.cu — launch wrappers and step orchestration of the GPU engine.
 #include "qb_engine.h"
 #include "qb_kernels.cuh"
+#include "qb_split128.cuh"
 #include "qb_transport.cuh"
 
 #include <algorithm>
@@ -35,7 +36,7 @@ std::string last_error() {
 	return g_last_error;
 }
 
-bool supported_n(int N) { return N == 8 || N == 16 || N == 32; }
+bool supported_n(int N) { return N == 8 || N == 16 || N == 32 || N == 64; }
 
 // ---------------------------------------------------------------------------
 // launch accounting
@@ -403,11 +404,198 @@ template <int P, class C> struct Rhs {
 	}
 };
 
+// ---------------------------------------------------------------------------
+// N = 64: padded grids of 128 x 128 split over CTA pairs (qb_split128.cuh)
+
+// launch with thread-block clusters of `cdim` CTAs (cdim = 1: plain launch)
+template <class... KA, class... A>
+void launch128(void (*kern)(KA...), const char *name, long nblocks, int cdim, size_t smem, cudaStream_t s, A... args) {
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)nblocks);
+	cfg.blockDim = dim3(G128::NT);
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = s;
+	cudaLaunchAttribute attr;
+	attr.id = cudaLaunchAttributeClusterDimension;
+	attr.val.clusterDim.x = cdim; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+	cfg.attrs = &attr;
+	cfg.numAttrs = cdim > 1 ? 1 : 0;
+	ProfScope ps(name, s);
+	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
+template <class K> void set_smem_once(K kern, size_t bytes, bool &done) {
+	if (!done) { set_smem(kern, bytes); done = true; }
+}
+
+// active 8-CTA clusters of the 128 I3 kernel (occupancy query, cached per C)
+template <class C> int active_i3_clusters128() {
+	static int cached = -1;
+	if (cached < 0) {
+		auto kern = k_i3_128<4, C>;
+		set_smem(kern, smem128<C>());
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(8);
+		cfg.blockDim = dim3(G128::NT);
+		cfg.dynamicSmemBytes = smem128<C>();
+		cudaLaunchAttribute attr;
+		attr.id = cudaLaunchAttributeClusterDimension;
+		attr.val.clusterDim.x = 8; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+		cfg.attrs = &attr;
+		cfg.numAttrs = 1;
+		int n = 0;
+		if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
+			cudaGetLastError();
+			n = std::max(1, num_sms() / 8);
+		}
+		cached = n;
+	}
+	return cached;
+}
+
+template <class C> void launch_pad_fft128(int ngrids, const double2 *src, C *out, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_pad_fft128<C>, smem128<C>(), init);
+	launch128(k_pad_fft128<C>, "pad_fft", 2L * ngrids, 1, smem128<C>(), s, src, out);
+}
+template <class C> void launch_i1_128(const I1ParamsT<C> &p, long units, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_i1_terms128<C>, smem128<C>(), init);
+	launch128(k_i1_terms128<C>, "i1_terms", 2 * units, 2, smem128<C>(), s, p);
+}
+template <class C> void launch_fft_full128(const FullParamsT<C> &p, long ngrids, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_fft_full128<C>, smem128<C>(), init);
+	launch128(k_fft_full128<C>, "fft_full", 2 * ngrids, 1, smem128<C>(), s, p);
+}
+template <class C> void launch_i2_128(const I2ParamsT<C> &p, long units, C *tmp, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_i2_terms128<C>, smem128<C>(), init);
+	launch128(k_i2_terms128<C>, "i2_terms", 2 * units, 1, smem128<C>(), s, p, tmp);
+}
+template <int CS, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_i3_128<CS, C>, smem128<C>(), init);
+	launch128(k_i3_128<CS, C>, "i3_cluster", nclusters * 2 * CS, 2 * CS, smem128<C>(), s, p, pscr);
+}
+template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_assemble128<C>, smem128<C>(), init);
+	launch128(k_assemble128<C>, "assemble", 2 * 4 * ncells, 2, smem128<C>(), s, p);
+}
+
+template <class C> struct Rhs<128, C> {
+	static constexpr int P = 128, N = 64;
+	static constexpr long NN = (long)N * N, PP = (long)P * P;
+	using T = Tab<C>;
+
+	static void spectra(Workspace &ws, int ncells, const double2 *W, cudaStream_t s) {
+		ws.What.ensure(sizeof(C) * 4 * ncells * PP);
+		launch_pad_fft128(4 * ncells, W, ws.What.as<C>(), s);
+	}
+
+	static void i1_sums(Workspace &ws, const DevI1 &t, int ncells, const double2 *W, bool cc, DevBuf &part, DevBuf &fs, int nchunk, cudaStream_t s) {
+		const int ntask = cc ? 3 : 4;
+		part.ensure(sizeof(C) * ncells * ntask * nchunk * PP);
+		I1ParamsT<C> p{};
+		p.ntask = ntask; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.g = W; p.g_cell = 4 * NN;
+		for (int k = 0; k < 4; k++) p.g_comp[k] = cc ? std::min(k + 1, 3) : k;
+		p.What = ws.What.as<C>(); p.w_cell = 4 * PP; p.f_comp = 0;
+		p.fa = cc ? -4.0 : 2.0; p.fb = cc ? 2.0 : -1.0;
+		p.psi2 = T::i1_psi2(t); p.phi = T::i1_phi(t);
+		p.out = part.as<C>();
+		launch_i1_128(p, (long)ncells * ntask * nchunk, s);
+		fs.ensure(sizeof(C) * ncells * ntask * PP);
+		FullParamsT<C> f{};
+		f.in = part.as<C>(); f.grid_stride = nchunk * PP; f.part_stride = PP; f.nparts = nchunk;
+		f.out = fs.as<C>();
+		launch_fft_full128(f, (long)ncells * ntask, s);
+	}
+
+	static void i2_sums(Workspace &ws, const DevI2 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
+		const long units = (long)ncells * 4 * nchunk;
+		ws.i2p.ensure(sizeof(C) * units * PP);
+		ws.scr128b.ensure(sizeof(C) * units * PP);
+		I2ParamsT<C> p{};
+		p.ntask = 4; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = W; p.cell_stride = 4 * NN;
+		for (int k = 0; k < 4; k++) { p.f_comp[k] = k; p.g_comp[k] = k; }
+		p.psi1 = T::i2_psi1(t); p.psi2 = T::i2_psi2(t);
+		p.out = ws.i2p.as<C>();
+		launch_i2_128(p, units, ws.scr128b.as<C>(), s);
+	}
+
+	static void i3_sums(Workspace &ws, const DevI3 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
+		const long ncl = (long)ncells * nchunk;
+		ws.i3p.ensure(sizeof(C) * ncl * 4 * PP);
+		ws.scr128a.ensure(sizeof(C) * ncl * 4 * PP);
+		I3ParamsT<C> p{};
+		p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = W; p.src_cell = 4 * NN;
+		for (int r = 0; r < 4; r++) p.src_comp[r] = r;
+		p.Ghat = ws.What.as<C>(); p.g_cell = 4 * PP;
+		const double eta[4] = { 1, -1, -1, -1 };
+		for (int r = 0; r < 4; r++) {
+			p.ncombo[r] = 4;
+			for (int i = 0; i < 4; i++) { p.ca[r][i] = i; p.cgi[r][i] = i; p.ccoef[r][i] = eta[i]; }
+		}
+		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
+		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
+		p.out = ws.i3p.as<C>();
+		launch_i3_128<4>(p, ncl, ws.scr128a.as<C>(), s);
+	}
+
+	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
+		T::prepare(q, s);
+		const int pairs = std::max(1, num_sms() / 2);
+		if (q.i1) ch.i1 = best_chunks((long)ncells * 7, std::max(1, q.i1->nterms), pairs, 64, 0.15);
+		if (q.i2) ch.i2 = best_chunks((long)ncells * 4, std::max(1, q.i2->nterms), pairs, 64, 0.15);
+		if (q.i3) ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), active_i3_clusters128<C>(), 256, 0.15);
+		spectra(ws, ncells, W, s);
+		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
+		if (parts & RHS_CD) {
+			i1_sums(ws, *q.i4, ncells, W, false, ws.i1i4, ws.fs4, ch.i1, s);
+			i2_sums(ws, *q.i2, ncells, W, ch.i2, s);
+			i3_sums(ws, *q.i3, ncells, W, ch.i3, s);
+		}
+	}
+
+	static AsmParamsT<C> asm_params(Workspace &ws, int parts, const Chunks &ch) {
+		AsmParamsT<C> a{};
+		a.What = ws.What.as<C>();
+		a.FS = (parts & RHS_CC) ? ws.fs.as<C>() : nullptr;
+		a.FS4 = (parts & RHS_CD) ? ws.fs4.as<C>() : nullptr;
+		a.Qp = (parts & RHS_CD) ? ws.i2p.as<C>() : nullptr; a.nq = ch.i2;
+		a.Xp = (parts & RHS_CD) ? ws.i3p.as<C>() : nullptr; a.nx = ch.i3;
+		a.s2 = 1.0 / (double)PP;
+		a.s1 = a.s2 * a.s2;
+		return a;
+	}
+
+	static void operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
+		Chunks ch;
+		prepare(ws, q, ncells, W, parts, ch, s);
+		AsmParamsT<C> a = asm_params(ws, parts, ch);
+		a.mode = 0; a.out_cc = cc; a.out_cd = cd;
+		launch_assemble128(a, ncells, s);
+	}
+
+	static void update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
+		Chunks ch;
+		prepare(ws, q, ncells, wcur, RHS_ALL, ch, s);
+		AsmParamsT<C> a = asm_params(ws, RHS_ALL, ch);
+		a.mode = 1; a.base = base; a.wcur = wcur; a.B = B; a.dtc = dtc; a.out = out;
+		launch_assemble128(a, ncells, s);
+	}
+};
+
 template <template <int> class F, class... A> void by_n(int N, A &&...args) {
 	switch (N) {
 	case 8: F<16>::run(args...); break;
 	case 16: F<32>::run(args...); break;
 	case 32: F<64>::run(args...); break;
+	case 64: F<128>::run(args...); break;
 	default: QB_FAIL("grid size N=" + std::to_string(N) + " has no compiled kernels");
 	}
 }
@@ -622,6 +810,97 @@ template <int P> struct I3S {
 		extract_ifft<P>(ws.fs.as<double2>(), s2 * s2, out, s);
 	}
 };
+
+// N = 64 single integrals on the split kernels (FP64)
+void extract_ifft128(const double2 *Z, double scale, double2 *out, cudaStream_t s) {
+	static bool init = false;
+	set_smem_once(k_extract_ifft128, smem128<double2>(), init);
+	launch128(k_extract_ifft128, "assemble", 2, 2, smem128<double2>(), s, Z, scale, out);
+}
+
+template <> struct I1S<128> {
+	static void run(Workspace &ws, const DevI1 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+		constexpr long NN = 64 * 64, PP = 128 * 128;
+		ws.aux.ensure(sizeof(double2) * 2 * NN);
+		double2 *fh = ws.aux.as<double2>();
+		QB_CUDA(cudaMemcpyAsync(fh, f, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(fh + NN, h, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		ws.What.ensure(sizeof(double2) * 2 * PP);
+		launch_pad_fft128(2, fh, ws.What.as<double2>(), s);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), std::max(1, num_sms() / 2), 128);
+		ws.i1cc.ensure(sizeof(double2) * nchunk * PP);
+		I1Params p{};
+		p.ntask = 1; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.g = g; p.g_cell = 0; p.g_comp[0] = 0;
+		p.What = ws.What.as<double2>(); p.w_cell = 0; p.f_comp = 0; p.fa = 1.0; p.fb = 0.0;
+		p.psi2 = t.psi2.as<double>(); p.phi = t.phi.as<double>();
+		p.out = ws.i1cc.as<double2>();
+		launch_i1_128(p, nchunk, s);
+		ws.fs.ensure(sizeof(double2) * 2 * PP);
+		FullParams fp{};
+		fp.in = ws.i1cc.as<double2>(); fp.grid_stride = 0; fp.part_stride = PP; fp.nparts = nchunk;
+		fp.out = ws.fs.as<double2>();
+		launch_fft_full128(fp, 1, s);
+		mul_sum(PP, ws.What.as<double2>() + PP, ws.fs.as<double2>(), 1, 0, ws.fs.as<double2>() + PP, s);
+		const double s2 = 1.0 / (double)PP;
+		extract_ifft128(ws.fs.as<double2>() + PP, s2 * s2, out, s);
+	}
+};
+
+template <> struct I2S<128> {
+	static void run(Workspace &ws, const DevI2 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+		constexpr long NN = 64 * 64, PP = 128 * 128;
+		ws.aux.ensure(sizeof(double2) * 3 * NN);
+		double2 *fgh = ws.aux.as<double2>();
+		QB_CUDA(cudaMemcpyAsync(fgh, f, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(fgh + NN, g, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(fgh + 2 * NN, h, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		ws.What.ensure(sizeof(double2) * PP);
+		launch_pad_fft128(1, fgh + 2 * NN, ws.What.as<double2>(), s);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), std::max(1, num_sms() / 2), 128);
+		ws.i2p.ensure(sizeof(double2) * nchunk * PP);
+		ws.scr128b.ensure(sizeof(double2) * nchunk * PP);
+		I2Params p{};
+		p.ntask = 1; p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = fgh; p.cell_stride = 0; p.f_comp[0] = 0; p.g_comp[0] = 1;
+		p.psi1 = t.psi1.as<double>(); p.psi2 = t.psi2.as<double>();
+		p.out = ws.i2p.as<double2>();
+		launch_i2_128(p, nchunk, ws.scr128b.as<double2>(), s);
+		ws.fs.ensure(sizeof(double2) * PP);
+		mul_sum(PP, ws.What.as<double2>(), ws.i2p.as<double2>(), nchunk, PP, ws.fs.as<double2>(), s);
+		extract_ifft128(ws.fs.as<double2>(), 1.0 / (double)PP, out, s);
+	}
+};
+
+template <> struct I3S<128> {
+	static void run(Workspace &ws, const DevI3 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
+		constexpr long NN = 64 * 64, PP = 128 * 128;
+		ws.aux.ensure(sizeof(double2) * 3 * NN);
+		double2 *src = ws.aux.as<double2>();
+		QB_CUDA(cudaMemcpyAsync(src, h, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(src + NN, f, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		QB_CUDA(cudaMemcpyAsync(src + 2 * NN, g, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
+		ws.What.ensure(sizeof(double2) * PP);
+		launch_pad_fft128(1, src + 2 * NN, ws.What.as<double2>(), s);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), std::max(1, num_sms() / 4), 256);
+		ws.i3p.ensure(sizeof(double2) * nchunk * 2 * PP);
+		ws.scr128a.ensure(sizeof(double2) * nchunk * 2 * PP);
+		I3Params p{};
+		p.nchunk = nchunk; p.nterms = t.nterms;
+		p.src = src; p.src_cell = 0; p.src_comp[0] = 0; p.src_comp[1] = 1;
+		p.Ghat = ws.What.as<double2>(); p.g_cell = 0;
+		p.ncombo[0] = 1; p.ca[0][0] = 1; p.cgi[0][0] = 0; p.ccoef[0][0] = 1.0;
+		p.ncombo[1] = 0;
+		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
+		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
+		p.out = ws.i3p.as<double2>();
+		launch_i3_128<2>(p, nchunk, ws.scr128a.as<double2>(), s);
+		ws.fs.ensure(sizeof(double2) * PP);
+		mul_sum(PP, nullptr, ws.i3p.as<double2>(), nchunk, 2 * PP, ws.fs.as<double2>(), s);
+		const double s2 = 1.0 / (double)PP;
+		extract_ifft128(ws.fs.as<double2>(), s2 * s2, out, s);
+	}
+};
 }  // namespace
 
 void integral_i1(Workspace &ws, const DevI1 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s) {
@@ -639,12 +918,16 @@ void integral_i3(Workspace &ws, const DevI3 &t, const double2 *f, const double2 
 namespace {
 template <int N> void launch_to_fourier(int ngrids, const double *Wv, double2 *Wf, cudaStream_t s) {
 	const size_t sm = sizeof(double2) * (N * (N + 1) + N);
+	static bool init = false;
+	set_smem_once(k_to_fourier<N>, sm, init);
 	ProfScope ps("to_fourier", s);
 	k_to_fourier<N><<<ngrids, Len<N>::T * N, sm, s>>>(Wv, Wf);
 	QB_CUDA(cudaGetLastError());
 }
 template <int N> void launch_from_fourier(int ngrids, const double2 *Wf, double *Wv, cudaStream_t s) {
 	const size_t sm = sizeof(double2) * (N * (N + 1) + N);
+	static bool init = false;
+	set_smem_once(k_from_fourier<N>, sm, init);
 	ProfScope ps("from_fourier", s);
 	k_from_fourier<N><<<ngrids, Len<N>::T * N, sm, s>>>(Wf, Wv);
 	QB_CUDA(cudaGetLastError());
@@ -657,6 +940,7 @@ void to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s
 	case 8: launch_to_fourier<8>(ngrids, Wv, Wf, s); break;
 	case 16: launch_to_fourier<16>(ngrids, Wv, Wf, s); break;
 	case 32: launch_to_fourier<32>(ngrids, Wv, Wf, s); break;
+	case 64: launch_to_fourier<64>(ngrids, Wv, Wf, s); break;
 	default: QB_FAIL("to_fourier: unsupported N");
 	}
 }
@@ -667,6 +951,7 @@ void from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t
 	case 8: launch_from_fourier<8>(ngrids, Wf, Wv, s); break;
 	case 16: launch_from_fourier<16>(ngrids, Wf, Wv, s); break;
 	case 32: launch_from_fourier<32>(ngrids, Wf, Wv, s); break;
+	case 64: launch_from_fourier<64>(ngrids, Wf, Wv, s); break;
 	default: QB_FAIL("from_fourier: unsupported N");
 	}
 }

@@ -85,6 +85,7 @@ struct Workspace {
 	DevBuf io_in, io_out, bext, vgrid;       // staging for host-pointer calls
 	DevBuf aux, aux2;
 	DevBuf inv;                              // per-cell collision invariants (conservation on)
+	DevBuf scr128a, scr128b;                 // N = 64: per-cluster spectra of the I3 terms, first I2 spectra
 	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
 	// replay of a repeated Strang step (batched API): the launch sequence of
 	// one (pointers, parameters) key is captured once and relaunched

@@ -4,8 +4,9 @@ Two surfaces are checked:
   * the upstream C API (host buffers, N_GRID = 32) -- the drop-in boundary --
     on the upstream golden vectors with the upstream test drivers' parameters;
   * the batched device API (include/qbgpu.h) against the oracle on seeded
-    Gaussian-mixture states at N = 8, 16, 32, including magnetic fields and
-    all three boundary conditions.
+    Gaussian-mixture states at N = 8, 16, 32, 64, including magnetic fields and
+    all three boundary conditions.  N = 64 runs the split-grid kernels (one
+    padded 128 x 128 grid per CTA pair of a cluster).
 Tolerance: the plain FP64 path must match the upstream C code within 1e-12
 relative (L1, as test/Cc_test.c:177-189 measures); against the Matlab-made
 I-integral goldens the bound is the upstream C code's own 5e-12 average
@@ -140,6 +141,24 @@ def test_inhom_step_golden(up):
     assert rel_l1(out, golden_r("Wx_next_ref.dat", (8, 4, 32, 32))) < TOL
 
 
+def test_upstream_api_n_grid_64():
+    """the upstream entry points built with N_GRID = 64 (lib/libqbgpu_n64.so),
+    called as a driver compiled for that grid calls them, against the oracle"""
+    up64 = qbgpu.Upstream(64)
+    J, M, L, R = 4, 3, 6.0, 3.75
+    quads = _quads(up64, J, M, L, R)
+    o = orc.Oracle(64, J, M, L, R)
+    Wv = qbgpu.gaussian_mixture_state(64, L, seed=41, ncells=3)
+    WF = up64.to_fourier_r2c(Wv[0])
+    assert rel_l1(WF, orc.to_fourier(Wv[0])) < 1e-14
+    assert rel_l1(up64.cc(WF, quads[0]), o.cc(WF)) < TOL
+    assert rel_l1(up64.cd(WF, quads[1], quads[2], quads[3]), o.cd(WF)) < TOL
+    h, dt = 1 / 3, 0.4 / 3 / L
+    out = up64.inhom_step(Wv, quads, h, dt, L=L)
+    assert rel_l1(out, o.inhom_step(Wv, h, dt)) < TOL
+    _free(up64, quads)
+
+
 def test_simulation_inhom_periodic_frame_golden(up):
     """bin/params_periodic_example.txt: 10 cells, J = M = 32, h = 0.1, dt = 0.008"""
     quads = _quads(up, 32, 32)
@@ -196,7 +215,7 @@ def test_inhom_step_maxwell_upstream_api(up):
 
 # even J: with odd J the upstream I1 principal-value weight -1/cos(theta1_i - theta2_j)
 # (src/quadrature.c:224) hits cos = 0 and the operator is singular
-CASES = [(8, 4, 3), (16, 4, 3), (32, 2, 4)]
+CASES = [(8, 4, 3), (16, 4, 3), (32, 2, 4), (64, 4, 3)]
 
 
 def dev(a, dtype=None):

@@ -56,7 +56,7 @@ def test_fp32_operators_against_oracle():
     assert rel_l2(cd, ref_cd) <= C_TOL
 
 
-@pytest.mark.parametrize("N,J,M", [(32, 16, 16), (32, 8, 4), (8, 4, 3)])
+@pytest.mark.parametrize("N,J,M", [(32, 16, 16), (32, 8, 4), (8, 4, 3), (64, 4, 3)])
 def test_fp32_operators_against_fp64(N, J, M):
     q = qbgpu.Quad(N, J, M, L, R)
     ws64, ws32 = qbgpu.Workspace(N), qbgpu.Workspace(N, precision=32)

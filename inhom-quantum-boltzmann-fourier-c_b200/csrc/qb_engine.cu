@@ -428,25 +428,28 @@ template <class K> void set_smem_once(K kern, size_t bytes, bool &done) {
 	if (!done) { set_smem(kern, bytes); done = true; }
 }
 
-// active 8-CTA clusters of the 128 I3 kernel (occupancy query, cached per C)
+// I3 kernel of the collision operator at N = 64: 4 components on 2 CTA pairs
+constexpr int kI3Pairs128 = 2;
+
+// active clusters of the 128 I3 kernel (occupancy query, cached per C)
 template <class C> int active_i3_clusters128() {
 	static int cached = -1;
 	if (cached < 0) {
-		auto kern = k_i3_128<4, C>;
+		auto kern = k_i3_128<4, kI3Pairs128, C>;
 		set_smem(kern, smem128<C>());
 		cudaLaunchConfig_t cfg = {};
-		cfg.gridDim = dim3(8);
+		cfg.gridDim = dim3(2 * kI3Pairs128);
 		cfg.blockDim = dim3(G128::NT);
 		cfg.dynamicSmemBytes = smem128<C>();
 		cudaLaunchAttribute attr;
 		attr.id = cudaLaunchAttributeClusterDimension;
-		attr.val.clusterDim.x = 8; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+		attr.val.clusterDim.x = 2 * kI3Pairs128; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
 		cfg.attrs = &attr;
 		cfg.numAttrs = 1;
 		int n = 0;
 		if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
 			cudaGetLastError();
-			n = std::max(1, num_sms() / 8);
+			n = std::max(1, num_sms() / (2 * kI3Pairs128));
 		}
 		cached = n;
 	}
@@ -473,10 +476,10 @@ template <class C> void launch_i2_128(const I2ParamsT<C> &p, long units, C *tmp,
 	set_smem_once(k_i2_terms128<C>, smem128<C>(), init);
 	launch128(k_i2_terms128<C>, "i2_terms", 2 * units, 1, smem128<C>(), s, p, tmp);
 }
-template <int CS, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, cudaStream_t s) {
+template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, cudaStream_t s) {
 	static bool init = false;
-	set_smem_once(k_i3_128<CS, C>, smem128<C>(), init);
-	launch128(k_i3_128<CS, C>, "i3_cluster", nclusters * 2 * CS, 2 * CS, smem128<C>(), s, p, pscr);
+	set_smem_once(k_i3_128<CS, NPAIR, C>, smem128<C>(), init);
+	launch128(k_i3_128<CS, NPAIR, C>, "i3_cluster", nclusters * 2 * NPAIR, 2 * NPAIR, smem128<C>(), s, p, pscr);
 }
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
 	static bool init = false;
@@ -543,7 +546,7 @@ template <class C> struct Rhs<128, C> {
 		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
-		launch_i3_128<4>(p, ncl, ws.scr128a.as<C>(), s);
+		launch_i3_128<4, kI3Pairs128>(p, ncl, ws.scr128a.as<C>(), s);
 	}
 
 	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
@@ -882,7 +885,7 @@ template <> struct I3S<128> {
 		QB_CUDA(cudaMemcpyAsync(src + 2 * NN, g, sizeof(double2) * NN, cudaMemcpyDeviceToDevice, s));
 		ws.What.ensure(sizeof(double2) * PP);
 		launch_pad_fft128(1, src + 2 * NN, ws.What.as<double2>(), s);
-		const int nchunk = best_chunks(1, std::max(1, t.nterms), std::max(1, num_sms() / 4), 256);
+		const int nchunk = best_chunks(1, std::max(1, t.nterms), std::max(1, num_sms() / 2), 256);
 		ws.i3p.ensure(sizeof(double2) * nchunk * 2 * PP);
 		ws.scr128a.ensure(sizeof(double2) * nchunk * 2 * PP);
 		I3Params p{};
@@ -894,7 +897,7 @@ template <> struct I3S<128> {
 		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<double2>();
-		launch_i3_128<2>(p, nchunk, ws.scr128a.as<double2>(), s);
+		launch_i3_128<2, 1>(p, nchunk, ws.scr128a.as<double2>(), s);
 		ws.fs.ensure(sizeof(double2) * PP);
 		mul_sum(PP, nullptr, ws.i3p.as<double2>(), nchunk, 2 * PP, ws.fs.as<double2>(), s);
 		const double s2 = 1.0 / (double)PP;

@@ -393,38 +393,39 @@ __global__ void __launch_bounds__(512, 1) k_i2_terms128(const I2ParamsT<C> p, C 
 }
 
 // ---------------------------------------------------------------------------
-// K4 (128): I3-type sums on a cluster of 2 CS CTAs: component r = rank / 2 is
-// held by the pair (2r, 2r + 1).  Per term the pair of r writes
-// P_r = FFT2(Pad(psi1_t . src_r)) (B layout) to the cluster's scratch in
-// global memory (L2); after a cluster barrier every pair runs its combos
+// K4 (128): I3-type sums on a cluster of NPAIR CTA pairs; pair q holds the
+// CS / NPAIR components q * CS / NPAIR ... in turn.  Per term each pair writes
+// the P_r = FFT2(Pad(psi1_t . src_r)) of its components (B layout) to the
+// cluster's scratch in global memory (L2); after a cluster barrier every pair
+// runs the combos of its components
 //   X_r += coef P_a . FFT2(psi2_t . IFFT2(G_g . P_r))
 // with one pair exchange each (inverse butterfly, psi2, forward butterfly).
-// Pairs with fewer combos than the cluster maximum run the barriers only.
-template <int CS, class C>
+// Components with fewer combos than the largest count run the barriers only.
+template <int CS, int NPAIR, class C>
 __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr) {
 	using G = G128;
 	using R = typename CT<C>::R;
+	constexpr int CPP = CS / NPAIR;             // components per pair
+	static_assert(CS % NPAIR == 0, "components must divide over the pairs");
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *S = reinterpret_cast<C *>(smem_raw), *tw128 = S + G::GRID_H, *tw64 = tw128 + 128;
 	cg::cluster_group cl = cg::this_cluster();
 	const int rank = (int)cl.block_rank();
-	const int comp = rank >> 1, h = rank & 1;
+	const int pair = rank >> 1, h = rank & 1;
 	const C *peer = cl.map_shared_rank(S, rank ^ 1);
-	const long cid = blockIdx.x / (2 * CS);
+	const long cid = blockIdx.x / (2 * NPAIR);
 	const int chunk = (int)(cid % p.nchunk);
 	const long cell = cid / p.nchunk;
 	init_tw128(tw128, tw64);
-	const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[comp] * G::N * G::N;
 	C *Pall = pscr + cid * CS * G::PP;
-	C *Pown = Pall + comp * G::PP;
 	const C *Gcell = p.Ghat + cell * p.g_cell;
-	C *acc = p.out + ((cell * p.nchunk + chunk) * CS + comp) * G::PP;
 	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
 	int ncmax = 0;
 	for (int r = 0; r < CS; r++) ncmax = max(ncmax, p.ncombo[r]);
-	const int nc = p.ncombo[comp];
-	{   // zero this CTA's half of the accumulator at the final row-pass points
-		const int tau = threadIdx.x & 15;
+	const int tau = threadIdx.x & 15;
+#pragma unroll 1
+	for (int q = 0; q < CPP; q++) {           // zero this CTA's half of each accumulator at the final row-pass points
+		C *acc = p.out + ((cell * p.nchunk + chunk) * CS + pair * CPP + q) * G::PP;
 		for (int it = 0; it < 2; it++) {
 			const int row = it * 32 + (threadIdx.x >> 4);
 			for (int e = 0; e < 8; e++) acc[G::bidx(h, row, pos128(tau, e))] = czero<C>();
@@ -433,54 +434,67 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 	__syncthreads();
 #pragma unroll 1
 	for (int t = t0; t < t1; t++) {
-		col_pass<-1>(S, tw64, ColFromPad<C, MulCplx<C>>{src, MulCplx<C>{p.psi1 + (long)t * G::N * G::N}, h, tw128});
-		__syncthreads();
-		row_pass<-1>(S, tw128, tw64, RowFromS<C>{S}, RowToB<C>{Pown, h});
+#pragma unroll 1
+		for (int q = 0; q < CPP; q++) {
+			const int comp = pair * CPP + q;
+			const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[comp] * G::N * G::N;
+			col_pass<-1>(S, tw64, ColFromPad<C, MulCplx<C>>{src, MulCplx<C>{p.psi1 + (long)t * G::N * G::N}, h, tw128});
+			__syncthreads();
+			row_pass<-1>(S, tw128, tw64, RowFromS<C>{S}, RowToB<C>{Pall + comp * G::PP, h});
+			__syncthreads();
+		}
 		cl.sync();                               // every P_r of the term is in global memory
 		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * G::PP;
 		const R sc = (R)p.psi2_scale[t];
 #pragma unroll 1
-		for (int c = 0; c < ncmax; c++) {
-			const bool act = c < nc;
-			if (act) {
-				const C *Gg = Gcell + (long)p.cgi[comp][c] * G::PP;
-				// rows: inverse FFT of G_g . P_r
-				row_pass<+1>(S, tw128, tw64, [&](C (&x)[8], int row, int tau) {
+		for (int q = 0; q < CPP; q++) {
+			const int comp = pair * CPP + q;
+			const int nc = p.ncombo[comp];
+			const C *Pown = Pall + comp * G::PP;
+			C *acc = p.out + ((cell * p.nchunk + chunk) * CS + comp) * G::PP;
+#pragma unroll 1
+			for (int c = 0; c < ncmax; c++) {
+				const bool act = c < nc;
+				if (act) {
+					const C *Gg = Gcell + (long)p.cgi[comp][c] * G::PP;
+					// rows: inverse FFT of G_g . P_r
+					row_pass<+1>(S, tw128, tw64, [&](C (&x)[8], int row, int tl) {
 #pragma unroll
-					for (int r = 0; r < 8; r++) {
-						const long o = G::bidx(h, row, tau + 16 * r);
-						x[r] = cmul(Gg[o], Pown[o]);
-					}
-				}, RowToS<C>{S});
-				__syncthreads();
-				col_pass<+1>(S, tw64, ColFromS<C>{S});
-			}
-			// inverse butterfly -> psi2 -> forward butterfly, one exchange
-			pair_exchange<true>(S, peer, cl, [&](C own, C oth, int l, int k) {
-				if (!act) return own;
-				const C E = h ? oth : own, O = h ? own : oth;
-				const C w = tw128[l];
-				const C wo = cmul(conj_c(w), O);
-				const R f0 = sc * psi2[(long)k * G::P + l], f1 = sc * psi2[(long)k * G::P + l + 64];
-				const C z0 = cscale(cadd(E, wo), f0), z1 = cscale(csub(E, wo), f1);
-				return h ? cmul(csub(z0, z1), w) : cadd(z0, z1);
-			});
-			if (act) {
-				col_pass<-1>(S, tw64, ColFromS<C>{S});
-				__syncthreads();
-				const C *Pa = Pall + (long)p.ca[comp][c] * G::PP;
-				const R coef = (R)p.ccoef[comp][c];
-				row_pass<-1>(S, tw128, tw64, RowFromS<C>{S}, [&](C (&x)[8], int row, int tau) {
-#pragma unroll
-					for (int e = 0; e < 8; e++) {
-						const long o = G::bidx(h, row, pos128(tau, e));
-						const C v = cmul(Pa[o], x[e]);
-						C a = acc[o];
-						a.x += coef * v.x; a.y += coef * v.y;
-						acc[o] = a;
-					}
+						for (int r = 0; r < 8; r++) {
+							const long o = G::bidx(h, row, tl + 16 * r);
+							x[r] = cmul(Gg[o], Pown[o]);
+						}
+					}, RowToS<C>{S});
+					__syncthreads();
+					col_pass<+1>(S, tw64, ColFromS<C>{S});
+				}
+				// inverse butterfly -> psi2 -> forward butterfly, one exchange
+				pair_exchange<true>(S, peer, cl, [&](C own, C oth, int l, int k) {
+					if (!act) return own;
+					const C E = h ? oth : own, O = h ? own : oth;
+					const C w = tw128[l];
+					const C wo = cmul(conj_c(w), O);
+					const R f0 = sc * psi2[(long)k * G::P + l], f1 = sc * psi2[(long)k * G::P + l + 64];
+					const C z0 = cscale(cadd(E, wo), f0), z1 = cscale(csub(E, wo), f1);
+					return h ? cmul(csub(z0, z1), w) : cadd(z0, z1);
 				});
-				__syncthreads();
+				if (act) {
+					col_pass<-1>(S, tw64, ColFromS<C>{S});
+					__syncthreads();
+					const C *Pa = Pall + (long)p.ca[comp][c] * G::PP;
+					const R coef = (R)p.ccoef[comp][c];
+					row_pass<-1>(S, tw128, tw64, RowFromS<C>{S}, [&](C (&x)[8], int row, int tl) {
+#pragma unroll
+						for (int e = 0; e < 8; e++) {
+							const long o = G::bidx(h, row, pos128(tl, e));
+							const C v = cmul(Pa[o], x[e]);
+							C a = acc[o];
+							a.x += coef * v.x; a.y += coef * v.y;
+							acc[o] = a;
+						}
+					});
+					__syncthreads();
+				}
 			}
 		}
 		cl.sync();                               // every pair is done with this term's P grids

@@ -230,6 +230,57 @@ template <int P, int CS, class C> void launch_i3(const I3ParamsT<C> &p, long ncl
 	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p));
 }
 
+// k_i3p (P = 64): 2-CTA clusters, TMEM accumulators.  The allocation of
+// I3Tmem<C>::NCOLS columns never waits as long as no more CTAs share an SM
+// than its 512 columns hold; the shared-memory (FP64) or register (FP32)
+// footprint keeps it at one CTA per SM, checked here before the first launch.
+template <class C> size_t i3p_smem() { return sizeof(C) * ((size_t)3 * Geo<64>::GRID + 64); }
+
+template <class C> int active_i3p_clusters() {
+	static int cached = -1;
+	if (cached < 0) {
+		auto kern = k_i3p<64, C>;
+		set_smem(kern, i3p_smem<C>());
+		int per_sm = 0;
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Geo<64>::NT, i3p_smem<C>()));
+		if (per_sm * (int)I3Tmem<C>::NCOLS > 512)
+			QB_FAIL("k_i3p: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(2);
+		cfg.blockDim = dim3(Geo<64>::NT);
+		cfg.dynamicSmemBytes = i3p_smem<C>();
+		cudaLaunchAttribute attr;
+		attr.id = cudaLaunchAttributeClusterDimension;
+		attr.val.clusterDim.x = 2; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+		cfg.attrs = &attr;
+		cfg.numAttrs = 1;
+		int n = 0;
+		if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
+			cudaGetLastError();
+			n = std::max(1, num_sms() / 2);
+		}
+		cached = n;
+	}
+	return cached;
+}
+
+template <class C> void launch_i3p(const I3ParamsT<C> &p, long nclusters, cudaStream_t s) {
+	active_i3p_clusters<C>();                  // attribute + occupancy check
+	auto kern = k_i3p<64, C>;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)(nclusters * 2));
+	cfg.blockDim = dim3(Geo<64>::NT);
+	cfg.dynamicSmemBytes = i3p_smem<C>();
+	cfg.stream = s;
+	cudaLaunchAttribute attr;
+	attr.id = cudaLaunchAttributeClusterDimension;
+	attr.val.clusterDim.x = 2; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+	cfg.attrs = &attr;
+	cfg.numAttrs = 1;
+	ProfScope ps("i3_cluster", s);
+	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p));
+}
+
 template <int P, class C> void launch_fft_full(const FullParamsT<C> &p, long ngrids, cudaStream_t s) {
 	static bool init = false;
 	if (!init) { set_smem(k_fft_full<P, C>, smem_grids<P, C>(1)); init = true; }
@@ -360,7 +411,8 @@ template <int P, class C> struct Rhs {
 		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
-		launch_i3<P, 4>(p, (long)ncells * nchunk, s);
+		if constexpr (P == 64) launch_i3p<C>(p, (long)ncells * nchunk, s);
+		else launch_i3<P, 4>(p, (long)ncells * nchunk, s);
 	}
 
 	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
@@ -644,7 +696,7 @@ Chunks pick_chunks(int N, int ncells, const QuadSet &q, int prec) {
 		switch (N) {
 		case 8: act = f32 ? active_i3_clusters<16, float2>() : active_i3_clusters<16, double2>(); break;
 		case 16: act = f32 ? active_i3_clusters<32, float2>() : active_i3_clusters<32, double2>(); break;
-		default: act = f32 ? active_i3_clusters<64, float2>() : active_i3_clusters<64, double2>(); break;
+		default: act = f32 ? active_i3p_clusters<float2>() : active_i3p_clusters<double2>(); break;
 		}
 		// an I3 partial is 4 padded grids per cluster (256 KB at N = 32) written
 		// and read back at HBM speed; one term takes a cluster ~36 us there: 0.15

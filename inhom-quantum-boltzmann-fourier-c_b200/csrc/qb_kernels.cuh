@@ -360,6 +360,183 @@ __global__ void __launch_bounds__(Geo<P>::NT, Occ<C>::CTAS) k_i3(const I3ParamsT
 }
 
 // ---------------------------------------------------------------------------
+// Tensor memory (TMEM) as accumulator storage.  A CTA allocates `ncols`
+// columns of its SM's 128-lane TMEM; warp w reaches lanes 32 (w % 4) ..
+// 32 (w % 4) + 31 (thread = lane), and the four warps that share a lane
+// quarter split the columns (slot w / 4).  Loads and stores are warp-wide
+// (tcgen05.ld / st .32x32b) and asynchronous until tcgen05.wait.
+__device__ __forceinline__ void tmem_alloc(unsigned *slot_smem, unsigned ncols) {
+	const unsigned a = (unsigned)__cvta_generic_to_shared(slot_smem);
+	asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(a), "r"(ncols) : "memory");
+	asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+	asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// one complex value per thread at column `taddr` (+ 4 columns FP64, 2 FP32)
+__device__ __forceinline__ void tmem_ld(unsigned taddr, double2 &v) {
+	unsigned a, b, c, d;
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(a), "=r"(b), "=r"(c), "=r"(d) : "r"(taddr) : "memory");
+	v.x = __hiloint2double((int)b, (int)a);
+	v.y = __hiloint2double((int)d, (int)c);
+}
+__device__ __forceinline__ void tmem_st(unsigned taddr, double2 v) {
+	const unsigned a = (unsigned)__double2loint(v.x), b = (unsigned)__double2hiint(v.x);
+	const unsigned c = (unsigned)__double2loint(v.y), d = (unsigned)__double2hiint(v.y);
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+__device__ __forceinline__ void tmem_ld(unsigned taddr, float2 &v) {
+	unsigned a, b;
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(a), "=r"(b) : "r"(taddr) : "memory");
+	v.x = __uint_as_float(a);
+	v.y = __uint_as_float(b);
+}
+__device__ __forceinline__ void tmem_st(unsigned taddr, float2 v) {
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(__float_as_uint(v.x)), "r"(__float_as_uint(v.y)) : "memory");
+}
+
+// TMEM accumulators of k_i3p: 2 outputs x 8 values per thread
+template <class C> struct I3Tmem {
+	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
+	static constexpr unsigned PER_THREAD = 2 * 8 * WPC;       // columns of one thread's slice
+	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 4 warps share a lane quarter: 256 (FP64), 128 (FP32)
+	// column address of value e of output q of this thread
+	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int e) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + (w >> 2) * PER_THREAD + (unsigned)(q * 8 + e) * WPC;
+	}
+};
+
+// ---------------------------------------------------------------------------
+// K4p: the I3 sums of the collision operator on a cluster of 2 CTAs, CTA r
+// holding components 2r and 2r + 1: per term it computes both spectra
+// P_{t,c} = FFT2(Pad(psi1_t . W_c)) into its shared memory and, after a
+// cluster barrier, the 8 (pair, combo) chains of its two outputs
+//   X_j += eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j)),  j in {2r, 2r + 1}
+// with P_i of the partner's components read through distributed shared
+// memory.  The two 8-value accumulators of every thread live in TMEM, which
+// frees their registers and lets 2-CTA clusters use all 148 SMs (4-CTA
+// clusters of k_i3 fit 33 of 37 four-SM slots).  Output as k_i3 with CS = 4.
+template <int P, class C>
+__global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
+	using G = Geo<P>;
+	using Lp = Len<P>;
+	using R = typename CT<C>::R;
+	using TM = I3Tmem<C>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ unsigned tmem_slot;
+	C *Pq = reinterpret_cast<C *>(smem_raw);                 // P of components 2r, 2r + 1 (2 grids)
+	C *Ug = Pq + 2 * G::GRID, *tw = Pq + 3 * G::GRID;
+	cg::cluster_group cluster = cg::this_cluster();
+	const int rank = (int)cluster.block_rank();
+	const long cid = blockIdx.x / 2;
+	const int chunk = (int)(cid % p.nchunk);
+	const long cell = cid / p.nchunk;
+	const int warp = threadIdx.x >> 5;
+	if (warp == 0) tmem_alloc(&tmem_slot, TM::NCOLS);
+	init_twiddles<P>(tw);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const unsigned tbase = tmem_slot;
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+#pragma unroll
+	for (int q = 0; q < 2; q++)
+#pragma unroll
+		for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, e), czero<C>());
+	tmem_wait_st();
+	const C *Gcell = p.Ghat + cell * p.g_cell;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+	C *Ppeer = cluster.map_shared_rank(Pq, rank ^ 1);
+	for (int t = t0; t < t1; t++) {
+#pragma unroll 1
+		for (int q = 0; q < 2; q++) {
+			const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank + q] * G::N * G::N;
+			fft2_pad<P, -1>(Pq + q * G::GRID, tw, src, MulCplx<C>{p.psi1 + (long)t * G::N * G::N});
+		}
+		cluster.sync();
+		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
+		const R sc = (R)p.psi2_scale[t];
+#pragma unroll 1
+		for (int q = 0; q < 2; q++) {
+			const int j = 2 * rank + q;
+			const C *Pj = Pq + q * G::GRID;
+#pragma unroll 1
+			for (int c = 0; c < p.ncombo[j]; c++) {
+				const C *Gg = Gcell + (long)p.cgi[j][c] * P * P;
+				C x[8];
+				// rows: IFFT of G_g . P_j
+#pragma unroll
+				for (int r = 0; r < 8; r++) {
+					const int k = tau + G::T * r;
+					x[r] = cmul(Gg[line * P + k], Pj[line * G::LDP + k]);
+				}
+				fft1d<P, +1>(x, tau, Ug + line * G::LDP, 1, tw);
+#pragma unroll
+				for (int e = 0; e < 8; e++) Ug[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+				__syncthreads();
+				// columns: IFFT, multiply by psi2_t, FFT
+#pragma unroll
+				for (int r = 0; r < 8; r++) x[r] = Ug[(tau + G::T * r) * G::LDP + line];
+				fft1d<P, +1>(x, tau, Ug + line, G::LDP, tw);
+#pragma unroll
+				for (int e = 0; e < 8; e++) {
+					const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
+					x[e].x *= f;
+					x[e].y *= f;
+				}
+				out_to_in<P>(x, tau, Ug + line, G::LDP);
+				fft1d<P, -1>(x, tau, Ug + line, G::LDP, tw);
+#pragma unroll
+				for (int e = 0; e < 8; e++) Ug[Lp::out_pos(tau, e) * G::LDP + line] = x[e];
+				__syncthreads();
+				// rows: FFT, multiply by P_a (own or the partner's), accumulate in TMEM
+#pragma unroll
+				for (int r = 0; r < 8; r++) x[r] = Ug[line * G::LDP + tau + G::T * r];
+				fft1d<P, -1>(x, tau, Ug + line * G::LDP, 1, tw);
+				const int a = p.ca[j][c];
+				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
+				const R coef = (R)p.ccoef[j][c];
+				C acc[8];
+#pragma unroll
+				for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, e), acc[e]);
+				tmem_wait_ld();
+#pragma unroll
+				for (int e = 0; e < 8; e++) {
+					const C v = cmul(Pa[line * G::LDP + Lp::out_pos(tau, e)], x[e]);
+					acc[e].x += coef * v.x;
+					acc[e].y += coef * v.y;
+				}
+#pragma unroll
+				for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, e), acc[e]);
+				tmem_wait_st();
+				__syncthreads();
+			}
+		}
+		cluster.sync();
+	}
+#pragma unroll 1
+	for (int q = 0; q < 2; q++) {
+		C acc[8];
+#pragma unroll
+		for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, e), acc[e]);
+		tmem_wait_ld();
+		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * (long)P * P + line * P;
+#pragma unroll
+		for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
+}
+
+// ---------------------------------------------------------------------------
 // K5: out[b] = FFT2(sum_{k<nparts} in[b*grid_stride + k*part_stride]) (full grids)
 template <class C> struct FullParamsT {
 	const C *in; long grid_stride, part_stride; int nparts;

@@ -146,7 +146,7 @@ template <class K> void set_smem(K kernel, size_t bytes) {
 	QB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
-template <int P, class C = double2> constexpr size_t smem_grids(int ngrids) { return sizeof(C) * ((size_t)ngrids * Geo<P>::GRID + P); }
+template <int P, class C = double2> constexpr size_t smem_grids(int ngrids) { return sizeof(C) * ((size_t)ngrids * Geo<P, C>::GRID + P); }
 
 // active clusters of the I3 kernel (occupancy query, cached per P and C)
 template <int P, class C> int active_i3_clusters() {
@@ -234,7 +234,7 @@ template <int P, int CS, class C> void launch_i3(const I3ParamsT<C> &p, long ncl
 // I3Tmem<C>::NCOLS columns never waits as long as no more CTAs share an SM
 // than its 512 columns hold; the shared-memory (FP64) or register (FP32)
 // footprint keeps it at one CTA per SM, checked here before the first launch.
-template <class C> size_t i3p_smem() { return sizeof(C) * ((size_t)3 * Geo<64>::GRID + 64); }
+template <class C> size_t i3p_smem() { return sizeof(C) * ((size_t)3 * Geo<64, C>::GRID + 64); }
 
 template <class C> int active_i3p_clusters() {
 	static int cached = -1;

@@ -28,10 +28,14 @@ namespace qb {
 
 namespace cg = cooperative_groups;
 
-template <int P> struct Geo {
+template <int P, class C = double2> struct Geo {
 	static constexpr int N = P / 2;
 	static constexpr int T = Len<P>::T;
-	static constexpr int LDP = P + 1;
+	// row pitch: P + 1 makes every 16-byte (FP64) access pattern of the row,
+	// column and exchange passes conflict-free; with 8-byte (FP32) values a
+	// half-warp spans two lines, and the pads below halve the excess wavefronts
+	// of P + 1 (bank model of all the patterns, 1.5x of ideal instead of 2x)
+	static constexpr int LDP = P + (sizeof(C) == 16 ? 1 : (P == 32 ? 4 : 2));
 	static constexpr int NT = P * T;            // threads per CTA
 	static constexpr int GRID = P * LDP;        // smem slots of one padded grid
 	// padded index -> index in the N grid, or -1 inside the zero band
@@ -64,7 +68,7 @@ template <class C> struct MulCplx {           // psi (complex N x N) .* v   (Mul
 // lane's 8 inputs of padded row `prow` of Pad(mul . src)
 template <int P, class C, class Mul>
 __device__ __forceinline__ void load_pad_row(C (&x)[8], int prow, int tau, const double2 *__restrict__ src, const Mul &mul) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	const int l = G::src(prow);
 #pragma unroll
 	for (int r = 0; r < 8; r++) {
@@ -76,7 +80,7 @@ __device__ __forceinline__ void load_pad_row(C (&x)[8], int prow, int tau, const
 // FFT2 (direction DIR) of Pad(mul . src) into the smem grid S (in place, two passes)
 template <int P, int DIR, class C, class Mul>
 __device__ __forceinline__ void fft2_pad(C *S, const C *tw, const double2 *__restrict__ src, const Mul &mul) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
 	C x[8];
 	load_pad_row<P>(x, line, tau, src, mul);
@@ -95,7 +99,7 @@ __device__ __forceinline__ void fft2_pad(C *S, const C *tw, const double2 *__res
 // FFT2 of a full grid already in smem S (natural layout), in place
 template <int P, int DIR, class C>
 __device__ __forceinline__ void fft2_smem(C *S, const C *tw) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
 	C x[8];
 #pragma unroll
@@ -115,7 +119,7 @@ __device__ __forceinline__ void fft2_smem(C *S, const C *tw) {
 // copy smem grid (pitch LDP) to a dense global P x P grid, coalesced
 template <int P, class C>
 __device__ __forceinline__ void smem_to_global(C *__restrict__ out, const C *S) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	for (int i = threadIdx.x; i < P * P; i += G::NT) out[i] = S[(i / P) * G::LDP + (i % P)];
 }
 
@@ -123,7 +127,7 @@ __device__ __forceinline__ void smem_to_global(C *__restrict__ out, const C *S) 
 // K1: padded forward spectra  out[b] = FFT2(Pad(src[b]))   (one CTA per grid)
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT) k_pad_fft(const double2 *__restrict__ src, C *__restrict__ out) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *S = reinterpret_cast<C *>(smem_raw), *tw = S + G::GRID;
 	init_twiddles<P>(tw);
@@ -152,7 +156,7 @@ using I1Params = I1ParamsT<double2>;
 
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1ParamsT<C> p) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	using Lp = Len<P>;
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -227,7 +231,7 @@ using I2Params = I2ParamsT<double2>;
 
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2ParamsT<C> p) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	using Lp = Len<P>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *A = reinterpret_cast<C *>(smem_raw), *B = A + G::GRID, *tw = A + 2 * G::GRID;
@@ -286,7 +290,7 @@ using I3Params = I3ParamsT<double2>;
 
 template <int P, int CS, class C>
 __global__ void __launch_bounds__(Geo<P>::NT, Occ<C>::CTAS) k_i3(const I3ParamsT<C> p) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	using Lp = Len<P>;
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -424,7 +428,7 @@ template <class C> struct I3Tmem {
 // clusters of k_i3 fit 33 of 37 four-SM slots).  Output as k_i3 with CS = 4.
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	using Lp = Len<P>;
 	using R = typename CT<C>::R;
 	using TM = I3Tmem<C>;
@@ -546,7 +550,7 @@ using FullParams = FullParamsT<double2>;
 
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT) k_fft_full(const FullParamsT<C> p) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *S = reinterpret_cast<C *>(smem_raw), *tw = S + G::GRID;
 	init_twiddles<P>(tw);
@@ -589,7 +593,7 @@ using AsmParams = AsmParamsT<double2>;
 
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) {
-	using G = Geo<P>;
+	using G = Geo<P, C>;
 	using R = typename CT<C>::R;
 	constexpr int N = G::N, NN = N * N, PP = P * P;
 	constexpr int PER = (NN + G::NT - 1) / G::NT;

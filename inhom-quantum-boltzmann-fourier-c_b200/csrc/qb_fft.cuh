@@ -104,16 +104,23 @@ template <int L> struct Len {
 	__device__ __forceinline__ static int xpos(int q, int s) { return q * T + (s ^ (q & (T - 1))); }
 };
 
-// Length-L transform of the 8 values in x (see file comment).  `scratch` is
-// an L-slot region addressed scratch[pos * sstride]; its previous contents are
-// destroyed.  `tw` is the table of init_twiddles (tw[e] = w_L^e); a lane
-// reads only its base twiddle w_L^tau (the T lanes read T consecutive
-// entries: one conflict-free wavefront) and forms w_L^(tau*q), q = 2..7, by
-// repeated multiplication in registers, trading six shared-memory loads for
-// six complex multiplies (relative error of the powers below 1e-15).
+// Scratch of a transform: sc(pos) is the slot of position pos (0 .. L-1)
+// of the line being transformed (a row or a column of a grid in shared memory).
+template <class C> struct Strided {
+	C *p; int stride;
+	__device__ __forceinline__ C &operator()(int pos) const { return p[pos * stride]; }
+};
+
+// Length-L transform of the 8 values in x (see file comment) with the
+// scratch accessor sc; its previous contents are destroyed.  `tw` is the table
+// of init_twiddles (tw[e] = w_L^e); a lane reads only its base twiddle
+// w_L^tau (the T lanes read T consecutive entries: one conflict-free
+// wavefront) and forms w_L^(tau*q), q = 2..7, by repeated multiplication in
+// registers, trading six shared-memory loads for six complex multiplies
+// (relative error of the powers below 1e-15).
 // Must be called by all 32 lanes of the warp (contains __syncwarp).
-template <int L, int DIR, class C>
-__device__ __forceinline__ void fft1d(C (&x)[8], int tau, C *scratch, int sstride, const C *tw) {
+template <int L, int DIR, class C, class Acc>
+__device__ __forceinline__ void fft1d_acc(C (&x)[8], int tau, const Acc &sc, const C *tw) {
 	using G = Len<L>;
 	dft8<DIR>(x);
 	if constexpr (G::T > 1) {
@@ -128,12 +135,12 @@ __device__ __forceinline__ void fft1d(C (&x)[8], int tau, C *scratch, int sstrid
 		}
 		__syncwarp();
 #pragma unroll
-		for (int q = 0; q < 8; q++) scratch[G::xpos(q, tau) * sstride] = x[q];
+		for (int q = 0; q < 8; q++) sc(G::xpos(q, tau)) = x[q];
 		__syncwarp();
 #pragma unroll
 		for (int u = 0; u < G::U; u++)
 #pragma unroll
-			for (int s = 0; s < G::T; s++) x[u * G::T + s] = scratch[G::xpos(tau * G::U + u, s) * sstride];
+			for (int s = 0; s < G::T; s++) x[u * G::T + s] = sc(G::xpos(tau * G::U + u, s));
 		__syncwarp();
 #pragma unroll
 		for (int u = 0; u < G::U; u++) {
@@ -151,20 +158,30 @@ __device__ __forceinline__ void fft1d(C (&x)[8], int tau, C *scratch, int sstrid
 	}
 }
 
+// the same on an L-slot region addressed scratch[pos * sstride]
+template <int L, int DIR, class C>
+__device__ __forceinline__ void fft1d(C (&x)[8], int tau, C *scratch, int sstride, const C *tw) {
+	fft1d_acc<L, DIR>(x, tau, Strided<C>{scratch, sstride}, tw);
+}
+
 // Reorder a lane's transform outputs (positions out_pos) into the input
 // layout (positions tau + T*r) through the scratch; a no-op when T is 1 or 8.
-template <int L, class C>
-__device__ __forceinline__ void out_to_in(C (&x)[8], int tau, C *scratch, int sstride) {
+template <int L, class C, class Acc>
+__device__ __forceinline__ void out_to_in_acc(C (&x)[8], int tau, const Acc &sc) {
 	using G = Len<L>;
 	if constexpr (G::T != 1 && G::T != 8) {
 		__syncwarp();
 #pragma unroll
-		for (int e = 0; e < 8; e++) scratch[G::out_pos(tau, e) * sstride] = x[e];
+		for (int e = 0; e < 8; e++) sc(G::out_pos(tau, e)) = x[e];
 		__syncwarp();
 #pragma unroll
-		for (int r = 0; r < 8; r++) x[r] = scratch[(tau + G::T * r) * sstride];
+		for (int r = 0; r < 8; r++) x[r] = sc(tau + G::T * r);
 		__syncwarp();
 	}
+}
+template <int L, class C>
+__device__ __forceinline__ void out_to_in(C (&x)[8], int tau, C *scratch, int sstride) {
+	out_to_in_acc<L>(x, tau, Strided<C>{scratch, sstride});
 }
 
 // fill the twiddle table of fft1d<L>: tw[e] = exp(-2 pi i e / L), e < L,

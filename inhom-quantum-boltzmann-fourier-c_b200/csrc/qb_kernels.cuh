@@ -35,7 +35,19 @@ template <int P, class C = double2> struct Geo {
 	// column and exchange passes conflict-free; with 8-byte (FP32) values a
 	// half-warp spans two lines, and the pads below halve the excess wavefronts
 	// of P + 1 (bank model of all the patterns, 1.5x of ideal instead of 2x)
-	static constexpr int LDP = P + (sizeof(C) == 16 ? 1 : (P == 32 ? 4 : 2));
+	static constexpr int LDP = sizeof(C) == 16 ? P + 1 : (P == 64 ? P + 8 : (P == 32 ? P + 4 : P + 2));
+	// FP32 at P = 64: pitch P + 8 with the column index XOR-ed by 2 ((row >> 1) & 3)
+	// makes every pattern conflict-free (a half-warp's two lines land on
+	// opposite halves of the banks, and the swizzle spreads a column's rows)
+	static constexpr bool SWZ = sizeof(C) == 8 && P == 64;
+	__device__ __forceinline__ static int swz(int r) { return SWZ ? 2 * ((r >> 1) & 3) : 0; }
+	// slot of element (row r, column c) of a grid in shared memory
+	__device__ __forceinline__ static int at(int r, int c) { return r * LDP + (c ^ swz(r)); }
+	// scratch accessors of a row / a column for the transforms
+	struct RowA { C *p; int m; __device__ __forceinline__ C &operator()(int pos) const { return p[pos ^ m]; } };
+	struct ColA { C *S; int c; __device__ __forceinline__ C &operator()(int pos) const { return S[at(pos, c)]; } };
+	__device__ __forceinline__ static RowA row(C *S, int r) { return RowA{ S + r * LDP, swz(r) }; }
+	__device__ __forceinline__ static ColA col(C *S, int c) { return ColA{ S, c }; }
 	static constexpr int NT = P * T;            // threads per CTA
 	static constexpr int GRID = P * LDP;        // smem slots of one padded grid
 	// padded index -> index in the N grid, or -1 inside the zero band
@@ -84,15 +96,15 @@ __device__ __forceinline__ void fft2_pad(C *S, const C *tw, const double2 *__res
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
 	C x[8];
 	load_pad_row<P>(x, line, tau, src, mul);
-	fft1d<P, DIR>(x, tau, S + line * G::LDP, 1, tw);
+	fft1d_acc<P, DIR>(x, tau, G::row(S, line), tw);
 #pragma unroll
-	for (int e = 0; e < 8; e++) S[line * G::LDP + Len<P>::out_pos(tau, e)] = x[e];
+	for (int e = 0; e < 8; e++) S[G::at(line, Len<P>::out_pos(tau, e))] = x[e];
 	__syncthreads();
 #pragma unroll
-	for (int r = 0; r < 8; r++) x[r] = S[(tau + G::T * r) * G::LDP + line];
-	fft1d<P, DIR>(x, tau, S + line, G::LDP, tw);
+	for (int r = 0; r < 8; r++) x[r] = S[G::at(tau + G::T * r, line)];
+	fft1d_acc<P, DIR>(x, tau, G::col(S, line), tw);
 #pragma unroll
-	for (int e = 0; e < 8; e++) S[Len<P>::out_pos(tau, e) * G::LDP + line] = x[e];
+	for (int e = 0; e < 8; e++) S[G::at(Len<P>::out_pos(tau, e), line)] = x[e];
 	__syncthreads();
 }
 
@@ -103,16 +115,16 @@ __device__ __forceinline__ void fft2_smem(C *S, const C *tw) {
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
 	C x[8];
 #pragma unroll
-	for (int r = 0; r < 8; r++) x[r] = S[line * G::LDP + tau + G::T * r];
-	fft1d<P, DIR>(x, tau, S + line * G::LDP, 1, tw);
+	for (int r = 0; r < 8; r++) x[r] = S[G::at(line, tau + G::T * r)];
+	fft1d_acc<P, DIR>(x, tau, G::row(S, line), tw);
 #pragma unroll
-	for (int e = 0; e < 8; e++) S[line * G::LDP + Len<P>::out_pos(tau, e)] = x[e];
+	for (int e = 0; e < 8; e++) S[G::at(line, Len<P>::out_pos(tau, e))] = x[e];
 	__syncthreads();
 #pragma unroll
-	for (int r = 0; r < 8; r++) x[r] = S[(tau + G::T * r) * G::LDP + line];
-	fft1d<P, DIR>(x, tau, S + line, G::LDP, tw);
+	for (int r = 0; r < 8; r++) x[r] = S[G::at(tau + G::T * r, line)];
+	fft1d_acc<P, DIR>(x, tau, G::col(S, line), tw);
 #pragma unroll
-	for (int e = 0; e < 8; e++) S[Len<P>::out_pos(tau, e) * G::LDP + line] = x[e];
+	for (int e = 0; e < 8; e++) S[G::at(Len<P>::out_pos(tau, e), line)] = x[e];
 	__syncthreads();
 }
 
@@ -120,7 +132,7 @@ __device__ __forceinline__ void fft2_smem(C *S, const C *tw) {
 template <int P, class C>
 __device__ __forceinline__ void smem_to_global(C *__restrict__ out, const C *S) {
 	using G = Geo<P, C>;
-	for (int i = threadIdx.x; i < P * P; i += G::NT) out[i] = S[(i / P) * G::LDP + (i % P)];
+	for (int i = threadIdx.x; i < P * P; i += G::NT) out[i] = S[G::at(i / P, i % P)];
 }
 
 // ---------------------------------------------------------------------------
@@ -170,7 +182,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1ParamsT<C> p) {
 	for (int i = threadIdx.x; i < P * P; i += G::NT) {
 		const C w = W[i];
 		C f; f.x = fa * w.x + fb; f.y = fa * w.y;
-		F[(i / P) * G::LDP + (i % P)] = f;
+		F[G::at(i / P, i % P)] = f;
 	}
 	__syncthreads();
 	const double2 *g = p.g + cell * p.g_cell + (long)p.g_comp[task] * G::N * G::N;
@@ -183,25 +195,25 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1ParamsT<C> p) {
 		C x[8];
 		// rows: FFT of Pad(psi2_t . g)
 		load_pad_row<P>(x, line, tau, g, MulReal<C>{p.psi2 + (long)t * G::N * G::N});
-		fft1d<P, -1>(x, tau, S + line * G::LDP, 1, tw);
+		fft1d_acc<P, -1>(x, tau, G::row(S, line), tw);
 #pragma unroll
-		for (int e = 0; e < 8; e++) S[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+		for (int e = 0; e < 8; e++) S[G::at(line, Lp::out_pos(tau, e))] = x[e];
 		__syncthreads();
 		// columns: FFT, multiply by F (convolution with f), inverse FFT
 #pragma unroll
-		for (int r = 0; r < 8; r++) x[r] = S[(tau + G::T * r) * G::LDP + line];
-		fft1d<P, -1>(x, tau, S + line, G::LDP, tw);
+		for (int r = 0; r < 8; r++) x[r] = S[G::at(tau + G::T * r, line)];
+		fft1d_acc<P, -1>(x, tau, G::col(S, line), tw);
 #pragma unroll
-		for (int e = 0; e < 8; e++) x[e] = cmul(F[Lp::out_pos(tau, e) * G::LDP + line], x[e]);
-		out_to_in<P>(x, tau, S + line, G::LDP);
-		fft1d<P, +1>(x, tau, S + line, G::LDP, tw);
+		for (int e = 0; e < 8; e++) x[e] = cmul(F[G::at(Lp::out_pos(tau, e), line)], x[e]);
+		out_to_in_acc<P>(x, tau, G::col(S, line));
+		fft1d_acc<P, +1>(x, tau, G::col(S, line), tw);
 #pragma unroll
-		for (int e = 0; e < 8; e++) S[Lp::out_pos(tau, e) * G::LDP + line] = x[e];
+		for (int e = 0; e < 8; e++) S[G::at(Lp::out_pos(tau, e), line)] = x[e];
 		__syncthreads();
 		// rows: inverse FFT, multiply by phi_t, accumulate
 #pragma unroll
-		for (int r = 0; r < 8; r++) x[r] = S[line * G::LDP + tau + G::T * r];
-		fft1d<P, +1>(x, tau, S + line * G::LDP, 1, tw);
+		for (int r = 0; r < 8; r++) x[r] = S[G::at(line, tau + G::T * r)];
+		fft1d_acc<P, +1>(x, tau, G::row(S, line), tw);
 		const R *phi = p.phi + (long)t * P * P + line * P;
 #pragma unroll
 		for (int e = 0; e < 8; e++) {
@@ -251,20 +263,20 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2ParamsT<C> p) {
 		fft2_pad<P, -1>(A, tw, f, MulReal<C>{p.psi1 + (long)t * G::N * G::N});
 		C x[8];
 		load_pad_row<P>(x, line, tau, g, MulReal<C>{p.psi2 + (long)t * G::N * G::N});
-		fft1d<P, -1>(x, tau, B + line * G::LDP, 1, tw);
+		fft1d_acc<P, -1>(x, tau, G::row(B, line), tw);
 #pragma unroll
-		for (int e = 0; e < 8; e++) B[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+		for (int e = 0; e < 8; e++) B[G::at(line, Lp::out_pos(tau, e))] = x[e];
 		__syncthreads();
 #pragma unroll
-		for (int r = 0; r < 8; r++) x[r] = B[(tau + G::T * r) * G::LDP + line];
-		fft1d<P, -1>(x, tau, B + line, G::LDP, tw);
+		for (int r = 0; r < 8; r++) x[r] = B[G::at(tau + G::T * r, line)];
+		fft1d_acc<P, -1>(x, tau, G::col(B, line), tw);
 #pragma unroll
-		for (int e = 0; e < 8; e++) acc[e] = cfma(A[Lp::out_pos(tau, e) * G::LDP + line], x[e], acc[e]);
+		for (int e = 0; e < 8; e++) acc[e] = cfma(A[G::at(Lp::out_pos(tau, e), line)], x[e], acc[e]);
 		__syncthreads();
 	}
 	// column-mapped accumulator -> smem -> coalesced store
 #pragma unroll
-	for (int e = 0; e < 8; e++) A[Lp::out_pos(tau, e) * G::LDP + line] = acc[e];
+	for (int e = 0; e < 8; e++) A[G::at(Lp::out_pos(tau, e), line)] = acc[e];
 	__syncthreads();
 	smem_to_global<P>(p.out + ((cell * p.ntask + task) * p.nchunk + chunk) * (long)P * P, A);
 }
@@ -321,36 +333,36 @@ __global__ void __launch_bounds__(Geo<P>::NT, Occ<C>::CTAS) k_i3(const I3ParamsT
 #pragma unroll
 			for (int r = 0; r < 8; r++) {
 				const int k = tau + G::T * r;
-				x[r] = cmul(Gg[line * P + k], Pr[line * G::LDP + k]);
+				x[r] = cmul(Gg[line * P + k], Pr[G::at(line, k)]);
 			}
-			fft1d<P, +1>(x, tau, Ug + line * G::LDP, 1, tw);
+			fft1d_acc<P, +1>(x, tau, G::row(Ug, line), tw);
 #pragma unroll
-			for (int e = 0; e < 8; e++) Ug[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+			for (int e = 0; e < 8; e++) Ug[G::at(line, Lp::out_pos(tau, e))] = x[e];
 			__syncthreads();
 			// columns: IFFT, multiply by psi2_t, FFT
 #pragma unroll
-			for (int r = 0; r < 8; r++) x[r] = Ug[(tau + G::T * r) * G::LDP + line];
-			fft1d<P, +1>(x, tau, Ug + line, G::LDP, tw);
+			for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
+			fft1d_acc<P, +1>(x, tau, G::col(Ug, line), tw);
 #pragma unroll
 			for (int e = 0; e < 8; e++) {
 				const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
 				x[e].x *= f;
 				x[e].y *= f;
 			}
-			out_to_in<P>(x, tau, Ug + line, G::LDP);
-			fft1d<P, -1>(x, tau, Ug + line, G::LDP, tw);
+			out_to_in_acc<P>(x, tau, G::col(Ug, line));
+			fft1d_acc<P, -1>(x, tau, G::col(Ug, line), tw);
 #pragma unroll
-			for (int e = 0; e < 8; e++) Ug[Lp::out_pos(tau, e) * G::LDP + line] = x[e];
+			for (int e = 0; e < 8; e++) Ug[G::at(Lp::out_pos(tau, e), line)] = x[e];
 			__syncthreads();
 			// rows: FFT, multiply by P_a (remote), accumulate
 #pragma unroll
-			for (int r = 0; r < 8; r++) x[r] = Ug[line * G::LDP + tau + G::T * r];
-			fft1d<P, -1>(x, tau, Ug + line * G::LDP, 1, tw);
+			for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
+			fft1d_acc<P, -1>(x, tau, G::row(Ug, line), tw);
 			const C *Pa = cluster.map_shared_rank(Pr, p.ca[rank][c]);
 			const R coef = (R)p.ccoef[rank][c];
 #pragma unroll
 			for (int e = 0; e < 8; e++) {
-				const C v = cmul(Pa[line * G::LDP + Lp::out_pos(tau, e)], x[e]);
+				const C v = cmul(Pa[G::at(line, Lp::out_pos(tau, e))], x[e]);
 				acc[e].x += coef * v.x;
 				acc[e].y += coef * v.y;
 			}
@@ -478,31 +490,31 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 #pragma unroll
 				for (int r = 0; r < 8; r++) {
 					const int k = tau + G::T * r;
-					x[r] = cmul(Gg[line * P + k], Pj[line * G::LDP + k]);
+					x[r] = cmul(Gg[line * P + k], Pj[G::at(line, k)]);
 				}
-				fft1d<P, +1>(x, tau, Ug + line * G::LDP, 1, tw);
+				fft1d_acc<P, +1>(x, tau, G::row(Ug, line), tw);
 #pragma unroll
-				for (int e = 0; e < 8; e++) Ug[line * G::LDP + Lp::out_pos(tau, e)] = x[e];
+				for (int e = 0; e < 8; e++) Ug[G::at(line, Lp::out_pos(tau, e))] = x[e];
 				__syncthreads();
 				// columns: IFFT, multiply by psi2_t, FFT
 #pragma unroll
-				for (int r = 0; r < 8; r++) x[r] = Ug[(tau + G::T * r) * G::LDP + line];
-				fft1d<P, +1>(x, tau, Ug + line, G::LDP, tw);
+				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
+				fft1d_acc<P, +1>(x, tau, G::col(Ug, line), tw);
 #pragma unroll
 				for (int e = 0; e < 8; e++) {
 					const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
 					x[e].x *= f;
 					x[e].y *= f;
 				}
-				out_to_in<P>(x, tau, Ug + line, G::LDP);
-				fft1d<P, -1>(x, tau, Ug + line, G::LDP, tw);
+				out_to_in_acc<P>(x, tau, G::col(Ug, line));
+				fft1d_acc<P, -1>(x, tau, G::col(Ug, line), tw);
 #pragma unroll
-				for (int e = 0; e < 8; e++) Ug[Lp::out_pos(tau, e) * G::LDP + line] = x[e];
+				for (int e = 0; e < 8; e++) Ug[G::at(Lp::out_pos(tau, e), line)] = x[e];
 				__syncthreads();
 				// rows: FFT, multiply by P_a (own or the partner's), accumulate in TMEM
 #pragma unroll
-				for (int r = 0; r < 8; r++) x[r] = Ug[line * G::LDP + tau + G::T * r];
-				fft1d<P, -1>(x, tau, Ug + line * G::LDP, 1, tw);
+				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
+				fft1d_acc<P, -1>(x, tau, G::row(Ug, line), tw);
 				const int a = p.ca[j][c];
 				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
 				const R coef = (R)p.ccoef[j][c];
@@ -512,7 +524,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 				tmem_wait_ld();
 #pragma unroll
 				for (int e = 0; e < 8; e++) {
-					const C v = cmul(Pa[line * G::LDP + Lp::out_pos(tau, e)], x[e]);
+					const C v = cmul(Pa[G::at(line, Lp::out_pos(tau, e))], x[e]);
 					acc[e].x += coef * v.x;
 					acc[e].y += coef * v.y;
 				}
@@ -559,7 +571,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_fft_full(const FullParamsT<C> p)
 	for (int i = threadIdx.x; i < P * P; i += G::NT) {
 		C s = in[i];
 		for (int k = 1; k < p.nparts; k++) s = cadd(s, in[k * p.part_stride + i]);
-		S[(i / P) * G::LDP + (i % P)] = s;
+		S[G::at(i / P, i % P)] = s;
 	}
 	__syncthreads();
 	fft2_smem<P, -1>(S, tw);
@@ -615,7 +627,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) 
 		const C *FS = p.FS + cell * 3 * PP;
 		for (int i = threadIdx.x; i < PP; i += G::NT) {
 			const C z = csub(cmul(Wh[hi * PP + i], FS[(gi - 1) * PP + i]), cmul(Wh[gi * PP + i], FS[(hi - 1) * PP + i]));
-			S[(i / P) * G::LDP + (i % P)] = z;
+			S[G::at(i / P, i % P)] = z;
 		}
 		__syncthreads();
 		fft2_smem<P, +1>(S, tw);
@@ -623,7 +635,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) 
 		for (int u = 0; u < PER; u++) {
 			const int q = threadIdx.x + u * G::NT;
 			if (q < NN) {
-				const C v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+				const C v = S[G::at(G::pad(q / N), G::pad(q % N))];
 				cc[u] = make_double2(p.s1 * (double)v.x, p.s1 * (double)v.y);
 			}
 		}
@@ -661,7 +673,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) 
 				}
 				z.x += s1 * v.x; z.y += s1 * v.y;
 			}
-			S[(i / P) * G::LDP + (i % P)] = z;
+			S[G::at(i / P, i % P)] = z;
 		}
 		__syncthreads();
 		fft2_smem<P, +1>(S, tw);
@@ -669,7 +681,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) 
 		for (int u = 0; u < PER; u++) {
 			const int q = threadIdx.x + u * G::NT;
 			if (q < NN) {
-				const C v = S[G::pad(q / N) * G::LDP + G::pad(q % N)];
+				const C v = S[G::at(G::pad(q / N), G::pad(q % N))];
 				cd[u] = make_double2((double)v.x, (double)v.y);
 			}
 		}

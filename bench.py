@@ -261,12 +261,16 @@ def run_ours(args):
     per_launch_ms = kms.value / max(1, kn.value)
     flops_launch = cells * wl["J"] * wl["M"] * i3_flops_per_term(N)
     achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp64", "kernel": "k_i3 (I3 quadrature sums, 4-CTA cluster)", "achieved": round(achieved, 3),
+    i3name = "k_i3p" if N == 32 else ("k_i3_128" if N == 64 else "k_i3")
+    i3desc = {"k_i3p": "k_i3p (I3 quadrature sums, 2-CTA cluster, accumulators in tensor memory)",
+              "k_i3_128": "k_i3_128 (I3 quadrature sums, grids split over CTA pairs)",
+              "k_i3": "k_i3 (I3 quadrature sums, 4-CTA cluster)"}[i3name]
+    roofline = {"bound": "fp64", "kernel": i3desc, "achieved": round(achieved, 3),
                 "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak > 0 else None,
                 "peak_source": "measured live: DFMA loop on every SM (qb_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
                 "flops_per_launch": flops_launch, "launch_ms": round(per_launch_ms, 4), "launches": kn.value,
                 "share_of_step": round(kms.value / max(1e-9, tot_ms.value), 4),
-                "traffic": captured_traffic("k_i3", wl)}
+                "traffic": captured_traffic(i3name, wl)}
     state_bytes = cells * 4 * N * N * 8
     hbm = {"bound": "hbm", "note": "whole step: transport reads+writes the state twice, collision reads W^ and writes C (FP64)",
            "bytes_per_step": 4 * state_bytes + 2 * cells * 3 * 4 * N * N * 16,

@@ -528,9 +528,18 @@ template <class C> void launch_i2_128(const I2ParamsT<C> &p, long units, C *tmp,
 	set_smem_once(k_i2_terms128<C>, smem128<C>(), init);
 	launch128(k_i2_terms128<C>, "i2_terms", 2 * units, 1, smem128<C>(), s, p, tmp);
 }
+// The tensor-memory allocation of k_i3_128 never waits as long as no more
+// CTAs share an SM than its 512 columns hold; checked before the first launch.
 template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, cudaStream_t s) {
 	static bool init = false;
-	set_smem_once(k_i3_128<CS, NPAIR, C>, smem128<C>(), init);
+	if (!init) {
+		set_smem(k_i3_128<CS, NPAIR, C>, smem128<C>());
+		int per_sm = 0;
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_i3_128<CS, NPAIR, C>, G128::NT, smem128<C>()));
+		if (per_sm * (int)I3Tmem128<C, CS / NPAIR>::NCOLS > 512)
+			QB_FAIL("k_i3_128: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
+		init = true;
+	}
 	launch128(k_i3_128<CS, NPAIR, C>, "i3_cluster", nclusters * 2 * NPAIR, 2 * NPAIR, smem128<C>(), s, p, pscr);
 }
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {

@@ -23,9 +23,10 @@
 // Every kernel here runs 512 threads per CTA.  Row passes: 16 lanes per row
 // (thread t: row t/16 of 32 per iteration, lane t%16), 2 iterations.  Column
 // passes: 8 lanes per column (column t/8 of 64 per iteration), 2 iterations.
-// Accumulators live in global memory (L2) as read-modify-write of the
-// caller's partial-sum slot owned by the thread; a 16-point accumulator per
-// thread would not fit the FP64 register budget of 128.
+// Accumulators of the I1/I2 sums live in global memory (L2) as
+// read-modify-write of the caller's partial-sum slot owned by the thread (a
+// 16-point accumulator per thread would not fit the FP64 register budget of
+// 128); those of the I3 sums live in tensor memory.
 //
 // Cluster barriers: every loop that contains one has a trip count that is
 // uniform over the cluster (chunk bounds per cluster, combo count = the
@@ -392,6 +393,20 @@ __global__ void __launch_bounds__(512, 1) k_i2_terms128(const I2ParamsT<C> p, C 
 	}
 }
 
+// tensor-memory accumulators of k_i3_128: CPP components x 2 row iterations
+// x 8 values per thread; the four warps of a lane quarter split the columns
+// (512 columns for FP64 with two components per pair, 256 for FP32)
+template <class C, int CPP> struct I3Tmem128 {
+	static constexpr unsigned WPC = sizeof(C) / 4;
+	static constexpr unsigned PER_THREAD = CPP * 16 * WPC;
+	static constexpr unsigned NCOLS = 4 * PER_THREAD;
+	static_assert(NCOLS <= 512, "tensor memory holds 512 columns");
+	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int it, int e) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + (w >> 2) * PER_THREAD + (unsigned)((q * 2 + it) * 8 + e) * WPC;
+	}
+};
+
 // ---------------------------------------------------------------------------
 // K4 (128): I3-type sums on a cluster of NPAIR CTA pairs; pair q holds the
 // CS / NPAIR components q * CS / NPAIR ... in turn.  Per term each pair writes
@@ -423,14 +438,22 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 	int ncmax = 0;
 	for (int r = 0; r < CS; r++) ncmax = max(ncmax, p.ncombo[r]);
 	const int tau = threadIdx.x & 15;
+	// accumulators in tensor memory: value e of row iteration `it` of component q
+	using TM = I3Tmem128<C, CPP>;
+	__shared__ unsigned tmem_slot;
+	const int warp = threadIdx.x >> 5;
+	if (warp == 0) tmem_alloc(&tmem_slot, TM::NCOLS);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const unsigned tbase = tmem_slot;
 #pragma unroll 1
-	for (int q = 0; q < CPP; q++) {           // zero this CTA's half of each accumulator at the final row-pass points
-		C *acc = p.out + ((cell * p.nchunk + chunk) * CS + pair * CPP + q) * G::PP;
-		for (int it = 0; it < 2; it++) {
-			const int row = it * 32 + (threadIdx.x >> 4);
-			for (int e = 0; e < 8; e++) acc[G::bidx(h, row, pos128(tau, e))] = czero<C>();
-		}
-	}
+	for (int q = 0; q < CPP; q++)
+#pragma unroll 1
+		for (int it = 0; it < 2; it++)
+#pragma unroll
+			for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, it, e), czero<C>());
+	tmem_wait_st();
 	__syncthreads();
 #pragma unroll 1
 	for (int t = t0; t < t1; t++) {
@@ -451,7 +474,6 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 			const int comp = pair * CPP + q;
 			const int nc = p.ncombo[comp];
 			const C *Pown = Pall + comp * G::PP;
-			C *acc = p.out + ((cell * p.nchunk + chunk) * CS + comp) * G::PP;
 #pragma unroll 1
 			for (int c = 0; c < ncmax; c++) {
 				const bool act = c < nc;
@@ -484,14 +506,19 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 					const C *Pa = Pall + (long)p.ca[comp][c] * G::PP;
 					const R coef = (R)p.ccoef[comp][c];
 					row_pass<-1>(S, tw128, tw64, RowFromS<C>{S}, [&](C (&x)[8], int row, int tl) {
+						const int it = row >> 5;
+						C a[8];
+#pragma unroll
+						for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), a[e]);
+						tmem_wait_ld();
 #pragma unroll
 						for (int e = 0; e < 8; e++) {
-							const long o = G::bidx(h, row, pos128(tl, e));
-							const C v = cmul(Pa[o], x[e]);
-							C a = acc[o];
-							a.x += coef * v.x; a.y += coef * v.y;
-							acc[o] = a;
+							const C v = cmul(Pa[G::bidx(h, row, pos128(tl, e))], x[e]);
+							a[e].x += coef * v.x; a[e].y += coef * v.y;
 						}
+#pragma unroll
+						for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, it, e), a[e]);
+						tmem_wait_st();
 					});
 					__syncthreads();
 				}
@@ -499,6 +526,25 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 		}
 		cl.sync();                               // every pair is done with this term's P grids
 	}
+	// accumulators -> this CTA's half of the partial-sum slots
+#pragma unroll 1
+	for (int q = 0; q < CPP; q++) {
+		C *acc = p.out + ((cell * p.nchunk + chunk) * CS + pair * CPP + q) * G::PP;
+#pragma unroll 1
+		for (int it = 0; it < 2; it++) {
+			const int row = it * 32 + (threadIdx.x >> 4);
+			C a[8];
+#pragma unroll
+			for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), a[e]);
+			tmem_wait_ld();
+#pragma unroll
+			for (int e = 0; e < 8; e++) acc[G::bidx(h, row, pos128(tau, e))] = a[e];
+		}
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
 }
 
 // ---------------------------------------------------------------------------

@@ -39,6 +39,29 @@ template <class C> __device__ __forceinline__ C cscale(C a, typename CT<C>::R s)
 template <class C> __device__ __forceinline__ C cfma(C a, C b, C c) {   // c + a*b
 	C z; z.x = c.x + (a.x * b.x - a.y * b.y); z.y = c.y + (a.x * b.y + a.y * b.x); return z;
 }
+// FP32: complex add and subtract as one packed two-lane instruction (sm_100
+// add/sub.rn.f32x2: the same IEEE round-to-nearest result per lane as two
+// scalar ones, half the issue slots)
+__device__ __forceinline__ unsigned long long pack_f2(float2 a) {
+	unsigned long long r;
+	asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+	return r;
+}
+__device__ __forceinline__ float2 unpack_f2(unsigned long long r) {
+	float2 a;
+	asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+	return a;
+}
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+	unsigned long long d;
+	asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack_f2(a)), "l"(pack_f2(b)));
+	return unpack_f2(d);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+	unsigned long long d;
+	asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack_f2(a)), "l"(pack_f2(b)));
+	return unpack_f2(d);
+}
 // FP64 shorthands used by code that is FP64 only
 __device__ __forceinline__ double2 czero() { return czero<double2>(); }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return cadd<double2>(a, b); }

@@ -21,6 +21,11 @@ e2e    : same metric through the upstream C API (InhomStepPeriodic on host
          step with host staging at N > 1
 --impl reference : the upstream C sources (compiled here with the project's
          CPU FFTW-API shim) on the host cores, bounded sample per step.
+
+Extra blocks of the JSON line at N = 1: `precision_form` (the FP32 form on
+the same workload, with its error against FP64) and `config2_sample` (64 of
+the 1024 x-cells of the N = 64, J = M = 32 precision-form configuration, FP64
+and FP32 timed alike; --no-config2 skips it).
 """
 import argparse
 import importlib.util
@@ -281,6 +286,9 @@ def run_ours(args):
     prec = None
     if world == 1 and not args.no_precision_form:
         prec = run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value)
+    big = None
+    if world == 1 and not args.no_config2:
+        big = run_config2_sample(args, qbgpu, flush)
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
@@ -290,6 +298,8 @@ def run_ours(args):
             "gpu_launches": launches, "clocks": clk.summary()}
     if prec is not None:
         line["precision_form"] = prec
+    if big is not None:
+        line["config2_sample"] = big
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind = ref_kind()
         procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
@@ -303,6 +313,55 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_config2_sample(args, qbgpu, flush, cells=64, steps=2, warmup=1):
+    """A bounded sample of the precision-form configuration: N = 64 (padded
+    128 x 128), J = M = 32, seeded Gaussian mixture, periodic Strang steps on
+    `cells` of its 1024 x-cells (h, dt as for 1024 cells), FP64 and the FP32
+    form timed alike (CUDA events, L2 flushed before every step), with the
+    FP32 form's error against FP64 on the collision operator of the sample."""
+    import torch
+    N, J, M, L, R = 64, 32, 32, 6.0, 3.75
+    h = 1.0 / 1024
+    dt = 0.4 * h / L
+    q = qbgpu.Quad(N, J, M, L, R)
+    W0 = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=2, ncells=cells)).cuda()
+    B = torch.zeros((cells, 3), dtype=torch.float64, device="cuda")
+    out = {"workload": f"N={N} (padded {2 * N}), J={J}, M={M}, L={L}, R={R}, {cells} of the 1024 x-cells, h=1/1024, "
+                       f"dt=0.4h/L, periodic Strang step; {steps} timed steps after {warmup} warm-up per precision",
+           "unit": UNIT}
+    for prec in (64, 32):
+        ws = qbgpu.Workspace(N, precision=prec)
+        bufs = [W0.clone(), torch.empty_like(W0)]
+        for i in range(warmup):
+            qbgpu.inhom_step(ws, q, bufs[i % 2], h, dt, B, out=bufs[(i + 1) % 2])
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        cur = warmup % 2
+        for k in range(steps):
+            flush.zero_()
+            evs[k][0].record()
+            qbgpu.inhom_step(ws, q, bufs[cur], h, dt, B, out=bufs[1 - cur])
+            evs[k][1].record()
+            cur = 1 - cur
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        out[f"f{prec}"] = {"value": round(cells * 2 / (ms * 1e-3), 3), "ms_per_step": round(ms, 3),
+                           "sim_steps_per_s_at_1024_cells": round(1e3 / (ms * 1024 / cells), 5)}
+        del ws
+    out["speedup_f32_vs_f64"] = round(out["f32"]["value"] / out["f64"]["value"], 4)
+    Wf = torch.empty((cells, 4, N, N), dtype=torch.complex128, device="cuda")
+    qbgpu._check(qbgpu.lib().qb_to_fourier(N, 4 * cells, qbgpu._ptr(W0), qbgpu._ptr(Wf), qbgpu._stream()), "qb_to_fourier")
+    ws64, ws32 = qbgpu.Workspace(N), qbgpu.Workspace(N, precision=32)
+    cc64, cd64 = qbgpu.collision_operators(ws64, q, Wf)
+    cc32, cd32 = qbgpu.collision_operators(ws32, q, Wf)
+
+    def rel(a, b):
+        a, b = a.cpu().numpy().ravel(), b.cpu().numpy().ravel()
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["rel_err_f32_vs_f64"] = {"Cc_l2": rel(cc32, cc64), "Cd_l2": rel(cd32, cd64)}
+    return out
 
 
 def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
@@ -459,6 +518,7 @@ def main():
     ap.add_argument("--M", type=int, default=16)
     ap.add_argument("--cpu-procs", type=int, default=min(32, os.cpu_count() or 1))
     ap.add_argument("--no-precision-form", action="store_true", help="skip the FP32-form measurement")
+    ap.add_argument("--no-config2", action="store_true", help="skip the N = 64 precision-form sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -531,7 +531,9 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 #pragma unroll
 				for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, e), acc[e]);
 				tmem_wait_st();
-				__syncthreads();
+				// no barrier here: the row passes that end this pair and begin the
+				// next touch only the rows of their own 8-lane group, and the next
+				// column pass waits behind the next pair's first barrier
 			}
 		}
 		cluster.sync();

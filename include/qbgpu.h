@@ -68,6 +68,21 @@ int qb_collision_operators(qb_workspace *ws, const qb_quad *q, int ncells, const
 int qb_collision_step(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, const double *B,
                       double dt, void *Wnext, int rk4, void *stream);
 
+/* Spatially homogeneous collision steps for a batch of ninst independent
+ * instances of possibly different grid sizes (the time loop of
+ * SimulationHomogeneous, upstream src/simulation.c:1219-1281, over many
+ * instances): instance i has grid size n[i] (8, 16, 32 or 64) and its Fourier
+ * state at the device pointer W[i] (4 complex n[i] x n[i] grids, updated in
+ * place); B (host, may be NULL = 0) holds 3 doubles per instance.  Every
+ * instance advances `steps` collision steps of size dt: midpoint
+ * (CollisionStep), or classical RK4 with rk4 != 0.  Instances of equal size
+ * are gathered and advanced together, one batched launch sequence per size
+ * and step; the quadrature (J, M, L, R) is common and its tables are built
+ * once per size and kept.  Calls are serialised on the host; their GPU work
+ * shares internal buffers, so calls on different streams must not overlap. */
+int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
+                         int J, int M, double L, double R, void *stream);
+
 /* one Strang step of InhomStepPeriodic (bc = 0) / InhomStepDirichlet (bc = 1)
  * (upstream src/simulation.c:307-830) over ncells velocity-space cells with
  * box half-width L; Bext = 3 doubles per cell.  Wnext must not alias W.

@@ -3,10 +3,11 @@
 // form); the Wigner state itself is always FP64.
 //
 // Notation: N = velocity grid size, P = 2N padded size, all Fourier-space
-// grids complex (double2), element (l, k) at index k + n*l.  A P x P grid in
-// shared memory uses the row pitch LDP = P + 1 so that both row passes (one
-// row per quarter-warp) and column passes (one column per quarter-warp) are
-// free of bank conflicts.  A CTA has P*T threads (T = P/8 lanes per line,
+// grids complex, element (l, k) at index k + n*l.  A P x P grid in shared
+// memory is addressed through Geo::at(row, column): row pitch P + 1 for FP64
+// (row passes, column passes and the in-line exchanges free of bank
+// conflicts), a wider pitch and, at P = 64, an XOR column swizzle for FP32.
+// A CTA has P*T threads (T = P/8 lanes per line,
 // one line = one row or one column): thread tid works on line tid / T as
 // lane tau = tid % T.
 //
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i1_terms(const I1ParamsT<C> p) {
 			acc[e].x += f * x[e].x;
 			acc[e].y += f * x[e].y;
 		}
-		__syncthreads();
+		// no barrier: the next term's first pass writes only this group's row
 	}
 	C *o = p.out + ((cell * p.ntask + task) * p.nchunk + chunk) * (long)P * P + line * P;
 #pragma unroll

@@ -65,6 +65,7 @@ def lib(n_grid=N_GRID):
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
     L.qb_diagnostics.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp]
+    L.qb_homogeneous_batch.argtypes = [C.c_int, _vp, _vp, _vp, C.c_double, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp]
     L.qb_fermi_dirac_equilibrium.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.qb_relative_entropy.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.CalculateRightwardFlux.restype = C.c_double
@@ -178,6 +179,24 @@ def inhom_step(ws, q, W, h, dt, Bext=None, bc="periodic", out=None):
     _check(lib().qb_inhom_step(ws.h, q.h, n, _ptr(W), _ptr(out), h, dt, _ptr(Bext), 0 if bc == "periodic" else 1, _stream()),
            "qb_inhom_step")
     return out
+
+
+def homogeneous_batch(states, dt, steps, B=None, rk4=True, J=16, M=16, L=6.0, R=3.75):
+    """Advance independent homogeneous instances of possibly different grid
+    sizes in place: states is a list of complex128 CUDA tensors (4, N_i, N_i)
+    (Fourier space), B an optional (ninst, 3) array; `steps` collision steps
+    of size dt (RK4 or midpoint), one batched launch sequence per grid size."""
+    n = len(states)
+    sizes = (C.c_int * n)(*[int(s.shape[-1]) for s in states])
+    ptrs = (C.c_void_p * n)(*[s.data_ptr() for s in states])
+    for s in states:
+        assert s.is_cuda and s.is_contiguous() and s.dtype == _torch().complex128
+    Bh = None
+    if B is not None:
+        Bh = np.ascontiguousarray(np.asarray(B, dtype=np.float64).reshape(n, 3))
+    _check(lib().qb_homogeneous_batch(n, sizes, ptrs, Bh.ctypes.data_as(_vp) if Bh is not None else None, dt, steps,
+                                      1 if rk4 else 0, J, M, L, R, _stream()), "qb_homogeneous_batch")
+    return states
 
 
 def inhom_step_maxwell(ws, q, W, h, dt, lam, WL, WR, Bext=None, out=None):

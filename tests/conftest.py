@@ -4,6 +4,10 @@ import sys
 import numpy as np
 import pytest
 
+# tests exercise error paths: make libqbgpu report failures (qb_last_error,
+# RuntimeError in the binding) instead of aborting the process
+os.environ.setdefault("QB_ABORT_ON_ERROR", "0")
+
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(REPO, "inhom-quantum-boltzmann-fourier-c_b200")
 GOLDEN = os.path.join(REPO, "tests", "golden")

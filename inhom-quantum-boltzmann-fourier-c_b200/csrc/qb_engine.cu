@@ -1179,7 +1179,7 @@ void inhom_step(Workspace &ws, const QuadSet &q, int ncells, const double *W, do
 	double *Vt = ws.va.as<double>();
 	transport((int)cs, ncells, W, Vt, A_dev, h, 0.5 * dt, bc, s);
 	const int i0 = (bc == 1) ? 1 : 0, i1 = (bc == 1) ? ncells - 1 : ncells;
-	fourier_collision(ws, q, i1 - i0, Vt + i0 * cs, Bext + 3 * i0, dt, s);
+	fourier_collision(ws, q, i1 - i0, Vt + i0 * cs, Bext ? Bext + 3 * i0 : nullptr, dt, s);   // null Bext: no field
 	transport((int)cs, ncells, Vt, Wnext, A_dev, h, 0.5 * dt, bc, s);
 }
 

@@ -601,7 +601,7 @@ template <class C> struct AsmParamsT {
 	int mode;
 	double2 *out_cc, *out_cd;         // mode 0: [cell][4][N*N] (either may be null)
 	const double2 *base, *wcur;       // mode 1: [cell][4][N*N]; base may be null (= 0)
-	const double *B; double dtc;      // B: [cell][3]
+	const double *B; double dtc;      // B: [cell][3], or null (no magnetic field)
 	double2 *out;                     // mode 1
 };
 using AsmParams = AsmParamsT<double2>;
@@ -699,12 +699,14 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) 
 			if (p.out_cc) p.out_cc[o] = cc[u];
 			if (p.out_cd) p.out_cd[o] = cd[u];
 		} else {
-			const double *B = p.B + cell * 3;
 			const double2 *w = p.wcur + cell * 4 * NN + q;
 			double2 cb = czero();          // -i [B, W] = 2 (B x w) . sigma
-			if (j == 1) cb = make_double2(2 * (B[1] * w[3 * NN].x - B[2] * w[2 * NN].x), 2 * (B[1] * w[3 * NN].y - B[2] * w[2 * NN].y));
-			if (j == 2) cb = make_double2(2 * (B[2] * w[1 * NN].x - B[0] * w[3 * NN].x), 2 * (B[2] * w[1 * NN].y - B[0] * w[3 * NN].y));
-			if (j == 3) cb = make_double2(2 * (B[0] * w[2 * NN].x - B[1] * w[1 * NN].x), 2 * (B[0] * w[2 * NN].y - B[1] * w[1 * NN].y));
+			if (p.B != nullptr) {        // null B: no magnetic field
+				const double *B = p.B + cell * 3;
+				if (j == 1) cb = make_double2(2 * (B[1] * w[3 * NN].x - B[2] * w[2 * NN].x), 2 * (B[1] * w[3 * NN].y - B[2] * w[2 * NN].y));
+				if (j == 2) cb = make_double2(2 * (B[2] * w[1 * NN].x - B[0] * w[3 * NN].x), 2 * (B[2] * w[1 * NN].y - B[0] * w[3 * NN].y));
+				if (j == 3) cb = make_double2(2 * (B[0] * w[2 * NN].x - B[1] * w[1 * NN].x), 2 * (B[0] * w[2 * NN].y - B[1] * w[1 * NN].y));
+			}
 			const double2 b = p.base ? p.base[o] : czero();      // null base: the right-hand side itself
 			p.out[o] = make_double2(b.x + p.dtc * ((cc[u].x + cd[u].x) + cb.x), b.y + p.dtc * ((cc[u].y + cd[u].y) + cb.y));
 		}

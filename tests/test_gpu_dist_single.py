@@ -1,0 +1,38 @@
+"""GPU: the sharded Strang step of bench.py's multi-GPU path, driven by the
+same qbgpu calls (qb_transport, qb_fourier_collision) on one rank of a
+gloo process group, against the single-domain step (qb_inhom_step)."""
+import socket
+
+import numpy as np
+import pytest
+
+import qb_dist
+import qbgpu
+from conftest import rel_l1
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_sharded_step_with_the_library_calls_matches_inhom_step():
+    import torch.distributed as dist
+    N, J, M, L, R = 16, 4, 3, 6.0, 3.75
+    q, ws = qbgpu.Quad(N, J, M, L, R), qbgpu.Workspace(N)
+    ncells = 6
+    W = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=61, ncells=ncells)).cuda()
+    B = torch.from_numpy(np.random.default_rng(4).standard_normal((ncells, 3)) * 0.05).cuda()
+    h, dt = 1.0 / ncells, 0.4 / ncells / L
+    ref = qbgpu.inhom_step(ws, q, W, h, dt, B).cpu().numpy()
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{free_port()}", rank=0, world_size=1)
+    try:
+        out = qb_dist.sharded_strang_step(W, lambda e: qbgpu.transport(e, L, h, 0.5 * dt),
+                                          lambda Wt: qbgpu.fourier_collision(ws, q, Wt, dt, B))
+    finally:
+        dist.destroy_process_group()
+    assert rel_l1(out.cpu().numpy(), ref) < 1e-14

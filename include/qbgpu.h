@@ -63,8 +63,8 @@ int qb_collision_operators(qb_workspace *ws, const qb_quad *q, int ncells, const
                            void *cc, void *cd, void *stream);
 
 /* CollisionStep (midpoint, upstream src/simulation.c:105-136) of ncells
- * Fourier states, B = 3 doubles per cell; rk4 != 0 uses classical RK4 on the
- * same right-hand side instead.  Wnext must not alias W. */
+ * Fourier states, B = 3 doubles per cell (NULL: no field); rk4 != 0 uses
+ * classical RK4 on the same right-hand side instead.  Wnext must not alias W. */
 int qb_collision_step(qb_workspace *ws, const qb_quad *q, int ncells, const void *W, const double *B,
                       double dt, void *Wnext, int rk4, void *stream);
 
@@ -85,7 +85,8 @@ int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *
 
 /* one Strang step of InhomStepPeriodic (bc = 0) / InhomStepDirichlet (bc = 1)
  * (upstream src/simulation.c:307-830) over ncells velocity-space cells with
- * box half-width L; Bext = 3 doubles per cell.  Wnext must not alias W.
+ * box half-width L; Bext = 3 doubles per cell (NULL: no field).  Wnext must
+ * not alias W.
  * A repeated call with identical arguments replays a captured CUDA graph of
  * the step (QB_CUDA_GRAPHS=0 launches kernel by kernel instead). */
 int qb_inhom_step(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
@@ -185,6 +186,65 @@ int qb_integral_i3_noalloc(const qb_quad *q, const void *f, const void *g, const
  * free DFMA loop on every SM, ~tens of ms) -- the denominator of the FP64
  * roofline of the collision kernels. */
 double qb_fp64_peak_tflops(void);
+
+/* ---- learned surrogate of the collision operator (no upstream counterpart) --
+ * A Fourier neural operator maps one velocity-space cell W (4 real N x N
+ * grids, FP64) to an approximation of C[W] = Cc + Cd (velocity space, FP64).
+ * Its input features are the 4 Pauli components and their 10 pairwise
+ * products w_i w_j (i <= j, order (0,0), (0,1), ..., (3,3)), each times a
+ * fixed input scale; a lift to `width` channels, `layers` spectral layers
+ * (truncated DFT to `modes` x (2 modes - 1) frequencies, complex mode mixing,
+ * inverse DFT, plus a pointwise map; GELU between layers) and a projection to
+ * 4 channels follow, whose outputs are multiplied by the per-component output
+ * scales.  Arithmetic is FP32; the forward pass, the backward pass and Adam
+ * are the library's own kernels, and every reduction is in a fixed order, so
+ * gradients and trained weights are deterministic.  All state pointers are
+ * device pointers. */
+typedef struct qb_fno qb_fno;
+/* N even, 4..64; 1 <= width <= 64; 2 modes - 1 <= N; 1 <= layers <= 16.
+ * Weights are drawn from a seeded normal distribution.  NULL on error. */
+qb_fno *qb_fno_create(int N, int width, int modes, int layers, unsigned long long seed);
+void qb_fno_free(qb_fno *net);
+long qb_fno_num_params(const qb_fno *net);
+/* all weights as one FP32 array of qb_fno_num_params() values (host memory):
+ * A[width][14], a[width], per layer Rr[width][width][K], Ri[..], W[width][width],
+ * b[width], then Q[4][width], q[4]; K = (2 modes - 1) modes, frequency
+ * k = (kx + modes - 1) modes + ky */
+int qb_fno_get_params(const qb_fno *net, float *host);
+int qb_fno_set_params(qb_fno *net, const float *host);
+int qb_fno_set_scale(qb_fno *net, const double *scale);          /* 4 output scales (> 0) */
+int qb_fno_set_input_scale(qb_fno *net, const double *scale);    /* 14 input scales (> 0) */
+/* C[b] ~ C[W[b]] for `batch` cells */
+int qb_fno_forward(qb_fno *net, int batch, const double *W, double *C, void *stream);
+/* loss = mean over all outputs of (y - target / scale)^2 (y: the unscaled
+ * network output) and its gradient with respect to every weight (copied to
+ * grad_host when non-NULL, same layout as qb_fno_get_params); synchronises */
+int qb_fno_gradients(qb_fno *net, int batch, const double *W, const double *target, float *grad_host, double *loss, void *stream);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected) on that loss;
+ * the loss is read back, so the call synchronises */
+int qb_fno_train_step(qb_fno *net, int batch, const double *W, const double *target, float lr, double *loss, void *stream);
+
+/* Strang step (the step of qb_inhom_step, periodic boundaries) whose
+ * collision half uses the network with the exact operator as judge:
+ *  - every `check_every`-th step (the first included) evaluates both, takes
+ *    the exact collision for every cell, and marks for the following steps
+ *    each cell whose relative L1 error of C was above `tol`;
+ *  - the other steps take the network's C (a midpoint step with the magnetic
+ *    term and a network evaluation at the midpoint) for unmarked cells and
+ *    the exact collision for marked ones.
+ * The network's C is projected before use onto mass, momentum and energy
+ * conservation of the trace component w0 (the least change |w0| (l0 + l1 v_x +
+ * l2 v_y + l3 |v|^2), the same moments the exact operator conserves), so the
+ * surrogate steps keep them to round-off.  tol = 0 gives the exact step.
+ * The surrogate holds `net`, which must outlive it. */
+typedef struct qb_surrogate qb_surrogate;
+qb_surrogate *qb_surrogate_create(qb_fno *net, double tol, unsigned check_every);
+void qb_surrogate_free(qb_surrogate *s);
+int qb_surrogate_inhom_step(qb_surrogate *s, qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
+                            double h, double dt, const double *Bext, void *stream);
+/* cell-steps taken by the network and by the exact operator so far, and the
+ * largest residual of the last check step */
+int qb_surrogate_stats(const qb_surrogate *s, long *surrogate_cells, long *exact_cells, double *last_max_residual);
 
 #ifdef __cplusplus
 }

@@ -62,12 +62,33 @@ def lib(n_grid=N_GRID):
     L.qb_to_fourier.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
     L.qb_from_fourier.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
     L.qb_integral.argtypes = [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.qb_transport.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, C.c_double, C.c_double, C.c_int, _vp]
+    L.qb_fourier_collision.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, _vp]
+    L.qb_launch_count.restype = C.c_long
+    L.qb_fp64_peak_tflops.restype = C.c_double
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
     L.qb_diagnostics.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp]
     L.qb_homogeneous_batch.argtypes = [C.c_int, _vp, _vp, _vp, C.c_double, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp]
     L.qb_fermi_dirac_equilibrium.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.qb_relative_entropy.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
+    L.qb_fno_create.restype = _vp
+    L.qb_fno_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong]
+    L.qb_fno_free.argtypes = [_vp]
+    L.qb_fno_num_params.restype = C.c_long
+    L.qb_fno_num_params.argtypes = [_vp]
+    L.qb_fno_get_params.argtypes = [_vp, _vp]
+    L.qb_fno_set_params.argtypes = [_vp, _vp]
+    L.qb_fno_set_scale.argtypes = [_vp, _vp]
+    L.qb_fno_set_input_scale.argtypes = [_vp, _vp]
+    L.qb_fno_forward.argtypes = [_vp, C.c_int, _vp, _vp, _vp]
+    L.qb_fno_gradients.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.qb_fno_train_step.argtypes = [_vp, C.c_int, _vp, _vp, C.c_float, _vp, _vp]
+    L.qb_surrogate_create.restype = _vp
+    L.qb_surrogate_create.argtypes = [_vp, C.c_double, C.c_uint]
+    L.qb_surrogate_free.argtypes = [_vp]
+    L.qb_surrogate_inhom_step.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _vp, C.c_double, C.c_double, _vp, _vp]
+    L.qb_surrogate_stats.argtypes = [_vp, _vp, _vp, _vp]
     L.CalculateRightwardFlux.restype = C.c_double
     L.CalculateLeftwardFlux.restype = C.c_double
     _libs[n_grid] = L
@@ -197,6 +218,182 @@ def homogeneous_batch(states, dt, steps, B=None, rk4=True, J=16, M=16, L=6.0, R=
     _check(lib().qb_homogeneous_batch(n, sizes, ptrs, Bh.ctypes.data_as(_vp) if Bh is not None else None, dt, steps,
                                       1 if rk4 else 0, J, M, L, R, _stream()), "qb_homogeneous_batch")
     return states
+
+
+def transport(W, L, h, dt, bc="periodic", out=None):
+    """One limiter step (qb_transport) of step dt on every x-line of the cells
+    of W (float64 CUDA tensor (ncells, 4, N, N)) in a box of half-width L."""
+    out = _torch().empty_like(W) if out is None else out
+    N = W.shape[-1]
+    _check(lib().qb_transport(N, L, W.shape[0], _ptr(W), _ptr(out), h, dt, 0 if bc == "periodic" else 1, _stream()), "qb_transport")
+    return out
+
+
+def fourier_collision(ws, q, W, dt, Bext=None):
+    """The collision part of a Strang step in place on velocity-space cells
+    W (qb_fourier_collision); returns W."""
+    _check(lib().qb_fourier_collision(ws.h, q.h, W.shape[0], _ptr(W), _ptr(Bext) if Bext is not None else None, dt, _stream()),
+           "qb_fourier_collision")
+    return W
+
+
+# ---------------------------------------------------------------------------
+# learned surrogate of the collision operator (qb_fno_*, qb_surrogate_*)
+
+def _features_np(W):
+    """the 14 network input features of velocity-space states W (numpy,
+    (B, 4, N, N)): w_c, then w_i w_j for i <= j"""
+    W = np.asarray(W, dtype=np.float64).reshape(W.shape[0], 4, -1)
+    f = [W[:, c] for c in range(4)] + [W[:, i] * W[:, j] for i in range(4) for j in range(i, 4)]
+    return np.stack(f, axis=1)
+
+
+class FNO:
+    """Fourier neural operator W -> C~[W] ~ Cc + Cd on N x N velocity-space
+    cells (qb_fno_*): FP32 weights on the device, forward, gradients and Adam
+    steps in the library's own kernels."""
+
+    NFEAT = 14
+
+    def __init__(self, N, width=32, modes=8, layers=4, seed=0):
+        self.N, self.width, self.modes, self.layers = N, width, modes, layers
+        self.h = lib().qb_fno_create(N, width, modes, layers, seed)
+        if not self.h:
+            raise RuntimeError(f"qb_fno_create failed: {lib().qb_last_error().decode()}")
+        self._free = lib().qb_fno_free
+        self.scale = np.ones(4)
+        self.input_scale = np.ones(self.NFEAT)
+
+    def __del__(self):
+        if getattr(self, "h", None) and getattr(self, "_free", None):
+            self._free(self.h)
+            self.h = None
+
+    @property
+    def num_params(self):
+        return int(lib().qb_fno_num_params(self.h))
+
+    def get_params(self):
+        out = np.empty(self.num_params, dtype=np.float32)
+        _check(lib().qb_fno_get_params(self.h, out.ctypes.data_as(_vp)), "qb_fno_get_params")
+        return out
+
+    def set_params(self, theta):
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        assert theta.size == self.num_params
+        _check(lib().qb_fno_set_params(self.h, theta.ctypes.data_as(_vp)), "qb_fno_set_params")
+
+    def set_scale(self, scale):
+        s = np.ascontiguousarray(scale, dtype=np.float64)
+        assert s.size == 4
+        _check(lib().qb_fno_set_scale(self.h, s.ctypes.data_as(_vp)), "qb_fno_set_scale")
+        self.scale = s.copy()
+
+    def set_input_scale(self, scale):
+        s = np.ascontiguousarray(scale, dtype=np.float64)
+        assert s.size == self.NFEAT
+        _check(lib().qb_fno_set_input_scale(self.h, s.ctypes.data_as(_vp)), "qb_fno_set_input_scale")
+        self.input_scale = s.copy()
+
+    def fit_scales(self, X, Y):
+        """input scales = 1 / RMS of each feature over the states X, output
+        scales = RMS of each Pauli component of the targets Y (numpy or CUDA
+        tensors (B, 4, N, N))"""
+        X = X.cpu().numpy() if hasattr(X, "cpu") else np.asarray(X)
+        Y = Y.cpu().numpy() if hasattr(Y, "cpu") else np.asarray(Y)
+        f = _features_np(X)
+        rx = np.sqrt(np.mean(f * f, axis=(0, 2)))
+        ry = np.sqrt(np.mean(np.asarray(Y, dtype=np.float64).reshape(Y.shape[0], 4, -1) ** 2, axis=(0, 2)))
+        self.set_input_scale(1.0 / np.where(rx > 0, rx, 1.0))
+        self.set_scale(np.where(ry > 0, ry, 1.0))
+
+    def forward(self, W, out=None):
+        """C~[W] for float64 CUDA states W (B, 4, N, N)"""
+        out = _torch().empty_like(W) if out is None else out
+        _check(lib().qb_fno_forward(self.h, W.shape[0], _ptr(W), _ptr(out), _stream()), "qb_fno_forward")
+        return out
+
+    def gradients(self, W, target):
+        """(loss, flat float32 gradient) of mean((y - target / scale)^2)"""
+        g = np.empty(self.num_params, dtype=np.float32)
+        loss = C.c_double()
+        _check(lib().qb_fno_gradients(self.h, W.shape[0], _ptr(W), _ptr(target), g.ctypes.data_as(_vp), C.byref(loss), _stream()),
+               "qb_fno_gradients")
+        return loss.value, g
+
+    def train_step(self, W, target, lr):
+        loss = C.c_double()
+        _check(lib().qb_fno_train_step(self.h, W.shape[0], _ptr(W), _ptr(target), float(lr), C.byref(loss), _stream()),
+               "qb_fno_train_step")
+        return loss.value
+
+
+def mixture_cells(N, L, nseeds, seed):
+    """one velocity-space cell per seed, numpy (nseeds, 4, N, N): seed k's
+    Gaussian mixture at x-cell k mod 4 of a 4-cell box, so that the mixture
+    amplitudes vary as well"""
+    return np.stack([gaussian_mixture_state(N, L, seed=seed + k, ncells=4)[k % 4] for k in range(nseeds)])
+
+
+def relaxation_pairs(ws, q, W, samples, every=5, dt=0.02):
+    """training pairs (W, C[W] = Cc + Cd), both float64 CUDA tensors in
+    velocity space: the states W (B, 4, N, N) and every `every`-th state of
+    their spatially homogeneous relaxation (midpoint collision steps of size
+    dt), `samples` states per trajectory"""
+    torch = _torch()
+    Wf = to_fourier(W)
+    X, Y = [], []
+    for k in range(samples):
+        if k:
+            for _ in range(every):
+                Wf = collision_step(ws, q, Wf, dt)
+        cc, cd = collision_operators(ws, q, Wf)
+        X.append(from_fourier(Wf))
+        Y.append(from_fourier(cc + cd))
+    return torch.cat(X), torch.cat(Y)
+
+
+def train_fno(net, X, Y, iters, batch=64, lr=2e-3, seed=0):
+    """`iters` Adam steps on random minibatches of the pairs (X, Y) with a
+    cosine learning-rate schedule from lr to 0; returns the last loss"""
+    torch = _torch()
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    loss = float("nan")
+    for it in range(iters):
+        idx = torch.randint(0, X.shape[0], (batch,), generator=g).to(X.device)
+        a = lr * 0.5 * (1 + math.cos(math.pi * it / iters))
+        loss = net.train_step(X[idx].contiguous(), Y[idx].contiguous(), a)
+    return loss
+
+
+class Surrogate:
+    """Strang steps whose collision half takes the network's C~ with the exact
+    operator as judge every `check_every` steps and as per-cell fallback where
+    the relative L1 error of C~ exceeded `tol` (qb_surrogate_inhom_step)."""
+
+    def __init__(self, net, tol=0.3, check_every=10):
+        self.net = net                       # the surrogate holds the network: keep it alive
+        self.h = lib().qb_surrogate_create(net.h, tol, check_every)
+        if not self.h:
+            raise RuntimeError(f"qb_surrogate_create failed: {lib().qb_last_error().decode()}")
+        self._free = lib().qb_surrogate_free
+
+    def __del__(self):
+        if getattr(self, "h", None) and getattr(self, "_free", None):
+            self._free(self.h)
+            self.h = None
+
+    def step(self, ws, q, W, h, dt, Bext=None, out=None):
+        out = _torch().empty_like(W) if out is None else out
+        _check(lib().qb_surrogate_inhom_step(self.h, ws.h, q.h, W.shape[0], _ptr(W), _ptr(out), h, dt,
+                                             _ptr(Bext) if Bext is not None else None, _stream()), "qb_surrogate_inhom_step")
+        return out
+
+    def stats(self):
+        """(surrogate cell-steps, exact cell-steps, largest residual of the last check)"""
+        a, b, r = C.c_long(), C.c_long(), C.c_double()
+        _check(lib().qb_surrogate_stats(self.h, C.byref(a), C.byref(b), C.byref(r)), "qb_surrogate_stats")
+        return a.value, b.value, r.value
 
 
 def inhom_step_maxwell(ws, q, W, h, dt, lam, WL, WR, Bext=None, out=None):

@@ -2,6 +2,7 @@
 #include "qb_engine.h"
 #include "qb_kernels.cuh"
 #include "qb_split128.cuh"
+#include "qb_full128.cuh"
 #include "qb_transport.cuh"
 
 #include <algorithm>
@@ -542,6 +543,48 @@ template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, 
 	}
 	launch128(k_i3_128<CS, NPAIR, C>, "i3_cluster", nclusters * 2 * NPAIR, 2 * NPAIR, smem128<C>(), s, p, pscr);
 }
+// k_i3_full128 (FP32 at N = 64): 2-CTA clusters, a whole grid per CTA, all
+// 512 tensor-memory columns per CTA, so exactly one CTA per SM (checked).
+// QB_I3_KERNEL=pair selects the pair-split k_i3_128 instead (for comparisons).
+inline bool use_full128() {
+	static const bool on = [] { const char *e = getenv("QB_I3_KERNEL"); return !(e && strcmp(e, "pair") == 0); }();
+	return on;
+}
+constexpr size_t kFull128Smem = sizeof(float2) * ((size_t)F128::GRID + 128 + 64);
+
+int active_i3_full128_clusters() {
+	static int cached = -1;
+	if (cached < 0) {
+		auto kern = k_i3_full128<float2>;
+		set_smem(kern, kFull128Smem);
+		int per_sm = 0;
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, F128::NT, kFull128Smem));
+		if (per_sm * (int)F128Tmem::NCOLS > 512)
+			QB_FAIL("k_i3_full128: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(2);
+		cfg.blockDim = dim3(F128::NT);
+		cfg.dynamicSmemBytes = kFull128Smem;
+		cudaLaunchAttribute attr;
+		attr.id = cudaLaunchAttributeClusterDimension;
+		attr.val.clusterDim.x = 2; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+		cfg.attrs = &attr;
+		cfg.numAttrs = 1;
+		int n = 0;
+		if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
+			cudaGetLastError();
+			n = std::max(1, num_sms() / 2);
+		}
+		cached = n;
+	}
+	return cached;
+}
+
+void launch_i3_full128(const I3ParamsT<float2> &p, long nclusters, float2 *pscr, cudaStream_t s) {
+	active_i3_full128_clusters();              // attribute + occupancy check
+	launch128(k_i3_full128<float2>, "i3_cluster", nclusters * 2, 2, kFull128Smem, s, p, pscr);
+}
+
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
 	static bool init = false;
 	set_smem_once(k_assemble128<C>, smem128<C>(), init);
@@ -607,6 +650,9 @@ template <class C> struct Rhs<128, C> {
 		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
+		if constexpr (sizeof(C) == 8) {
+			if (use_full128()) { launch_i3_full128(p, ncl, ws.scr128a.as<C>(), s); return; }
+		}
 		launch_i3_128<4, kI3Pairs128>(p, ncl, ws.scr128a.as<C>(), s);
 	}
 
@@ -615,7 +661,10 @@ template <class C> struct Rhs<128, C> {
 		const int pairs = std::max(1, num_sms() / 2);
 		if (q.i1) ch.i1 = best_chunks((long)ncells * 7, std::max(1, q.i1->nterms), pairs, 64, 0.15);
 		if (q.i2) ch.i2 = best_chunks((long)ncells * 4, std::max(1, q.i2->nterms), pairs, 64, 0.15);
-		if (q.i3) ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), active_i3_clusters128<C>(), 256, 0.15);
+		if (q.i3) {
+			const int act = (sizeof(C) == 8 && use_full128()) ? active_i3_full128_clusters() : active_i3_clusters128<C>();
+			ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), act, 256, 0.15);
+		}
 		spectra(ws, ncells, W, s);
 		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
 		if (parts & RHS_CD) {

@@ -1,0 +1,264 @@
+// qb_full128.cuh — the I3 sums at N = 64 in the FP32 precision form, with
+// each padded 128 x 128 grid whole in one CTA's shared memory.
+//
+// An FP32 complex grid of 128 x 128 is 128 KB, so unlike FP64 it fits one CTA:
+// both dimensions of a transform are local, and an I3 chain
+//   X_j += eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j))
+// (upstream I3integral, src/integrals.c:283-379, summed over the quadrature
+// terms inside the outer transforms) is a row pass, a column pass (inverse
+// transform, psi2, forward transform) and a row pass, with two CTA barriers and
+// no exchange between CTAs.  The 4 components of a (cell, chunk) run on a
+// 2-CTA cluster: CTA r computes the spectra P_{t,c} = FFT2(Pad(psi1_t . W_c))
+// of its components 2r, 2r + 1 into a scratch grid in global memory (L2);
+// after a cluster barrier it runs the 8 chains of its two outputs, reading
+// W^_i, P_j and P_a from L2 and accumulating in tensor memory.
+//
+// Shared-memory grid: natural order, row pitch 129, the column index XOR-ed
+// by 8 when exactly one of (row, column) is in the upper half:
+//   slot(l, k) = 129 l + (k ^ 8 ((l >> 6) ^ (k >> 6)))
+// With 8-byte values a half-warp spans one line (16 lanes); the pitch makes
+// the column accesses conflict-free and the XOR separates the two 64-point
+// halves that the in-line exchange of a 128-point transform visits together.
+//
+// Global layouts: W^ and the outputs are in the B layout of the N = 64 kernels
+// (natural row l stored at row 64 (l & 1) + l / 2); P scratch is natural.
+#pragma once
+#include "qb_split128.cuh"
+
+namespace qb {
+
+struct F128 {
+	static constexpr int P = 128, N = 64, LDP = 129, NT = 512, GRID = P * LDP;
+	__device__ __forceinline__ static int at(int l, int k) { return l * LDP + (k ^ ((((l >> 6) ^ (k >> 6)) & 1) << 3)); }
+	__device__ __forceinline__ static int src(int p) { return p < N / 2 ? p : (p >= 3 * N / 2 ? p - N : -1); }
+	// offset of natural row l of a B-layout grid
+	__device__ __forceinline__ static long brow(int l) { return (long)(64 * (l & 1) + (l >> 1)) * P; }
+};
+
+// slots of a line of the shared grid as a transform scratch: one 64-point half
+template <class C> struct RowHalf {
+	C *S; int row, off;
+	__device__ __forceinline__ C &operator()(int pos) const { return S[F128::at(row, off + pos)]; }
+};
+template <class C> struct ColHalf {
+	C *S; int col, off;
+	__device__ __forceinline__ C &operator()(int pos) const { return S[F128::at(off + pos, col)]; }
+};
+
+// fft128 with the line given as row (ROW) or column `line` of the shared grid
+template <int DIR, bool ROW, class C>
+__device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, const C *tw128, const C *tw64) {
+	const int h = tau >> 3;
+	C u[4], v[4];
+#pragma unroll
+	for (int r = 0; r < 4; r++) {
+		C w = tw128[tau + 16 * r];
+		if (DIR > 0) w.y = -w.y;
+		u[r] = cadd(x[r], x[r + 4]);
+		v[r] = cmul(csub(x[r], x[r + 4]), w);
+	}
+#pragma unroll
+	for (int r = 0; r < 4; r++) {
+		const C send = h ? u[r] : v[r];
+		const C recv = shfl_xor_c(send, 8);
+		x[2 * r] = h ? recv : u[r];
+		x[2 * r + 1] = h ? v[r] : recv;
+	}
+	if constexpr (ROW) fft1d_acc<64, DIR>(x, tau & 7, RowHalf<C>{S, line, h * 64}, tw64);
+	else fft1d_acc<64, DIR>(x, tau & 7, ColHalf<C>{S, line, h * 64}, tw64);
+}
+
+// tensor-memory accumulators: 2 outputs x 4 row iterations x 8 values per
+// thread; the four warps of a lane quarter split the 512 columns
+struct F128Tmem {
+	static constexpr unsigned PER_THREAD = 2 * 4 * 8 * 2;     // 128 (FP32)
+	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 512
+	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int it, int e) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + (w >> 2) * PER_THREAD + (unsigned)((q * 4 + it) * 8 + e) * 2;
+	}
+};
+
+// Ghat: B layout; pscr: [cluster][4][P*P] natural; out: [cell][chunk][4][P*P] B layout
+template <class C>
+__global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p, C *pscr) {
+	static_assert(sizeof(C) == 8, "the whole-grid form is FP32 only");
+	using F = F128;
+	using R = typename CT<C>::R;
+	using TM = F128Tmem;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ unsigned tmem_slot;
+	C *S = reinterpret_cast<C *>(smem_raw), *tw128 = S + F::GRID, *tw64 = tw128 + 128;
+	cg::cluster_group cl = cg::this_cluster();
+	const int rank = (int)cl.block_rank();
+	const long cid = blockIdx.x / 2;
+	const int chunk = (int)(cid % p.nchunk);
+	const long cell = cid / p.nchunk;
+	const int tid = threadIdx.x, warp = tid >> 5, tau = tid & 15, sub = tid >> 4;   // line it * 32 + sub
+	if (warp == 0) tmem_alloc(&tmem_slot, TM::NCOLS);
+	init_tw128(tw128, tw64);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const unsigned tbase = tmem_slot;
+#pragma unroll 1
+	for (int q = 0; q < 2; q++)
+#pragma unroll 1
+		for (int it = 0; it < 4; it++)
+#pragma unroll
+			for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, it, e), czero<C>());
+	tmem_wait_st();
+	C *Pall = pscr + cid * 4 * (long)F::P * F::P;
+	const C *Gcell = p.Ghat + cell * p.g_cell;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+#pragma unroll 1
+	for (int t = t0; t < t1; t++) {
+		// spectra of components 2 rank + q (sign -1), natural layout, to L2
+#pragma unroll 1
+		for (int q = 0; q < 2; q++) {
+			const int comp = 2 * rank + q;
+			const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[comp] * F::N * F::N;
+			const C *psi1 = p.psi1 + (long)t * F::N * F::N;
+#pragma unroll 1
+			for (int it = 0; it < 4; it += 3) {             // rows outside the zero band: 0..31, 96..127
+				const int row = it * 32 + sub, ls = F::src(row);
+				C x[8];
+#pragma unroll
+				for (int r = 0; r < 8; r++) {
+					const int ks = F::src(tau + 16 * r);
+					C v = czero<C>();
+					if (ks >= 0) {
+						const int idx = ks + F::N * ls;
+						const double2 w = src[idx];
+						v = cmul(psi1[idx], mk<C>(w.x, w.y));
+					}
+					x[r] = v;
+				}
+				fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
+#pragma unroll
+				for (int e = 0; e < 8; e++) S[F::at(row, pos128(tau, e))] = x[e];
+			}
+			__syncthreads();
+#pragma unroll 1
+			for (int it = 0; it < 4; it++) {
+				const int col = it * 32 + sub;
+				C x[8];
+#pragma unroll
+				for (int r = 0; r < 8; r++) {
+					const int row = tau + 16 * r;              // rows 32..95 are the zero band
+					x[r] = (r >= 2 && r < 6) ? czero<C>() : S[F::at(row, col)];
+				}
+				fft128_line<-1, false>(x, tau, S, col, tw128, tw64);
+#pragma unroll
+				for (int e = 0; e < 8; e++) S[F::at(pos128(tau, e), col)] = x[e];
+			}
+			__syncthreads();
+			C *Pq = Pall + (long)comp * F::P * F::P;
+#pragma unroll 4
+			for (int i = tid; i < F::P * F::P; i += F::NT) Pq[i] = S[F::at(i >> 7, i & 127)];
+			__syncthreads();
+		}
+		cl.sync();                                          // both CTAs' spectra of term t are in L2
+		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * F::P * F::P;
+		const R sc = (R)p.psi2_scale[t];
+#pragma unroll 1
+		for (int q = 0; q < 2; q++) {
+			const int j = 2 * rank + q;
+			const C *Pj = Pall + (long)j * F::P * F::P;
+#pragma unroll 1
+			for (int cmb = 0; cmb < p.ncombo[j]; cmb++) {
+				const C *Gg = Gcell + (long)p.cgi[j][cmb] * F::P * F::P;
+				// rows: inverse transform along k of W^_i . P_j
+#pragma unroll 1
+				for (int it = 0; it < 4; it++) {
+					const int row = it * 32 + sub;
+					const C *g = Gg + F::brow(row), *pj = Pj + (long)row * F::P;
+					C x[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = cmul(g[tau + 16 * r], pj[tau + 16 * r]);
+					fft128_line<+1, true>(x, tau, S, row, tw128, tw64);
+#pragma unroll
+					for (int e = 0; e < 8; e++) S[F::at(row, pos128(tau, e))] = x[e];
+				}
+				__syncthreads();
+				// columns: inverse transform along l, psi2, forward transform
+#pragma unroll 1
+				for (int it = 0; it < 4; it++) {
+					const int col = it * 32 + sub;
+					C x[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = S[F::at(tau + 16 * r, col)];
+					fft128_line<+1, false>(x, tau, S, col, tw128, tw64);
+					const R *ps = psi2 + (long)col * F::P;
+#pragma unroll
+					for (int e = 0; e < 8; e++) {
+						const R f = sc * ps[pos128(tau, e)];
+						x[e].x *= f;
+						x[e].y *= f;
+					}
+					// outputs (rows pos128) back into the input order (rows tau + 16 r)
+					__syncwarp();
+#pragma unroll
+					for (int e = 0; e < 8; e++) S[F::at(pos128(tau, e), col)] = x[e];
+					__syncwarp();
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = S[F::at(tau + 16 * r, col)];
+					__syncwarp();
+					fft128_line<-1, false>(x, tau, S, col, tw128, tw64);
+#pragma unroll
+					for (int e = 0; e < 8; e++) S[F::at(pos128(tau, e), col)] = x[e];
+				}
+				__syncthreads();
+				// rows: forward transform along k, times P_a, accumulate
+				const int a = p.ca[j][cmb];
+				const C *Pa = Pall + (long)a * F::P * F::P;
+				const R coef = (R)p.ccoef[j][cmb];
+#pragma unroll 1
+				for (int it = 0; it < 4; it++) {
+					const int row = it * 32 + sub;
+					C x[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = S[F::at(row, tau + 16 * r)];
+					fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
+					const C *pa = Pa + (long)row * F::P;
+					C acc[8];
+#pragma unroll
+					for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), acc[e]);
+					tmem_wait_ld();
+#pragma unroll
+					for (int e = 0; e < 8; e++) {
+						const C v = cmul(pa[pos128(tau, e)], x[e]);
+						acc[e].x += coef * v.x;
+						acc[e].y += coef * v.y;
+					}
+#pragma unroll
+					for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, it, e), acc[e]);
+					tmem_wait_st();
+				}
+				// no barrier: the next chain's first row pass writes only the
+				// rows this thread's 16-lane group has just read
+			}
+		}
+		cl.sync();                                          // the partner is done with this term's spectra
+	}
+#pragma unroll 1
+	for (int q = 0; q < 2; q++) {
+		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * (long)F::P * F::P;
+#pragma unroll 1
+		for (int it = 0; it < 4; it++) {
+			const int row = it * 32 + sub;
+			C acc[8];
+#pragma unroll
+			for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), acc[e]);
+			tmem_wait_ld();
+#pragma unroll
+			for (int e = 0; e < 8; e++) o[F::brow(row) + pos128(tau, e)] = acc[e];
+		}
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
+}
+
+}  // namespace qb

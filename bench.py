@@ -286,7 +286,7 @@ def run_ours(args):
         prec = run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value)
     big = None
     if world == 1 and not args.no_config2:
-        big = run_config2_sample(args, qbgpu, flush)
+        big = run_config2_sample(args, qbgpu, flush, cells=args.config2_cells)
     sur = None
     if world == 1 and not args.no_surrogate:
         sur = run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value)
@@ -587,6 +587,7 @@ def main():
     ap.add_argument("--cpu-procs", type=int, default=min(32, os.cpu_count() or 1))
     ap.add_argument("--no-precision-form", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--no-config2", action="store_true", help="skip the N = 64 precision-form sample")
+    ap.add_argument("--config2-cells", type=int, default=64, help="x-cells of the N = 64 sample (of its 1024)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

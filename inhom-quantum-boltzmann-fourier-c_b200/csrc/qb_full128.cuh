@@ -6,8 +6,9 @@
 //   X_j += eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j))
 // (upstream I3integral, src/integrals.c:283-379, summed over the quadrature
 // terms inside the outer transforms) is a row pass, a column pass (inverse
-// transform, psi2, forward transform) and a row pass, with two CTA barriers and
-// no exchange between CTAs.  The 4 components of a (cell, chunk) run on a
+// transform by decimation in frequency, psi2, forward transform by decimation
+// in time, all in registers) and a row pass, with two CTA barriers and no
+// exchange between CTAs.  The 4 components of a (cell, chunk) run on a
 // 2-CTA cluster: CTA r computes the spectra P_{t,c} = FFT2(Pad(psi1_t . W_c))
 // of its components 2r, 2r + 1 into a scratch grid in global memory (L2);
 // after a cluster barrier it runs the 8 chains of its two outputs, reading
@@ -66,6 +67,37 @@ __device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, 
 	}
 	if constexpr (ROW) fft1d_acc<64, DIR>(x, tau & 7, RowHalf<C>{S, line, h * 64}, tw64);
 	else fft1d_acc<64, DIR>(x, tau & 7, ColHalf<C>{S, line, h * 64}, tw64);
+}
+
+// 128-point transform by decimation in time of a column whose lane tau holds
+// the samples at rows pos128(tau, e) (the output order of fft128_line):
+// lanes 0-7 hold the even samples 2m, lanes 8-15 the odd ones, m = (tau & 7) +
+// 8 e, which is the input order of fft1d<64> on each half.  After the two
+// 64-point transforms E and O, the butterfly Z[k] = E[k] + w^k O[k],
+// Z[k + 64] = E[k] - w^k O[k] is split between the lane pair: lanes 0-7 take
+// k = (tau & 7) + 16 j, lanes 8-15 k = (tau & 7) + 16 j + 8, one shuffle of four
+// values each way.  Output i of lane tau is Z[dpos128(tau, i)].  Applied after
+// fft128_line it needs no reordering in between.
+__device__ __forceinline__ int dpos128(int tau, int i) { return (tau & 7) + 16 * (i >> 1) + 8 * (tau >> 3) + 64 * (i & 1); }
+
+template <int DIR, class C>
+__device__ __forceinline__ void fft128_dit_col(C (&x)[8], int tau, C *S, int col, const C *tw128, const C *tw64) {
+	const int h = tau >> 3, t = tau & 7;
+	fft1d_acc<64, DIR>(x, t, ColHalf<C>{S, col, h * 64}, tw64);
+	C y[8];
+#pragma unroll
+	for (int j = 0; j < 4; j++) {
+		const C send = h ? x[2 * j] : x[2 * j + 1];
+		const C recv = shfl_xor_c(send, 8);
+		const C E = h ? recv : x[2 * j], O = h ? x[2 * j + 1] : recv;
+		C w = tw128[t + 16 * j + 8 * h];
+		if (DIR > 0) w.y = -w.y;
+		const C wo = cmul(w, O);
+		y[2 * j] = cadd(E, wo);
+		y[2 * j + 1] = csub(E, wo);
+	}
+#pragma unroll
+	for (int i = 0; i < 8; i++) x[i] = y[i];
 }
 
 // tensor-memory accumulators: 2 outputs x 4 row iterations x 8 values per
@@ -196,17 +228,9 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 						x[e].x *= f;
 						x[e].y *= f;
 					}
-					// outputs (rows pos128) back into the input order (rows tau + 16 r)
-					__syncwarp();
+					fft128_dit_col<-1>(x, tau, S, col, tw128, tw64);
 #pragma unroll
-					for (int e = 0; e < 8; e++) S[F::at(pos128(tau, e), col)] = x[e];
-					__syncwarp();
-#pragma unroll
-					for (int r = 0; r < 8; r++) x[r] = S[F::at(tau + 16 * r, col)];
-					__syncwarp();
-					fft128_line<-1, false>(x, tau, S, col, tw128, tw64);
-#pragma unroll
-					for (int e = 0; e < 8; e++) S[F::at(pos128(tau, e), col)] = x[e];
+					for (int i = 0; i < 8; i++) S[F::at(dpos128(tau, i), col)] = x[i];
 				}
 				__syncthreads();
 				// rows: forward transform along k, times P_a, accumulate

@@ -246,8 +246,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 					fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
 					const C *pa = Pa + (long)row * F::P;
 					C acc[8];
-#pragma unroll
-					for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), acc[e]);
+					tmem_ld8(TM::addr(tbase, q, it, 0), acc);
 					tmem_wait_ld();
 #pragma unroll
 					for (int e = 0; e < 8; e++) {
@@ -255,8 +254,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 						acc[e].x += coef * v.x;
 						acc[e].y += coef * v.y;
 					}
-#pragma unroll
-					for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, it, e), acc[e]);
+					tmem_st8(TM::addr(tbase, q, it, 0), acc);
 					tmem_wait_st();
 				}
 				// no barrier: the next chain's first row pass writes only the
@@ -272,8 +270,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 		for (int it = 0; it < 4; it++) {
 			const int row = it * 32 + sub;
 			C acc[8];
-#pragma unroll
-			for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), acc[e]);
+			tmem_ld8(TM::addr(tbase, q, it, 0), acc);
 			tmem_wait_ld();
 #pragma unroll
 			for (int e = 0; e < 8; e++) o[F::brow(row) + pos128(tau, e)] = acc[e];

@@ -417,6 +417,45 @@ __device__ __forceinline__ void tmem_st(unsigned taddr, float2 v) {
 	asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(__float_as_uint(v.x)), "r"(__float_as_uint(v.y)) : "memory");
 }
 
+// eight consecutive complex values (32 columns FP64, 16 FP32) of this
+// thread's lane in one warp-wide load or store
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, double2 (&v)[8]) {
+	unsigned r[32];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int e = 0; e < 8; e++) {
+		v[e].x = __hiloint2double((int)r[4 * e + 1], (int)r[4 * e]);
+		v[e].y = __hiloint2double((int)r[4 * e + 3], (int)r[4 * e + 2]);
+	}
+}
+__device__ __forceinline__ void tmem_st8(unsigned taddr, const double2 (&v)[8]) {
+	unsigned r[32];
+#pragma unroll
+	for (int e = 0; e < 8; e++) {
+		r[4 * e] = (unsigned)__double2loint(v[e].x); r[4 * e + 1] = (unsigned)__double2hiint(v[e].x);
+		r[4 * e + 2] = (unsigned)__double2loint(v[e].y); r[4 * e + 3] = (unsigned)__double2hiint(v[e].y);
+	}
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};"
+	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31]) : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float2 (&v)[8]) {
+	unsigned r[16];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int e = 0; e < 8; e++) { v[e].x = __uint_as_float(r[2 * e]); v[e].y = __uint_as_float(r[2 * e + 1]); }
+}
+__device__ __forceinline__ void tmem_st8(unsigned taddr, const float2 (&v)[8]) {
+	unsigned r[16];
+#pragma unroll
+	for (int e = 0; e < 8; e++) { r[2 * e] = __float_as_uint(v[e].x); r[2 * e + 1] = __float_as_uint(v[e].y); }
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
+}
+
 // TMEM accumulators of k_i3p: 2 outputs x 8 values per thread
 template <class C> struct I3Tmem {
 	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
@@ -520,8 +559,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
 				const R coef = (R)p.ccoef[j][c];
 				C acc[8];
-#pragma unroll
-				for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, e), acc[e]);
+				tmem_ld8(TM::addr(tbase, q, 0), acc);
 				tmem_wait_ld();
 #pragma unroll
 				for (int e = 0; e < 8; e++) {
@@ -529,8 +567,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					acc[e].x += coef * v.x;
 					acc[e].y += coef * v.y;
 				}
-#pragma unroll
-				for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, e), acc[e]);
+				tmem_st8(TM::addr(tbase, q, 0), acc);
 				tmem_wait_st();
 				// no barrier here: the row passes that end this pair and begin the
 				// next touch only the rows of their own 8-lane group, and the next
@@ -542,8 +579,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 #pragma unroll 1
 	for (int q = 0; q < 2; q++) {
 		C acc[8];
-#pragma unroll
-		for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, e), acc[e]);
+		tmem_ld8(TM::addr(tbase, q, 0), acc);
 		tmem_wait_ld();
 		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * (long)P * P + line * P;
 #pragma unroll

@@ -508,16 +508,14 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 					row_pass<-1>(S, tw128, tw64, RowFromS<C>{S}, [&](C (&x)[8], int row, int tl) {
 						const int it = row >> 5;
 						C a[8];
-#pragma unroll
-						for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), a[e]);
+						tmem_ld8(TM::addr(tbase, q, it, 0), a);
 						tmem_wait_ld();
 #pragma unroll
 						for (int e = 0; e < 8; e++) {
 							const C v = cmul(Pa[G::bidx(h, row, pos128(tl, e))], x[e]);
 							a[e].x += coef * v.x; a[e].y += coef * v.y;
 						}
-#pragma unroll
-						for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, it, e), a[e]);
+						tmem_st8(TM::addr(tbase, q, it, 0), a);
 						tmem_wait_st();
 					});
 					__syncthreads();
@@ -534,8 +532,7 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 		for (int it = 0; it < 2; it++) {
 			const int row = it * 32 + (threadIdx.x >> 4);
 			C a[8];
-#pragma unroll
-			for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, it, e), a[e]);
+			tmem_ld8(TM::addr(tbase, q, it, 0), a);
 			tmem_wait_ld();
 #pragma unroll
 			for (int e = 0; e < 8; e++) acc[G::bidx(h, row, pos128(tau, e))] = a[e];

@@ -36,15 +36,46 @@ struct F128 {
 	__device__ __forceinline__ static long brow(int l) { return (long)(64 * (l & 1) + (l >> 1)) * P; }
 };
 
-// slots of a line of the shared grid as a transform scratch: one 64-point half
+// slots of a line of the shared grid as a transform scratch: one 64-point
+// half.  Within half h of row l the swizzle is one XOR of the position with
+// 8 ((l >> 6) ^ h); within half h of column k it is a constant column offset.
 template <class C> struct RowHalf {
-	C *S; int row, off;
-	__device__ __forceinline__ C &operator()(int pos) const { return S[F128::at(row, off + pos)]; }
+	C *S; int base, m;                         // base = 129 l + 64 h, m = 8 ((l >> 6) ^ h)
+	__device__ __forceinline__ RowHalf(C *S_, int row, int h) : S(S_), base(row * F128::LDP + 64 * h), m((((row >> 6) ^ h) & 1) << 3) {}
+	__device__ __forceinline__ C &operator()(int pos) const { return S[base + (pos ^ m)]; }
 };
 template <class C> struct ColHalf {
-	C *S; int col, off;
-	__device__ __forceinline__ C &operator()(int pos) const { return S[F128::at(off + pos, col)]; }
+	C *S; int base;                            // base = 129 * 64 h + (k ^ 8 (h ^ (k >> 6)))
+	__device__ __forceinline__ ColHalf(C *S_, int col, int h) : S(S_), base(64 * h * F128::LDP + (col ^ ((((col >> 6) ^ h) & 1) << 3))) {}
+	__device__ __forceinline__ C &operator()(int pos) const { return S[base + pos * F128::LDP]; }
 };
+
+// slots of the 8 inputs (positions tau + 16 r) and outputs (positions
+// pos128(tau, e)) of lane tau on a row or column of the shared grid: the
+// swizzle depends only on which half a position is in (r / 4, e / 4)
+struct LineSlots {
+	int in[2], out[2], step, cx[2];            // cx: a column's swizzled index in the lower / upper half (columns only)
+	__device__ __forceinline__ int at_in(int r) const { return in[r >> 2] + step * r; }
+	__device__ __forceinline__ int at_out(int e) const { return out[e >> 2] + step * e; }
+};
+__device__ __forceinline__ LineSlots row_slots(int row, int tau) {
+	const int p0 = 2 * (tau & 7) + (tau >> 3), rb = row * F128::LDP, m = ((row >> 6) & 1) << 3;
+	LineSlots L;
+	L.in[0] = rb + (tau ^ m); L.in[1] = rb + (tau ^ m ^ 8);
+	L.out[0] = rb + (p0 ^ m); L.out[1] = rb + (p0 ^ m ^ 8);
+	L.step = 16;
+	L.cx[0] = L.cx[1] = 0;
+	return L;
+}
+__device__ __forceinline__ LineSlots col_slots(int col, int tau) {
+	const int p0 = 2 * (tau & 7) + (tau >> 3), c0 = col ^ (((col >> 6) & 1) << 3), c1 = c0 ^ 8;
+	LineSlots L;
+	L.in[0] = tau * F128::LDP + c0; L.in[1] = tau * F128::LDP + c1;
+	L.out[0] = p0 * F128::LDP + c0; L.out[1] = p0 * F128::LDP + c1;
+	L.step = 16 * F128::LDP;
+	L.cx[0] = c0; L.cx[1] = c1;
+	return L;
+}
 
 // fft128 with the line given as row (ROW) or column `line` of the shared grid
 template <int DIR, bool ROW, class C>
@@ -65,8 +96,8 @@ __device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, 
 		x[2 * r] = h ? recv : u[r];
 		x[2 * r + 1] = h ? v[r] : recv;
 	}
-	if constexpr (ROW) fft1d_acc<64, DIR>(x, tau & 7, RowHalf<C>{S, line, h * 64}, tw64);
-	else fft1d_acc<64, DIR>(x, tau & 7, ColHalf<C>{S, line, h * 64}, tw64);
+	if constexpr (ROW) fft1d_acc<64, DIR>(x, tau & 7, RowHalf<C>(S, line, h), tw64);
+	else fft1d_acc<64, DIR>(x, tau & 7, ColHalf<C>(S, line, h), tw64);
 }
 
 // 128-point transform by decimation in time of a column whose lane tau holds
@@ -83,7 +114,7 @@ __device__ __forceinline__ int dpos128(int tau, int i) { return (tau & 7) + 16 *
 template <int DIR, class C>
 __device__ __forceinline__ void fft128_dit_col(C (&x)[8], int tau, C *S, int col, const C *tw128, const C *tw64) {
 	const int h = tau >> 3, t = tau & 7;
-	fft1d_acc<64, DIR>(x, t, ColHalf<C>{S, col, h * 64}, tw64);
+	fft1d_acc<64, DIR>(x, t, ColHalf<C>(S, col, h), tw64);
 	C y[8];
 #pragma unroll
 	for (int j = 0; j < 4; j++) {
@@ -167,22 +198,22 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 					x[r] = v;
 				}
 				fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
+				const LineSlots ls_ = row_slots(row, tau);
 #pragma unroll
-				for (int e = 0; e < 8; e++) S[F::at(row, pos128(tau, e))] = x[e];
+				for (int e = 0; e < 8; e++) S[ls_.at_out(e)] = x[e];
 			}
 			__syncthreads();
 #pragma unroll 1
 			for (int it = 0; it < 4; it++) {
 				const int col = it * 32 + sub;
+				const LineSlots cs_ = col_slots(col, tau);
 				C x[8];
 #pragma unroll
-				for (int r = 0; r < 8; r++) {
-					const int row = tau + 16 * r;              // rows 32..95 are the zero band
-					x[r] = (r >= 2 && r < 6) ? czero<C>() : S[F::at(row, col)];
-				}
+				for (int r = 0; r < 8; r++)                     // rows tau + 16 r; 32..95 are the zero band
+					x[r] = (r >= 2 && r < 6) ? czero<C>() : S[cs_.at_in(r)];
 				fft128_line<-1, false>(x, tau, S, col, tw128, tw64);
 #pragma unroll
-				for (int e = 0; e < 8; e++) S[F::at(pos128(tau, e), col)] = x[e];
+				for (int e = 0; e < 8; e++) S[cs_.at_out(e)] = x[e];
 			}
 			__syncthreads();
 			C *Pq = Pall + (long)comp * F::P * F::P;
@@ -209,17 +240,19 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 #pragma unroll
 					for (int r = 0; r < 8; r++) x[r] = cmul(g[tau + 16 * r], pj[tau + 16 * r]);
 					fft128_line<+1, true>(x, tau, S, row, tw128, tw64);
+					const LineSlots ls_ = row_slots(row, tau);
 #pragma unroll
-					for (int e = 0; e < 8; e++) S[F::at(row, pos128(tau, e))] = x[e];
+					for (int e = 0; e < 8; e++) S[ls_.at_out(e)] = x[e];
 				}
 				__syncthreads();
 				// columns: inverse transform along l, psi2, forward transform
 #pragma unroll 1
 				for (int it = 0; it < 4; it++) {
 					const int col = it * 32 + sub;
+					const LineSlots cs_ = col_slots(col, tau);
 					C x[8];
 #pragma unroll
-					for (int r = 0; r < 8; r++) x[r] = S[F::at(tau + 16 * r, col)];
+					for (int r = 0; r < 8; r++) x[r] = S[cs_.at_in(r)];
 					fft128_line<+1, false>(x, tau, S, col, tw128, tw64);
 					const R *ps = psi2 + (long)col * F::P;
 #pragma unroll
@@ -229,8 +262,9 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 						x[e].y *= f;
 					}
 					fft128_dit_col<-1>(x, tau, S, col, tw128, tw64);
+					const int d0 = (tau & 7) + 8 * (tau >> 3);   // rows d0 + 16 (i / 2) + 64 (i % 2)
 #pragma unroll
-					for (int i = 0; i < 8; i++) S[F::at(dpos128(tau, i), col)] = x[i];
+					for (int i = 0; i < 8; i++) S[(d0 + 16 * (i >> 1) + 64 * (i & 1)) * F::LDP + cs_.cx[i & 1]] = x[i];
 				}
 				__syncthreads();
 				// rows: forward transform along k, times P_a, accumulate
@@ -240,9 +274,10 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 #pragma unroll 1
 				for (int it = 0; it < 4; it++) {
 					const int row = it * 32 + sub;
+					const LineSlots ls_ = row_slots(row, tau);
 					C x[8];
 #pragma unroll
-					for (int r = 0; r < 8; r++) x[r] = S[F::at(row, tau + 16 * r)];
+					for (int r = 0; r < 8; r++) x[r] = S[ls_.at_in(r)];
 					fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
 					const C *pa = Pa + (long)row * F::P;
 					C acc[8];

@@ -134,6 +134,35 @@ template <class C> struct Strided {
 	__device__ __forceinline__ C &operator()(int pos) const { return p[pos * stride]; }
 };
 
+// steps 3 and 4 of a length-L transform (see file comment): the transpose
+// among the T lanes through the scratch accessor sc, then the radix-T DFTs
+template <int L, int DIR, class C, class Acc>
+__device__ __forceinline__ void fft1d_tail(C (&x)[8], int tau, const Acc &sc) {
+	using G = Len<L>;
+	__syncwarp();
+#pragma unroll
+	for (int q = 0; q < 8; q++) sc(G::xpos(q, tau)) = x[q];
+	__syncwarp();
+#pragma unroll
+	for (int u = 0; u < G::U; u++)
+#pragma unroll
+		for (int s = 0; s < G::T; s++) x[u * G::T + s] = sc(G::xpos(tau * G::U + u, s));
+	__syncwarp();
+#pragma unroll
+	for (int u = 0; u < G::U; u++) {
+		if constexpr (G::T == 2) dft2(x[2 * u], x[2 * u + 1]);
+		else if constexpr (G::T == 4) dft4<DIR>(x[4 * u], x[4 * u + 1], x[4 * u + 2], x[4 * u + 3]);
+		else {
+			C y[8];
+#pragma unroll
+			for (int s = 0; s < 8; s++) y[s] = x[s];
+			dft8<DIR>(y);
+#pragma unroll
+			for (int s = 0; s < 8; s++) x[s] = y[s];
+		}
+	}
+}
+
 // Length-L transform of the 8 values in x (see file comment) with the
 // scratch accessor sc; its previous contents are destroyed.  `tw` is the table
 // of init_twiddles (tw[e] = w_L^e); a lane reads only its base twiddle
@@ -156,28 +185,25 @@ __device__ __forceinline__ void fft1d_acc(C (&x)[8], int tau, const Acc &sc, con
 			w = cmul(w, w1);
 			x[q] = cmul(x[q], w);
 		}
-		__syncwarp();
+		fft1d_tail<L, DIR>(x, tau, sc);
+	}
+}
+
+// the same with the lane's twiddle powers given: wp[q] = w_L^(tau q) of the
+// forward sign (conjugated here for DIR = +1), q = 1..7, e.g. computed once
+// per kernel by a lane whose tau does not change
+template <int L, int DIR, class C, class Acc>
+__device__ __forceinline__ void fft1d_accw(C (&x)[8], int tau, const Acc &sc, const C (&wp)[8]) {
+	using G = Len<L>;
+	dft8<DIR>(x);
+	if constexpr (G::T > 1) {
 #pragma unroll
-		for (int q = 0; q < 8; q++) sc(G::xpos(q, tau)) = x[q];
-		__syncwarp();
-#pragma unroll
-		for (int u = 0; u < G::U; u++)
-#pragma unroll
-			for (int s = 0; s < G::T; s++) x[u * G::T + s] = sc(G::xpos(tau * G::U + u, s));
-		__syncwarp();
-#pragma unroll
-		for (int u = 0; u < G::U; u++) {
-			if constexpr (G::T == 2) dft2(x[2 * u], x[2 * u + 1]);
-			else if constexpr (G::T == 4) dft4<DIR>(x[4 * u], x[4 * u + 1], x[4 * u + 2], x[4 * u + 3]);
-			else {
-				C y[8];
-#pragma unroll
-				for (int s = 0; s < 8; s++) y[s] = x[s];
-				dft8<DIR>(y);
-#pragma unroll
-				for (int s = 0; s < 8; s++) x[s] = y[s];
-			}
+		for (int q = 1; q < 8; q++) {
+			C w = wp[q];
+			if (DIR > 0) w.y = -w.y;
+			x[q] = cmul(x[q], w);
 		}
+		fft1d_tail<L, DIR>(x, tau, sc);
 	}
 }
 

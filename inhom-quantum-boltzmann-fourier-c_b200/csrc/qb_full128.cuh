@@ -79,7 +79,7 @@ __device__ __forceinline__ LineSlots col_slots(int col, int tau) {
 
 // fft128 with the line given as row (ROW) or column `line` of the shared grid
 template <int DIR, bool ROW, class C>
-__device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, const C *tw128, const C *tw64) {
+__device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, const C *tw128, const C (&wp)[8]) {
 	const int h = tau >> 3;
 	C u[4], v[4];
 #pragma unroll
@@ -96,8 +96,8 @@ __device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, 
 		x[2 * r] = h ? recv : u[r];
 		x[2 * r + 1] = h ? v[r] : recv;
 	}
-	if constexpr (ROW) fft1d_acc<64, DIR>(x, tau & 7, RowHalf<C>(S, line, h), tw64);
-	else fft1d_acc<64, DIR>(x, tau & 7, ColHalf<C>(S, line, h), tw64);
+	if constexpr (ROW) fft1d_accw<64, DIR>(x, tau & 7, RowHalf<C>(S, line, h), wp);
+	else fft1d_accw<64, DIR>(x, tau & 7, ColHalf<C>(S, line, h), wp);
 }
 
 // 128-point transform by decimation in time of a column whose lane tau holds
@@ -112,9 +112,9 @@ __device__ __forceinline__ void fft128_line(C (&x)[8], int tau, C *S, int line, 
 __device__ __forceinline__ int dpos128(int tau, int i) { return (tau & 7) + 16 * (i >> 1) + 8 * (tau >> 3) + 64 * (i & 1); }
 
 template <int DIR, class C>
-__device__ __forceinline__ void fft128_dit_col(C (&x)[8], int tau, C *S, int col, const C *tw128, const C *tw64) {
+__device__ __forceinline__ void fft128_dit_col(C (&x)[8], int tau, C *S, int col, const C *tw128, const C (&wp)[8]) {
 	const int h = tau >> 3, t = tau & 7;
-	fft1d_acc<64, DIR>(x, t, ColHalf<C>(S, col, h), tw64);
+	fft1d_accw<64, DIR>(x, t, ColHalf<C>(S, col, h), wp);
 	C y[8];
 #pragma unroll
 	for (int j = 0; j < 4; j++) {
@@ -164,6 +164,11 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 	__syncthreads();
 	tmem_fence_after();
 	const unsigned tbase = tmem_slot;
+	// the 64-point twiddle powers of this lane, w64^((tau & 7) q), for every transform of the kernel
+	C wp[8];
+	wp[0] = tw64[0];
+#pragma unroll
+	for (int q = 1; q < 8; q++) wp[q] = tw64[((tau & 7) * q) & 63];
 #pragma unroll 1
 	for (int q = 0; q < 2; q++)
 #pragma unroll 1
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 					}
 					x[r] = v;
 				}
-				fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
+				fft128_line<-1, true>(x, tau, S, row, tw128, wp);
 				const LineSlots ls_ = row_slots(row, tau);
 #pragma unroll
 				for (int e = 0; e < 8; e++) S[ls_.at_out(e)] = x[e];
@@ -211,7 +216,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 #pragma unroll
 				for (int r = 0; r < 8; r++)                     // rows tau + 16 r; 32..95 are the zero band
 					x[r] = (r >= 2 && r < 6) ? czero<C>() : S[cs_.at_in(r)];
-				fft128_line<-1, false>(x, tau, S, col, tw128, tw64);
+				fft128_line<-1, false>(x, tau, S, col, tw128, wp);
 #pragma unroll
 				for (int e = 0; e < 8; e++) S[cs_.at_out(e)] = x[e];
 			}
@@ -239,7 +244,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 					C x[8];
 #pragma unroll
 					for (int r = 0; r < 8; r++) x[r] = cmul(g[tau + 16 * r], pj[tau + 16 * r]);
-					fft128_line<+1, true>(x, tau, S, row, tw128, tw64);
+					fft128_line<+1, true>(x, tau, S, row, tw128, wp);
 					const LineSlots ls_ = row_slots(row, tau);
 #pragma unroll
 					for (int e = 0; e < 8; e++) S[ls_.at_out(e)] = x[e];
@@ -253,7 +258,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 					C x[8];
 #pragma unroll
 					for (int r = 0; r < 8; r++) x[r] = S[cs_.at_in(r)];
-					fft128_line<+1, false>(x, tau, S, col, tw128, tw64);
+					fft128_line<+1, false>(x, tau, S, col, tw128, wp);
 					const R *ps = psi2 + (long)col * F::P;
 #pragma unroll
 					for (int e = 0; e < 8; e++) {
@@ -261,7 +266,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 						x[e].x *= f;
 						x[e].y *= f;
 					}
-					fft128_dit_col<-1>(x, tau, S, col, tw128, tw64);
+					fft128_dit_col<-1>(x, tau, S, col, tw128, wp);
 					const int d0 = (tau & 7) + 8 * (tau >> 3);   // rows d0 + 16 (i / 2) + 64 (i % 2)
 #pragma unroll
 					for (int i = 0; i < 8; i++) S[(d0 + 16 * (i >> 1) + 64 * (i & 1)) * F::LDP + cs_.cx[i & 1]] = x[i];
@@ -278,7 +283,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 					C x[8];
 #pragma unroll
 					for (int r = 0; r < 8; r++) x[r] = S[ls_.at_in(r)];
-					fft128_line<-1, true>(x, tau, S, row, tw128, tw64);
+					fft128_line<-1, true>(x, tau, S, row, tw128, wp);
 					const C *pa = Pa + (long)row * F::P;
 					C acc[8];
 					tmem_ld8(TM::addr(tbase, q, it, 0), acc);

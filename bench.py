@@ -28,7 +28,8 @@ the 1024 x-cells of the N = 64, J = M = 32 precision-form configuration, FP64
 and FP32 timed alike; --no-config2 skips it), and `surrogate` (a Fourier
 neural operator trained here on homogeneous relaxation data, used for the
 collision half of the same Strang steps with the exact operator as judge
-every 10th step and as per-cell fallback; --no-surrogate skips it).
+every 10th step and as per-cell fallback; --no-surrogate skips it);
+--surrogate-n64 adds the same at N = 64, J = M = 32 (`surrogate_n64`).
 """
 import argparse
 import importlib.util
@@ -290,6 +291,9 @@ def run_ours(args):
     sur = None
     if world == 1 and not args.no_surrogate:
         sur = run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value)
+    sur64 = None
+    if world == 1 and args.surrogate_n64:
+        sur64 = run_surrogate64(args, qbgpu, flush)
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
@@ -303,6 +307,8 @@ def run_ours(args):
         line["config2_sample"] = big
     if sur is not None:
         line["surrogate"] = sur
+    if sur64 is not None:
+        line["surrogate_n64"] = sur64
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind = ref_kind()
         procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
@@ -415,11 +421,12 @@ def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
             "bound": 1e-5}
 
 
-def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=2048, samples=3, iters=8000, lr=5e-3):
+def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samples=3, iters=8000, lr=5e-3):
     """The learned collision operator on the same workload and timing
     protocol.  A Fourier neural operator (width 32, 12 modes, 4 layers) is
     trained on (W, Cc + Cd) pairs of `nseeds` seeded mixture cells and their
-    homogeneous relaxation (exact FP64 operator), then drives the collision
+    homogeneous relaxation (exact FP64 operator), each minibatch turned by
+    random spin rotations (the operator commutes with them), then drives the collision
     half of the Strang steps: the exact operator judges every 10th step and
     takes over, until the next check, the cells whose relative L1 error of C
     was above 0.5.  Reported: the rate, the training cost, the network's error
@@ -435,7 +442,7 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=2048, samp
     net = qbgpu.FNO(N, width=32, modes=12, layers=4, seed=1)
     net.fit_scales(X, Y)
     t0 = time.perf_counter()
-    loss = qbgpu.train_fno(net, X, Y, iters, batch=64, lr=lr)
+    loss = qbgpu.train_fno(net, X, Y, iters, batch=64, lr=lr, spin_rotations=True)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     del X, Y
@@ -473,11 +480,81 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=2048, samp
                     f"the timed region",
             "value": round(value, 3), "unit": UNIT, "ms_per_step": round(ms / args.steps, 4),
             "speedup_vs_fp64": round(value / value64, 4),
-            "training": {"pairs": nseeds * samples, "iterations": iters, "batch": 64, "lr": lr, "final_loss": loss,
+            "training": {"pairs": nseeds * samples, "iterations": iters, "batch": 64, "lr": lr, "spin_rotations": True, "final_loss": loss,
                          "data_s": round(t_data, 2), "train_s": round(t_train, 2), "params": net.num_params},
             "C_rel_l1_on_initial_state": round(c_err, 5),
             "cell_steps": {"surrogate": ns, "exact": ne}, "last_max_residual": round(res, 5),
             f"W_rel_l1_vs_fp64_after_{args.warmup + args.steps}_steps": rel(bufs[cur], a)}
+
+
+def run_surrogate64(args, qbgpu, flush, cells=64, nseeds=1024, samples=3, iters=8000, lr=5e-3, steps=10, warmup=3):
+    """The learned collision operator at N = 64 (the shape of the surrogate
+    configuration: J = M = 32, FNO of 4 layers, width 32, 12 modes), on `cells`
+    of a 4096-cell periodic domain (h = 1/4096).  Training pairs and the judge
+    use the FP32 form of the exact operator (its C error against FP64 is about
+    1e-6); the plain FP64 Strang step is timed alike for the ratio.  The exact
+    operator judges every 10th step and takes over the cells whose relative L1
+    error of C was above 0.5 until the next check."""
+    import torch
+    N, J, M, L, R = 64, 32, 32, 6.0, 3.75
+    h = 1.0 / 4096
+    dt = 0.4 * h / L
+    q = qbgpu.Quad(N, J, M, L, R)
+    ws32, ws64 = qbgpu.Workspace(N, precision=32), qbgpu.Workspace(N)
+    t0 = time.perf_counter()
+    X, Y = qbgpu.relaxation_pairs(ws32, q, torch.from_numpy(qbgpu.mixture_cells(N, L, nseeds, 7000)).cuda(), samples)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net = qbgpu.FNO(N, width=32, modes=12, layers=4, seed=1)
+    net.fit_scales(X, Y)
+    t0 = time.perf_counter()
+    loss = qbgpu.train_fno(net, X, Y, iters, batch=64, lr=lr, spin_rotations=True)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del X, Y
+
+    def rel(a, b):
+        a, b = a.cpu().numpy().ravel(), b.cpu().numpy().ravel()
+        return float(np.abs(a - b).sum() / np.abs(b).sum())
+    W0 = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=4, ncells=cells)).cuda()
+    B = torch.zeros((cells, 3), dtype=torch.float64, device="cuda")
+    cc, cd = qbgpu.collision_operators(ws64, q, qbgpu.to_fourier(W0))
+    c_err = rel(net.forward(W0), qbgpu.from_fourier(cc + cd))
+
+    def timed(stepfn, n, w):
+        bufs = [W0.clone(), torch.empty_like(W0)]
+        for i in range(w):
+            stepfn(bufs[i % 2], bufs[(i + 1) % 2])
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        cur = w % 2
+        for k in range(n):
+            flush.zero_()
+            evs[k][0].record()
+            stepfn(bufs[cur], bufs[1 - cur])
+            evs[k][1].record()
+            cur = 1 - cur
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / n, bufs[cur]
+    ms64, W64 = timed(lambda a, b: qbgpu.inhom_step(ws64, q, a, h, dt, B, out=b), 2, 1)
+    tol, every = 0.5, 10
+    sur = qbgpu.Surrogate(net, tol=tol, check_every=every)
+    ms_sur, Wsur = timed(lambda a, b: sur.step(ws32, q, a, h, dt, B, out=b), steps, warmup)
+    ns, ne, res = sur.stats()
+    a = W0.clone()
+    for _ in range(warmup + steps):
+        a = qbgpu.inhom_step(ws64, q, a, h, dt, B)
+    torch.cuda.synchronize()
+    return {"workload": f"N={N} (padded {2 * N}), J={J}, M={M}, {cells} of 4096 x-cells, h=1/4096, dt=0.4h/L, periodic; "
+                        f"FNO width 32, 12 modes, 4 layers; judge: FP32 form of the exact operator every {every}th step "
+                        f"(inside the timed region), per-cell fallback above relative L1 error {tol}",
+            "unit": UNIT, "fp64": {"value": round(cells * 2 / (ms64 * 1e-3), 3), "ms_per_step": round(ms64, 3)},
+            "surrogate": {"value": round(cells * 2 / (ms_sur * 1e-3), 3), "ms_per_step": round(ms_sur, 3)},
+            "speedup_vs_fp64": round(ms64 / ms_sur, 3),
+            "training": {"pairs": nseeds * samples, "data": "FP32 form", "iterations": iters, "batch": 64, "lr": lr,
+                         "spin_rotations": True, "final_loss": loss, "data_s": round(t_data, 2), "train_s": round(t_train, 2)},
+            "C_rel_l1_on_initial_state": round(c_err, 5), "cell_steps": {"surrogate": ns, "exact": ne},
+            "last_max_residual": round(res, 5), f"W_rel_l1_vs_fp64_after_{warmup + steps}_steps": rel(Wsur, a)}
 
 
 def run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall):
@@ -589,6 +666,7 @@ def main():
     ap.add_argument("--no-config2", action="store_true", help="skip the N = 64 precision-form sample")
     ap.add_argument("--config2-cells", type=int, default=64, help="x-cells of the N = 64 sample (of its 1024)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
+    ap.add_argument("--surrogate-n64", action="store_true", help="add the learned operator at N = 64 (about two minutes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -559,7 +559,11 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
 				const R coef = (R)p.ccoef[j][c];
 				C acc[8];
-				tmem_ld8(TM::addr(tbase, q, 0), acc);
+				if constexpr (sizeof(C) == 16) tmem_ld8(TM::addr(tbase, q, 0), acc);   // one load (FP64); FP32 per value measured faster
+				else {
+#pragma unroll
+					for (int e = 0; e < 8; e++) tmem_ld(TM::addr(tbase, q, e), acc[e]);
+				}
 				tmem_wait_ld();
 #pragma unroll
 				for (int e = 0; e < 8; e++) {
@@ -567,7 +571,11 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					acc[e].x += coef * v.x;
 					acc[e].y += coef * v.y;
 				}
-				tmem_st8(TM::addr(tbase, q, 0), acc);
+				if constexpr (sizeof(C) == 16) tmem_st8(TM::addr(tbase, q, 0), acc);
+				else {
+#pragma unroll
+					for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, e), acc[e]);
+				}
 				tmem_wait_st();
 				// no barrier here: the row passes that end this pair and begin the
 				// next touch only the rows of their own 8-lane group, and the next

@@ -353,16 +353,45 @@ def relaxation_pairs(ws, q, W, samples, every=5, dt=0.02):
     return torch.cat(X), torch.cat(Y)
 
 
-def train_fno(net, X, Y, iters, batch=64, lr=2e-3, seed=0):
+def random_rotations(n, generator):
+    """n uniformly distributed 3 x 3 rotation matrices (float64, CPU): unit
+    quaternions from normal variates"""
+    import torch
+    qv = torch.randn((n, 4), dtype=torch.float64, generator=generator)
+    a, b, c, d = (qv / qv.norm(dim=1, keepdim=True)).unbind(1)
+    return torch.stack([
+        torch.stack([a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)], 1),
+        torch.stack([2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)], 1),
+        torch.stack([2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d], 1)], 1)
+
+
+def rotate_spin(W, Rm):
+    """the Pauli vector components (1..3) of states or operators W (B, 4, N, N)
+    rotated by the matrices Rm (B, 3, 3); component 0 is unchanged"""
+    import torch
+    out = W.clone()
+    out[:, 1:4] = torch.einsum("bij,bjkl->bikl", Rm, W[:, 1:4])
+    return out
+
+
+def train_fno(net, X, Y, iters, batch=64, lr=2e-3, seed=0, spin_rotations=False):
     """`iters` Adam steps on random minibatches of the pairs (X, Y) with a
-    cosine learning-rate schedule from lr to 0; returns the last loss"""
+    cosine learning-rate schedule from lr to 0; returns the last loss.
+    spin_rotations: rotate the Pauli vector of every pair of a minibatch by a
+    random rotation, which maps a pair (W, C[W]) to the pair (RW, RC[W]) =
+    (RW, C[RW]) of the same operator (the collision operator commutes with
+    global spin rotations)."""
     torch = _torch()
     g = torch.Generator(device="cpu").manual_seed(seed)
     loss = float("nan")
     for it in range(iters):
         idx = torch.randint(0, X.shape[0], (batch,), generator=g).to(X.device)
         a = lr * 0.5 * (1 + math.cos(math.pi * it / iters))
-        loss = net.train_step(X[idx].contiguous(), Y[idx].contiguous(), a)
+        xb, yb = X[idx], Y[idx]
+        if spin_rotations:
+            Rm = random_rotations(batch, g).to(X.device)
+            xb, yb = rotate_spin(xb, Rm), rotate_spin(yb, Rm)
+        loss = net.train_step(xb.contiguous(), yb.contiguous(), a)
     return loss
 
 

@@ -90,7 +90,7 @@ def trained16():
     net = qbgpu.FNO(N, width=32, modes=6, layers=4, seed=2)
     net.fit_scales(X, Y)
     e0 = rel_l1(net.forward(Xt).cpu().numpy(), Yt.cpu().numpy())
-    qbgpu.train_fno(net, X, Y, 4000, lr=5e-3)
+    qbgpu.train_fno(net, X, Y, 4000, lr=5e-3, spin_rotations=True)
     e1 = rel_l1(net.forward(Xt).cpu().numpy(), Yt.cpu().numpy())
     return dict(N=N, J=J, M=M, net=net, e0=e0, e1=e1)
 

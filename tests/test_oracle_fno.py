@@ -3,6 +3,7 @@
 analytic gradient is pinned by central finite differences of its own loss, and
 its spectral layer by the properties of the transform it restates."""
 import numpy as np
+import pytest
 
 import fno_ref
 
@@ -69,3 +70,29 @@ def test_flatten_roundtrip():
     w, m, L = 3, 2, 2
     theta = np.arange(fno_ref.num_params(w, m, L), dtype=np.float64)
     assert np.array_equal(fno_ref.flatten(fno_ref.unflatten(theta, w, m, L), w, m, L), theta)
+
+
+def test_collision_operator_commutes_with_spin_rotations():
+    """the premise of training the surrogate on spin-rotated pairs: for a global
+    rotation R of the Pauli vector, C[R W] = R C[W] (oracle, N = 8)"""
+    import orc
+    import qbgpu
+    N, J, M, L, R = 8, 4, 3, 6.0, 3.75
+    o = orc.Oracle(N, J, M, L, R)
+    W = qbgpu.gaussian_mixture_state(N, L, seed=3, ncells=1)[0]
+    torch = pytest.importorskip("torch")
+    Rm = qbgpu.random_rotations(1, torch.Generator().manual_seed(1))
+    assert float((Rm[0] @ Rm[0].T - torch.eye(3, dtype=torch.float64)).abs().max()) < 1e-14
+    Q = Rm[0].numpy()
+
+    def rot(X):
+        Y = X.copy()
+        Y[1:4] = np.einsum("ij,jkl->ikl", Q, X[1:4])
+        return Y
+    # the device helper applies the same rotation
+    Wt = torch.from_numpy(W[None].copy())
+    assert np.abs(qbgpu.rotate_spin(Wt, Rm)[0].numpy() - rot(W)).max() < 1e-15
+    Wf, WRf = orc.to_fourier(W[None])[0], orc.to_fourier(rot(W)[None])[0]
+    c0 = o.cc(Wf) + o.cd(Wf)
+    c1 = o.cc(WRf) + o.cd(WRf)
+    assert np.abs(c1 - rot(c0)).max() <= 1e-12 * np.abs(c0).max()

@@ -456,6 +456,15 @@ __device__ __forceinline__ void tmem_st8(unsigned taddr, const float2 (&v)[8]) {
 	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
 }
 
+// FP32: the lane's twiddle powers precomputed once (wp, fft1d_accw), fewer
+// instructions in an issue-bound kernel; FP64: the power recurrence of
+// fft1d_acc (registers are exhausted there)
+template <int L, int DIR, class C, class Acc>
+__device__ __forceinline__ void fft1d_lane(C (&x)[8], int tau, const Acc &sc, const C *tw, const C (&wp)[8]) {
+	if constexpr (sizeof(C) == 8) fft1d_accw<L, DIR>(x, tau, sc, wp);
+	else fft1d_acc<L, DIR>(x, tau, sc, tw);
+}
+
 // TMEM accumulators of k_i3p: 2 outputs x 8 values per thread
 template <class C> struct I3Tmem {
 	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
@@ -501,6 +510,11 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 	tmem_fence_after();
 	const unsigned tbase = tmem_slot;
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	C wp[8];
+	if constexpr (sizeof(C) == 8) {
+#pragma unroll
+		for (int q = 0; q < 8; q++) wp[q] = tw[(tau * q) & (P - 1)];
+	}
 #pragma unroll
 	for (int q = 0; q < 2; q++)
 #pragma unroll
@@ -532,14 +546,14 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					const int k = tau + G::T * r;
 					x[r] = cmul(Gg[line * P + k], Pj[G::at(line, k)]);
 				}
-				fft1d_acc<P, +1>(x, tau, G::row(Ug, line), tw);
+				fft1d_lane<P, +1>(x, tau, G::row(Ug, line), tw, wp);
 #pragma unroll
 				for (int e = 0; e < 8; e++) Ug[G::at(line, Lp::out_pos(tau, e))] = x[e];
 				__syncthreads();
 				// columns: IFFT, multiply by psi2_t, FFT
 #pragma unroll
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
-				fft1d_acc<P, +1>(x, tau, G::col(Ug, line), tw);
+				fft1d_lane<P, +1>(x, tau, G::col(Ug, line), tw, wp);
 #pragma unroll
 				for (int e = 0; e < 8; e++) {
 					const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
@@ -547,14 +561,14 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					x[e].y *= f;
 				}
 				out_to_in_acc<P>(x, tau, G::col(Ug, line));
-				fft1d_acc<P, -1>(x, tau, G::col(Ug, line), tw);
+				fft1d_lane<P, -1>(x, tau, G::col(Ug, line), tw, wp);
 #pragma unroll
 				for (int e = 0; e < 8; e++) Ug[G::at(Lp::out_pos(tau, e), line)] = x[e];
 				__syncthreads();
 				// rows: FFT, multiply by P_a (own or the partner's), accumulate in TMEM
 #pragma unroll
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
-				fft1d_acc<P, -1>(x, tau, G::row(Ug, line), tw);
+				fft1d_lane<P, -1>(x, tau, G::row(Ug, line), tw, wp);
 				const int a = p.ca[j][c];
 				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
 				const R coef = (R)p.ccoef[j][c];

@@ -428,8 +428,8 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samp
     homogeneous relaxation (exact FP64 operator), each minibatch turned by
     random spin rotations (the operator commutes with them), then drives the collision
     half of the Strang steps: the exact operator judges every 10th step and
-    takes over, until the next check, the cells whose relative L1 error of C
-    was above 0.5.  Reported: the rate, the training cost, the network's error
+    takes over, until the next check, the cells whose collision increment from
+    the network differed from the exact one by more than 0.5 (relative L1).  Reported: the rate, the training cost, the network's error
     on the workload's initial state, how many cell-steps each operator took,
     and the state's deviation from the FP64 run after the same steps."""
     import torch
@@ -476,7 +476,8 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samp
         a = qbgpu.inhom_step(ws, q, a, wl["h"], wl["dt"], B)
     torch.cuda.synchronize()
     return {"what": f"Strang steps with the collision half from a Fourier neural operator (FP32), exact FP64 operator as judge "
-                    f"every {every}th step and per-cell fallback above relative L1 error {tol}; the checking steps are inside "
+                    f"every {every}th step and per-cell fallback above a relative L1 difference {tol} of the collision increment; "
+                    f"the checking steps are inside "
                     f"the timed region",
             "value": round(value, 3), "unit": UNIT, "ms_per_step": round(ms / args.steps, 4),
             "speedup_vs_fp64": round(value / value64, 4),
@@ -493,8 +494,9 @@ def run_surrogate64(args, qbgpu, flush, cells=64, nseeds=1024, samples=3, iters=
     of a 4096-cell periodic domain (h = 1/4096).  Training pairs and the judge
     use the FP32 form of the exact operator (its C error against FP64 is about
     1e-6); the plain FP64 Strang step is timed alike for the ratio.  The exact
-    operator judges every 10th step and takes over the cells whose relative L1
-    error of C was above 0.5 until the next check."""
+    operator judges every 10th step and takes over the cells whose collision
+    increment from the network differed from the exact one by more than 0.5
+    (relative L1) until the next check."""
     import torch
     N, J, M, L, R = 64, 32, 32, 6.0, 3.75
     h = 1.0 / 4096
@@ -547,7 +549,7 @@ def run_surrogate64(args, qbgpu, flush, cells=64, nseeds=1024, samples=3, iters=
     torch.cuda.synchronize()
     return {"workload": f"N={N} (padded {2 * N}), J={J}, M={M}, {cells} of 4096 x-cells, h=1/4096, dt=0.4h/L, periodic; "
                         f"FNO width 32, 12 modes, 4 layers; judge: FP32 form of the exact operator every {every}th step "
-                        f"(inside the timed region), per-cell fallback above relative L1 error {tol}",
+                        f"(inside the timed region), per-cell fallback above a relative L1 difference {tol} of the collision increment",
             "unit": UNIT, "fp64": {"value": round(cells * 2 / (ms64 * 1e-3), 3), "ms_per_step": round(ms64, 3)},
             "surrogate": {"value": round(cells * 2 / (ms_sur * 1e-3), 3), "ms_per_step": round(ms_sur, 3)},
             "speedup_vs_fp64": round(ms64 / ms_sur, 3),

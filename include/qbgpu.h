@@ -226,9 +226,10 @@ int qb_fno_train_step(qb_fno *net, int batch, const double *W, const double *tar
 
 /* Strang step (the step of qb_inhom_step, periodic boundaries) whose
  * collision half uses the network with the exact operator as judge:
- *  - every `check_every`-th step (the first included) evaluates both, takes
- *    the exact collision for every cell, and marks for the following steps
- *    each cell whose relative L1 error of C was above `tol`;
+ *  - every `check_every`-th step (the first included) runs both collision
+ *    steps on every cell, keeps the exact one, and marks for the following
+ *    steps each cell whose collision increment from the network differs from
+ *    the exact increment by more than `tol` (relative L1);
  *  - the other steps take the network's C (a midpoint step with the magnetic
  *    term and a network evaluation at the midpoint) for unmarked cells and
  *    the exact collision for marked ones.
@@ -243,7 +244,7 @@ void qb_surrogate_free(qb_surrogate *s);
 int qb_surrogate_inhom_step(qb_surrogate *s, qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
                             double h, double dt, const double *Bext, void *stream);
 /* cell-steps taken by the network and by the exact operator so far, and the
- * largest residual of the last check step */
+ * largest residual (relative increment difference) of the last check step */
 int qb_surrogate_stats(const qb_surrogate *s, long *surrogate_cells, long *exact_cells, double *last_max_residual);
 
 #ifdef __cplusplus

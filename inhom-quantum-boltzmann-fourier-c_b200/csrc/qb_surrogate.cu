@@ -14,12 +14,14 @@
 // projected so that the trace component conserves mass, momentum and energy:
 // c0 -= |w0| (l0 + l1 i + l2 j + l3 (i^2 + j^2)) with the l solving the 4 x 4
 // normal equations, (i, j) the velocity in units of the grid spacing (the
-// same span as the physical velocities).  Every `check_every`-th step evaluates both operators
-// on every cell, takes the exact step, and marks the cells whose relative
-// L1 error of C~ exceeds `tol`; marked cells take the exact step until the
-// next check.  Only the library's public entry points are used for the exact
-// operator (qb_to_fourier, qb_collision_operators, qb_from_fourier,
-// qb_fourier_collision), so the judge is the same code the parity tests pin.
+// same span as the physical velocities).  Every `check_every`-th step runs
+// both the network's step and the exact one on every cell, keeps the exact one, and
+// marks the cells whose collision increment from the network differs from the
+// exact increment by more than `tol` (relative L1); marked cells take the
+// exact step until the next check.  Judging the step rather than C itself
+// costs no evaluation of the exact operator beyond the exact step.  The exact
+// operator is reached only through the library's public entry point
+// qb_fourier_collision, so the judge is the same code the parity tests pin.
 #include "qb_engine.h"
 
 extern "C" {
@@ -131,24 +133,20 @@ __global__ void k_stage(int NN, int ncells, const double *__restrict__ V, const 
 	}
 }
 
-// out[cell] = sum |A - B| / sum |B| over the cell's `per` values
-__global__ void __launch_bounds__(kThreads) k_residual(long per, const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ out) {
+// out[cell] = sum |A - B| / sum |B - V| over the cell's `per` values: the
+// relative L1 difference of two steps A, B from the same state V, measured on
+// the increment B - V
+__global__ void __launch_bounds__(kThreads) k_step_residual(long per, const double *__restrict__ A, const double *__restrict__ B,
+                                                            const double *__restrict__ V, double *__restrict__ out) {
 	__shared__ double red[2];
-	const double *a = A + blockIdx.x * per, *b = B + blockIdx.x * per;
+	const double *a = A + blockIdx.x * per, *b = B + blockIdx.x * per, *v = V + blockIdx.x * per;
 	double acc[2] = { 0, 0 };
 	for (long p = threadIdx.x; p < per; p += kThreads) {
 		acc[0] += fabs(a[p] - b[p]);
-		acc[1] += fabs(b[p]);
+		acc[1] += fabs(b[p] - v[p]);
 	}
 	block_sums<2>(acc, red);
 	if (threadIdx.x == 0) out[blockIdx.x] = red[1] > 0 ? red[0] / red[1] : (red[0] > 0 ? INFINITY : 0.0);
-}
-
-__global__ void k_add2(long n, double2 *__restrict__ a, const double2 *__restrict__ b) {
-	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-		const double2 x = a[i], y = b[i];
-		a[i] = make_double2(x.x + y.x, x.y + y.y);
-	}
 }
 
 // dst[k] = src[idx[k]] (to_gathered) or dst[idx[k]] = src[k], cells of `per` doubles
@@ -186,7 +184,7 @@ struct qb_surrogate {
 	std::vector<unsigned char> exact;            // per cell: take the exact step until the next check
 	std::vector<int> idx;
 	std::vector<double> resid_h;
-	qb::DevBuf vt, vm, vc, c1, cx, f, fc, fd, resid, gath, bg, didx;
+	qb::DevBuf vt, vm, vc, c1, vs, resid, gath, bg, didx;
 };
 
 extern "C" {
@@ -235,23 +233,30 @@ int qb_surrogate_inhom_step(qb_surrogate *sg, qb_workspace *ws, const qb_quad *q
 
 		api(qb_transport(N, L, ncells, W, Vt, h, 0.5 * dt, 0, s), "transport");
 		const bool check = (sg->step % sg->check_every == 0) || sg->exact.size() != (size_t)ncells;
-		if (check) {
-			sg->cx.ensure(sizeof(double) * cs * ncells);
-			sg->f.ensure(sizeof(double2) * cs * ncells);
-			sg->fc.ensure(sizeof(double2) * cs * ncells);
-			sg->fd.ensure(sizeof(double2) * cs * ncells);
-			sg->resid.ensure(sizeof(double) * ncells);
+		// the network's midpoint step of every cell from Vt into out
+		auto network_step = [&](double *out) {
+			sg->vm.ensure(sizeof(double) * cs * ncells);
+			double *Vm = sg->vm.as<double>();
+			const long nv = (long)ncells * NN;
 			api(qb_fno_forward(sg->net, ncells, Vt, C1, s), "network");
 			launch("surrogate_project", k_project, ncells, kThreads, s, N, C1, (const double *)Vt);
-			api(qb_to_fourier(N, 4 * ncells, Vt, sg->f.p, s), "to_fourier");
-			api(qb_collision_operators(ws, q, ncells, sg->f.p, 3, sg->fc.p, sg->fd.p, s), "collision operators");
-			launch("surrogate_add", k_add2, grid_for(cs * ncells), 256, s, cs * ncells, sg->fc.as<double2>(), (const double2 *)sg->fd.as<double2>());
-			api(qb_from_fourier(N, 4 * ncells, sg->fc.p, sg->cx.as<double>(), s), "from_fourier");
-			launch("surrogate_residual", k_residual, ncells, kThreads, s, cs, (const double *)C1, (const double *)sg->cx.as<double>(), sg->resid.as<double>());
-			sg->resid_h.resize(ncells);
-			QB_CUDA(cudaMemcpyAsync(sg->resid_h.data(), sg->resid.p, sizeof(double) * ncells, cudaMemcpyDeviceToHost, s));
+			launch("surrogate_stage", k_stage, grid_for(nv), 256, s, NN, ncells, (const double *)Vt, (const double *)Vt, (const double *)C1, Bext, 0.5 * dt, Vm);
+			api(qb_fno_forward(sg->net, ncells, Vm, C1, s), "network");
+			launch("surrogate_project", k_project, ncells, kThreads, s, N, C1, (const double *)Vm);
+			launch("surrogate_stage", k_stage, grid_for(nv), 256, s, NN, ncells, (const double *)Vt, (const double *)Vm, (const double *)C1, Bext, dt, out);
+		};
+		if (check) {
+			// both steps on every cell; the exact one is kept, the network's is
+			// judged by the relative L1 difference of its collision increment
+			sg->vs.ensure(sizeof(double) * cs * ncells);
+			sg->resid.ensure(sizeof(double) * ncells);
+			network_step(sg->vs.as<double>());
 			QB_CUDA(cudaMemcpyAsync(Vc, Vt, sizeof(double) * cs * ncells, cudaMemcpyDeviceToDevice, s));
 			api(qb_fourier_collision(ws, q, ncells, Vc, Bext, dt, s), "exact collision");
+			launch("surrogate_residual", k_step_residual, ncells, kThreads, s, cs, (const double *)sg->vs.as<double>(), (const double *)Vc,
+			       (const double *)Vt, sg->resid.as<double>());
+			sg->resid_h.resize(ncells);
+			QB_CUDA(cudaMemcpyAsync(sg->resid_h.data(), sg->resid.p, sizeof(double) * ncells, cudaMemcpyDeviceToHost, s));
 			QB_CUDA(cudaStreamSynchronize(s));
 			sg->exact.assign(ncells, 0);
 			double mx = 0;
@@ -263,15 +268,7 @@ int qb_surrogate_inhom_step(qb_surrogate *sg, qb_workspace *ws, const qb_quad *q
 			sg->last_res = mx;
 			sg->n_ex += ncells;
 		} else {
-			sg->vm.ensure(sizeof(double) * cs * ncells);
-			double *Vm = sg->vm.as<double>();
-			const long nv = (long)ncells * NN;
-			api(qb_fno_forward(sg->net, ncells, Vt, C1, s), "network");
-			launch("surrogate_project", k_project, ncells, kThreads, s, N, C1, (const double *)Vt);
-			launch("surrogate_stage", k_stage, grid_for(nv), 256, s, NN, ncells, (const double *)Vt, (const double *)Vt, (const double *)C1, Bext, 0.5 * dt, Vm);
-			api(qb_fno_forward(sg->net, ncells, Vm, C1, s), "network");
-			launch("surrogate_project", k_project, ncells, kThreads, s, N, C1, (const double *)Vm);
-			launch("surrogate_stage", k_stage, grid_for(nv), 256, s, NN, ncells, (const double *)Vt, (const double *)Vm, (const double *)C1, Bext, dt, Vc);
+			network_step(Vc);
 			sg->idx.clear();
 			for (int c = 0; c < ncells; c++) if (sg->exact[c]) sg->idx.push_back(c);
 			const int nf = (int)sg->idx.size();

@@ -398,7 +398,8 @@ def train_fno(net, X, Y, iters, batch=64, lr=2e-3, seed=0, spin_rotations=False)
 class Surrogate:
     """Strang steps whose collision half takes the network's C~ with the exact
     operator as judge every `check_every` steps and as per-cell fallback where
-    the relative L1 error of C~ exceeded `tol` (qb_surrogate_inhom_step)."""
+    the network's collision increment differed from the exact one by more
+    than `tol`, relative L1 (qb_surrogate_inhom_step)."""
 
     def __init__(self, net, tol=0.3, check_every=10):
         self.net = net                       # the surrogate holds the network: keep it alive
@@ -419,7 +420,8 @@ class Surrogate:
         return out
 
     def stats(self):
-        """(surrogate cell-steps, exact cell-steps, largest residual of the last check)"""
+        """(surrogate cell-steps, exact cell-steps, largest residual of the last check:
+        the relative L1 difference of the network's collision increment)"""
         a, b, r = C.c_long(), C.c_long(), C.c_double()
         _check(lib().qb_surrogate_stats(self.h, C.byref(a), C.byref(b), C.byref(r)), "qb_surrogate_stats")
         return a.value, b.value, r.value

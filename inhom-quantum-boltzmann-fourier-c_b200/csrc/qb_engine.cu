@@ -244,7 +244,7 @@ template <class C> int active_i3p_clusters() {
 		set_smem(kern, i3p_smem<C>());
 		int per_sm = 0;
 		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Geo<64>::NT, i3p_smem<C>()));
-		if (per_sm * (int)I3Tmem<C>::NCOLS > 512)
+		if (per_sm * (int)I3Tmem<C>::ALLOC > 512)
 			QB_FAIL("k_i3p: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
 		cudaLaunchConfig_t cfg = {};
 		cfg.gridDim = dim3(2);

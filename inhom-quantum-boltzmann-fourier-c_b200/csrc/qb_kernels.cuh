@@ -456,13 +456,64 @@ __device__ __forceinline__ void tmem_st8(unsigned taddr, const float2 (&v)[8]) {
 	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
 }
 
-// FP32: the lane's twiddle powers precomputed once (wp, fft1d_accw), fewer
-// instructions in an issue-bound kernel; FP64: the power recurrence of
-// fft1d_acc (registers are exhausted there)
+// four consecutive FP64 complex values (16 columns) in one load or store
+__device__ __forceinline__ void tmem_ld4(unsigned taddr, double2 (&v)[4]) {
+	unsigned r[16];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int e = 0; e < 4; e++) {
+		v[e].x = __hiloint2double((int)r[4 * e + 1], (int)r[4 * e]);
+		v[e].y = __hiloint2double((int)r[4 * e + 3], (int)r[4 * e + 2]);
+	}
+}
+__device__ __forceinline__ void tmem_st4(unsigned taddr, const double2 (&v)[4]) {
+	unsigned r[16];
+#pragma unroll
+	for (int e = 0; e < 4; e++) {
+		r[4 * e] = (unsigned)__double2loint(v[e].x); r[4 * e + 1] = (unsigned)__double2hiint(v[e].x);
+		r[4 * e + 2] = (unsigned)__double2loint(v[e].y); r[4 * e + 3] = (unsigned)__double2hiint(v[e].y);
+	}
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
+}
+
+// length-L transform with the lane's twiddle powers w_L^(tau q), q = 1..7
+// (forward sign), read from tensor memory at taddr (4 complex FP64 values at
+// taddr, 3 more at taddr + 16): the loads are issued before the first
+// radix-8 stage and waited for after it
+template <int L, int DIR, class Acc>
+__device__ __forceinline__ void fft1d_acct(double2 (&x)[8], int tau, const Acc &sc, unsigned taddr) {
+	double2 w[4];
+	tmem_ld4(taddr, w);
+	dft8<DIR>(x);
+	tmem_wait_ld();
+#pragma unroll
+	for (int q = 1; q <= 4; q++) {
+		double2 v = w[q - 1];
+		if (DIR > 0) v.y = -v.y;
+		x[q] = cmul(x[q], v);
+	}
+	tmem_ld4(taddr + 16, w);
+	tmem_wait_ld();
+#pragma unroll
+	for (int q = 5; q < 8; q++) {
+		double2 v = w[q - 5];
+		if (DIR > 0) v.y = -v.y;
+		x[q] = cmul(x[q], v);
+	}
+	fft1d_tail<L, DIR>(x, tau, sc);
+}
+
+// the lane's twiddle powers computed once per kernel: FP32 in registers (wp,
+// fft1d_accw), FP64 in tensor memory (registers are exhausted there; the
+// loads replace the six complex multiplies of the power recurrence and add
+// no shared-memory traffic)
 template <int L, int DIR, class C, class Acc>
-__device__ __forceinline__ void fft1d_lane(C (&x)[8], int tau, const Acc &sc, const C *tw, const C (&wp)[8]) {
+__device__ __forceinline__ void fft1d_lane(C (&x)[8], int tau, const Acc &sc, const C (&wp)[8], unsigned twaddr) {
 	if constexpr (sizeof(C) == 8) fft1d_accw<L, DIR>(x, tau, sc, wp);
-	else fft1d_acc<L, DIR>(x, tau, sc, tw);
+	else fft1d_acct<L, DIR>(x, tau, sc, twaddr);
 }
 
 // TMEM accumulators of k_i3p: 2 outputs x 8 values per thread
@@ -470,10 +521,16 @@ template <class C> struct I3Tmem {
 	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
 	static constexpr unsigned PER_THREAD = 2 * 8 * WPC;       // columns of one thread's slice
 	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 4 warps share a lane quarter: 256 (FP64), 128 (FP32)
+	// FP64 also keeps each thread's 7 twiddle powers (32 columns a slot) after the accumulators
+	static constexpr unsigned ALLOC = sizeof(C) == 16 ? 512 : NCOLS;
 	// column address of value e of output q of this thread
 	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int e) {
 		const unsigned w = threadIdx.x >> 5;
 		return base + ((32u * (w & 3u)) << 16) + (w >> 2) * PER_THREAD + (unsigned)(q * 8 + e) * WPC;
+	}
+	__device__ __forceinline__ static unsigned twaddr(unsigned base) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + NCOLS + (w >> 2) * 32u;
 	}
 };
 
@@ -503,7 +560,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 	const int chunk = (int)(cid % p.nchunk);
 	const long cell = cid / p.nchunk;
 	const int warp = threadIdx.x >> 5;
-	if (warp == 0) tmem_alloc(&tmem_slot, TM::NCOLS);
+	if (warp == 0) tmem_alloc(&tmem_slot, TM::ALLOC);
 	init_twiddles<P>(tw);
 	tmem_fence_before();
 	__syncthreads();
@@ -511,9 +568,16 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 	const unsigned tbase = tmem_slot;
 	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
 	C wp[8];
+	const unsigned twaddr = TM::twaddr(tbase);
 	if constexpr (sizeof(C) == 8) {
 #pragma unroll
 		for (int q = 0; q < 8; q++) wp[q] = tw[(tau * q) & (P - 1)];
+	} else {
+		double2 a[4], b[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++) { a[q] = tw[(tau * (q + 1)) & (P - 1)]; b[q] = q < 3 ? tw[(tau * (q + 5)) & (P - 1)] : czero(); }
+		tmem_st4(twaddr, a);
+		tmem_st4(twaddr + 16, b);
 	}
 #pragma unroll
 	for (int q = 0; q < 2; q++)
@@ -546,14 +610,14 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					const int k = tau + G::T * r;
 					x[r] = cmul(Gg[line * P + k], Pj[G::at(line, k)]);
 				}
-				fft1d_lane<P, +1>(x, tau, G::row(Ug, line), tw, wp);
+				fft1d_lane<P, +1>(x, tau, G::row(Ug, line), wp, twaddr);
 #pragma unroll
 				for (int e = 0; e < 8; e++) Ug[G::at(line, Lp::out_pos(tau, e))] = x[e];
 				__syncthreads();
 				// columns: IFFT, multiply by psi2_t, FFT
 #pragma unroll
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
-				fft1d_lane<P, +1>(x, tau, G::col(Ug, line), tw, wp);
+				fft1d_lane<P, +1>(x, tau, G::col(Ug, line), wp, twaddr);
 #pragma unroll
 				for (int e = 0; e < 8; e++) {
 					const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
@@ -561,14 +625,14 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					x[e].y *= f;
 				}
 				out_to_in_acc<P>(x, tau, G::col(Ug, line));
-				fft1d_lane<P, -1>(x, tau, G::col(Ug, line), tw, wp);
+				fft1d_lane<P, -1>(x, tau, G::col(Ug, line), wp, twaddr);
 #pragma unroll
 				for (int e = 0; e < 8; e++) Ug[G::at(Lp::out_pos(tau, e), line)] = x[e];
 				__syncthreads();
 				// rows: FFT, multiply by P_a (own or the partner's), accumulate in TMEM
 #pragma unroll
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
-				fft1d_lane<P, -1>(x, tau, G::row(Ug, line), tw, wp);
+				fft1d_lane<P, -1>(x, tau, G::row(Ug, line), wp, twaddr);
 				const int a = p.ca[j][c];
 				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
 				const R coef = (R)p.ccoef[j][c];
@@ -610,7 +674,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 	tmem_fence_before();
 	__syncthreads();
 	tmem_fence_after();
-	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
+	if (warp == 0) tmem_dealloc(tbase, TM::ALLOC);
 }
 
 // ---------------------------------------------------------------------------

@@ -479,6 +479,23 @@ __device__ __forceinline__ void tmem_st4(unsigned taddr, const double2 (&v)[4]) 
 	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
 }
 
+// eight FP64 reals (16 columns) in one load or store
+__device__ __forceinline__ void tmem_ld8r(unsigned taddr, double (&v)[8]) {
+	unsigned r[16];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int e = 0; e < 8; e++) v[e] = __hiloint2double((int)r[2 * e + 1], (int)r[2 * e]);
+}
+__device__ __forceinline__ void tmem_st8r(unsigned taddr, const double (&v)[8]) {
+	unsigned r[16];
+#pragma unroll
+	for (int e = 0; e < 8; e++) { r[2 * e] = (unsigned)__double2loint(v[e]); r[2 * e + 1] = (unsigned)__double2hiint(v[e]); }
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
+}
+
 // length-L transform with the lane's twiddle powers w_L^(tau q), q = 1..7
 // (forward sign), read from tensor memory at taddr (4 complex FP64 values at
 // taddr, 3 more at taddr + 16): the loads are issued before the first
@@ -521,7 +538,8 @@ template <class C> struct I3Tmem {
 	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
 	static constexpr unsigned PER_THREAD = 2 * 8 * WPC;       // columns of one thread's slice
 	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 4 warps share a lane quarter: 256 (FP64), 128 (FP32)
-	// FP64 also keeps each thread's 7 twiddle powers (32 columns a slot) after the accumulators
+	// FP64 also keeps each thread's 7 twiddle powers (32 columns a slot) and its
+	// 8 psi2 values of the current term (16 columns a slot) after the accumulators
 	static constexpr unsigned ALLOC = sizeof(C) == 16 ? 512 : NCOLS;
 	// column address of value e of output q of this thread
 	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int e) {
@@ -531,6 +549,10 @@ template <class C> struct I3Tmem {
 	__device__ __forceinline__ static unsigned twaddr(unsigned base) {
 		const unsigned w = threadIdx.x >> 5;
 		return base + ((32u * (w & 3u)) << 16) + NCOLS + (w >> 2) * 32u;
+	}
+	__device__ __forceinline__ static unsigned psiaddr(unsigned base) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + NCOLS + 128u + (w >> 2) * 16u;
 	}
 };
 
@@ -596,6 +618,16 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 		cluster.sync();
 		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
 		const R sc = (R)p.psi2_scale[t];
+		if constexpr (sizeof(C) == 16) {
+			// this thread's psi2 values of the term (column line, rows out_pos(tau, e)), read
+			// once from L2 for the term's 8 chains; the previous term's reads of the slot
+			// have completed (tcgen05.wait::ld in every chain)
+			double f[8];
+#pragma unroll
+			for (int e = 0; e < 8; e++) f[e] = sc * psi2[line * P + Lp::out_pos(tau, e)];
+			tmem_st8r(TM::psiaddr(tbase), f);
+			tmem_wait_st();
+		}
 #pragma unroll 1
 		for (int q = 0; q < 2; q++) {
 			const int j = 2 * rank + q;
@@ -618,11 +650,19 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 #pragma unroll
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
 				fft1d_lane<P, +1>(x, tau, G::col(Ug, line), wp, twaddr);
+				if constexpr (sizeof(C) == 16) {
+					double f[8];
+					tmem_ld8r(TM::psiaddr(tbase), f);
+					tmem_wait_ld();
 #pragma unroll
-				for (int e = 0; e < 8; e++) {
-					const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
-					x[e].x *= f;
-					x[e].y *= f;
+					for (int e = 0; e < 8; e++) { x[e].x *= f[e]; x[e].y *= f[e]; }
+				} else {
+#pragma unroll
+					for (int e = 0; e < 8; e++) {
+						const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
+						x[e].x *= f;
+						x[e].y *= f;
+					}
 				}
 				out_to_in_acc<P>(x, tau, G::col(Ug, line));
 				fft1d_lane<P, -1>(x, tau, G::col(Ug, line), wp, twaddr);

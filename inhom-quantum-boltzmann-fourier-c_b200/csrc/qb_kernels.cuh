@@ -496,30 +496,24 @@ __device__ __forceinline__ void tmem_st8r(unsigned taddr, const double (&v)[8]) 
 	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
 }
 
-// length-L transform with the lane's twiddle powers w_L^(tau q), q = 1..7
-// (forward sign), read from tensor memory at taddr (4 complex FP64 values at
-// taddr, 3 more at taddr + 16): the loads are issued before the first
-// radix-8 stage and waited for after it
+// length-L transform with the lane's twiddle powers w_L^(tau q), q = 1..4
+// (forward sign), read from tensor memory at taddr (4 complex FP64 values);
+// w^5..w^7 = w^4 w^1..w^3.  The load is issued before the first radix-8
+// stage and waited for after it.
 template <int L, int DIR, class Acc>
 __device__ __forceinline__ void fft1d_acct(double2 (&x)[8], int tau, const Acc &sc, unsigned taddr) {
 	double2 w[4];
 	tmem_ld4(taddr, w);
 	dft8<DIR>(x);
 	tmem_wait_ld();
+	if (DIR > 0) {
 #pragma unroll
-	for (int q = 1; q <= 4; q++) {
-		double2 v = w[q - 1];
-		if (DIR > 0) v.y = -v.y;
-		x[q] = cmul(x[q], v);
+		for (int q = 0; q < 4; q++) w[q].y = -w[q].y;
 	}
-	tmem_ld4(taddr + 16, w);
-	tmem_wait_ld();
 #pragma unroll
-	for (int q = 5; q < 8; q++) {
-		double2 v = w[q - 5];
-		if (DIR > 0) v.y = -v.y;
-		x[q] = cmul(x[q], v);
-	}
+	for (int q = 1; q <= 4; q++) x[q] = cmul(x[q], w[q - 1]);
+#pragma unroll
+	for (int q = 5; q < 8; q++) x[q] = cmul(x[q], cmul(w[3], w[q - 5]));
 	fft1d_tail<L, DIR>(x, tau, sc);
 }
 
@@ -538,8 +532,9 @@ template <class C> struct I3Tmem {
 	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
 	static constexpr unsigned PER_THREAD = 2 * 8 * WPC;       // columns of one thread's slice
 	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 4 warps share a lane quarter: 256 (FP64), 128 (FP32)
-	// FP64 also keeps each thread's 7 twiddle powers (32 columns a slot) and its
-	// 8 psi2 values of the current term (16 columns a slot) after the accumulators
+	// FP64 also keeps, after the accumulators, each thread's twiddle powers w^1..w^4
+	// (16 columns a slot), its 8 psi2 values of the current term (16 columns a slot)
+	// and its 8 values of the current P_j (32 columns a slot)
 	static constexpr unsigned ALLOC = sizeof(C) == 16 ? 512 : NCOLS;
 	// column address of value e of output q of this thread
 	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int e) {
@@ -548,11 +543,15 @@ template <class C> struct I3Tmem {
 	}
 	__device__ __forceinline__ static unsigned twaddr(unsigned base) {
 		const unsigned w = threadIdx.x >> 5;
-		return base + ((32u * (w & 3u)) << 16) + NCOLS + (w >> 2) * 32u;
+		return base + ((32u * (w & 3u)) << 16) + NCOLS + (w >> 2) * 16u;
 	}
 	__device__ __forceinline__ static unsigned psiaddr(unsigned base) {
 		const unsigned w = threadIdx.x >> 5;
-		return base + ((32u * (w & 3u)) << 16) + NCOLS + 128u + (w >> 2) * 16u;
+		return base + ((32u * (w & 3u)) << 16) + NCOLS + 64u + (w >> 2) * 16u;
+	}
+	__device__ __forceinline__ static unsigned pjaddr(unsigned base) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + NCOLS + 128u + (w >> 2) * 32u;
 	}
 };
 
@@ -595,11 +594,10 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 #pragma unroll
 		for (int q = 0; q < 8; q++) wp[q] = tw[(tau * q) & (P - 1)];
 	} else {
-		double2 a[4], b[4];
+		double2 a[4];
 #pragma unroll
-		for (int q = 0; q < 4; q++) { a[q] = tw[(tau * (q + 1)) & (P - 1)]; b[q] = q < 3 ? tw[(tau * (q + 5)) & (P - 1)] : czero(); }
+		for (int q = 0; q < 4; q++) a[q] = tw[(tau * (q + 1)) & (P - 1)];
 		tmem_st4(twaddr, a);
-		tmem_st4(twaddr + 16, b);
 	}
 #pragma unroll
 	for (int q = 0; q < 2; q++)
@@ -632,15 +630,35 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 		for (int q = 0; q < 2; q++) {
 			const int j = 2 * rank + q;
 			const C *Pj = Pq + q * G::GRID;
+			if constexpr (sizeof(C) == 16) {
+				// this thread's 8 values of P_j (row line, columns tau + 8 r), read once from
+				// shared memory for the 4 chains of output j
+				C v[8];
+#pragma unroll
+				for (int r = 0; r < 8; r++) v[r] = Pj[G::at(line, tau + G::T * r)];
+				tmem_st8(TM::pjaddr(tbase), v);
+				tmem_wait_st();
+			}
 #pragma unroll 1
 			for (int c = 0; c < p.ncombo[j]; c++) {
 				const C *Gg = Gcell + (long)p.cgi[j][c] * P * P;
 				C x[8];
 				// rows: IFFT of G_g . P_j
+				if constexpr (sizeof(C) == 16) {
+					C pj[8];
+					tmem_ld8(TM::pjaddr(tbase), pj);
+					C g[8];
 #pragma unroll
-				for (int r = 0; r < 8; r++) {
-					const int k = tau + G::T * r;
-					x[r] = cmul(Gg[line * P + k], Pj[G::at(line, k)]);
+					for (int r = 0; r < 8; r++) g[r] = Gg[line * P + tau + G::T * r];
+					tmem_wait_ld();
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = cmul(g[r], pj[r]);
+				} else {
+#pragma unroll
+					for (int r = 0; r < 8; r++) {
+						const int k = tau + G::T * r;
+						x[r] = cmul(Gg[line * P + k], Pj[G::at(line, k)]);
+					}
 				}
 				fft1d_lane<P, +1>(x, tau, G::row(Ug, line), wp, twaddr);
 #pragma unroll

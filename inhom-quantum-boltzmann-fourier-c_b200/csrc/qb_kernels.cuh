@@ -496,6 +496,23 @@ __device__ __forceinline__ void tmem_st8r(unsigned taddr, const double (&v)[8]) 
 	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
 }
 
+// eight FP32 reals (8 columns) in one load or store
+__device__ __forceinline__ void tmem_ld8r(unsigned taddr, float (&v)[8]) {
+	unsigned r[8];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+	             : "r"(taddr) : "memory");
+#pragma unroll
+	for (int e = 0; e < 8; e++) v[e] = __uint_as_float(r[e]);
+}
+__device__ __forceinline__ void tmem_st8r(unsigned taddr, const float (&v)[8]) {
+	unsigned r[8];
+#pragma unroll
+	for (int e = 0; e < 8; e++) r[e] = __float_as_uint(v[e]);
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
+	             :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]) : "memory");
+}
+
 // length-L transform with the lane's twiddle powers w_L^(tau q), q = 1..4
 // (forward sign), read from tensor memory at taddr (4 complex FP64 values);
 // w^5..w^7 = w^4 w^1..w^3.  The load is issued before the first radix-8
@@ -532,27 +549,21 @@ template <class C> struct I3Tmem {
 	static constexpr unsigned WPC = sizeof(C) / 4;            // 32-bit columns per complex value
 	static constexpr unsigned PER_THREAD = 2 * 8 * WPC;       // columns of one thread's slice
 	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 4 warps share a lane quarter: 256 (FP64), 128 (FP32)
-	// FP64 also keeps, after the accumulators, each thread's twiddle powers w^1..w^4
-	// (16 columns a slot), its 8 psi2 values of the current term (16 columns a slot)
-	// and its 8 values of the current P_j (32 columns a slot)
-	static constexpr unsigned ALLOC = sizeof(C) == 16 ? 512 : NCOLS;
+	// after the accumulators each thread keeps its 8 psi2 values of the current
+	// term, its 8 values of the current P_j and (FP64) its twiddle powers w^1..w^4;
+	// columns a slot: 16 / 32 / 16 (FP64), 8 / 16 (FP32)
+	static constexpr unsigned ALLOC = sizeof(C) == 16 ? 512 : 256;
 	// column address of value e of output q of this thread
 	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int e) {
 		const unsigned w = threadIdx.x >> 5;
 		return base + ((32u * (w & 3u)) << 16) + (w >> 2) * PER_THREAD + (unsigned)(q * 8 + e) * WPC;
 	}
-	__device__ __forceinline__ static unsigned twaddr(unsigned base) {
-		const unsigned w = threadIdx.x >> 5;
-		return base + ((32u * (w & 3u)) << 16) + NCOLS + (w >> 2) * 16u;
-	}
-	__device__ __forceinline__ static unsigned psiaddr(unsigned base) {
-		const unsigned w = threadIdx.x >> 5;
-		return base + ((32u * (w & 3u)) << 16) + NCOLS + 64u + (w >> 2) * 16u;
-	}
-	__device__ __forceinline__ static unsigned pjaddr(unsigned base) {
-		const unsigned w = threadIdx.x >> 5;
-		return base + ((32u * (w & 3u)) << 16) + NCOLS + 128u + (w >> 2) * 32u;
-	}
+	static constexpr unsigned PSI = 8 * WPC / 2, PJ = 8 * WPC;   // columns a slot
+	__device__ __forceinline__ static unsigned lanes() { return (32u * ((threadIdx.x >> 5) & 3u)) << 16; }
+	__device__ __forceinline__ static unsigned slot() { return threadIdx.x >> 7; }
+	__device__ __forceinline__ static unsigned psiaddr(unsigned base) { return base + lanes() + NCOLS + slot() * PSI; }
+	__device__ __forceinline__ static unsigned pjaddr(unsigned base) { return base + lanes() + NCOLS + 4 * PSI + slot() * PJ; }
+	__device__ __forceinline__ static unsigned twaddr(unsigned base) { return base + lanes() + NCOLS + 4 * (PSI + PJ) + slot() * 16u; }
 };
 
 // ---------------------------------------------------------------------------
@@ -616,11 +627,11 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 		cluster.sync();
 		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
 		const R sc = (R)p.psi2_scale[t];
-		if constexpr (sizeof(C) == 16) {
+		{
 			// this thread's psi2 values of the term (column line, rows out_pos(tau, e)), read
 			// once from L2 for the term's 8 chains; the previous term's reads of the slot
 			// have completed (tcgen05.wait::ld in every chain)
-			double f[8];
+			R f[8];
 #pragma unroll
 			for (int e = 0; e < 8; e++) f[e] = sc * psi2[line * P + Lp::out_pos(tau, e)];
 			tmem_st8r(TM::psiaddr(tbase), f);
@@ -630,7 +641,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 		for (int q = 0; q < 2; q++) {
 			const int j = 2 * rank + q;
 			const C *Pj = Pq + q * G::GRID;
-			if constexpr (sizeof(C) == 16) {
+			{
 				// this thread's 8 values of P_j (row line, columns tau + 8 r), read once from
 				// shared memory for the 4 chains of output j
 				C v[8];
@@ -644,7 +655,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 				const C *Gg = Gcell + (long)p.cgi[j][c] * P * P;
 				C x[8];
 				// rows: IFFT of G_g . P_j
-				if constexpr (sizeof(C) == 16) {
+				{
 					C pj[8];
 					tmem_ld8(TM::pjaddr(tbase), pj);
 					C g[8];
@@ -653,12 +664,6 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 					tmem_wait_ld();
 #pragma unroll
 					for (int r = 0; r < 8; r++) x[r] = cmul(g[r], pj[r]);
-				} else {
-#pragma unroll
-					for (int r = 0; r < 8; r++) {
-						const int k = tau + G::T * r;
-						x[r] = cmul(Gg[line * P + k], Pj[G::at(line, k)]);
-					}
 				}
 				fft1d_lane<P, +1>(x, tau, G::row(Ug, line), wp, twaddr);
 #pragma unroll
@@ -668,19 +673,12 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 #pragma unroll
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
 				fft1d_lane<P, +1>(x, tau, G::col(Ug, line), wp, twaddr);
-				if constexpr (sizeof(C) == 16) {
-					double f[8];
+				{
+					R f[8];
 					tmem_ld8r(TM::psiaddr(tbase), f);
 					tmem_wait_ld();
 #pragma unroll
 					for (int e = 0; e < 8; e++) { x[e].x *= f[e]; x[e].y *= f[e]; }
-				} else {
-#pragma unroll
-					for (int e = 0; e < 8; e++) {
-						const R f = sc * psi2[line * P + Lp::out_pos(tau, e)];
-						x[e].x *= f;
-						x[e].y *= f;
-					}
 				}
 				out_to_in_acc<P>(x, tau, G::col(Ug, line));
 				fft1d_lane<P, -1>(x, tau, G::col(Ug, line), wp, twaddr);

@@ -139,3 +139,29 @@ def test_fp32_graph_replay_equals_direct(monkeypatch):
     monkeypatch.setenv("QB_CUDA_GRAPHS", "0")
     ws2 = qbgpu.Workspace(N, precision=32)
     assert torch.equal(qbgpu.inhom_step(ws2, q, W, 0.25, 0.01, B), results[0])
+
+
+def test_eigenvalues_stay_in_unit_interval_over_200_steps():
+    """0 <= W <= 1 (the Pauli principle: eigenvalues w0 -+ |w|) along 200 Strang
+    steps of the inhomogeneous workload (64 cells, N = 32, J = M = 16), in both
+    precisions; the tails of the state dip below 0 by the discrete operator's
+    error only (about 1e-7), and the FP32 form tracks the FP64 bounds"""
+    N, J, M, cells, steps = 32, 16, 16, 64, 200
+    q = qbgpu.Quad(N, J, M, L, R)
+    h = 1.0 / cells
+    dt = 0.4 * h / L
+    W0 = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=1, ncells=cells)).cuda()
+    bounds = {}
+    for prec in (64, 32):
+        ws = qbgpu.Workspace(N, precision=prec)
+        w, nxt = W0.clone(), torch.empty_like(W0)
+        lo, hi = np.inf, -np.inf
+        for k in range(steps):
+            qbgpu.inhom_step(ws, q, w, h, dt, out=nxt)
+            w, nxt = nxt, w
+            if k % 20 == 19:
+                d = qbgpu.diagnostics(w, L).cpu().numpy()
+                lo, hi = min(lo, d[:, 7].min()), max(hi, d[:, 8].max())
+        assert -1e-6 <= lo and hi <= 1.0, (prec, lo, hi)
+        bounds[prec] = (lo, hi)
+    assert abs(bounds[32][0] - bounds[64][0]) <= 1e-8 and abs(bounds[32][1] - bounds[64][1]) <= 1e-8, bounds

@@ -165,3 +165,24 @@ def test_eigenvalues_stay_in_unit_interval_over_200_steps():
         assert -1e-6 <= lo and hi <= 1.0, (prec, lo, hi)
         bounds[prec] = (lo, hi)
     assert abs(bounds[32][0] - bounds[64][0]) <= 1e-8 and abs(bounds[32][1] - bounds[64][1]) <= 1e-8, bounds
+
+
+def test_fp32_state_after_1000_steps():
+    """the FP32 form's W against the FP64 path after 1000 Strang steps (8 cells,
+    N = 32, J = M = 16, magnetic field on): within the 1e-5 bound of C"""
+    N, J, M, cells, steps = 32, 16, 16, 8, 1000
+    q = qbgpu.Quad(N, J, M, L, R)
+    h = 1.0 / cells
+    dt = 0.4 * h / L
+    W0 = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=76, ncells=cells)).cuda()
+    B = torch.from_numpy(np.random.default_rng(11).standard_normal((cells, 3)) * 0.05).cuda()
+    out = {}
+    for prec in (64, 32):
+        ws = qbgpu.Workspace(N, precision=prec)
+        w, nxt = W0.clone(), torch.empty_like(W0)
+        for _ in range(steps):
+            qbgpu.inhom_step(ws, q, w, h, dt, B, out=nxt)
+            w, nxt = nxt, w
+        out[prec] = w.cpu().numpy()
+    e = rel_l1(out[32], out[64])
+    assert 0 < e <= 1e-5, e

@@ -206,6 +206,7 @@ typedef struct qb_fno qb_fno;
 qb_fno *qb_fno_create(int N, int width, int modes, int layers, unsigned long long seed);
 void qb_fno_free(qb_fno *net);
 long qb_fno_num_params(const qb_fno *net);
+int qb_fno_grid_size(const qb_fno *net);                         /* N, or -1 for NULL */
 /* all weights as one FP32 array of qb_fno_num_params() values (host memory):
  * A[width][14], a[width], per layer Rr[width][width][K], Ri[..], W[width][width],
  * b[width], then Q[4][width], q[4]; K = (2 modes - 1) modes, frequency

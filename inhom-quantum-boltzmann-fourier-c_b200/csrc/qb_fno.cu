@@ -494,16 +494,25 @@ void qb_fno_free(qb_fno *net) { delete net; }
 
 long qb_fno_num_params(const qb_fno *net) { return net ? net->off.total : -1; }
 
+int qb_fno_grid_size(const qb_fno *net) { return net ? net->N : -1; }
+
 int qb_fno_get_params(const qb_fno *net, float *host) {
-	return fno_guard([&] { QB_CUDA(cudaMemcpy(host, net->params.p, sizeof(float) * net->off.total, cudaMemcpyDeviceToHost)); });
+	return fno_guard([&] {
+		if (net == nullptr || host == nullptr) QB_FAIL("qb_fno_get_params: null network or buffer");
+		QB_CUDA(cudaMemcpy(host, net->params.p, sizeof(float) * net->off.total, cudaMemcpyDeviceToHost));
+	});
 }
 
 int qb_fno_set_params(qb_fno *net, const float *host) {
-	return fno_guard([&] { QB_CUDA(cudaMemcpy(net->params.p, host, sizeof(float) * net->off.total, cudaMemcpyHostToDevice)); });
+	return fno_guard([&] {
+		if (net == nullptr || host == nullptr) QB_FAIL("qb_fno_set_params: null network or buffer");
+		QB_CUDA(cudaMemcpy(net->params.p, host, sizeof(float) * net->off.total, cudaMemcpyHostToDevice));
+	});
 }
 
 int qb_fno_set_scale(qb_fno *net, const double *scale) {
 	return fno_guard([&] {
+		if (net == nullptr || scale == nullptr) QB_FAIL("qb_fno_set_scale: null network or scales");
 		for (int c = 0; c < 4; c++) {
 			if (!(scale[c] > 0)) QB_FAIL("qb_fno_set_scale: scales must be positive");
 			net->scale[c] = scale[c];
@@ -513,6 +522,7 @@ int qb_fno_set_scale(qb_fno *net, const double *scale) {
 
 int qb_fno_set_input_scale(qb_fno *net, const double *scale) {
 	return fno_guard([&] {
+		if (net == nullptr || scale == nullptr) QB_FAIL("qb_fno_set_input_scale: null network or scales");
 		for (int f = 0; f < kFnoIn; f++) {
 			if (!(scale[f] > 0)) QB_FAIL("qb_fno_set_input_scale: scales must be positive");
 			net->inscale.s[f] = scale[f];
@@ -523,6 +533,7 @@ int qb_fno_set_input_scale(qb_fno *net, const double *scale) {
 int qb_fno_forward(qb_fno *net, int batch, const double *W, double *C, void *stream) {
 	return fno_guard([&] {
 		if (batch <= 0) return;
+		if (net == nullptr || W == nullptr || C == nullptr) QB_FAIL("qb_fno_forward: null network or state");
 		cudaStream_t s = (cudaStream_t)stream;
 		net->forward(batch, W, s);
 		const long n4 = (long)batch * 4 * net->P;
@@ -534,6 +545,7 @@ int qb_fno_forward(qb_fno *net, int batch, const double *W, double *C, void *str
 int qb_fno_gradients(qb_fno *net, int batch, const double *W, const double *target, float *grad_host, double *loss, void *stream) {
 	return fno_guard([&] {
 		if (batch <= 0) QB_FAIL("qb_fno_gradients: empty batch");
+		if (net == nullptr || W == nullptr || target == nullptr) QB_FAIL("qb_fno_gradients: null network, state or target");
 		cudaStream_t s = (cudaStream_t)stream;
 		net->forward(batch, W, s);
 		const double l = net->loss_backward(batch, target, s);
@@ -548,6 +560,7 @@ int qb_fno_gradients(qb_fno *net, int batch, const double *W, const double *targ
 int qb_fno_train_step(qb_fno *net, int batch, const double *W, const double *target, float lr, double *loss, void *stream) {
 	return fno_guard([&] {
 		if (batch <= 0) QB_FAIL("qb_fno_train_step: empty batch");
+		if (net == nullptr || W == nullptr || target == nullptr) QB_FAIL("qb_fno_train_step: null network, state or target");
 		cudaStream_t s = (cudaStream_t)stream;
 		net->forward(batch, W, s);
 		const double l = net->loss_backward(batch, target, s);

@@ -207,7 +207,10 @@ qb_surrogate *qb_surrogate_create(qb_fno *net, double tol, unsigned check_every)
 void qb_surrogate_free(qb_surrogate *s) { delete s; }
 
 int qb_surrogate_stats(const qb_surrogate *s, long *surrogate_cells, long *exact_cells, double *last_max_residual) {
-	if (s == nullptr) return -1;
+	if (s == nullptr) {
+		try { QB_FAIL("qb_surrogate_stats: null handle"); } catch (const std::exception &) {}
+		return -1;
+	}
 	if (surrogate_cells) *surrogate_cells = s->n_sur;
 	if (exact_cells) *exact_cells = s->n_ex;
 	if (last_max_residual) *last_max_residual = s->last_res;
@@ -218,6 +221,8 @@ int qb_surrogate_inhom_step(qb_surrogate *sg, qb_workspace *ws, const qb_quad *q
                             double h, double dt, const double *Bext, void *stream) {
 	try {
 		if (sg == nullptr || ws == nullptr || q == nullptr) QB_FAIL("qb_surrogate_inhom_step: null handle");
+		if (W == nullptr || Wnext == nullptr) QB_FAIL("qb_surrogate_inhom_step: null state");
+		if (qb_fno_grid_size(sg->net) != ws->N) QB_FAIL("qb_surrogate_inhom_step: the network and the workspace are for different grid sizes");
 		const int N = ws->N;
 		if (q->q->N != N) QB_FAIL("qb_surrogate_inhom_step: workspace and quadrature tables are for different grid sizes");
 		if (N > 64 || ncells <= 0) QB_FAIL("qb_surrogate_inhom_step: bad grid size or cell count");

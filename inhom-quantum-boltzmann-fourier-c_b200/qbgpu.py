@@ -77,6 +77,7 @@ def lib(n_grid=N_GRID):
     L.qb_fno_free.argtypes = [_vp]
     L.qb_fno_num_params.restype = C.c_long
     L.qb_fno_num_params.argtypes = [_vp]
+    L.qb_fno_grid_size.argtypes = [_vp]
     L.qb_fno_get_params.argtypes = [_vp, _vp]
     L.qb_fno_set_params.argtypes = [_vp, _vp]
     L.qb_fno_set_scale.argtypes = [_vp, _vp]

@@ -80,6 +80,12 @@ def test_parameters_roundtrip_and_bad_arguments():
         qbgpu.FNO(8, width=4, modes=5, layers=1)      # 2 modes - 1 > N
     with pytest.raises(RuntimeError):
         qbgpu.FNO(7, width=4, modes=2, layers=1)      # odd N
+    # a network for another grid size than the workspace's
+    q, ws = qbgpu.Quad(16, 4, 3, L, R), qbgpu.Workspace(16)
+    sur = qbgpu.Surrogate(net, tol=1.0, check_every=2)
+    W = torch.from_numpy(qbgpu.gaussian_mixture_state(16, L, seed=1, ncells=2)).cuda()
+    with pytest.raises(RuntimeError):
+        sur.step(ws, q, W, 0.5, 0.01)
 
 
 @pytest.fixture(scope="module")

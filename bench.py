@@ -586,8 +586,7 @@ def run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall):
         t0 = time.perf_counter()
         a, b = hin, hout
         for _ in range(steps):
-            out = up.inhom_step(a, quads, wl["h"], wl["dt"], hB, L=wl["L"], interm=it)
-            b[...] = out
+            up.inhom_step(a, quads, wl["h"], wl["dt"], hB, L=wl["L"], interm=it, out=b)
             a, b = b, a
         wall = time.perf_counter() - t0
         up.L.InhomStepInterm_Delete(qbgpu.C.byref(it))

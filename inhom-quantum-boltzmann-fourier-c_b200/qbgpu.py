@@ -633,12 +633,17 @@ class Upstream:
         self.L.InhomStepInterm_Create(C.c_uint(numVol), C.c_double(L), C.byref(it))
         return it
 
-    def inhom_step(self, W, quads, h, dt, Bext=None, bc="periodic", L=12.0, interm=None):
+    def inhom_step(self, W, quads, h, dt, Bext=None, bc="periodic", L=12.0, interm=None, out=None):
+        """InhomStepPeriodic / InhomStepDirichlet on host arrays; `out` (a
+        C-contiguous float64 array shaped like W, e.g. pinned) receives Wnext"""
         n = W.shape[0]
         it = interm or self.inhom_interm(n, L)
         W, pW = _np(W, np.float64)
         Bv, pB = _np(np.zeros((n, 3)) if Bext is None else Bext, np.float64)
-        out = np.zeros_like(W)
+        if out is None:
+            out = np.zeros_like(W)
+        elif not (out.flags["C_CONTIGUOUS"] and out.dtype == np.float64 and out.shape == W.shape):
+            raise ValueError("out must be a C-contiguous float64 array shaped like W")
         fn = {"periodic": self.L.InhomStepPeriodic, "dirichlet": self.L.InhomStepDirichlet}[bc]
         fn(pW, *[C.byref(q) for q in quads], C.c_double(h), C.c_double(dt), pB, C.byref(it), out.ctypes.data_as(_dp))
         if interm is None:

@@ -575,7 +575,12 @@ template <class C> struct I3Tmem {
 // with P_i of the partner's components read through distributed shared
 // memory.  The two 8-value accumulators of every thread live in TMEM, which
 // frees their registers and lets 2-CTA clusters use all 148 SMs (4-CTA
-// clusters of k_i3 fit 33 of 37 four-SM slots).  Output as k_i3 with CS = 4.
+// clusters of k_i3 fit 33 of 37 four-SM slots).  The rest of the TMEM
+// allocation caches values each thread reuses at its own positions: its psi2
+// values of the current term (one L2 read for the term's 8 chains), its P_j
+// values of the current output (one shared-memory read for the output's 4
+// chains) and, in FP64, its twiddle powers (FP32 keeps them in registers).
+// Output as k_i3 with CS = 4.
 template <int P, class C>
 __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 	using G = Geo<P, C>;

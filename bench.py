@@ -25,7 +25,8 @@ e2e    : same metric through the upstream C API (InhomStepPeriodic on host
 Extra blocks of the JSON line at N = 1: `precision_form` (the FP32 form on
 the same workload, with its error against FP64) and `config2_sample` (64 of
 the 1024 x-cells of the N = 64, J = M = 32 precision-form configuration, FP64
-and FP32 timed alike; --no-config2 skips it), and `surrogate` (a Fourier
+and FP32 timed alike; --no-config2 skips it), `config3_sample` (256 homogeneous
+instances of mixed N, RK4, FP64 and FP32; --no-config3 skips it), and `surrogate` (a Fourier
 neural operator trained here on homogeneous relaxation data, used for the
 collision half of the same Strang steps with the exact operator as judge
 every 10th step and as per-cell fallback; --no-surrogate skips it);
@@ -288,6 +289,9 @@ def run_ours(args):
     big = None
     if world == 1 and not args.no_config2:
         big = run_config2_sample(args, qbgpu, flush, cells=args.config2_cells)
+    big3 = None
+    if world == 1 and not args.no_config3:
+        big3 = run_config3_sample(args, qbgpu, flush)
     sur = None
     if world == 1 and not args.no_surrogate:
         sur = run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value)
@@ -305,6 +309,8 @@ def run_ours(args):
         line["precision_form"] = prec
     if big is not None:
         line["config2_sample"] = big
+    if big3 is not None:
+        line["config3_sample"] = big3
     if sur is not None:
         line["surrogate"] = sur
     if sur64 is not None:
@@ -370,6 +376,44 @@ def run_config2_sample(args, qbgpu, flush, cells=64, steps=2, warmup=1):
         a, b = a.cpu().numpy().ravel(), b.cpu().numpy().ravel()
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
     out["rel_err_f32_vs_f64"] = {"Cc_l2": rel(cc32, cc64), "Cd_l2": rel(cd32, cd64)}
+    return out
+
+
+def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
+    """A sample of the mixed-size batch configuration: `ninst` independent
+    homogeneous instances with N drawn from the configuration's sizes this
+    build supports (16, 32, 64, weights 0.1, 0.25, 0.2 renormalised), seeded
+    Gaussian mixtures, RK4 steps of dt = 0.01 (J = M = 16), FP64 and the FP32
+    form timed alike (CUDA events, L2 flushed before every step), with the
+    FP32 form's deviation from FP64 on the final states."""
+    import torch
+    L, R, J, M, dt = 6.0, 3.75, 16, 16, 0.01
+    rng = np.random.default_rng(3)
+    w = np.array([0.1, 0.25, 0.2])
+    sizes = rng.choice([16, 32, 64], size=ninst, p=w / w.sum())
+    Wf = [qbgpu.to_fourier(torch.from_numpy(qbgpu.gaussian_mixture_state(int(n), L, seed=3000 + i, ncells=1)).cuda())[0].contiguous()
+          for i, n in enumerate(sizes)]
+    out = {"workload": f"{ninst} homogeneous instances, N in (16, 32, 64) with weights (0.1, 0.25, 0.2) renormalised, "
+                       f"J={J}, M={M}, RK4 dt={dt}, {steps} timed steps after {warmup} warm-up per precision",
+           "unit": "instance-steps/s", "instances_per_N": {str(k): int((sizes == k).sum()) for k in (16, 32, 64)}}
+    final = {}
+    for prec in (64, 32):
+        states = [x.clone() for x in Wf]
+        for _ in range(warmup):
+            qbgpu.homogeneous_batch(states, dt, 1, rk4=True, J=J, M=M, L=L, R=R, precision=prec)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            evs[k][0].record()
+            qbgpu.homogeneous_batch(states, dt, 1, rk4=True, J=J, M=M, L=L, R=R, precision=prec)
+            evs[k][1].record()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        out[f"f{prec}"] = {"value": round(ninst / (ms * 1e-3), 3), "ms_per_step": round(ms, 3)}
+        final[prec] = torch.cat([x.reshape(-1) for x in states]).cpu().numpy()
+    out["speedup_f32_vs_f64"] = round(out["f32"]["value"] / out["f64"]["value"], 4)
+    out["rel_l2_f32_vs_f64_final_states"] = float(np.linalg.norm(final[32] - final[64]) / np.linalg.norm(final[64]))
     return out
 
 
@@ -676,6 +720,7 @@ def main():
     ap.add_argument("--no-precision-form", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--no-config2", action="store_true", help="skip the N = 64 precision-form sample")
     ap.add_argument("--config2-cells", type=int, default=64, help="x-cells of the N = 64 sample (of its 1024)")
+    ap.add_argument("--no-config3", action="store_true", help="skip the mixed-size batch sample")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
     ap.add_argument("--surrogate-n64", action="store_true", help="add the learned operator at N = 64 (about two minutes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -82,6 +82,11 @@ int qb_collision_step(qb_workspace *ws, const qb_quad *q, int ncells, const void
  * shares internal buffers, so calls on different streams must not overlap. */
 int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
                          int J, int M, double L, double R, void *stream);
+/* the same in a chosen working precision: 64 (the call above) or 32 (the
+ * FP32 form of qb_workspace_set_precision: FP32 spectra, tables and FFTs, FP64
+ * state and update).  The first FP32 call with a table set synchronises. */
+int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
+                            int precision, int J, int M, double L, double R, void *stream);
 
 /* one Strang step of InhomStepPeriodic (bc = 0) / InhomStepDirichlet (bc = 1)
  * (upstream src/simulation.c:307-830) over ncells velocity-space cells with

@@ -38,7 +38,7 @@ __global__ void k_scatter(const double2 *__restrict__ src, long per, int count, 
 using QuadKey = std::tuple<int, int, int, int, double, double>;   // device, N, J, M, L, R
 std::mutex g_mu;
 std::map<QuadKey, std::unique_ptr<qb::Quad>> g_quads;
-std::map<std::pair<int, int>, std::unique_ptr<qb::Workspace>> g_ws;   // (device, N)
+std::map<std::tuple<int, int, int>, std::unique_ptr<qb::Workspace>> g_ws;   // (device, N, precision)
 
 struct Group {
 	qb::DevBuf ptrs, state_a, state_b, bfield;
@@ -47,9 +47,10 @@ std::map<std::pair<int, int>, std::unique_ptr<Group>> g_groups;      // (device,
 
 }  // namespace
 
-extern "C" int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
-                                    int J, int M, double L, double R, void *stream) {
+extern "C" int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
+                                       int precision, int J, int M, double L, double R, void *stream) {
 	try {
+		if (precision != 64 && precision != 32) QB_FAIL("qb_homogeneous_batch_ex: precision must be 64 or 32");
 		if (ninst <= 0 || steps == 0) return 0;
 		if (n == nullptr || W == nullptr) QB_FAIL("qb_homogeneous_batch: null size or state array");
 		std::lock_guard<std::mutex> lk(g_mu);
@@ -69,8 +70,11 @@ extern "C" int qb_homogeneous_batch(int ninst, const int *n, void *const *W, con
 			const long per = 4L * N * N;
 			auto &quad = g_quads[QuadKey(dev, N, J, M, L, R)];
 			if (!quad) quad = qb::make_quad(N, J, M, L, R, s);
-			auto &ws = g_ws[{ dev, N }];
-			if (!ws) ws = std::make_unique<qb::Workspace>(N);
+			auto &ws = g_ws[std::make_tuple(dev, N, precision)];
+			if (!ws) {
+				ws = std::make_unique<qb::Workspace>(N);
+				ws->prec = precision;
+			}
 			auto &grp = g_groups[{ dev, N }];
 			if (!grp) grp = std::make_unique<Group>();
 			std::vector<const double2 *> src(g);
@@ -105,4 +109,9 @@ extern "C" int qb_homogeneous_batch(int ninst, const int *n, void *const *W, con
 	} catch (const std::exception &) {
 		return -1;
 	}
+}
+
+extern "C" int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
+                                    int J, int M, double L, double R, void *stream) {
+	return qb_homogeneous_batch_ex(ninst, n, W, B, dt, steps, rk4, 64, J, M, L, R, stream);
 }

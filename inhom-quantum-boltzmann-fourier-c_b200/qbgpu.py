@@ -70,6 +70,8 @@ def lib(n_grid=N_GRID):
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
     L.qb_diagnostics.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp]
     L.qb_homogeneous_batch.argtypes = [C.c_int, _vp, _vp, _vp, C.c_double, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp]
+    L.qb_homogeneous_batch_ex.argtypes = [C.c_int, _vp, _vp, _vp, C.c_double, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                          C.c_double, _vp]
     L.qb_fermi_dirac_equilibrium.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.qb_relative_entropy.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.qb_fno_create.restype = _vp
@@ -203,11 +205,12 @@ def inhom_step(ws, q, W, h, dt, Bext=None, bc="periodic", out=None):
     return out
 
 
-def homogeneous_batch(states, dt, steps, B=None, rk4=True, J=16, M=16, L=6.0, R=3.75):
+def homogeneous_batch(states, dt, steps, B=None, rk4=True, J=16, M=16, L=6.0, R=3.75, precision=64):
     """Advance independent homogeneous instances of possibly different grid
     sizes in place: states is a list of complex128 CUDA tensors (4, N_i, N_i)
     (Fourier space), B an optional (ninst, 3) array; `steps` collision steps
-    of size dt (RK4 or midpoint), one batched launch sequence per grid size."""
+    of size dt (RK4 or midpoint), one batched launch sequence per grid size;
+    precision 64 or 32 (the FP32 form)."""
     n = len(states)
     sizes = (C.c_int * n)(*[int(s.shape[-1]) for s in states])
     ptrs = (C.c_void_p * n)(*[s.data_ptr() for s in states])
@@ -216,8 +219,8 @@ def homogeneous_batch(states, dt, steps, B=None, rk4=True, J=16, M=16, L=6.0, R=
     Bh = None
     if B is not None:
         Bh = np.ascontiguousarray(np.asarray(B, dtype=np.float64).reshape(n, 3))
-    _check(lib().qb_homogeneous_batch(n, sizes, ptrs, Bh.ctypes.data_as(_vp) if Bh is not None else None, dt, steps,
-                                      1 if rk4 else 0, J, M, L, R, _stream()), "qb_homogeneous_batch")
+    _check(lib().qb_homogeneous_batch_ex(n, sizes, ptrs, Bh.ctypes.data_as(_vp) if Bh is not None else None, dt, steps,
+                                         1 if rk4 else 0, precision, J, M, L, R, _stream()), "qb_homogeneous_batch_ex")
     return states
 
 

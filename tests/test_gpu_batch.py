@@ -36,3 +36,22 @@ def test_batch_rejects_unsupported_size():
     bad = [torch.zeros((4, 24, 24), dtype=torch.complex128, device="cuda")]
     with pytest.raises(RuntimeError, match="N=24"):
         qbgpu.homogeneous_batch(bad, 0.01, 1, J=J, M=M, L=L, R=R)
+
+
+def test_fp32_batch_tracks_fp64_batch():
+    """the FP32 form of the mixed-size batch (N = 8, 16, 32 and 64, the last
+    through the whole-grid FP32 I3 kernel) within the 1e-5 bound of the FP64 one"""
+    sizes = [8, 16, 32, 64, 16, 32]
+    Wf = [orc.to_fourier(qbgpu.gaussian_mixture_state(n, L, seed=300 + i, ncells=1))[0] for i, n in enumerate(sizes)]
+    B = np.random.default_rng(12).standard_normal((len(sizes), 3)) * 0.1
+    out = {}
+    for prec in (64, 32):
+        states = [torch.from_numpy(w.copy()).cuda() for w in Wf]
+        qbgpu.homogeneous_batch(states, 0.01, 2, B=B, rk4=True, J=J, M=M, L=L, R=R, precision=prec)
+        out[prec] = [s.cpu().numpy() for s in states]
+    for i in range(len(sizes)):
+        a, b = out[32][i], out[64][i]
+        e = float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+        assert 0 < e <= 1e-5, (sizes[i], e)
+    with pytest.raises(RuntimeError):
+        qbgpu.homogeneous_batch([torch.from_numpy(Wf[0].copy()).cuda()], 0.01, 1, precision=16)

@@ -335,7 +335,8 @@ def run_config2_sample(args, qbgpu, flush, cells=64, steps=2, warmup=1):
     128 x 128), J = M = 32, seeded Gaussian mixture, periodic Strang steps on
     `cells` of its 1024 x-cells (h, dt as for 1024 cells), FP64 and the FP32
     form timed alike (CUDA events, L2 flushed before every step), with the
-    FP32 form's error against FP64 on the collision operator of the sample."""
+    FP32 form's error against FP64 on the collision operator of the sample and
+    how many cell evaluations of its timed steps ran the I3 sums in real form."""
     import torch
     N, J, M, L, R = 64, 32, 32, 6.0, 3.75
     h = 1.0 / 1024
@@ -352,6 +353,7 @@ def run_config2_sample(args, qbgpu, flush, cells=64, steps=2, warmup=1):
         for i in range(warmup):
             qbgpu.inhom_step(ws, q, bufs[i % 2], h, dt, B, out=bufs[(i + 1) % 2])
         torch.cuda.synchronize()
+        ws.i3_forms(reset=True)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         cur = warmup % 2
         for k in range(steps):
@@ -364,6 +366,9 @@ def run_config2_sample(args, qbgpu, flush, cells=64, steps=2, warmup=1):
         ms = sum(a.elapsed_time(b) for a, b in evs) / steps
         out[f"f{prec}"] = {"value": round(cells * 2 / (ms * 1e-3), 3), "ms_per_step": round(ms, 3),
                            "sim_steps_per_s_at_1024_cells": round(1e3 / (ms * 1024 / cells), 5)}
+        if prec == 32:
+            real, total = ws.i3_forms()      # cell evaluations of the timed steps, by I3 form
+            out["f32"]["i3_real_form_cells"] = f"{real} of {total}"
         del ws
     out["speedup_f32_vs_f64"] = round(out["f32"]["value"] / out["f64"]["value"], 4)
     Wf = torch.empty((cells, 4, N, N), dtype=torch.complex128, device="cuda")

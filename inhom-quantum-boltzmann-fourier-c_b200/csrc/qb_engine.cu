@@ -119,6 +119,8 @@ Workspace::Workspace(int n) : N(n) {
 	if (!supported_n(N)) QB_FAIL("grid size N=" + std::to_string(N) + " has no compiled kernels");
 	QB_CUDA(cudaGetDevice(&device));
 	QB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+	i3stats.ensure(2 * sizeof(unsigned long long));
+	QB_CUDA(cudaMemset(i3stats.p, 0, 2 * sizeof(unsigned long long)));
 }
 
 Workspace::~Workspace() {
@@ -545,11 +547,23 @@ template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, 
 }
 // k_i3_full128 (FP32 at N = 64): 2-CTA clusters, a whole grid per CTA, all
 // 512 tensor-memory columns per CTA, so exactly one CTA per SM (checked).
-// QB_I3_KERNEL=pair selects the pair-split k_i3_128 instead (for comparisons).
+// By default the cells whose Nyquist content is at most kRealFormBound take
+// the real form k_i3_full128r and the others k_i3_full128.  QB_I3_KERNEL
+// selects one kernel for every cell instead (for comparisons): "complex" the
+// complex k_i3_full128, "pair" the pair-split k_i3_128.
+inline const char *i3_kernel_env() {
+	static const char *e = getenv("QB_I3_KERNEL");
+	return e ? e : "";
+}
 inline bool use_full128() {
-	static const bool on = [] { const char *e = getenv("QB_I3_KERNEL"); return !(e && strcmp(e, "pair") == 0); }();
+	static const bool on = strcmp(i3_kernel_env(), "pair") != 0;
 	return on;
 }
+inline bool use_real_form() {
+	static const bool on = use_full128() && strcmp(i3_kernel_env(), "complex") != 0;
+	return on;
+}
+constexpr double kRealFormBound = 1e-6;
 constexpr size_t kFull128Smem = sizeof(float2) * ((size_t)F128::GRID + 128 + 64);
 
 int active_i3_full128_clusters() {
@@ -580,9 +594,29 @@ int active_i3_full128_clusters() {
 	return cached;
 }
 
-void launch_i3_full128(const I3ParamsT<float2> &p, long nclusters, float2 *pscr, cudaStream_t s) {
+void launch_i3_full128(const I3ParamsT<float2> &p, long nclusters, float2 *pscr, const int *kind, cudaStream_t s) {
 	active_i3_full128_clusters();              // attribute + occupancy check
-	launch128(k_i3_full128<float2>, "i3_cluster", nclusters * 2, 2, kFull128Smem, s, p, pscr);
+	launch128(k_i3_full128<float2>, "i3_cluster", nclusters * 2, 2, kFull128Smem, s, p, pscr, kind);
+}
+
+// the real form: same shared memory, 256 tensor-memory columns
+void launch_i3_full128r(const I3ParamsT<float2> &p, long nclusters, float *pscr, const int *kind, cudaStream_t s) {
+	static bool init = false;
+	if (!init) {
+		set_smem(k_i3_full128r, kFull128Smem);
+		int per_sm = 0;
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_i3_full128r, F128::NT, kFull128Smem));
+		if (per_sm * (int)F128TmemR::NCOLS > 512)
+			QB_FAIL("k_i3_full128r: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
+		init = true;
+	}
+	launch128(k_i3_full128r, "i3_cluster", nclusters * 2, 2, kFull128Smem, s, p, pscr, kind);
+}
+
+void launch_nyquist_kind(int N, int ncells, const double2 *W, double bound, int *kind, unsigned long long *stats, cudaStream_t s) {
+	ProfScope ps("nyquist_kind", s);
+	k_nyquist_kind<<<ncells, kNyqThreads, 0, s>>>(N, W, bound, kind, stats);
+	QB_CUDA(cudaGetLastError());
 }
 
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
@@ -651,7 +685,18 @@ template <class C> struct Rhs<128, C> {
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
 		if constexpr (sizeof(C) == 8) {
-			if (use_full128()) { launch_i3_full128(p, ncl, ws.scr128a.as<C>(), s); return; }
+			if (use_full128()) {
+				if (use_real_form()) {
+					ws.i3kind.ensure(sizeof(int) * ncells);
+					int *kind = ws.i3kind.as<int>();
+					launch_nyquist_kind(N, ncells, W, kRealFormBound, kind, ws.i3stats.as<unsigned long long>(), s);
+					launch_i3_full128r(p, ncl, reinterpret_cast<float *>(ws.scr128a.as<C>()), kind, s);
+					launch_i3_full128(p, ncl, ws.scr128a.as<C>(), kind, s);     // cells above the bound
+				} else {
+					launch_i3_full128(p, ncl, ws.scr128a.as<C>(), nullptr, s);
+				}
+				return;
+			}
 		}
 		launch_i3_128<4, kI3Pairs128>(p, ncl, ws.scr128a.as<C>(), s);
 	}

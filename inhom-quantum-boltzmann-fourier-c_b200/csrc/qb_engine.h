@@ -86,6 +86,8 @@ struct Workspace {
 	DevBuf aux, aux2;
 	DevBuf inv;                              // per-cell collision invariants (conservation on)
 	DevBuf scr128a, scr128b;                 // N = 64: per-cluster spectra of the I3 terms, first I2 spectra
+	DevBuf i3kind;                           // N = 64, FP32: per-cell I3 kernel (0 real form, 1 complex)
+	DevBuf i3stats;                          // N = 64, FP32: cells evaluated by the real form, by either form (2 x u64)
 	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
 	// replay of a repeated Strang step (batched API): the launch sequence of
 	// one (pointers, parameters) key is captured once and relaunched

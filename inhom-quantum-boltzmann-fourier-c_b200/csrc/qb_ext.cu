@@ -142,6 +142,19 @@ int qb_workspace_set_precision(qb_workspace *ws, int bits) {
 
 int qb_workspace_precision(const qb_workspace *ws) { return ws ? ws->prec : -1; }
 
+int qb_workspace_i3_forms(qb_workspace *ws, long long *real_cells, long long *all_cells, int reset) {
+	return guarded([&] {
+		if (ws == nullptr || real_cells == nullptr || all_cells == nullptr) QB_FAIL("null argument");
+		unsigned long long h[2] = { 0, 0 };
+		QB_CUDA(cudaSetDevice(ws->device));
+		QB_CUDA(cudaDeviceSynchronize());
+		QB_CUDA(cudaMemcpy(h, ws->i3stats.p, sizeof(h), cudaMemcpyDeviceToHost));
+		*real_cells = (long long)h[0];
+		*all_cells = (long long)h[1];
+		if (reset) QB_CUDA(cudaMemset(ws->i3stats.p, 0, sizeof(h)));
+	});
+}
+
 int qb_workspace_set_conservation(qb_workspace *ws, int on) {
 	return guarded([&] {
 		if (ws == nullptr) QB_FAIL("null workspace");

@@ -142,9 +142,11 @@ struct F128Tmem {
 	}
 };
 
-// Ghat: B layout; pscr: [cluster][4][P*P] natural; out: [cell][chunk][4][P*P] B layout
+// Ghat: B layout; pscr: [cluster][4][P*P] natural; out: [cell][chunk][4][P*P] B layout.
+// kind: null (every cell) or the per-cell form of k_nyquist_kind; this kernel
+// then takes the cells of kind 1 (the real form k_i3_full128r takes kind 0).
 template <class C>
-__global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p, C *pscr) {
+__global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p, C *pscr, const int *kind) {
 	static_assert(sizeof(C) == 8, "the whole-grid form is FP32 only");
 	using F = F128;
 	using R = typename CT<C>::R;
@@ -157,6 +159,7 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 	const long cid = blockIdx.x / 2;
 	const int chunk = (int)(cid % p.nchunk);
 	const long cell = cid / p.nchunk;
+	if (kind != nullptr && kind[cell] != 1) return;     // both CTAs of the cluster leave before any barrier
 	const int tid = threadIdx.x, warp = tid >> 5, tau = tid & 15, sub = tid >> 4;   // line it * 32 + sub
 	if (warp == 0) tmem_alloc(&tmem_slot, TM::NCOLS);
 	init_tw128(tw128, tw64);
@@ -320,6 +323,265 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128(const I3ParamsT<C> p
 	__syncthreads();
 	tmem_fence_after();
 	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
+}
+
+
+// ---------------------------------------------------------------------------
+// Real form of the same sums.
+//
+// Let Pad(X) be Hermitian, Pad(X)(-k) = conj Pad(X)(k) on the 128 x 128
+// frequency grid.  Then its forward transform is real.  Pad(W_c) and
+// Pad(psi1_t . W_c) are Hermitian up to the Nyquist row and column of W_c:
+// the N x N Fourier state of a real velocity-space component is Hermitian,
+// psi1_t = exp(i a_t . k) is too, and padding keeps every pair (k, -k) except
+// k = -N/2 (stored at 3N/2), whose partner +N/2 is not on the padded grid.
+// So when the Nyquist content of W is negligible, W^_i and P_{t,c} are real
+// and so is every chain input a = W^_i . P_j.  psi2_t is real and even, so
+// a -> FFT2(psi2_t . IFFT2(a)) maps real grids to real grids.  Two chains
+// therefore share one complex transform, one in the real part and one in
+// the imaginary part, and the spectra of two components come out of one
+// transform of psi1_t . (W_a + i W_b).  That halves the transforms of the
+// complex kernel.
+//
+// What is dropped: the imaginary parts of W^ and P, which come from the
+// Nyquist entries only.  The sums move by at most about the Nyquist fraction
+// (sum of |W| on the Nyquist row and column over sum of |W|, all 4
+// components): 0.2-0.3 of it on the extracted I3 of Gaussian-mixture states at
+// N = 64, 0.5-1.1 of it on the raw sums at N = 16.  k_nyquist_kind marks each
+// cell against a bound (1e-6 in the engine); cells above it go to the complex
+// kernel, so the error this form adds stays at the FP32 rounding of the
+// precision form.
+//
+// pscr: [cluster][4][P*P] real, natural order; out as k_i3_full128 (real
+// parts; imaginary parts written as zero).
+struct F128TmemR {
+	static constexpr unsigned PER_THREAD = 2 * 4 * 8;         // 64 (real FP32)
+	static constexpr unsigned NCOLS = 4 * PER_THREAD;         // 256
+	__device__ __forceinline__ static unsigned addr(unsigned base, int q, int it) {
+		const unsigned w = threadIdx.x >> 5;
+		return base + ((32u * (w & 3u)) << 16) + (w >> 2) * PER_THREAD + (unsigned)(q * 4 + it) * 8;
+	}
+};
+
+__global__ void __launch_bounds__(F128::NT, 1) k_i3_full128r(const I3ParamsT<float2> p, float *pscr, const int *kind) {
+	using C = float2;
+	using F = F128;
+	using TM = F128TmemR;
+	constexpr long PP = (long)F::P * F::P;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ unsigned tmem_slot;
+	C *S = reinterpret_cast<C *>(smem_raw), *tw128 = S + F::GRID, *tw64 = tw128 + 128;
+	cg::cluster_group cl = cg::this_cluster();
+	const int rank = (int)cl.block_rank();
+	const long cid = blockIdx.x / 2;
+	const int chunk = (int)(cid % p.nchunk);
+	const long cell = cid / p.nchunk;
+	if (kind[cell] != 0) return;                          // both CTAs of the cluster leave before any barrier
+	const int tid = threadIdx.x, warp = tid >> 5, tau = tid & 15, sub = tid >> 4;
+	if (warp == 0) tmem_alloc(&tmem_slot, TM::NCOLS);
+	init_tw128(tw128, tw64);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const unsigned tbase = tmem_slot;
+	C wp[8];
+	wp[0] = tw64[0];
+#pragma unroll
+	for (int q = 1; q < 8; q++) wp[q] = tw64[((tau & 7) * q) & 63];
+	{
+		const float z[8] = { 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f };
+#pragma unroll 1
+		for (int q = 0; q < 2; q++)
+#pragma unroll 1
+			for (int it = 0; it < 4; it++) tmem_st8r(TM::addr(tbase, q, it), z);
+	}
+	tmem_wait_st();
+	float *Pall = pscr + cid * 4 * PP;
+	const C *Gcell = p.Ghat + cell * p.g_cell;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+#pragma unroll 1
+	for (int t = t0; t < t1; t++) {
+		// spectra of components 2 rank (real part) and 2 rank + 1 (imaginary part)
+		{
+			const double2 *sa = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank] * F::N * F::N;
+			const double2 *sb = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank + 1] * F::N * F::N;
+			const C *psi1 = p.psi1 + (long)t * F::N * F::N;
+#pragma unroll 1
+			for (int it = 0; it < 4; it += 3) {             // rows outside the zero band: 0..31, 96..127
+				const int row = it * 32 + sub, ls = F::src(row);
+				C x[8];
+#pragma unroll
+				for (int r = 0; r < 8; r++) {
+					const int ks = F::src(tau + 16 * r);
+					C v = czero<C>();
+					if (ks >= 0) {
+						const int idx = ks + F::N * ls;
+						const double2 a = sa[idx], b = sb[idx];
+						v = cmul(psi1[idx], mk<C>(a.x - b.y, a.y + b.x));
+					}
+					x[r] = v;
+				}
+				fft128_line<-1, true>(x, tau, S, row, tw128, wp);
+				const LineSlots ls_ = row_slots(row, tau);
+#pragma unroll
+				for (int e = 0; e < 8; e++) S[ls_.at_out(e)] = x[e];
+			}
+			__syncthreads();
+#pragma unroll 1
+			for (int it = 0; it < 4; it++) {
+				const int col = it * 32 + sub;
+				const LineSlots cs_ = col_slots(col, tau);
+				C x[8];
+#pragma unroll
+				for (int r = 0; r < 8; r++)
+					x[r] = (r >= 2 && r < 6) ? czero<C>() : S[cs_.at_in(r)];
+				fft128_line<-1, false>(x, tau, S, col, tw128, wp);
+#pragma unroll
+				for (int e = 0; e < 8; e++) S[cs_.at_out(e)] = x[e];
+			}
+			__syncthreads();
+			float *Pa = Pall + (long)(2 * rank) * PP, *Pb = Pa + PP;
+#pragma unroll 4
+			for (int i = tid; i < F::P * F::P; i += F::NT) {
+				const C v = S[F::at(i >> 7, i & 127)];
+				Pa[i] = v.x;
+				Pb[i] = v.y;
+			}
+		}
+		cl.sync();                                          // both CTAs' spectra of term t are in L2
+		const float *psi2 = p.psi2T + (long)p.psi2_idx[t] * PP;
+		const float sc = (float)p.psi2_scale[t];
+#pragma unroll 1
+		for (int q = 0; q < 2; q++) {
+			const int j = 2 * rank + q;
+			const float *Pj = Pall + (long)j * PP;
+#pragma unroll 1
+			for (int cmb = 0; cmb + 1 < p.ncombo[j]; cmb += 2) {
+				const C *G0 = Gcell + (long)p.cgi[j][cmb] * PP, *G1 = Gcell + (long)p.cgi[j][cmb + 1] * PP;
+				// rows: inverse transform along k of (W^_i0 + i W^_i1) . P_j
+#pragma unroll 1
+				for (int it = 0; it < 4; it++) {
+					const int row = it * 32 + sub;
+					const C *g0 = G0 + F::brow(row), *g1 = G1 + F::brow(row);
+					const float *pj = Pj + (long)row * F::P;
+					C x[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) {
+						const int n = tau + 16 * r;
+						const float pv = pj[n];
+						x[r] = mk<C>(pv * g0[n].x, pv * g1[n].x);
+					}
+					fft128_line<+1, true>(x, tau, S, row, tw128, wp);
+					const LineSlots ls_ = row_slots(row, tau);
+#pragma unroll
+					for (int e = 0; e < 8; e++) S[ls_.at_out(e)] = x[e];
+				}
+				__syncthreads();
+				// columns: inverse transform along l, psi2, forward transform
+#pragma unroll 1
+				for (int it = 0; it < 4; it++) {
+					const int col = it * 32 + sub;
+					const LineSlots cs_ = col_slots(col, tau);
+					C x[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = S[cs_.at_in(r)];
+					fft128_line<+1, false>(x, tau, S, col, tw128, wp);
+					const float *ps = psi2 + (long)col * F::P;
+#pragma unroll
+					for (int e = 0; e < 8; e++) {
+						const float f = sc * ps[pos128(tau, e)];
+						x[e].x *= f;
+						x[e].y *= f;
+					}
+					fft128_dit_col<-1>(x, tau, S, col, tw128, wp);
+					const int d0 = (tau & 7) + 8 * (tau >> 3);
+#pragma unroll
+					for (int i = 0; i < 8; i++) S[(d0 + 16 * (i >> 1) + 64 * (i & 1)) * F::LDP + cs_.cx[i & 1]] = x[i];
+				}
+				__syncthreads();
+				// rows: forward transform along k; the real part belongs to i0,
+				// the imaginary part to i1
+				const float *P0 = Pall + (long)p.ca[j][cmb] * PP, *P1 = Pall + (long)p.ca[j][cmb + 1] * PP;
+				const float c0 = (float)p.ccoef[j][cmb], c1 = (float)p.ccoef[j][cmb + 1];
+#pragma unroll 1
+				for (int it = 0; it < 4; it++) {
+					const int row = it * 32 + sub;
+					const LineSlots ls_ = row_slots(row, tau);
+					C x[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = S[ls_.at_in(r)];
+					fft128_line<-1, true>(x, tau, S, row, tw128, wp);
+					const float *p0 = P0 + (long)row * F::P, *p1 = P1 + (long)row * F::P;
+					float acc[8];
+					tmem_ld8r(TM::addr(tbase, q, it), acc);
+					tmem_wait_ld();
+#pragma unroll
+					for (int e = 0; e < 8; e++) {
+						const int n = pos128(tau, e);
+						acc[e] += c0 * (p0[n] * x[e].x) + c1 * (p1[n] * x[e].y);
+					}
+					tmem_st8r(TM::addr(tbase, q, it), acc);
+					tmem_wait_st();
+				}
+				// no barrier: the next chain's first row pass writes only the
+				// rows this thread's 16-lane group has just read
+			}
+		}
+		cl.sync();                                          // the partner is done with this term's spectra
+	}
+#pragma unroll 1
+	for (int q = 0; q < 2; q++) {
+		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * PP;
+#pragma unroll 1
+		for (int it = 0; it < 4; it++) {
+			const int row = it * 32 + sub;
+			float acc[8];
+			tmem_ld8r(TM::addr(tbase, q, it), acc);
+			tmem_wait_ld();
+#pragma unroll
+			for (int e = 0; e < 8; e++) o[F::brow(row) + pos128(tau, e)] = mk<C>(acc[e], 0.0);
+		}
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
+}
+
+// per cell: 1 when the Nyquist content of the Fourier state W ([cell][4][N*N],
+// natural order k + N l) exceeds `bound` times its total (sums of |W| over the
+// 4 components; Nyquist = row l = N/2 and column k = N/2), else 0.  stats
+// (may be null) counts the cells of kind 0 and all cells.
+constexpr int kNyqThreads = 256;
+__global__ void __launch_bounds__(kNyqThreads) k_nyquist_kind(int N, const double2 *__restrict__ W, double bound, int *__restrict__ kind,
+                                                             unsigned long long *stats) {
+	__shared__ double red[2][kNyqThreads / 32];
+	const long NN = (long)N * N;
+	const double2 *w = W + blockIdx.x * 4 * NN;
+	double tot = 0.0, nyq = 0.0;
+	for (long i = threadIdx.x; i < 4 * NN; i += kNyqThreads) {
+		const int g = (int)(i % NN), k = g % N, l = g / N;
+		const double a = hypot(w[i].x, w[i].y);
+		tot += a;
+		if (k == N / 2 || l == N / 2) nyq += a;
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		tot += __shfl_xor_sync(0xffffffffu, tot, o);
+		nyq += __shfl_xor_sync(0xffffffffu, nyq, o);
+	}
+	if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = tot; red[1][threadIdx.x >> 5] = nyq; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0, n = 0.0;
+		for (int i = 0; i < kNyqThreads / 32; i++) { t += red[0][i]; n += red[1][i]; }
+		const int k = (n <= bound * t) ? 0 : 1;           // NaN sums take the complex kernel
+		kind[blockIdx.x] = k;
+		if (stats != nullptr) {
+			atomicAdd(&stats[0], (unsigned long long)(k == 0));
+			atomicAdd(&stats[1], 1ull);
+		}
+	}
 }
 
 }  // namespace qb

@@ -55,6 +55,7 @@ def lib(n_grid=N_GRID):
     L.qb_workspace_set_precision.argtypes = [_vp, C.c_int]
     L.qb_workspace_precision.argtypes = [_vp]
     L.qb_workspace_set_conservation.argtypes = [_vp, C.c_int]
+    L.qb_workspace_i3_forms.argtypes = [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.c_int]
     L.qb_collision_operators.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp]
     L.qb_collision_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, _vp, C.c_int, _vp]
     L.qb_inhom_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, C.c_double, _vp, C.c_int, _vp]
@@ -165,6 +166,13 @@ class Workspace:
     @property
     def precision(self):
         return lib().qb_workspace_precision(self.h)
+
+    def i3_forms(self, reset=False):
+        """(cells whose I3 sums ran in the real form, all cells) evaluated so
+        far through this workspace at N = 64 in FP32 (zero otherwise)."""
+        r, a = C.c_longlong(), C.c_longlong()
+        _check(lib().qb_workspace_i3_forms(self.h, C.byref(r), C.byref(a), 1 if reset else 0), "qb_workspace_i3_forms")
+        return r.value, a.value
 
     def __del__(self):
         if getattr(self, "h", None) and getattr(self, "_free", None):

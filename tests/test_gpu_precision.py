@@ -71,6 +71,31 @@ def test_fp32_operators_against_fp64(N, J, M):
     assert e_cc > 0 and e_cd > 0
 
 
+def test_fp32_n64_real_form_and_guard():
+    """N = 64 in FP32: cells with negligible Nyquist content run the I3 sums in
+    real form (two chains per complex transform), cells with Nyquist content
+    take the complex kernel; both stay within the FP32 bound of the oracle"""
+    N, J, M = 64, 4, 3
+    o = orc.Oracle(N, J, M, L, R)
+    q = qbgpu.Quad(N, J, M, L, R)
+    Wv = qbgpu.gaussian_mixture_state(N, L, seed=2, ncells=4)
+    rng = np.random.default_rng(5)
+    Wv[2:] += 1e-3 * rng.standard_normal(Wv[2:].shape)      # white noise: Nyquist fraction far above 1e-6
+    Wf = np.stack([orc.to_fourier(w) for w in Wv])
+    ws32, ws64 = qbgpu.Workspace(N, precision=32), qbgpu.Workspace(N)
+    cc, cd = qbgpu.collision_operators(ws32, q, torch.from_numpy(Wf).cuda())
+    qbgpu.collision_operators(ws64, q, torch.from_numpy(Wf).cuda())
+    assert ws32.i3_forms() == (2, 4)
+    assert ws64.i3_forms() == (0, 0)
+    assert ws32.i3_forms(reset=True) == (2, 4) and ws32.i3_forms() == (0, 0)
+    cc, cd = cc.cpu().numpy(), cd.cpu().numpy()
+    for sl in (slice(0, 2), slice(2, 4)):
+        ref_cc = np.stack([o.cc(w) for w in Wf[sl]])
+        ref_cd = np.stack([o.cd(w) for w in Wf[sl]])
+        assert rel_l2(cc[sl], ref_cc) <= C_TOL
+        assert rel_l2(cd[sl], ref_cd) <= C_TOL
+
+
 def conserved_totals(W):
     """mass, momentum (x, y) and kinetic energy of the trace component summed over all cells"""
     d = orc.diagnostics(W, L)

@@ -233,6 +233,33 @@ template <int P, int CS, class C> void launch_i3(const I3ParamsT<C> &p, long ncl
 	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p));
 }
 
+// I3 kernels of the FP32 form at N = 32 (k_i3p) and N = 64 (k_i3_full128:
+// 2-CTA clusters, a whole grid per CTA, all 512 tensor-memory columns per CTA,
+// so exactly one CTA per SM, checked).  By default the cells whose Nyquist
+// content is at most kRealFormBound take the real forms (k_i3pr,
+// k_i3_full128r) and the others the complex kernels.  QB_I3_KERNEL selects one
+// kernel for every cell instead (for comparisons): "complex" the complex
+// kernels, "pair" the complex k_i3p and the pair-split k_i3_128.
+inline const char *i3_kernel_env() {
+	static const char *e = getenv("QB_I3_KERNEL");
+	return e ? e : "";
+}
+inline bool use_full128() {
+	static const bool on = strcmp(i3_kernel_env(), "pair") != 0;
+	return on;
+}
+inline bool use_real_form() {
+	static const bool on = use_full128() && strcmp(i3_kernel_env(), "complex") != 0;
+	return on;
+}
+constexpr double kRealFormBound = 1e-6;
+
+void launch_nyquist_kind(int N, int ncells, const double2 *W, double bound, int *kind, unsigned long long *stats, cudaStream_t s) {
+	ProfScope ps("nyquist_kind", s);
+	k_nyquist_kind<<<ncells, kNyqThreads, 0, s>>>(N, W, bound, kind, stats);
+	QB_CUDA(cudaGetLastError());
+}
+
 // k_i3p (P = 64): 2-CTA clusters, TMEM accumulators.  The allocation of
 // I3Tmem<C>::NCOLS columns never waits as long as no more CTAs share an SM
 // than its 512 columns hold; the shared-memory (FP64) or register (FP32)
@@ -267,7 +294,7 @@ template <class C> int active_i3p_clusters() {
 	return cached;
 }
 
-template <class C> void launch_i3p(const I3ParamsT<C> &p, long nclusters, cudaStream_t s) {
+template <class C> void launch_i3p(const I3ParamsT<C> &p, long nclusters, const int *kind, cudaStream_t s) {
 	active_i3p_clusters<C>();                  // attribute + occupancy check
 	auto kern = k_i3p<64, C>;
 	cudaLaunchConfig_t cfg = {};
@@ -281,7 +308,33 @@ template <class C> void launch_i3p(const I3ParamsT<C> &p, long nclusters, cudaSt
 	cfg.attrs = &attr;
 	cfg.numAttrs = 1;
 	ProfScope ps("i3_cluster", s);
-	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p));
+	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p, kind));
+}
+
+// the real form at P = 64 (FP32): same shared memory as k_i3p, 128 tensor-memory columns
+void launch_i3pr(const I3ParamsT<float2> &p, long nclusters, const int *kind, cudaStream_t s) {
+	static bool init = false;
+	auto kern = k_i3pr<64>;
+	if (!init) {
+		set_smem(kern, i3p_smem<float2>());
+		int per_sm = 0;
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Geo<64>::NT, i3p_smem<float2>()));
+		if (per_sm * (int)I3TmemR::ALLOC > 512)
+			QB_FAIL("k_i3pr: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
+		init = true;
+	}
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)(nclusters * 2));
+	cfg.blockDim = dim3(Geo<64>::NT);
+	cfg.dynamicSmemBytes = i3p_smem<float2>();
+	cfg.stream = s;
+	cudaLaunchAttribute attr;
+	attr.id = cudaLaunchAttributeClusterDimension;
+	attr.val.clusterDim.x = 2; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+	cfg.attrs = &attr;
+	cfg.numAttrs = 1;
+	ProfScope ps("i3_cluster", s);
+	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, p, kind));
 }
 
 template <int P, class C> void launch_fft_full(const FullParamsT<C> &p, long ngrids, cudaStream_t s) {
@@ -414,8 +467,21 @@ template <int P, class C> struct Rhs {
 		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
-		if constexpr (P == 64) launch_i3p<C>(p, (long)ncells * nchunk, s);
-		else launch_i3<P, 4>(p, (long)ncells * nchunk, s);
+		if constexpr (P == 64) {
+			if constexpr (sizeof(C) == 8) {
+				if (use_real_form()) {
+					ws.i3kind.ensure(sizeof(int) * ncells);
+					int *kind = ws.i3kind.as<int>();
+					launch_nyquist_kind(P / 2, ncells, W, kRealFormBound, kind, ws.i3stats.as<unsigned long long>(), s);
+					launch_i3pr(p, (long)ncells * nchunk, kind, s);
+					launch_i3p<C>(p, (long)ncells * nchunk, kind, s);       // cells above the bound
+					return;
+				}
+			}
+			launch_i3p<C>(p, (long)ncells * nchunk, nullptr, s);
+		} else {
+			launch_i3<P, 4>(p, (long)ncells * nchunk, s);
+		}
 	}
 
 	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
@@ -545,25 +611,6 @@ template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, 
 	}
 	launch128(k_i3_128<CS, NPAIR, C>, "i3_cluster", nclusters * 2 * NPAIR, 2 * NPAIR, smem128<C>(), s, p, pscr);
 }
-// k_i3_full128 (FP32 at N = 64): 2-CTA clusters, a whole grid per CTA, all
-// 512 tensor-memory columns per CTA, so exactly one CTA per SM (checked).
-// By default the cells whose Nyquist content is at most kRealFormBound take
-// the real form k_i3_full128r and the others k_i3_full128.  QB_I3_KERNEL
-// selects one kernel for every cell instead (for comparisons): "complex" the
-// complex k_i3_full128, "pair" the pair-split k_i3_128.
-inline const char *i3_kernel_env() {
-	static const char *e = getenv("QB_I3_KERNEL");
-	return e ? e : "";
-}
-inline bool use_full128() {
-	static const bool on = strcmp(i3_kernel_env(), "pair") != 0;
-	return on;
-}
-inline bool use_real_form() {
-	static const bool on = use_full128() && strcmp(i3_kernel_env(), "complex") != 0;
-	return on;
-}
-constexpr double kRealFormBound = 1e-6;
 constexpr size_t kFull128Smem = sizeof(float2) * ((size_t)F128::GRID + 128 + 64);
 
 int active_i3_full128_clusters() {
@@ -613,11 +660,6 @@ void launch_i3_full128r(const I3ParamsT<float2> &p, long nclusters, float *pscr,
 	launch128(k_i3_full128r, "i3_cluster", nclusters * 2, 2, kFull128Smem, s, p, pscr, kind);
 }
 
-void launch_nyquist_kind(int N, int ncells, const double2 *W, double bound, int *kind, unsigned long long *stats, cudaStream_t s) {
-	ProfScope ps("nyquist_kind", s);
-	k_nyquist_kind<<<ncells, kNyqThreads, 0, s>>>(N, W, bound, kind, stats);
-	QB_CUDA(cudaGetLastError());
-}
 
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
 	static bool init = false;

@@ -77,6 +77,14 @@ template <class C> struct MulCplx {           // psi (complex N x N) .* v   (Mul
 	const C *psi;
 	__device__ __forceinline__ C operator()(int idx, double2 v) const { return cmul(psi[idx], mk<C>(v.x, v.y)); }
 };
+template <class C> struct MulCplxPair {       // psi .* (v + i b): two grids packed in one transform
+	const C *psi;
+	const double2 *b;
+	__device__ __forceinline__ C operator()(int idx, double2 v) const {
+		const double2 w = b[idx];
+		return cmul(psi[idx], mk<C>(v.x - w.y, v.y + w.x));
+	}
+};
 
 // lane's 8 inputs of padded row `prow` of Pad(mul . src)
 template <int P, class C, class Mul>
@@ -581,8 +589,11 @@ template <class C> struct I3Tmem {
 // values of the current output (one shared-memory read for the output's 4
 // chains) and, in FP64, its twiddle powers (FP32 keeps them in registers).
 // Output as k_i3 with CS = 4.
+//
+// kind: null (every cell) or the per-cell form of k_nyquist_kind; this kernel
+// then takes the cells of kind 1 (the real form k_i3pr takes kind 0).
 template <int P, class C>
-__global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
+__global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, const int *kind) {
 	using G = Geo<P, C>;
 	using Lp = Len<P>;
 	using R = typename CT<C>::R;
@@ -596,6 +607,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 	const long cid = blockIdx.x / 2;
 	const int chunk = (int)(cid % p.nchunk);
 	const long cell = cid / p.nchunk;
+	if (kind != nullptr && kind[cell] != 1) return;     // both CTAs of the cluster leave before any barrier
 	const int warp = threadIdx.x >> 5;
 	if (warp == 0) tmem_alloc(&tmem_slot, TM::ALLOC);
 	init_twiddles<P>(tw);
@@ -731,6 +743,165 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p) {
 		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * (long)P * P + line * P;
 #pragma unroll
 		for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tbase, TM::ALLOC);
+}
+
+// k_i3p in real arithmetic (FP32 form, cells without Nyquist content): the
+// identity of k_i3_full128r at P = 64.  One transform of psi1_t . (W_2r +
+// i W_2r+1) gives the real spectra P_2r (real part) and P_2r+1 (imaginary
+// part) in one shared grid; the chains of combos (i0, i1) of an output share
+// one complex transform of P_j . (W^_i0 + i W^_i1), and the real accumulators
+// take eta_i0 P_i0 . Re + eta_i1 P_i1 . Im.  Same shared-memory layout as k_i3p
+// (the second P grid unused); tensor memory: 2 x 8 real accumulators, 8 psi2
+// and 8 P_j values per thread.
+struct I3TmemR {
+	static constexpr unsigned PER_THREAD = 16, NCOLS = 64, PSI = 8, PJ = 8, ALLOC = 128;
+	__device__ __forceinline__ static unsigned lanes() { return (32u * ((threadIdx.x >> 5) & 3u)) << 16; }
+	__device__ __forceinline__ static unsigned slot() { return threadIdx.x >> 7; }
+	__device__ __forceinline__ static unsigned addr(unsigned base, int q) { return base + lanes() + (threadIdx.x >> 7) * PER_THREAD + (unsigned)q * 8; }
+	__device__ __forceinline__ static unsigned psiaddr(unsigned base) { return base + lanes() + NCOLS + slot() * PSI; }
+	__device__ __forceinline__ static unsigned pjaddr(unsigned base) { return base + lanes() + NCOLS + 4 * PSI + slot() * PJ; }
+};
+
+template <int P>
+__global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3pr(const I3ParamsT<float2> p, const int *kind) {
+	using C = float2;
+	using G = Geo<P, C>;
+	using Lp = Len<P>;
+	using TM = I3TmemR;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ unsigned tmem_slot;
+	C *Pq = reinterpret_cast<C *>(smem_raw);                 // P_2r + i P_2r+1
+	C *Ug = Pq + 2 * G::GRID, *tw = Pq + 3 * G::GRID;
+	cg::cluster_group cluster = cg::this_cluster();
+	const int rank = (int)cluster.block_rank();
+	const long cid = blockIdx.x / 2;
+	const int chunk = (int)(cid % p.nchunk);
+	const long cell = cid / p.nchunk;
+	if (kind[cell] != 0) return;                          // both CTAs of the cluster leave before any barrier
+	const int warp = threadIdx.x >> 5;
+	if (warp == 0) tmem_alloc(&tmem_slot, TM::ALLOC);
+	init_twiddles<P>(tw);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const unsigned tbase = tmem_slot;
+	const int line = threadIdx.x / G::T, tau = threadIdx.x % G::T;
+	C wp[8];
+#pragma unroll
+	for (int q = 0; q < 8; q++) wp[q] = tw[(tau * q) & (P - 1)];
+	{
+		const float z[8] = { 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f };
+		tmem_st8r(TM::addr(tbase, 0), z);
+		tmem_st8r(TM::addr(tbase, 1), z);
+		tmem_wait_st();
+	}
+	const C *Gcell = p.Ghat + cell * p.g_cell;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+	const C *Ppeer = cluster.map_shared_rank(Pq, rank ^ 1);
+	for (int t = t0; t < t1; t++) {
+		{
+			const double2 *sa = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank] * G::N * G::N;
+			const double2 *sb = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank + 1] * G::N * G::N;
+			fft2_pad<P, -1>(Pq, tw, sa, MulCplxPair<C>{p.psi1 + (long)t * G::N * G::N, sb});
+		}
+		cluster.sync();
+		const float *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
+		const float sc = (float)p.psi2_scale[t];
+		{
+			float f[8];
+#pragma unroll
+			for (int e = 0; e < 8; e++) f[e] = sc * psi2[line * P + Lp::out_pos(tau, e)];
+			tmem_st8r(TM::psiaddr(tbase), f);
+			tmem_wait_st();
+		}
+#pragma unroll 1
+		for (int q = 0; q < 2; q++) {
+			const int j = 2 * rank + q;
+			{
+				float v[8];
+#pragma unroll
+				for (int r = 0; r < 8; r++) {
+					const C pv = Pq[G::at(line, tau + G::T * r)];
+					v[r] = q ? pv.y : pv.x;
+				}
+				tmem_st8r(TM::pjaddr(tbase), v);
+				tmem_wait_st();
+			}
+#pragma unroll 1
+			for (int c = 0; c + 1 < p.ncombo[j]; c += 2) {
+				const C *G0 = Gcell + (long)p.cgi[j][c] * P * P, *G1 = Gcell + (long)p.cgi[j][c + 1] * P * P;
+				C x[8];
+				// rows: IFFT of P_j . (W^_i0 + i W^_i1)
+				{
+					float pj[8];
+					tmem_ld8r(TM::pjaddr(tbase), pj);
+					float g0[8], g1[8];
+#pragma unroll
+					for (int r = 0; r < 8; r++) {
+						g0[r] = G0[line * P + tau + G::T * r].x;
+						g1[r] = G1[line * P + tau + G::T * r].x;
+					}
+					tmem_wait_ld();
+#pragma unroll
+					for (int r = 0; r < 8; r++) x[r] = mk<C>(pj[r] * g0[r], pj[r] * g1[r]);
+				}
+				fft1d_lane<P, +1>(x, tau, G::row(Ug, line), wp, 0u);
+#pragma unroll
+				for (int e = 0; e < 8; e++) Ug[G::at(line, Lp::out_pos(tau, e))] = x[e];
+				__syncthreads();
+				// columns: IFFT, multiply by psi2_t, FFT
+#pragma unroll
+				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(tau + G::T * r, line)];
+				fft1d_lane<P, +1>(x, tau, G::col(Ug, line), wp, 0u);
+				{
+					float f[8];
+					tmem_ld8r(TM::psiaddr(tbase), f);
+					tmem_wait_ld();
+#pragma unroll
+					for (int e = 0; e < 8; e++) { x[e].x *= f[e]; x[e].y *= f[e]; }
+				}
+				out_to_in_acc<P>(x, tau, G::col(Ug, line));
+				fft1d_lane<P, -1>(x, tau, G::col(Ug, line), wp, 0u);
+#pragma unroll
+				for (int e = 0; e < 8; e++) Ug[G::at(Lp::out_pos(tau, e), line)] = x[e];
+				__syncthreads();
+				// rows: FFT; the real part belongs to i0, the imaginary part to i1
+#pragma unroll
+				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
+				fft1d_lane<P, -1>(x, tau, G::row(Ug, line), wp, 0u);
+				const int a0 = p.ca[j][c], a1 = p.ca[j][c + 1];
+				const C *Pa0 = ((a0 >> 1) == rank ? Pq : Ppeer), *Pa1 = ((a1 >> 1) == rank ? Pq : Ppeer);
+				const float c0 = (float)p.ccoef[j][c], c1 = (float)p.ccoef[j][c + 1];
+				float acc[8];
+				tmem_ld8r(TM::addr(tbase, q), acc);
+				tmem_wait_ld();
+#pragma unroll
+				for (int e = 0; e < 8; e++) {
+					const int n = G::at(line, Lp::out_pos(tau, e));
+					const C v0 = Pa0[n], v1 = Pa1[n];
+					const float p0 = (a0 & 1) ? v0.y : v0.x, p1 = (a1 & 1) ? v1.y : v1.x;
+					acc[e] += c0 * (p0 * x[e].x) + c1 * (p1 * x[e].y);
+				}
+				tmem_st8r(TM::addr(tbase, q), acc);
+				tmem_wait_st();
+				// no barrier here, as in k_i3p
+			}
+		}
+		cluster.sync();
+	}
+#pragma unroll 1
+	for (int q = 0; q < 2; q++) {
+		float acc[8];
+		tmem_ld8r(TM::addr(tbase, q), acc);
+		tmem_wait_ld();
+		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * (long)P * P + line * P;
+#pragma unroll
+		for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = mk<C>(acc[e], 0.0);
 	}
 	tmem_fence_before();
 	__syncthreads();

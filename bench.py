@@ -438,6 +438,7 @@ def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
     for i in range(args.warmup):
         step(bufs[i % 2], bufs[(i + 1) % 2])
     torch.cuda.synchronize()
+    ws32.i3_forms(reset=True)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     cur = args.warmup % 2
     for k in range(args.steps):
@@ -449,6 +450,7 @@ def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in evs)
     value32 = cells * 2 * args.steps / (ms * 1e-3)
+    real, total = ws32.i3_forms()      # cell evaluations of the timed steps, by I3 form
 
     def rel(a, b, o):
         a, b = a.cpu().numpy().ravel(), b.cpu().numpy().ravel()
@@ -473,7 +475,7 @@ def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
     torch.cuda.synchronize()
     return {"dtype": "f32 (FFTs, spectra, tables); f64 state, assembly and update", "value": round(value32, 3), "unit": UNIT,
             "ms_per_step": round(ms / args.steps, 4), "sim_steps_per_s": round(args.steps / (ms * 1e-3), 4),
-            "speedup_vs_fp64": round(value32 / value64, 4),
+            "speedup_vs_fp64": round(value32 / value64, 4), "i3_real_form_cells": f"{real} of {total}",
             "rel_err_vs_fp64": {"Cc_l2": rel(cc32, cc64, 2), "Cd_l2": rel(cd32, cd64, 2), "Cc_l1": rel(cc32, cc64, 1),
                                 "Cd_l1": rel(cd32, cd64, 1), f"W_l1_after_{args.steps}_steps": rel(b, a, 1),
                                 f"W_l1_after_{long_steps}_steps_first_{long_cells}_cells": rel(b8, a8, 1)},

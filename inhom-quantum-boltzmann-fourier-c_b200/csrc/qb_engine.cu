@@ -253,6 +253,12 @@ inline bool use_real_form() {
 	return on;
 }
 constexpr double kRealFormBound = 1e-6;
+// the real forms pack the combos of an output in pairs
+template <class C> bool even_combos(const I3ParamsT<C> &p) {
+	for (int r = 0; r < 4; r++)
+		if (p.ncombo[r] & 1) return false;
+	return true;
+}
 
 void launch_nyquist_kind(int N, int ncells, const double2 *W, double bound, int *kind, unsigned long long *stats, cudaStream_t s) {
 	ProfScope ps("nyquist_kind", s);
@@ -469,7 +475,7 @@ template <int P, class C> struct Rhs {
 		p.out = ws.i3p.as<C>();
 		if constexpr (P == 64) {
 			if constexpr (sizeof(C) == 8) {
-				if (use_real_form()) {
+				if (use_real_form() && even_combos(p)) {
 					ws.i3kind.ensure(sizeof(int) * ncells);
 					int *kind = ws.i3kind.as<int>();
 					launch_nyquist_kind(P / 2, ncells, W, kRealFormBound, kind, ws.i3stats.as<unsigned long long>(), s);
@@ -728,7 +734,7 @@ template <class C> struct Rhs<128, C> {
 		p.out = ws.i3p.as<C>();
 		if constexpr (sizeof(C) == 8) {
 			if (use_full128()) {
-				if (use_real_form()) {
+				if (use_real_form() && even_combos(p)) {
 					ws.i3kind.ensure(sizeof(int) * ncells);
 					int *kind = ws.i3kind.as<int>();
 					launch_nyquist_kind(N, ncells, W, kRealFormBound, kind, ws.i3stats.as<unsigned long long>(), s);

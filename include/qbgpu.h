@@ -101,8 +101,10 @@ int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, const doubl
  * (upstream src/simulation.c:307-830) over ncells velocity-space cells with
  * box half-width L; Bext = 3 doubles per cell (NULL: no field).  Wnext must
  * not alias W.
- * A repeated call with identical arguments replays a captured CUDA graph of
- * the step (QB_CUDA_GRAPHS=0 launches kernel by kernel instead). */
+ * The workspace keeps the CUDA graphs of its last 4 distinct argument sets:
+ * a call whose arguments match one of them (e.g. steps that alternate two
+ * state buffers) relaunches the graph captured on that set's second call.
+ * QB_CUDA_GRAPHS=0, or kernel profiling being on, launches kernel by kernel. */
 int qb_inhom_step(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext,
                   double h, double dt, const double *Bext, int bc, void *stream);
 
@@ -181,7 +183,11 @@ int qb_relative_entropy(int N, double L, int ncells, const double *W, const doub
 int qb_profile_enable(int on);
 int qb_profile_reset(void);
 int qb_profile_read(const char *prefix, double *ms, long *launches);
+/* kernels launched so far by this library, the kernel nodes of replayed CUDA
+ * graphs included */
 long qb_launch_count(void);
+/* Strang steps of qb_inhom_step served by relaunching a captured CUDA graph */
+long qb_workspace_graph_replays(const qb_workspace *ws);
 
 /* The I3 integral of qb_integral(q, 3, ...) for callers that cannot allocate
  * device memory (a stream being captured into a CUDA graph, a host

@@ -50,7 +50,9 @@ std::atomic<long> g_launches{0};
 }  // namespace
 
 void prof_enable(bool on) { g_prof_on = on; }
+bool prof_enabled() { return g_prof_on.load(); }
 long launch_count() { return g_launches.load(); }
+void add_launches(long n) { g_launches += n; }
 
 void prof_reset() {
 	std::lock_guard<std::mutex> lk(g_prof_mu);
@@ -95,9 +97,16 @@ ProfScope::~ProfScope() {
 
 // ---------------------------------------------------------------------------
 // buffers
+namespace {
+std::atomic<unsigned long long> g_buffer_generation{0};
+}
+
+unsigned long long buffer_generation() { return g_buffer_generation.load(std::memory_order_acquire); }
+
 void DevBuf::ensure(size_t n) {
 	if (n <= bytes && p != nullptr) return;
 	release();
+	g_buffer_generation.fetch_add(1, std::memory_order_acq_rel);
 	QB_CUDA(cudaGetDevice(&device));
 	QB_CUDA(cudaMalloc(&p, n));
 	bytes = n;
@@ -105,6 +114,7 @@ void DevBuf::ensure(size_t n) {
 
 void DevBuf::release() {
 	if (p != nullptr) {
+		g_buffer_generation.fetch_add(1, std::memory_order_acq_rel);
 		int cur = -1;
 		cudaGetDevice(&cur);
 		if (device >= 0 && cur != device) cudaSetDevice(device);
@@ -124,7 +134,8 @@ Workspace::Workspace(int n) : N(n) {
 }
 
 Workspace::~Workspace() {
-	if (graph_exec) cudaGraphExecDestroy(graph_exec);
+	for (auto &g : graphs)
+		if (g.exec) cudaGraphExecDestroy(g.exec);
 	if (ev_in) cudaEventDestroy(ev_in);
 	if (ev_out) cudaEventDestroy(ev_out);
 	if (stream) cudaStreamDestroy(stream);
@@ -134,16 +145,48 @@ Workspace::~Workspace() {
 // launch helpers (templated on the padded size P)
 namespace {
 
+// Kernel attributes (dynamic shared-memory limits) and occupancy results are
+// per CUDA device.  These two wrappers keep one value per device, selected by
+// the device current at each access, so that a process driving several GPUs
+// sets every attribute on each of them.  Racing first calls from several host
+// threads at worst repeat an idempotent attribute call or occupancy query.
+constexpr int kMaxDevices = 64;
+inline int cur_dev() {
+	int d = 0;
+	cudaGetDevice(&d);
+	return d & (kMaxDevices - 1);
+}
+struct DeviceFlag {
+	std::atomic<unsigned long long> bits{0};
+	explicit operator bool() const { return (bits.load(std::memory_order_acquire) >> cur_dev()) & 1ull; }
+	bool operator!() const { return !static_cast<bool>(*this); }
+	DeviceFlag &operator=(bool v) {
+		const unsigned long long b = 1ull << cur_dev();
+		if (v) bits.fetch_or(b, std::memory_order_acq_rel);
+		else bits.fetch_and(~b, std::memory_order_acq_rel);
+		return *this;
+	}
+};
+struct DeviceInt {
+	std::atomic<int> v[kMaxDevices];
+	explicit DeviceInt(int init) { for (auto &x : v) x.store(init); }
+	operator int() const { return v[cur_dev()].load(std::memory_order_acquire); }
+	DeviceInt &operator=(int x) { v[cur_dev()].store(x, std::memory_order_release); return *this; }
+};
+
 int num_sms() {
-	static int sms = 0;
+	static DeviceInt sms{0};
 	if (sms == 0) {
-		int dev = 0;
+		int dev = 0, n = 0;
 		cudaGetDevice(&dev);
-		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		if (sms <= 0) sms = 148;
+		cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+		sms = n > 0 ? n : 148;
 	}
 	return sms;
 }
+
+// before the first launch of any tensor-memory kernel on a device (defined below)
+void check_tmem_coresidency();
 
 template <class K> void set_smem(K kernel, size_t bytes) {
 	QB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -153,7 +196,7 @@ template <int P, class C = double2> constexpr size_t smem_grids(int ngrids) { re
 
 // active clusters of the I3 kernel (occupancy query, cached per P and C)
 template <int P, class C> int active_i3_clusters() {
-	static int cached = -1;
+	static DeviceInt cached{-1};
 	if (cached < 0) {
 		auto kern = k_i3<P, 4, C>;
 		set_smem(kern, smem_grids<P, C>(2));
@@ -192,7 +235,7 @@ int best_chunks(long units, int nterms, int slots, int max_chunks, double penalt
 }
 
 template <int P, class C> void launch_pad_fft(int ngrids, const double2 *src, C *out, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_pad_fft<P, C>, smem_grids<P, C>(1)); init = true; }
 	ProfScope ps("pad_fft", s);
 	k_pad_fft<P, C><<<ngrids, Geo<P>::NT, smem_grids<P, C>(1), s>>>(src, out);
@@ -200,7 +243,7 @@ template <int P, class C> void launch_pad_fft(int ngrids, const double2 *src, C 
 }
 
 template <int P, class C> void launch_i1(const I1ParamsT<C> &p, long nblocks, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_i1_terms<P, C>, smem_grids<P, C>(2)); init = true; }
 	ProfScope ps("i1_terms", s);
 	k_i1_terms<P, C><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P, C>(2), s>>>(p);
@@ -208,7 +251,7 @@ template <int P, class C> void launch_i1(const I1ParamsT<C> &p, long nblocks, cu
 }
 
 template <int P, class C> void launch_i2(const I2ParamsT<C> &p, long nblocks, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_i2_terms<P, C>, smem_grids<P, C>(2)); init = true; }
 	ProfScope ps("i2_terms", s);
 	k_i2_terms<P, C><<<(unsigned)nblocks, Geo<P>::NT, smem_grids<P, C>(2), s>>>(p);
@@ -216,7 +259,7 @@ template <int P, class C> void launch_i2(const I2ParamsT<C> &p, long nblocks, cu
 }
 
 template <int P, int CS, class C> void launch_i3(const I3ParamsT<C> &p, long nclusters, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	auto kern = k_i3<P, CS, C>;
 	if (!init) { set_smem(kern, smem_grids<P, C>(2)); init = true; }
 	cudaLaunchConfig_t cfg = {};
@@ -253,7 +296,10 @@ inline bool use_real_form() {
 	return on;
 }
 constexpr double kRealFormBound = 1e-6;
-// the real forms pack the combos of an output in pairs
+// The real forms pack the combos of an output in pairs.  Both callers of the
+// I3 sums (the Cd assembly and the single-integral path) set 4 combos per
+// output, so this holds today; it guards the real-form launch against a
+// future caller with an odd count, which then takes the complex kernel.
 template <class C> bool even_combos(const I3ParamsT<C> &p) {
 	for (int r = 0; r < 4; r++)
 		if (p.ncombo[r] & 1) return false;
@@ -273,8 +319,9 @@ void launch_nyquist_kind(int N, int ncells, const double2 *W, double bound, int 
 template <class C> size_t i3p_smem() { return sizeof(C) * ((size_t)3 * Geo<64, C>::GRID + 64); }
 
 template <class C> int active_i3p_clusters() {
-	static int cached = -1;
+	static DeviceInt cached{-1};
 	if (cached < 0) {
+		check_tmem_coresidency();
 		auto kern = k_i3p<64, C>;
 		set_smem(kern, i3p_smem<C>());
 		int per_sm = 0;
@@ -319,9 +366,10 @@ template <class C> void launch_i3p(const I3ParamsT<C> &p, long nclusters, const 
 
 // the real form at P = 64 (FP32): same shared memory as k_i3p, 128 tensor-memory columns
 void launch_i3pr(const I3ParamsT<float2> &p, long nclusters, const int *kind, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	auto kern = k_i3pr<64>;
 	if (!init) {
+		check_tmem_coresidency();
 		set_smem(kern, i3p_smem<float2>());
 		int per_sm = 0;
 		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Geo<64>::NT, i3p_smem<float2>()));
@@ -344,7 +392,7 @@ void launch_i3pr(const I3ParamsT<float2> &p, long nclusters, const int *kind, cu
 }
 
 template <int P, class C> void launch_fft_full(const FullParamsT<C> &p, long ngrids, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_fft_full<P, C>, smem_grids<P, C>(1)); init = true; }
 	ProfScope ps("fft_full", s);
 	k_fft_full<P, C><<<(unsigned)ngrids, Geo<P>::NT, smem_grids<P, C>(1), s>>>(p);
@@ -352,7 +400,7 @@ template <int P, class C> void launch_fft_full(const FullParamsT<C> &p, long ngr
 }
 
 template <int P, class C> void launch_assemble(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_assemble<P, C>, smem_grids<P, C>(1)); init = true; }
 	ProfScope ps("assemble", s);
 	k_assemble<P, C><<<(unsigned)(ncells * 4), Geo<P>::NT, smem_grids<P, C>(1), s>>>(p);
@@ -551,7 +599,7 @@ void launch128(void (*kern)(KA...), const char *name, long nblocks, int cdim, si
 	QB_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
 }
 
-template <class K> void set_smem_once(K kern, size_t bytes, bool &done) {
+template <class K> void set_smem_once(K kern, size_t bytes, DeviceFlag &done) {
 	if (!done) { set_smem(kern, bytes); done = true; }
 }
 
@@ -560,7 +608,7 @@ constexpr int kI3Pairs128 = 2;
 
 // active clusters of the 128 I3 kernel (occupancy query, cached per C)
 template <class C> int active_i3_clusters128() {
-	static int cached = -1;
+	static DeviceInt cached{-1};
 	if (cached < 0) {
 		auto kern = k_i3_128<4, kI3Pairs128, C>;
 		set_smem(kern, smem128<C>());
@@ -584,30 +632,31 @@ template <class C> int active_i3_clusters128() {
 }
 
 template <class C> void launch_pad_fft128(int ngrids, const double2 *src, C *out, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_pad_fft128<C>, smem128<C>(), init);
 	launch128(k_pad_fft128<C>, "pad_fft", 2L * ngrids, 1, smem128<C>(), s, src, out);
 }
 template <class C> void launch_i1_128(const I1ParamsT<C> &p, long units, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_i1_terms128<C>, smem128<C>(), init);
 	launch128(k_i1_terms128<C>, "i1_terms", 2 * units, 2, smem128<C>(), s, p);
 }
 template <class C> void launch_fft_full128(const FullParamsT<C> &p, long ngrids, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_fft_full128<C>, smem128<C>(), init);
 	launch128(k_fft_full128<C>, "fft_full", 2 * ngrids, 1, smem128<C>(), s, p);
 }
 template <class C> void launch_i2_128(const I2ParamsT<C> &p, long units, C *tmp, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_i2_terms128<C>, smem128<C>(), init);
 	launch128(k_i2_terms128<C>, "i2_terms", 2 * units, 1, smem128<C>(), s, p, tmp);
 }
 // The tensor-memory allocation of k_i3_128 never waits as long as no more
 // CTAs share an SM than its 512 columns hold; checked before the first launch.
 template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) {
+		check_tmem_coresidency();
 		set_smem(k_i3_128<CS, NPAIR, C>, smem128<C>());
 		int per_sm = 0;
 		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_i3_128<CS, NPAIR, C>, G128::NT, smem128<C>()));
@@ -620,8 +669,9 @@ template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, 
 constexpr size_t kFull128Smem = sizeof(float2) * ((size_t)F128::GRID + 128 + 64);
 
 int active_i3_full128_clusters() {
-	static int cached = -1;
+	static DeviceInt cached{-1};
 	if (cached < 0) {
+		check_tmem_coresidency();
 		auto kern = k_i3_full128<float2>;
 		set_smem(kern, kFull128Smem);
 		int per_sm = 0;
@@ -654,8 +704,9 @@ void launch_i3_full128(const I3ParamsT<float2> &p, long nclusters, float2 *pscr,
 
 // the real form: same shared memory, 256 tensor-memory columns
 void launch_i3_full128r(const I3ParamsT<float2> &p, long nclusters, float *pscr, const int *kind, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) {
+		check_tmem_coresidency();
 		set_smem(k_i3_full128r, kFull128Smem);
 		int per_sm = 0;
 		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_i3_full128r, F128::NT, kFull128Smem));
@@ -667,8 +718,84 @@ void launch_i3_full128r(const I3ParamsT<float2> &p, long nclusters, float *pscr,
 }
 
 
+// ---- tensor memory: why no allocation ever waits -----------------------------
+// tcgen05.alloc blocks while the columns it asks for are held by other CTAs
+// on its SM.  With clusters that could deadlock: CTA a1 of cluster A holds
+// columns on SM 1 that CTA b1 of cluster B waits for, while b2 holds columns
+// on SM 2 that a2 waits for, and each cluster's CTAs wait for one another at
+// a cluster barrier.  Launches from two workspaces on two streams could set
+// that up.  The library excludes the wait itself, by construction: for every
+// set of CTAs of its tensor-memory kernels that the SM's shared memory,
+// registers, thread slots and block slots allow to be resident at the same
+// time, their columns sum to at most the SM's 512.  Then every allocation is
+// granted at once, whatever launches run beside it, and each kernel frees its
+// columns before it exits.  This function checks that property from the
+// compiled resource footprint of every tensor-memory kernel on the current
+// device, by enumerating the multisets of co-resident CTAs (shared-memory
+// capacity counted at its largest carve-out, which only admits more sets),
+// once per device before the first launch of any of them, and fails loudly
+// if a set could oversubscribe.
+void check_tmem_coresidency() {
+	static DeviceFlag done;
+	if (done) return;
+	struct Info { const void *fn; size_t dyn_smem; int threads; int cols; const char *name; };
+	const Info ks[] = {
+		{ (const void *)k_i3p<64, double2>, i3p_smem<double2>(), Geo<64>::NT, (int)I3Tmem<double2>::ALLOC, "k_i3p<f64>" },
+		{ (const void *)k_i3p<64, float2>, i3p_smem<float2>(), Geo<64>::NT, (int)I3Tmem<float2>::ALLOC, "k_i3p<f32>" },
+		{ (const void *)k_i3pr<64>, i3p_smem<float2>(), Geo<64>::NT, (int)I3TmemR::ALLOC, "k_i3pr" },
+		{ (const void *)k_i3_128<4, kI3Pairs128, double2>, smem128<double2>(), G128::NT,
+		  (int)I3Tmem128<double2, 4 / kI3Pairs128>::NCOLS, "k_i3_128<f64>" },
+		{ (const void *)k_i3_128<4, kI3Pairs128, float2>, smem128<float2>(), G128::NT,
+		  (int)I3Tmem128<float2, 4 / kI3Pairs128>::NCOLS, "k_i3_128<f32>" },
+		{ (const void *)k_i3_128<2, 1, double2>, smem128<double2>(), G128::NT, (int)I3Tmem128<double2, 2>::NCOLS,
+		  "k_i3_128<f64, single integral>" },
+		{ (const void *)k_i3_full128<float2>, kFull128Smem, F128::NT, (int)F128Tmem::NCOLS, "k_i3_full128" },
+		{ (const void *)k_i3_full128r, kFull128Smem, F128::NT, (int)F128TmemR::NCOLS, "k_i3_full128r" },
+	};
+	constexpr int n = (int)(sizeof(ks) / sizeof(ks[0]));
+	int dev = 0, sm_smem = 0, sm_regs = 0, sm_threads = 0, sm_blocks = 0, reserved = 0;
+	QB_CUDA(cudaGetDevice(&dev));
+	QB_CUDA(cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+	QB_CUDA(cudaDeviceGetAttribute(&sm_regs, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+	QB_CUDA(cudaDeviceGetAttribute(&sm_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+	QB_CUDA(cudaDeviceGetAttribute(&sm_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, dev));
+	QB_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+	struct Use { long smem, regs; int threads, cols; };
+	Use u[n];
+	for (int i = 0; i < n; i++) {
+		cudaFuncAttributes a;
+		QB_CUDA(cudaFuncGetAttributes(&a, ks[i].fn));
+		const long warps = (ks[i].threads + 31) / 32;
+		const long regs_warp = (long)((a.numRegs + 7) / 8) * 8 * 32;      // registers are granted per warp, 8 per thread at a time
+		u[i] = { (long)a.sharedSizeBytes + (long)ks[i].dyn_smem + reserved, warps * regs_warp, ks[i].threads, ks[i].cols };
+	}
+	int count[n] = {};
+	// depth-first over multisets in non-decreasing kernel order
+	struct Dfs {
+		const Use *u; const Info *ks; int *count; int sm_smem, sm_regs, sm_threads, sm_blocks;
+		void go(int from, long smem, long regs, int thr, int blocks, int cols) {
+			for (int i = from; i < n; i++) {
+				const long s2 = smem + u[i].smem, r2 = regs + u[i].regs;
+				const int t2 = thr + u[i].threads, b2 = blocks + 1, c2 = cols + u[i].cols;
+				if (s2 > sm_smem || r2 > sm_regs || t2 > sm_threads || b2 > sm_blocks) continue;
+				count[i]++;
+				if (c2 > 512) {
+					std::string set;
+					for (int k = 0; k < n; k++)
+						if (count[k]) set += (set.empty() ? "" : " + ") + std::to_string(count[k]) + " x " + ks[k].name;
+					QB_FAIL("tensor memory: " + set + " can share an SM and would ask for " + std::to_string(c2) + " of 512 columns");
+				}
+				go(i, s2, r2, t2, b2, c2);
+				count[i]--;
+			}
+		}
+	} dfs{ u, ks, count, sm_smem, sm_regs, sm_threads, sm_blocks };
+	dfs.go(0, 0, 0, 0, 0, 0);
+	done = true;
+}
+
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_assemble128<C>, smem128<C>(), init);
 	launch128(k_assemble128<C>, "assemble", 2 * 4 * ncells, 2, smem128<C>(), s, p);
 }
@@ -925,7 +1052,7 @@ void mul_sum(long n, const double2 *a, const double2 *b, int nparts, long stride
 }
 
 template <int P> void extract_ifft(const double2 *Z, double scale, double2 *out, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_extract_ifft<P>, smem_grids<P>(1)); init = true; }
 	k_extract_ifft<P><<<1, Geo<P>::NT, smem_grids<P>(1), s>>>(Z, scale, out);
 	QB_CUDA(cudaGetLastError());
@@ -1019,7 +1146,7 @@ template <int P> struct I3S {
 
 // N = 64 single integrals on the split kernels (FP64)
 void extract_ifft128(const double2 *Z, double scale, double2 *out, cudaStream_t s) {
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_extract_ifft128, smem128<double2>(), init);
 	launch128(k_extract_ifft128, "assemble", 2, 2, smem128<double2>(), s, Z, scale, out);
 }
@@ -1124,7 +1251,7 @@ void integral_i3(Workspace &ws, const DevI3 &t, const double2 *f, const double2 
 namespace {
 template <int N> void launch_to_fourier(int ngrids, const double *Wv, double2 *Wf, cudaStream_t s) {
 	const size_t sm = sizeof(double2) * (N * (N + 1) + N);
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_to_fourier<N>, sm, init);
 	ProfScope ps("to_fourier", s);
 	k_to_fourier<N><<<ngrids, Len<N>::T * N, sm, s>>>(Wv, Wf);
@@ -1132,7 +1259,7 @@ template <int N> void launch_to_fourier(int ngrids, const double *Wv, double2 *W
 }
 template <int N> void launch_from_fourier(int ngrids, const double2 *Wf, double *Wv, cudaStream_t s) {
 	const size_t sm = sizeof(double2) * (N * (N + 1) + N);
-	static bool init = false;
+	static DeviceFlag init;
 	set_smem_once(k_from_fourier<N>, sm, init);
 	ProfScope ps("from_fourier", s);
 	k_from_fourier<N><<<ngrids, Len<N>::T * N, sm, s>>>(Wf, Wv);
@@ -1358,7 +1485,7 @@ bool fft2_generic_supported(int n0, int n1) {
 namespace {
 template <int L, int DIR> void launch_generic(bool r2c, const void *in, double2 *out, cudaStream_t s) {
 	const size_t sm = sizeof(double2) * (L * (L + 1) + L);
-	static bool init = false;
+	static DeviceFlag init;
 	if (!init) { set_smem(k_fft2_generic<L, DIR>, sm); init = true; }
 	k_fft2_generic<L, DIR><<<1, Len<L>::T * L, sm, s>>>(in, out, r2c ? 1 : 0);
 	QB_CUDA(cudaGetLastError());

@@ -24,6 +24,10 @@ void fail(const char *file, int line, const std::string &msg);
 bool supported_n(int N);      // grid sizes with compiled kernels
 
 // ---- device buffers ---------------------------------------------------------
+// Process-wide count of device-buffer reallocations and releases: a captured
+// CUDA graph holds raw buffer addresses, so it is replayed only while this
+// count is unchanged since its capture.
+unsigned long long buffer_generation();
 struct DevBuf {
 	void *p = nullptr;
 	size_t bytes = 0;
@@ -89,10 +93,20 @@ struct Workspace {
 	DevBuf i3kind;                           // N = 64, FP32: per-cell I3 kernel (0 real form, 1 complex)
 	DevBuf i3stats;                          // N = 64, FP32: cells evaluated by the real form, by either form (2 x u64)
 	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
-	// replay of a repeated Strang step (batched API): the launch sequence of
-	// one (pointers, parameters) key is captured once and relaunched
-	std::vector<double> graph_key;
-	cudaGraphExec_t graph_exec = nullptr;
+	// replay of repeated Strang steps (batched API): the launch sequence of a
+	// (pointers, parameters) key is captured on its second call and relaunched
+	// afterwards; a few keys are kept, so that ping-pong buffers replay too
+	struct GraphEntry {
+		std::vector<double> key;
+		cudaGraphExec_t exec = nullptr;
+		unsigned long long generation = 0;   // buffer_generation() when the key was sized / captured
+		unsigned long long last_use = 0;
+		long kernels = 0;                    // kernel nodes of the captured sequence
+	};
+	static constexpr int kGraphSlots = 4;
+	std::vector<GraphEntry> graphs;
+	unsigned long long graph_clock = 0;
+	long graph_replays = 0;                  // launches served by an instantiated graph
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 	explicit Workspace(int N);
 	~Workspace();
@@ -163,8 +177,11 @@ std::string last_error();
 // launches and, while profiling is enabled, brackets the launch with CUDA
 // events on its stream so per-kernel device time can be read back.
 void prof_enable(bool on);
+bool prof_enabled();
 void prof_reset();
+// kernels launched so far, the nodes of replayed CUDA graphs included
 long launch_count();
+void add_launches(long n);
 // total device milliseconds and launches recorded for kernels whose name starts with `prefix`
 void prof_read(const char *prefix, double *ms, long *launches);
 struct ProfScope {

@@ -24,6 +24,21 @@ template <class F> int guarded(F &&f) {
 	}
 }
 
+// makes `dev` current for its scope and restores the caller's device on every exit path
+struct DeviceGuard {
+	int prev = -1;
+	explicit DeviceGuard(int dev) {
+		QB_CUDA(cudaGetDevice(&prev));
+		if (dev != prev) QB_CUDA(cudaSetDevice(dev));
+	}
+	~DeviceGuard() {
+		int cur = -1;
+		if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+	}
+	DeviceGuard(const DeviceGuard &) = delete;
+	DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 // the caller's stream as given; NULL is the legacy default stream (torch's default stream)
 cudaStream_t pick(const qb_workspace *, void *stream) { return (cudaStream_t)stream; }
 
@@ -61,36 +76,70 @@ bool graphs_enabled() {
 	return e == nullptr || strcmp(e, "0") != 0;
 }
 
-// One Strang step through a CUDA graph: the first call with a new key runs
-// the launch sequence directly (sizing every buffer), the second captures it
-// on the workspace stream, later calls relaunch the instantiated graph.  The
-// caller's stream is ordered before and after through events.
+// One Strang step through a CUDA graph.  The workspace keeps up to
+// kGraphSlots keys (pointers and parameters of a call).  A key's first call
+// runs the launch sequence directly (sizing every buffer); its second call
+// captures the sequence on the workspace stream; later calls relaunch the
+// instantiated graph.  A graph is dropped when any device buffer was
+// reallocated or released since it was sized (buffer_generation), because
+// it holds raw addresses.  While kernel profiling is on (qb_profile_enable),
+// steps launch kernel by kernel, because per-kernel event timing needs
+// individual launches.  The caller's stream is ordered before and after
+// through events.
 void inhom_step_graphed(qb_workspace *ws, const qb_quad *q, int ncells, const double *W, double *Wnext, double h, double dt,
                         const double *Bext, int bc, cudaStream_t caller) {
 	const double *A = velocity_tables(ws, q->q->L, caller);
 	const std::vector<double> key = { (double)ncells, (double)(uintptr_t)W, (double)(uintptr_t)Wnext, h, dt,
 	                                  (double)(uintptr_t)Bext, (double)bc, (double)(uintptr_t)q, q->q->L, (double)ws->prec, (double)ws->conserve };
-	if (!graphs_enabled() || key != ws->graph_key) {
-		if (ws->graph_exec) { cudaGraphExecDestroy(ws->graph_exec); ws->graph_exec = nullptr; }
-		ws->graph_key = key;
-		qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, caller);
+	auto direct = [&] { qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, caller); };
+	if (!graphs_enabled() || qb::prof_enabled()) { direct(); return; }
+	qb::Workspace::GraphEntry *e = nullptr;
+	for (auto &g : ws->graphs)
+		if (g.key == key) { e = &g; break; }
+	if (e == nullptr) {
+		if ((int)ws->graphs.size() < qb::Workspace::kGraphSlots) {
+			ws->graphs.emplace_back();
+			e = &ws->graphs.back();
+		} else {
+			e = &*std::min_element(ws->graphs.begin(), ws->graphs.end(),
+			                       [](const qb::Workspace::GraphEntry &a, const qb::Workspace::GraphEntry &b) { return a.last_use < b.last_use; });
+			if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+		}
+		e->key = key;
+		e->last_use = ++ws->graph_clock;
+		direct();
+		e->generation = qb::buffer_generation();
+		return;
+	}
+	e->last_use = ++ws->graph_clock;
+	if (e->generation != qb::buffer_generation()) {
+		// buffers moved since this key was sized or captured: run directly, capture on the next call
+		if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+		direct();
+		e->generation = qb::buffer_generation();
 		return;
 	}
 	if (ws->ev_in == nullptr) {
 		QB_CUDA(cudaEventCreateWithFlags(&ws->ev_in, cudaEventDisableTiming));
 		QB_CUDA(cudaEventCreateWithFlags(&ws->ev_out, cudaEventDisableTiming));
 	}
-	if (ws->graph_exec == nullptr) {
+	if (e->exec == nullptr) {
 		cudaGraph_t g = nullptr;
+		const long before = qb::launch_count();
 		QB_CUDA(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal));
 		qb::inhom_step(*ws, q->q->set(), ncells, W, Wnext, A, h, dt, Bext, bc, ws->stream);
 		QB_CUDA(cudaStreamEndCapture(ws->stream, &g));
-		QB_CUDA(cudaGraphInstantiate(&ws->graph_exec, g, 0));
+		QB_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
 		cudaGraphDestroy(g);
+		e->kernels = qb::launch_count() - before;     // counted once here, for this first launch of the graph
+		e->generation = qb::buffer_generation();
+	} else {
+		ws->graph_replays++;
+		qb::add_launches(e->kernels);
 	}
 	QB_CUDA(cudaEventRecord(ws->ev_in, caller));
 	QB_CUDA(cudaStreamWaitEvent(ws->stream, ws->ev_in, 0));
-	QB_CUDA(cudaGraphLaunch(ws->graph_exec, ws->stream));
+	QB_CUDA(cudaGraphLaunch(e->exec, ws->stream));
 	QB_CUDA(cudaEventRecord(ws->ev_out, ws->stream));
 	QB_CUDA(cudaStreamWaitEvent(caller, ws->ev_out, 0));
 }
@@ -146,7 +195,7 @@ int qb_workspace_i3_forms(qb_workspace *ws, long long *real_cells, long long *al
 	return guarded([&] {
 		if (ws == nullptr || real_cells == nullptr || all_cells == nullptr) QB_FAIL("null argument");
 		unsigned long long h[2] = { 0, 0 };
-		QB_CUDA(cudaSetDevice(ws->device));
+		DeviceGuard dg(ws->device);
 		QB_CUDA(cudaDeviceSynchronize());
 		QB_CUDA(cudaMemcpy(h, ws->i3stats.p, sizeof(h), cudaMemcpyDeviceToHost));
 		*real_cells = (long long)h[0];
@@ -311,6 +360,7 @@ int qb_profile_read(const char *prefix, double *ms, long *launches) {
 	return guarded([&] { qb::prof_read(prefix ? prefix : "", ms, launches); });
 }
 long qb_launch_count(void) { return qb::launch_count(); }
+long qb_workspace_graph_replays(const qb_workspace *ws) { return ws ? ws->graph_replays : -1; }
 
 }  // extern "C"
 

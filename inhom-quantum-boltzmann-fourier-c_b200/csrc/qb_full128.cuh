@@ -548,34 +548,47 @@ __global__ void __launch_bounds__(F128::NT, 1) k_i3_full128r(const I3ParamsT<flo
 	if (warp == 0) tmem_dealloc(tbase, TM::NCOLS);
 }
 
-// per cell: 1 when the Nyquist content of the Fourier state W ([cell][4][N*N],
-// natural order k + N l) exceeds `bound` times its total (sums of |W| over the
-// 4 components; Nyquist = row l = N/2 and column k = N/2), else 0.  stats
-// (may be null) counts the cells of kind 0 and all cells.
+// per cell: 0 (real form) when both
+//   - the Nyquist content of the Fourier state W ([cell][4][N*N], natural
+//     order k + N l; Nyquist = row l = N/2 and column k = N/2), and
+//   - its anti-Hermitian part, sum of |W(k) - conj W(-k)| over the other
+//     entries (nonzero when a velocity-space component is not real)
+// are at most `bound` times the total (sums of |W| over the 4 components),
+// else 1 (complex kernel).  stats (may be null) counts the cells of kind 0
+// and all cells.
 constexpr int kNyqThreads = 256;
 __global__ void __launch_bounds__(kNyqThreads) k_nyquist_kind(int N, const double2 *__restrict__ W, double bound, int *__restrict__ kind,
                                                              unsigned long long *stats) {
-	__shared__ double red[2][kNyqThreads / 32];
+	__shared__ double red[3][kNyqThreads / 32];
 	const long NN = (long)N * N;
 	const double2 *w = W + blockIdx.x * 4 * NN;
-	double tot = 0.0, nyq = 0.0;
+	double tot = 0.0, nyq = 0.0, anti = 0.0;
 	for (long i = threadIdx.x; i < 4 * NN; i += kNyqThreads) {
+		const long c = i / NN;
 		const int g = (int)(i % NN), k = g % N, l = g / N;
-		const double a = hypot(w[i].x, w[i].y);
+		const double2 v = w[i];
+		const double a = hypot(v.x, v.y);
 		tot += a;
-		if (k == N / 2 || l == N / 2) nyq += a;
+		if (k == N / 2 || l == N / 2) {
+			nyq += a;
+		} else {
+			const int kc = (N - k) & (N - 1), lc = (N - l) & (N - 1);      // N is a power of 2
+			const double2 p = w[c * NN + kc + (long)N * lc];
+			anti += hypot(v.x - p.x, v.y + p.y);
+		}
 	}
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		tot += __shfl_xor_sync(0xffffffffu, tot, o);
 		nyq += __shfl_xor_sync(0xffffffffu, nyq, o);
+		anti += __shfl_xor_sync(0xffffffffu, anti, o);
 	}
-	if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = tot; red[1][threadIdx.x >> 5] = nyq; }
+	if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = tot; red[1][threadIdx.x >> 5] = nyq; red[2][threadIdx.x >> 5] = anti; }
 	__syncthreads();
 	if (threadIdx.x == 0) {
-		double t = 0.0, n = 0.0;
-		for (int i = 0; i < kNyqThreads / 32; i++) { t += red[0][i]; n += red[1][i]; }
-		const int k = (n <= bound * t) ? 0 : 1;           // NaN sums take the complex kernel
+		double t = 0.0, n = 0.0, h = 0.0;
+		for (int i = 0; i < kNyqThreads / 32; i++) { t += red[0][i]; n += red[1][i]; h += red[2][i]; }
+		const int k = (n <= bound * t && h <= bound * t) ? 0 : 1;     // NaN sums take the complex kernel
 		kind[blockIdx.x] = k;
 		if (stats != nullptr) {
 			atomicAdd(&stats[0], (unsigned long long)(k == 0));

@@ -66,6 +66,8 @@ def lib(n_grid=N_GRID):
     L.qb_transport.argtypes = [C.c_int, C.c_double, C.c_int, _vp, _vp, C.c_double, C.c_double, C.c_int, _vp]
     L.qb_fourier_collision.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, _vp]
     L.qb_launch_count.restype = C.c_long
+    L.qb_workspace_graph_replays.restype = C.c_long
+    L.qb_workspace_graph_replays.argtypes = [_vp]
     L.qb_fp64_peak_tflops.restype = C.c_double
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
@@ -173,6 +175,11 @@ class Workspace:
         r, a = C.c_longlong(), C.c_longlong()
         _check(lib().qb_workspace_i3_forms(self.h, C.byref(r), C.byref(a), 1 if reset else 0), "qb_workspace_i3_forms")
         return r.value, a.value
+
+    @property
+    def graph_replays(self):
+        """Strang steps of inhom_step served by relaunching a captured CUDA graph."""
+        return lib().qb_workspace_graph_replays(self.h)
 
     def __del__(self):
         if getattr(self, "h", None) and getattr(self, "_free", None):

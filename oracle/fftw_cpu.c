@@ -31,6 +31,12 @@ static pthread_mutex_t tw_lock = PTHREAD_MUTEX_INITIALIZER;
 
 static const cplx *twiddles(int n)
 {
+	/* lock-free hit path: a slot's table is published before its size */
+	for (int i = 0; i < TW_MAX; i++) {
+		int ni = __atomic_load_n(&tw_cache[i].n, __ATOMIC_ACQUIRE);
+		if (ni == n) return tw_cache[i].w;
+		if (ni == 0) break;
+	}
 	pthread_mutex_lock(&tw_lock);
 	for (int i = 0; i < TW_MAX; i++) {
 		if (tw_cache[i].n == n) { const cplx *w = tw_cache[i].w; pthread_mutex_unlock(&tw_lock); return w; }
@@ -51,16 +57,18 @@ static const cplx *twiddles(int n)
 	int slot = -1;
 	for (int i = 0; i < TW_MAX; i++) if (tw_cache[i].n == 0) { slot = i; break; }
 	if (slot < 0) { pthread_mutex_unlock(&tw_lock); abort(); }   /* more distinct sizes than any caller uses */
-	tw_cache[slot].n = n;
 	tw_cache[slot].w = w;
+	__atomic_store_n(&tw_cache[slot].n, n, __ATOMIC_RELEASE);
 	pthread_mutex_unlock(&tw_lock);
 	return w;
 }
 
-/* twiddle exp(sign * 2 pi i e / n) from the forward table */
+/* twiddle exp(sign * 2 pi i e / n) from the forward table; every caller
+ * passes 0 <= e < n (exponents are reduced by construction) */
 static inline cplx tw_get(const cplx *w, int n, long e, int sign)
 {
-	cplx t = w[e % n];
+	(void)n;
+	cplx t = w[e];
 	if (sign > 0) t.im = -t.im;
 	return t;
 }

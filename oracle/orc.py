@@ -211,7 +211,8 @@ def ref_lib():
         L.ref_ctx_create.restype = C.c_void_p
         L.ref_ctx_create.argtypes = [C.c_uint, C.c_uint, C.c_double, C.c_double]
         for n in ("ref_ctx_free", "ref_table_num", "ref_table_copy", "ref_i1", "ref_i2", "ref_i3", "ref_cc", "ref_cd",
-                  "ref_collision_step", "ref_inhom_step", "ref_inhom_step_maxwell", "ref_sim_hom"):
+                  "ref_collision_step", "ref_inhom_step", "ref_inhom_step_maxwell", "ref_sim_hom",
+                  "ref_sim_inhom_periodic"):
             getattr(L, n).argtypes = None
         L.ref_table_num.restype = C.c_uint
         L.CalculateRightwardFlux.restype = C.c_double
@@ -288,6 +289,15 @@ class Ref:
     def simulation_homogeneous(self, W0, dt, numsteps, B=(0.0, 0.0, 0.0)):
         W0 = _r(W0); out = np.zeros((numsteps,) + W0.shape); Bv = _r(B)
         ref_lib().ref_sim_hom(self.h, _ptr(W0), C.c_double(dt), C.c_uint(numsteps), _ptr(Bv), _ptr(out)); return out
+
+    def sim_inhom_periodic(self, W0, h, dt, steps, Bext=None):
+        """SimulationInhomogeneousPeriodic over `steps` Strang steps: frames
+        (steps + 1, cells, 4, N, N), frame 0 = W0."""
+        W0 = _r(W0); n = W0.shape[0]; out = np.zeros((steps + 1,) + W0.shape)
+        Bext = _r(np.zeros((n, 3)) if Bext is None else Bext)
+        ref_lib().ref_sim_inhom_periodic(self.h, C.c_uint(n), C.c_double(self.L), _ptr(W0), C.c_double(h), C.c_double(dt),
+                                         C.c_uint(steps + 1), _ptr(Bext), _ptr(out))
+        return out
 
 
 def ref_to_fourier(Wv):

@@ -167,3 +167,15 @@ void ref_to_fourier(const double *Wv, double *Wf)
 	fftw_free(in);
 	fftw_free(WFh);
 }
+
+/* SimulationInhomogeneousPeriodic (src/simulation.c:1288-1301): numsteps
+ * frames of numVol cells, frame 0 = W0, written to Wevolv */
+void ref_sim_inhom_periodic(void *p, unsigned numVol, double L, const double *W0, double h, double dt,
+                            unsigned numsteps, const double *Bext, double *Wevolv)
+{
+	ref_ctx *c = p;
+	inhomStepInterm_t it; InhomStepInterm_Create(numVol, L, &it);
+	SimulationInhomogeneousPeriodic((const wignerV_t *)W0, &c->q1, &c->q2, &c->q3, &c->q4, h, dt, numsteps, Bext, &it,
+	                                (wignerV_t *)Wevolv);
+	InhomStepInterm_Delete(&it);
+}

@@ -12,7 +12,22 @@ import qbgpu
 from conftest import REPO
 
 INCLUDE = os.path.join(REPO, "include")
-UPSTREAM = "/root/reference"
+
+
+def _upstream_dir():
+    """The upstream checkout: $QB_REFERENCE_DIR, else the REF default of the
+    oracle's build recipe (oracle/Makefile), which is overridable the same way."""
+    d = os.environ.get("QB_REFERENCE_DIR")
+    if d:
+        return d
+    try:
+        r = subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "print-ref"], capture_output=True, text=True, timeout=30)
+        return r.stdout.strip() if r.returncode == 0 else ""
+    except (OSError, subprocess.SubprocessError):
+        return ""
+
+
+UPSTREAM = _upstream_dir()
 
 
 def declared_functions():
@@ -67,7 +82,7 @@ DRIVERS = ["test/I1_test.c", "test/I2_test.c", "test/I2_test2.c", "test/I3_test.
            "test/slope_lim_test2.c", "src/main_hom.c", "src/main_inhom.c"]
 
 
-@pytest.mark.skipif(not os.path.isdir(UPSTREAM) or shutil.which("gcc") is None, reason="upstream drivers not available here")
+@pytest.mark.skipif(not UPSTREAM or not os.path.isdir(UPSTREAM) or shutil.which("gcc") is None, reason="upstream drivers not available here")
 @pytest.mark.parametrize("driver", DRIVERS)
 def test_upstream_driver_links_unchanged(driver, tmp_path):
     """Compile the unmodified upstream driver with its own flags against

@@ -65,3 +65,39 @@ def test_graph_replay_equals_direct_launches(env, monkeypatch):
     direct = qbgpu.inhom_step(ws2, q, W, h, dt, B)
     torch.cuda.synchronize()
     assert torch.equal(direct, results[0])
+
+
+def test_alternating_buffers_replay_their_graphs(env):
+    """Steps that alternate two state buffers (A -> B, B -> A, ...) keep one
+    graph per direction: from the third step of each direction on, every
+    step is a graph replay, its kernels are counted, and the trajectory is
+    bit-identical to kernel-by-kernel launches."""
+    q, _, _ = env
+    L_ = qbgpu.lib()
+    ws = qbgpu.Workspace(N)
+    W = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=54, ncells=4)).cuda()
+    B = torch.zeros((4, 3), dtype=torch.float64, device="cuda")
+    h, dt = 0.25, 0.01
+    bufs = [W.clone(), torch.empty_like(W)]
+    steps = 10
+    counts = []
+    for k in range(steps):
+        c0 = L_.qb_launch_count()
+        qbgpu.inhom_step(ws, q, bufs[k % 2], h, dt, B, out=bufs[(k + 1) % 2])
+        counts.append(L_.qb_launch_count() - c0)
+    torch.cuda.synchronize()
+    # calls 0, 1 run directly (one per key), 2, 3 capture, 4.. replay
+    assert ws.graph_replays == steps - 4
+    assert len(set(counts)) == 1 and counts[0] > 0      # replays count the graph's kernel nodes
+    ref = W.clone()
+    wsd = qbgpu.Workspace(N)
+    L_.qb_profile_enable(1)                             # profiling on: kernel-by-kernel launches
+    try:
+        for k in range(steps):
+            ref = qbgpu.inhom_step(wsd, q, ref, h, dt, B)
+        torch.cuda.synchronize()
+    finally:
+        L_.qb_profile_enable(0)
+        L_.qb_profile_reset()
+    assert wsd.graph_replays == 0
+    assert torch.equal(bufs[steps % 2], ref)

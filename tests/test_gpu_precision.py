@@ -96,6 +96,35 @@ def test_fp32_n64_real_form_and_guard():
         assert rel_l2(cd[sl], ref_cd) <= C_TOL
 
 
+@pytest.mark.parametrize("N,J,M", [(32, 4, 3), (64, 4, 3)])
+def test_fp32_real_form_guard_routes_non_hermitian_states(N, J, M):
+    """The real form of the FP32 I3 sums (N = 32: k_i3pr, N = 64:
+    k_i3_full128r) holds only for Fourier states of real velocity-space
+    components (Hermitian, W(-k) = conj W(k)) without Nyquist content.  Two
+    smooth cells take it; two cells with an anti-Hermitian part (a complex
+    perturbation kept off the Nyquist row and column, so that only the
+    Hermitian check can catch it) take the complex kernel, and all four stay
+    within the FP32 bound of the oracle, which evaluates general complex
+    states."""
+    o = orc.Oracle(N, J, M, L, R)
+    q = qbgpu.Quad(N, J, M, L, R)
+    _, Wf = fourier_states(N, 4, seed=90 + N)
+    rng = np.random.default_rng(N)
+    noise = rng.standard_normal(Wf[2:].shape) + 1j * rng.standard_normal(Wf[2:].shape)
+    noise[..., N // 2, :] = 0
+    noise[..., :, N // 2] = 0
+    Wf[2:] += 1e-4 * np.abs(Wf[2:]).max() * noise
+    ws32 = qbgpu.Workspace(N, precision=32)
+    cc, cd = qbgpu.collision_operators(ws32, q, torch.from_numpy(Wf).cuda())
+    assert ws32.i3_forms() == (2, 4)
+    cc, cd = cc.cpu().numpy(), cd.cpu().numpy()
+    for sl in (slice(0, 2), slice(2, 4)):
+        ref_cc = np.stack([o.cc(w) for w in Wf[sl]])
+        ref_cd = np.stack([o.cd(w) for w in Wf[sl]])
+        assert rel_l2(cc[sl], ref_cc) <= C_TOL, sl
+        assert rel_l2(cd[sl], ref_cd) <= C_TOL, sl
+
+
 def conserved_totals(W):
     """mass, momentum (x, y) and kinetic energy of the trace component summed over all cells"""
     d = orc.diagnostics(W, L)

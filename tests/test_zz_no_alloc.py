@@ -14,6 +14,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import orc
 import qbgpu
 from conftest import rel_l1
 
@@ -36,10 +37,13 @@ def _grids(N, seed):
     return [torch.from_numpy(rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))).cuda() for _ in range(3)]
 
 
-@pytest.mark.parametrize("N,J,M", [(32, 32, 7), (16, 6, 5)])
+@pytest.mark.parametrize("N,J,M", [(32, 32, 7), (16, 6, 5), (8, 4, 3)])
 def test_noalloc_matches_allocating_entry_point(N, J, M):
+    """every grid size the entry point dispatches (N = 8, 16, 32), against the
+    allocating entry point and against the CPU oracle's I3integral"""
     fn = _noalloc_fn()
     q, ws = qbgpu.Quad(N, J, M, 12.0, 7.5), qbgpu.Workspace(N)
+    o = orc.Oracle(N, J, M, 12.0, 7.5)
     for seed in (1, 2):                       # two calls in a row sharing the static scratch
         f, g, h = _grids(N, seed)
         ref = qbgpu.integral(ws, q, 3, f, g, h)
@@ -47,5 +51,8 @@ def test_noalloc_matches_allocating_entry_point(N, J, M):
         rc = fn(q.h, qbgpu._ptr(f), qbgpu._ptr(g), qbgpu._ptr(h), qbgpu._ptr(out), qbgpu._stream())
         assert rc == 0, qbgpu.lib().qb_last_error().decode()
         torch.cuda.synchronize()
-        err = rel_l1(out.cpu().numpy(), ref.cpu().numpy())
+        got = out.cpu().numpy()
+        err = rel_l1(got, ref.cpu().numpy())
         assert err < TOL, (seed, err)
+        want = o.i3(f.cpu().numpy(), g.cpu().numpy(), h.cpu().numpy())
+        assert rel_l1(got, want) < TOL, seed

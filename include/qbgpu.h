@@ -48,6 +48,19 @@ void qb_workspace_free(qb_workspace *ws);
 int qb_workspace_set_precision(qb_workspace *ws, int bits);
 int qb_workspace_precision(const qb_workspace *ws);
 
+/* I3 sums of the collision operator (no upstream counterpart): variant 0
+ * (default) runs the hand-written FFT kernels; variant 1 runs every 1-D pass
+ * of the I3 chains as a GEMM against the DFT matrix on the tensor cores
+ * (tcgen05.mma, TF32 operands split hi + lo, FP32 accumulation).  Variant 1
+ * applies to the FP32 form at N = 16; other sizes and FP64 ignore it. */
+int qb_workspace_set_i3_variant(qb_workspace *ws, int variant);
+
+/* Synchronises the workspace's device and returns (then clears) its device
+ * error word: 0 when no kernel with a bounded wait (the tensor-core I3
+ * variant) gave up on a wait since the last call, 1 if one did (its outputs
+ * are NaN), -1 on a host error. */
+int qb_workspace_device_errors(qb_workspace *ws);
+
 /* on != 0: the velocity-space steps through `ws` (qb_inhom_step,
  * qb_inhom_step_maxwell, qb_fourier_collision, qb_simulate_record) restore,
  * after each collision, the mass, momentum and energy of the trace component
@@ -183,6 +196,13 @@ int qb_relative_entropy(int N, double L, int ncells, const double *W, const doub
 int qb_profile_enable(int on);
 int qb_profile_reset(void);
 int qb_profile_read(const char *prefix, double *ms, long *launches);
+/* Tensor-core self-check (no upstream counterpart): D (128 x 64) = A (128 x 64)
+ * x B (64 x 64) through tcgen05.mma kind::tf32 in one CTA, with both
+ * operands in the K-major shared-memory layout that the DFT-as-GEMM kernels
+ * use; Bt is B transposed (row n = column n of B).  Operands are rounded to
+ * TF32 (nearest); device pointers, row-major FP32. */
+int qb_umma_selftest(const float *A, const float *Bt, float *D, void *stream);
+
 /* kernels launched so far by this library, the kernel nodes of replayed CUDA
  * graphs included */
 long qb_launch_count(void);

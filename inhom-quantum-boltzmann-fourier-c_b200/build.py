@@ -26,7 +26,7 @@ LIB = os.path.join(HERE, "lib")
 OBJ = os.path.join(HERE, "_build")
 
 SOURCES = ["qb_engine.cu", "qb_tables.cu", "qb_abi.cu", "qb_fftw.cu", "qb_ext.cu", "qb_noalloc.cu", "qb_diag.cu", "qb_batch.cu",
-           "qb_fno.cu", "qb_surrogate.cu"]
+           "qb_fno.cu", "qb_surrogate.cu", "qb_dftmma.cu"]
 # sources that depend on N_GRID (the upstream ABI); the others are grid-size independent
 NGRID_SOURCES = {"qb_abi.cu", "qb_ext.cu"}
 

@@ -580,20 +580,24 @@ void SlopeLimiterStepMaxwell(const double h, const double dt, const unsigned int
 // ---- util.h (upstream src/util.c): raw binary I/O ---------------------------------------
 int ReadData(const char *filename, void *data, const size_t size, const size_t n) {
 	FILE *fd = fopen(filename, "rb");
-	if (fd == NULL) { fprintf(stderr, "'fopen()' failed during call of 'ReadData()'.\n"); return -1; }
+	if (fd == NULL) { fprintf(stderr, "ReadData: cannot open '%s' for reading\n", filename); return -1; }
 	fseek(fd, 0, SEEK_END);
 	const long filesize = ftell(fd);
 	rewind(fd);
-	if ((size_t)filesize != n * size) { fprintf(stderr, "'ReadData()' failed: expected file size does not match.\n"); fclose(fd); return -2; }
-	if (fread(data, size, n, fd) != n) { fprintf(stderr, "'fread()' failed during call of 'ReadData()'.\n"); fclose(fd); return -3; }
+	if ((size_t)filesize != n * size) {
+		fprintf(stderr, "ReadData: '%s' holds %ld bytes, the caller expects %zu\n", filename, filesize, n * size);
+		fclose(fd);
+		return -2;
+	}
+	if (fread(data, size, n, fd) != n) { fprintf(stderr, "ReadData: short read from '%s'\n", filename); fclose(fd); return -3; }
 	fclose(fd);
 	return 0;
 }
 
 int WriteData(const char *filename, const void *data, const size_t size, const size_t n, const bool append) {
 	FILE *fd = fopen(filename, append ? "ab" : "wb");
-	if (fd == NULL) { fprintf(stderr, "'fopen()' failed during call of 'WriteData()'.\n"); return -1; }
-	if (fwrite(data, size, n, fd) != n) { fprintf(stderr, "'fwrite()' failed during call of 'WriteData()'.\n"); fclose(fd); return -3; }
+	if (fd == NULL) { fprintf(stderr, "WriteData: cannot open '%s' for writing\n", filename); return -1; }
+	if (fwrite(data, size, n, fd) != n) { fprintf(stderr, "WriteData: short write to '%s'\n", filename); fclose(fd); return -3; }
 	fclose(fd);
 	return 0;
 }

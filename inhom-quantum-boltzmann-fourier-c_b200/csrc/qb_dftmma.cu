@@ -1,0 +1,441 @@
+// qb_dftmma.cu — DFT-as-GEMM on the tensor cores (tcgen05.mma, kind::tf32).
+//
+// A length-P complex DFT along the rows of a batch of grids is a real GEMM:
+// with row vectors x = xr + i xi and F[k][k'] = exp(-2 pi i k k' / P),
+//   [yr | yi] = [xr | xi] x [[Fr, Fi], [-Fi, Fr]]        (K = N = 2P).
+// The inverse transform is conj(DFT(conj(x))), so one matrix serves both
+// directions.  TF32 keeps 10 explicit mantissa bits; three products of a
+// hi/lo split, A_hi B_hi + A_hi B_lo + A_lo B_hi with X_hi = tf32(X) and
+// X_lo = tf32(X - X_hi), give about 2^-21 relative accuracy per GEMM, which
+// the FP32 form's 1e-5 bound allows.
+#include "qb_engine.h"
+#include "qb_kernels.cuh"
+#include "qb_umma.cuh"
+
+#include <vector>
+
+extern "C" {
+#include "qbgpu.h"
+}
+
+namespace qb {
+namespace {
+
+constexpr unsigned kWaitPolls = 1u << 24;      // bounded mbarrier waits (about a second)
+
+__device__ __forceinline__ unsigned char *align1024(unsigned char *p) {
+	const uintptr_t a = (uintptr_t)p;
+	return (unsigned char *)((a + 1023) & ~(uintptr_t)1023);
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// D (128 x 64) = A (128 x 64) x B (64 x 64) with B given transposed (Bt: 64 x 64,
+// row n = column n of B), one CTA of 128 threads: a check of the K-major
+// operand layouts and descriptors on the device.  err[0] is set when the MMA
+// did not complete within the poll limit.
+__global__ void __launch_bounds__(128, 1) k_umma_selftest(const float *__restrict__ A, const float *__restrict__ Bt,
+                                                          float *__restrict__ D, int *err) {
+	extern __shared__ unsigned char smem_raw[];
+	unsigned char *base = align1024(smem_raw);
+	unsigned char *sA = base, *sB = base + 128 * 64 * 4;
+	__shared__ uint64_t mbar;
+	__shared__ uint32_t tslot;
+	const int t = threadIdx.x, warp = t >> 5;
+	for (int k = 0; k < 64; k++) {
+		const float v = umma::tf32_round(A[t * 64 + k]);
+		*reinterpret_cast<float *>(sA + umma::kmajor_off(128, t, k)) = v;
+	}
+	if (t < 64)
+		for (int k = 0; k < 64; k++) *reinterpret_cast<float *>(sB + umma::kmajor_off(64, t, k)) = umma::tf32_round(Bt[t * 64 + k]);
+	if (t == 0) {
+		umma::mbar_init(&mbar, 1);
+		fence_mbar_init();
+	}
+	if (warp == 0) tmem_alloc(&tslot, 64);
+	umma::fence_async_smem();
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const uint32_t d = tslot;
+	if (t == 0) {
+		const uint32_t a0 = umma::smem_u32(sA), b0 = umma::smem_u32(sB);
+		for (int kk = 0; kk < 8; kk++) {
+			const uint64_t ad = umma::desc_sw128(a0 + (kk >> 2) * 16384 + (kk & 3) * 32, 16, 1024);
+			const uint64_t bd = umma::desc_sw128(b0 + (kk >> 2) * 8192 + (kk & 3) * 32, 16, 1024);
+			umma::mma_tf32(d, ad, bd, umma::idesc_tf32<128, 64>(), kk > 0);
+		}
+		umma::commit(&mbar);
+	}
+	__syncwarp();
+	const bool ok = umma::mbar_wait(&mbar, 0, kWaitPolls);
+	tmem_fence_after();
+	if (!ok) {
+		if ((t & 31) == 0) atomicExch(err, 1);
+	} else {
+		for (int c = 0; c < 64; c += 16) {
+			float v[16];
+			umma::tmem_ld16(d + ((uint32_t)(32 * warp) << 16) + c, v);
+			tmem_wait_ld();
+#pragma unroll
+			for (int i = 0; i < 16; i++) D[t * 64 + c + i] = v[i];
+		}
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(d, 64);
+}
+
+constexpr size_t kSelftestSmem = 128 * 64 * 4 + 64 * 64 * 4 + 1024;
+
+// ---------------------------------------------------------------------------
+// I3 sums of the FP32 form at N = 16 (padded grids of P = 32) as DFT-GEMMs.
+//
+// One CTA per (cell, chunk of terms), two warpgroups.  A tile is 4 grids of
+// 32 rows (128 rows, row (q, lane) in tensor-memory lane 32 q + lane); every
+// 1-D pass of a chain is one tile GEMM against the real-ified DFT matrix,
+// K = N = 64, as 3 x 8 tcgen05.mma of M128 N64 K8 (TF32 hi/lo split).
+// Between passes each thread reads its row of D from tensor memory and
+// writes the next A tile: its own row (a pass along the same axis) or, for
+// a pass along the other axis, one column of the next tile (the transpose).
+// Per term:
+//   P_c = FFT2(Pad(psi1_t . W_c))   warpgroup 0, tile rows (c, l)
+//   for combos c = wg, wg + 2:      tile rows (r, l) of outputs r = 0..3
+//     a = G_g . P_r -> IFFT along k -> IFFT along l -> x psi2_t
+//       -> FFT along l -> FFT along k -> X_r += coef P_a . (result)
+// with IFFT = conj . FFT . conj, so one DFT matrix serves every pass.  The
+// sums X of a warpgroup live in tensor memory beside its D (row (r, l) of
+// X_r: real parts in 32 columns, imaginary parts in the next 32); the two
+// warpgroups' sums are added in a fixed order at the end.
+namespace dm {
+constexpr int P = 32, N = 16, K2 = 2 * P;
+constexpr int kThreads = 256;
+constexpr uint32_t kTile = 128 * K2 * 4;           // one A operand tile (32 KB)
+constexpr uint32_t kBmat = K2 * K2 * 4;            // the DFT matrix (16 KB)
+constexpr int kPitch = P + 1;                      // P grids in shared memory (complex pitch)
+constexpr uint32_t oBhi = 0, oBlo = kBmat, oA = 2 * kBmat;
+constexpr uint32_t oP = oA + 4 * kTile;            // A tiles: [warpgroup][hi, lo]
+constexpr uint32_t kSmem = oP + 4 * P * kPitch * 8 + 1024;
+constexpr uint32_t kCols = 256;                    // tensor memory: per warpgroup a 64-column D and its 64-column sums X
+}  // namespace dm
+
+__device__ __forceinline__ int pad_src(int p) { return p < dm::N / 2 ? p : (p >= 3 * dm::N / 2 ? p - dm::N : -1); }
+
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(128) : "memory"); }
+
+// this thread's row r of the hi and lo tiles: values v[0..63] (real parts, then imaginary parts)
+__device__ __forceinline__ void put_row(unsigned char *hi, unsigned char *lo, int r, const float (&v)[64]) {
+#pragma unroll
+	for (int k = 0; k < 64; k += 4) {
+		float4 h, l;
+		h.x = umma::tf32_round(v[k]);     l.x = umma::tf32_round(v[k] - h.x);
+		h.y = umma::tf32_round(v[k + 1]); l.y = umma::tf32_round(v[k + 1] - h.y);
+		h.z = umma::tf32_round(v[k + 2]); l.z = umma::tf32_round(v[k + 2] - h.z);
+		h.w = umma::tf32_round(v[k + 3]); l.w = umma::tf32_round(v[k + 3] - h.w);
+		const uint32_t o = umma::kmajor_off(128, r, k);
+		*reinterpret_cast<float4 *>(hi + o) = h;
+		*reinterpret_cast<float4 *>(lo + o) = l;
+	}
+}
+
+// the transpose: row j of this thread's D (values d[j], d[32 + j]) becomes
+// column `col` (real) and 32 + col (imaginary) of row r0 + j of the next tile
+__device__ __forceinline__ void put_col(unsigned char *hi, unsigned char *lo, int r0, int col, const float (&d)[64]) {
+#pragma unroll
+	for (int j = 0; j < 32; j++) {
+		const float hr = umma::tf32_round(d[j]), hi_ = umma::tf32_round(d[32 + j]);
+		const uint32_t o0 = umma::kmajor_off(128, r0 + j, col), o1 = umma::kmajor_off(128, r0 + j, 32 + col);
+		*reinterpret_cast<float *>(hi + o0) = hr;
+		*reinterpret_cast<float *>(lo + o0) = umma::tf32_round(d[j] - hr);
+		*reinterpret_cast<float *>(hi + o1) = hi_;
+		*reinterpret_cast<float *>(lo + o1) = umma::tf32_round(d[32 + j] - hi_);
+	}
+}
+
+// D = A_lo B_hi + A_hi B_lo + A_hi B_hi over K = 64 (8 steps of 8), issued by one thread
+__device__ __forceinline__ void issue_pass(uint32_t d, uint32_t ahi, uint32_t alo, uint32_t bhi, uint32_t blo) {
+	constexpr uint32_t id = umma::idesc_tf32<128, 64>();
+	uint32_t acc = 0;
+#pragma unroll 1
+	for (int pass = 0; pass < 3; pass++) {
+		const uint32_t a = pass == 0 ? alo : ahi, b = pass == 1 ? blo : bhi;
+#pragma unroll
+		for (int kk = 0; kk < 8; kk++) {
+			const uint64_t ad = umma::desc_sw128(a + (kk >> 2) * (128 * 128) + (kk & 3) * 32, 16, 1024);
+			const uint64_t bd = umma::desc_sw128(b + (kk >> 2) * (64 * 128) + (kk & 3) * 32, 16, 1024);
+			umma::mma_tf32(d, ad, bd, id, acc);
+			acc = 1;
+		}
+	}
+}
+
+struct MmaCtx {
+	int wg;
+	bool issuer;
+	uint32_t dcol, trow, ahi, alo, bhi, blo;
+	uint64_t *mbar;
+	volatile int *abort;          // this warpgroup's flag: set on a wait that ran out
+	unsigned phase;
+};
+
+// one pass: the staged A tile times the DFT matrix into D; on return d[] is
+// this thread's row of D.  A wait that runs out marks the warpgroup aborted;
+// later passes then issue and wait for nothing (every barrier still runs).
+__device__ __forceinline__ void mma_pass(MmaCtx &c, float (&d)[64]) {
+	umma::fence_async_smem();
+	tmem_fence_before();
+	wg_sync(c.wg);
+	tmem_fence_after();
+	const bool skip = *c.abort != 0;
+	if (!skip) {
+		if (c.issuer) {
+			issue_pass(c.dcol, c.ahi, c.alo, c.bhi, c.blo);
+			umma::commit(c.mbar);
+		}
+		__syncwarp();
+		if (!umma::mbar_wait(c.mbar, c.phase, kWaitPolls)) *c.abort = 1;
+		c.phase ^= 1u;
+		tmem_fence_after();
+	}
+#pragma unroll
+	for (int q = 0; q < 4; q++) {
+		float v[16];
+		umma::tmem_ld16(c.trow + 16 * q, v);
+		tmem_wait_ld();
+#pragma unroll
+		for (int i = 0; i < 16; i++) d[16 * q + i] = v[i];
+	}
+}
+
+__global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<float2> p, int *err) {
+	using namespace dm;
+	extern __shared__ unsigned char smem_raw[];
+	unsigned char *base = align1024(smem_raw);
+	__shared__ uint64_t mbar[2];
+	__shared__ uint32_t tslot;
+	__shared__ int abort_flag[2];
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, wg = warp >> 2, q = warp & 3;
+	const long cid = blockIdx.x;
+	const int chunk = (int)(cid % p.nchunk);
+	const long cell = cid / p.nchunk;
+	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
+	unsigned char *Ahi = base + oA + wg * 2 * kTile, *Alo = Ahi + kTile;
+	float2 *Pg = reinterpret_cast<float2 *>(base + oP);       // [4][P][kPitch], P_c[l][k] natural
+	// the real-ified DFT matrix B (K x N) as its transpose, row n = column n of B, split hi / lo
+	for (int i = tid; i < K2 * K2; i += kThreads) {
+		const int n = i / K2, k = i % K2;
+		const int e = ((k & 31) * (n & 31)) & (P - 1);
+		double sn, cs;
+		sincospi(2.0 * e / P, &sn, &cs);                     // F = exp(-2 pi i e / P) = cs - i sn
+		const double fr = cs, fi = -sn;
+		const double v = k < 32 ? (n < 32 ? fr : fi) : (n < 32 ? -fi : fr);
+		const float h = umma::tf32_round((float)v);
+		const float l = umma::tf32_round((float)(v - (double)h));
+		const uint32_t o = umma::kmajor_off(64, n, k);
+		*reinterpret_cast<float *>(base + oBhi + o) = h;
+		*reinterpret_cast<float *>(base + oBlo + o) = l;
+	}
+	if (tid == 0) {
+		umma::mbar_init(&mbar[0], 1);
+		umma::mbar_init(&mbar[1], 1);
+		fence_mbar_init();
+		abort_flag[0] = abort_flag[1] = 0;
+	}
+	if (warp == 0) tmem_alloc(&tslot, kCols);
+	umma::fence_async_smem();
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	MmaCtx mc;
+	mc.wg = wg;
+	mc.issuer = (tid & 127) == 0;
+	mc.dcol = tslot + 64u * wg;
+	mc.trow = mc.dcol + ((uint32_t)(32 * q) << 16);
+	mc.ahi = umma::smem_u32(Ahi); mc.alo = umma::smem_u32(Alo);
+	mc.bhi = umma::smem_u32(base + oBhi); mc.blo = umma::smem_u32(base + oBlo);
+	mc.mbar = &mbar[wg];
+	mc.abort = &abort_flag[wg];
+	mc.phase = 0;
+	const int row = 32 * q + lane;
+	const uint32_t xrow = mc.trow + 128;                       // this thread's row of X (sums)
+	int ncmax = 0;
+	for (int r = 0; r < 4; r++) ncmax = max(ncmax, p.ncombo[r]);
+	{
+		float z[16];
+#pragma unroll
+		for (int i = 0; i < 16; i++) z[i] = 0.0f;
+#pragma unroll
+		for (int c = 0; c < 64; c += 16) umma::tmem_st16(xrow + c, z);
+		tmem_wait_st();
+	}
+	float d[64];                                            // this thread's row: operand in, result out
+#pragma unroll 1
+	for (int t = t0; t < t1; t++) {
+		if (wg == 0) {
+			// P_q = FFT2(Pad(psi1_t . W_q)): row l = lane of the padded grid, along k, then along l
+			const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[q] * N * N;
+			const float2 *ps1 = p.psi1 + (long)t * N * N;
+			const int ls = pad_src(lane);
+#pragma unroll
+			for (int k = 0; k < P; k++) {
+				const int ks = pad_src(k);
+				float2 x = make_float2(0.0f, 0.0f);
+				if (ls >= 0 && ks >= 0) {
+					const double2 w = src[ks + N * ls];
+					x = cmul(ps1[ks + N * ls], make_float2((float)w.x, (float)w.y));
+				}
+				d[k] = x.x;
+				d[32 + k] = x.y;
+			}
+			put_row(Ahi, Alo, row, d);
+			mma_pass(mc, d);
+			put_col(Ahi, Alo, 32 * q, lane, d);
+			mma_pass(mc, d);                                    // row (q, k = lane): P_q[l][k] over l
+#pragma unroll
+			for (int l = 0; l < P; l++) Pg[(q * P + l) * kPitch + lane] = make_float2(d[l], d[32 + l]);
+		}
+		__syncthreads();                                        // P grids of the term are in place
+		const float *ps2 = p.psi2T + (long)p.psi2_idx[t] * P * P + lane * P;    // psi2[l][k = lane] at ps2[l]
+		const float sc = (float)p.psi2_scale[t];
+#pragma unroll 1
+		for (int c = wg; c < ncmax; c += 2) {
+			const bool act = c < p.ncombo[q];
+			// a = G_g . P_q on row l = lane, conjugated (inverse transforms as conj . FFT . conj)
+			if (act) {
+				const float2 *Gg = p.Ghat + cell * p.g_cell + (long)p.cgi[q][c] * P * P + lane * P;
+				const float2 *Pq = Pg + (q * P + lane) * kPitch;
+#pragma unroll
+				for (int k = 0; k < P; k++) {
+					const float2 a = cmul(Gg[k], Pq[k]);
+					d[k] = a.x;
+					d[32 + k] = -a.y;
+				}
+			} else {
+#pragma unroll
+				for (int k = 0; k < 64; k++) d[k] = 0.0f;
+			}
+			put_row(Ahi, Alo, row, d);
+			mma_pass(mc, d);                                    // along k
+			put_col(Ahi, Alo, 32 * q, lane, d);
+			mma_pass(mc, d);                                    // along l: row (q, k = lane), conj IFFT2(a) over l
+#pragma unroll
+			for (int l = 0; l < P; l++) {
+				const float f = sc * ps2[l];
+				d[l] = d[l] * f;
+				d[32 + l] = -d[32 + l] * f;
+			}
+			put_row(Ahi, Alo, row, d);
+			mma_pass(mc, d);                                    // FFT along l
+			put_col(Ahi, Alo, 32 * q, lane, d);
+			mma_pass(mc, d);                                    // FFT along k: row (q, l = lane) over k
+			if (act) {
+				const float2 *Pa = Pg + (p.ca[q][c] * P + lane) * kPitch;
+				const float coef = (float)p.ccoef[q][c];
+#pragma unroll
+				for (int h = 0; h < 2; h++) {                    // k = 16 h .. 16 h + 15
+					float xr[16], xi[16];
+					umma::tmem_ld16(xrow + 16 * h, xr);
+					umma::tmem_ld16(xrow + 32 + 16 * h, xi);
+					tmem_wait_ld();
+#pragma unroll
+					for (int i = 0; i < 16; i++) {
+						const int k = 16 * h + i;
+						const float2 y = cmul(Pa[k], make_float2(d[k], d[32 + k]));
+						xr[i] += coef * y.x;
+						xi[i] += coef * y.y;
+					}
+					umma::tmem_st16(xrow + 16 * h, xr);
+					umma::tmem_st16(xrow + 32 + 16 * h, xi);
+				}
+				tmem_wait_st();
+			}
+		}
+		__syncthreads();                                        // every chain of the term is done with Pg
+	}
+	// the two warpgroups' sums, added in a fixed order (0 + 1), to the partial-sum slot
+#pragma unroll
+	for (int c = 0; c < 64; c += 16) {
+		float x[16];
+		umma::tmem_ld16(xrow + c, x);
+		tmem_wait_ld();
+#pragma unroll
+		for (int i = 0; i < 16; i++) d[c + i] = x[i];
+	}
+	float *red = reinterpret_cast<float *>(base + oA);          // the operand tiles are free now
+	if (wg == 1) {
+#pragma unroll
+		for (int i = 0; i < 64; i++) red[i * 128 + row] = d[i];
+	}
+	__syncthreads();
+	const bool failed = abort_flag[0] != 0 || abort_flag[1] != 0;
+	if (wg == 0) {
+		float2 *o = p.out + ((cell * p.nchunk + chunk) * 4 + q) * (long)P * P + lane * P;
+		const float nanv = __int_as_float(0x7fc00000);
+#pragma unroll
+		for (int k = 0; k < P; k++)
+			o[k] = failed ? make_float2(nanv, nanv) : make_float2(d[k] + red[k * 128 + row], d[32 + k] + red[(32 + k) * 128 + row]);
+	}
+	if (failed) {
+		if (tid == 0) atomicExch(err, 1);
+		// an MMA may still be in flight after a wait ran out: give it one more bounded wait
+		if ((tid & 127) == 0 && abort_flag[wg]) umma::mbar_wait(&mbar[wg], mc.phase, kWaitPolls);
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tslot, kCols);
+}
+
+}  // namespace
+
+// launcher (engine): ncl = cells x chunks CTAs
+void launch_i3_mma32(const I3ParamsT<float2> &p, long ncl, int *err, cudaStream_t s) {
+	static bool attr_done[64] = {};
+	int dev = 0;
+	QB_CUDA(cudaGetDevice(&dev));
+	if (!attr_done[dev & 63]) {
+		QB_CUDA(cudaFuncSetAttribute(k_i3_mma32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::kSmem));
+		attr_done[dev & 63] = true;
+	}
+	ProfScope ps("i3_cluster", s);
+	k_i3_mma32<<<(unsigned)ncl, dm::kThreads, dm::kSmem, s>>>(p, err);
+	QB_CUDA(cudaGetLastError());
+}
+
+// the tensor-memory kernels of this file, for the co-residency check of the engine
+std::vector<TmemKernel> dftmma_tmem_kernels() {
+	return { { (const void *)k_i3_mma32, dm::kSmem, dm::kThreads, (int)dm::kCols, "k_i3_mma32" },
+	         { (const void *)k_umma_selftest, kSelftestSmem, 128, 64, "k_umma_selftest" } };
+}
+
+}  // namespace qb
+
+namespace {
+template <class F> int guarded_dm(F &&f) {
+	try {
+		f();
+		return 0;
+	} catch (const std::exception &) {
+		return -1;
+	}
+}
+}  // namespace
+
+extern "C" int qb_umma_selftest(const float *A, const float *Bt, float *D, void *stream) {
+	return guarded_dm([&] {
+		if (A == nullptr || Bt == nullptr || D == nullptr) QB_FAIL("qb_umma_selftest: null pointer");
+		cudaStream_t s = (cudaStream_t)stream;
+		int *err = nullptr;
+		QB_CUDA(cudaMallocAsync(&err, sizeof(int), s));
+		QB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+		QB_CUDA(cudaFuncSetAttribute(qb::k_umma_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qb::kSelftestSmem));
+		qb::k_umma_selftest<<<1, 128, qb::kSelftestSmem, s>>>(A, Bt, D, err);
+		QB_CUDA(cudaGetLastError());
+		int h = 0;
+		QB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+		QB_CUDA(cudaStreamSynchronize(s));
+		cudaFreeAsync(err, s);
+		if (h) QB_FAIL("qb_umma_selftest: the tensor-core MMA did not complete within the poll limit");
+	});
+}

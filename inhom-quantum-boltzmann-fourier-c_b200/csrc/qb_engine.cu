@@ -131,6 +131,8 @@ Workspace::Workspace(int n) : N(n) {
 	QB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 	i3stats.ensure(2 * sizeof(unsigned long long));
 	QB_CUDA(cudaMemset(i3stats.p, 0, 2 * sizeof(unsigned long long)));
+	kerr.ensure(sizeof(int));
+	QB_CUDA(cudaMemset(kerr.p, 0, sizeof(int)));
 }
 
 Workspace::~Workspace() {
@@ -187,6 +189,10 @@ int num_sms() {
 
 // before the first launch of any tensor-memory kernel on a device (defined below)
 void check_tmem_coresidency();
+}  // namespace
+// I3 sums of the FP32 form at N = 16 as DFT-GEMMs on the tensor cores (qb_dftmma.cu)
+void launch_i3_mma32(const I3ParamsT<float2> &p, long ncl, int *err, cudaStream_t s);
+namespace {
 
 template <class K> void set_smem(K kernel, size_t bytes) {
 	QB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -534,6 +540,12 @@ template <int P, class C> struct Rhs {
 			}
 			launch_i3p<C>(p, (long)ncells * nchunk, nullptr, s);
 		} else {
+			if constexpr (P == 32 && sizeof(C) == 8) {
+				if (ws.i3_variant == 1) {
+					launch_i3_mma32(p, (long)ncells * nchunk, ws.kerr.as<int>(), s);
+					return;
+				}
+			}
 			launch_i3<P, 4>(p, (long)ncells * nchunk, s);
 		}
 	}
@@ -541,6 +553,10 @@ template <int P, class C> struct Rhs {
 	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
 		T::prepare(q, s);
 		ch = pick_chunks(N, ncells, q, (int)(8 * sizeof(typename CT<C>::R)));
+		if (P == 32 && sizeof(C) == 8 && ws.i3_variant == 1 && q.i3) {
+			check_tmem_coresidency();
+			ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), num_sms(), 256, 0.15);      // one CTA per SM
+		}
 		spectra(ws, ncells, W, s);
 		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
 		if (parts & RHS_CD) {
@@ -738,8 +754,7 @@ void launch_i3_full128r(const I3ParamsT<float2> &p, long nclusters, float *pscr,
 void check_tmem_coresidency() {
 	static DeviceFlag done;
 	if (done) return;
-	struct Info { const void *fn; size_t dyn_smem; int threads; int cols; const char *name; };
-	const Info ks[] = {
+	std::vector<TmemKernel> ks = {
 		{ (const void *)k_i3p<64, double2>, i3p_smem<double2>(), Geo<64>::NT, (int)I3Tmem<double2>::ALLOC, "k_i3p<f64>" },
 		{ (const void *)k_i3p<64, float2>, i3p_smem<float2>(), Geo<64>::NT, (int)I3Tmem<float2>::ALLOC, "k_i3p<f32>" },
 		{ (const void *)k_i3pr<64>, i3p_smem<float2>(), Geo<64>::NT, (int)I3TmemR::ALLOC, "k_i3pr" },
@@ -752,7 +767,8 @@ void check_tmem_coresidency() {
 		{ (const void *)k_i3_full128<float2>, kFull128Smem, F128::NT, (int)F128Tmem::NCOLS, "k_i3_full128" },
 		{ (const void *)k_i3_full128r, kFull128Smem, F128::NT, (int)F128TmemR::NCOLS, "k_i3_full128r" },
 	};
-	constexpr int n = (int)(sizeof(ks) / sizeof(ks[0]));
+	for (const TmemKernel &k : dftmma_tmem_kernels()) ks.push_back(k);
+	const int n = (int)ks.size();
 	int dev = 0, sm_smem = 0, sm_regs = 0, sm_threads = 0, sm_blocks = 0, reserved = 0;
 	QB_CUDA(cudaGetDevice(&dev));
 	QB_CUDA(cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
@@ -761,7 +777,7 @@ void check_tmem_coresidency() {
 	QB_CUDA(cudaDeviceGetAttribute(&sm_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, dev));
 	QB_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
 	struct Use { long smem, regs; int threads, cols; };
-	Use u[n];
+	std::vector<Use> u(n);
 	for (int i = 0; i < n; i++) {
 		cudaFuncAttributes a;
 		QB_CUDA(cudaFuncGetAttributes(&a, ks[i].fn));
@@ -769,10 +785,10 @@ void check_tmem_coresidency() {
 		const long regs_warp = (long)((a.numRegs + 7) / 8) * 8 * 32;      // registers are granted per warp, 8 per thread at a time
 		u[i] = { (long)a.sharedSizeBytes + (long)ks[i].dyn_smem + reserved, warps * regs_warp, ks[i].threads, ks[i].cols };
 	}
-	int count[n] = {};
+	std::vector<int> count(n, 0);
 	// depth-first over multisets in non-decreasing kernel order
 	struct Dfs {
-		const Use *u; const Info *ks; int *count; int sm_smem, sm_regs, sm_threads, sm_blocks;
+		const Use *u; const TmemKernel *ks; int *count; int n, sm_smem, sm_regs, sm_threads, sm_blocks;
 		void go(int from, long smem, long regs, int thr, int blocks, int cols) {
 			for (int i = from; i < n; i++) {
 				const long s2 = smem + u[i].smem, r2 = regs + u[i].regs;
@@ -789,7 +805,7 @@ void check_tmem_coresidency() {
 				count[i]--;
 			}
 		}
-	} dfs{ u, ks, count, sm_smem, sm_regs, sm_threads, sm_blocks };
+	} dfs{ u.data(), ks.data(), count.data(), n, sm_smem, sm_regs, sm_threads, sm_blocks };
 	dfs.go(0, 0, 0, 0, 0, 0);
 	done = true;
 }

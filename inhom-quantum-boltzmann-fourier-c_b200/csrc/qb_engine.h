@@ -92,6 +92,8 @@ struct Workspace {
 	DevBuf scr128a, scr128b;                 // N = 64: per-cluster spectra of the I3 terms, first I2 spectra
 	DevBuf i3kind;                           // N = 64, FP32: per-cell I3 kernel (0 real form, 1 complex)
 	DevBuf i3stats;                          // N = 64, FP32: cells evaluated by the real form, by either form (2 x u64)
+	DevBuf kerr;                             // device error word of kernels with bounded waits (nonzero: a wait ran out)
+	int i3_variant = 0;                      // I3 sums: 0 the FFT kernels, 1 DFT-GEMMs on the tensor cores (FP32 form, N = 16)
 	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
 	// replay of repeated Strang steps (batched API): the launch sequence of a
 	// (pointers, parameters) key is captured on its second call and relaunched
@@ -111,6 +113,10 @@ struct Workspace {
 	explicit Workspace(int N);
 	~Workspace();
 };
+
+// a kernel that allocates tensor memory, for the co-residency check
+struct TmemKernel { const void *fn; size_t dyn_smem; int threads; int cols; const char *name; };
+std::vector<TmemKernel> dftmma_tmem_kernels();
 
 // chunking of the quadrature-term sums over CTAs (picked per launch shape)
 struct Chunks { int i1 = 1, i2 = 1, i3 = 1; };

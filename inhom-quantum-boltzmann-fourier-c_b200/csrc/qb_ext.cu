@@ -204,6 +204,26 @@ int qb_workspace_i3_forms(qb_workspace *ws, long long *real_cells, long long *al
 	});
 }
 
+int qb_workspace_set_i3_variant(qb_workspace *ws, int variant) {
+	return guarded([&] {
+		if (ws == nullptr) QB_FAIL("null workspace");
+		if (variant != 0 && variant != 1) QB_FAIL("I3 variant must be 0 (FFT kernels) or 1 (DFT-GEMMs on the tensor cores)");
+		ws->i3_variant = variant;
+	});
+}
+
+int qb_workspace_device_errors(qb_workspace *ws) {
+	int h = -1;
+	const int rc = guarded([&] {
+		if (ws == nullptr) QB_FAIL("null workspace");
+		DeviceGuard dg(ws->device);
+		QB_CUDA(cudaDeviceSynchronize());
+		QB_CUDA(cudaMemcpy(&h, ws->kerr.p, sizeof(int), cudaMemcpyDeviceToHost));
+		QB_CUDA(cudaMemset(ws->kerr.p, 0, sizeof(int)));
+	});
+	return rc == 0 ? h : -1;
+}
+
 int qb_workspace_set_conservation(qb_workspace *ws, int on) {
 	return guarded([&] {
 		if (ws == nullptr) QB_FAIL("null workspace");

@@ -68,6 +68,9 @@ def lib(n_grid=N_GRID):
     L.qb_launch_count.restype = C.c_long
     L.qb_workspace_graph_replays.restype = C.c_long
     L.qb_workspace_graph_replays.argtypes = [_vp]
+    L.qb_workspace_set_i3_variant.argtypes = [_vp, C.c_int]
+    L.qb_workspace_device_errors.argtypes = [_vp]
+    L.qb_umma_selftest.argtypes = [_vp, _vp, _vp, _vp]
     L.qb_fp64_peak_tflops.restype = C.c_double
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
@@ -175,6 +178,15 @@ class Workspace:
         r, a = C.c_longlong(), C.c_longlong()
         _check(lib().qb_workspace_i3_forms(self.h, C.byref(r), C.byref(a), 1 if reset else 0), "qb_workspace_i3_forms")
         return r.value, a.value
+
+    def set_i3_variant(self, variant):
+        """0: FFT kernels for the I3 sums; 1: DFT-GEMMs on the tensor cores
+        (FP32 form at N = 16)."""
+        _check(lib().qb_workspace_set_i3_variant(self.h, variant), "qb_workspace_set_i3_variant")
+
+    def device_errors(self):
+        """device error word since the last call (0: no bounded wait ran out)"""
+        return lib().qb_workspace_device_errors(self.h)
 
     @property
     def graph_replays(self):

@@ -72,14 +72,21 @@ def run(name, source, outdir=HERE):
         for _ in range(spec["steps"]):
             W = o.inhom_step(W, H, DT)
     sel = np.ascontiguousarray(W[spec["cells"]], dtype="<f8")
+    sel.tofile(os.path.join(outdir, spec["file"]))
+    return name, describe(name, source, outdir, seconds=round(time.time() - t0, 1))
+
+
+def describe(name, source, outdir, seconds=None):
+    """manifest entry of an already written fixture file"""
+    spec = FIXTURES[name]
     path = os.path.join(outdir, spec["file"])
-    sel.tofile(path)
-    return name, dict(source=("upstream SimulationInhomogeneousPeriodic (oracle/_ref)" if source == "ref"
-                              else "oracle restatement (oracle/_build)"),
-                      N=N, J=spec["J"], M=spec["M"], L=L, R=R, cells_total=CELLS, seed=SEED, h=H, dt=DT,
-                      steps=spec["steps"], cells_stored=spec["cells"], bytes=os.path.getsize(path),
-                      sha256=sha(open(path, "rb").read()), initial_state_sha256=sha(W0.astype("<f8").tobytes()),
-                      seconds=round(time.time() - t0, 1))
+    W0 = np.ascontiguousarray(initial_state())
+    return dict(source=("upstream SimulationInhomogeneousPeriodic (oracle/_ref)" if source == "ref"
+                        else "oracle restatement (oracle/_build)"),
+                N=N, J=spec["J"], M=spec["M"], L=L, R=R, cells_total=CELLS, seed=SEED, h=H, dt=DT,
+                steps=spec["steps"], cells_stored=spec["cells"], bytes=os.path.getsize(path),
+                sha256=sha(open(path, "rb").read()), initial_state_sha256=sha(W0.astype("<f8").tobytes()),
+                seconds=seconds)
 
 
 def main():
@@ -87,11 +94,16 @@ def main():
     ap.add_argument("--only", choices=sorted(FIXTURES))
     ap.add_argument("--source", choices=("ref", "oracle"), default="ref")
     ap.add_argument("--out", default=HERE, help="output directory (default: next to this script)")
+    ap.add_argument("--record", action="store_true",
+                    help="only (re)write the manifest entries of fixture files already written by --source")
     a = ap.parse_args()
     names = [a.only] if a.only else sorted(FIXTURES)
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(len(names)) as pool:
-        results = pool.starmap(run, [(n, a.source, a.out) for n in names])
+    if a.record:
+        results = [(n, describe(n, a.source, a.out)) for n in names]
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(len(names)) as pool:
+            results = pool.starmap(run, [(n, a.source, a.out) for n in names])
     man_path = os.path.join(a.out, "SEEDED.json")
     man = json.load(open(man_path)) if os.path.exists(man_path) else {}
     for name, entry in results:

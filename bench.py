@@ -306,6 +306,9 @@ def run_ours(args):
     big3 = None
     if world == 1 and not args.no_config3:
         big3 = run_config3_sample(args, qbgpu, flush)
+    dmm = None
+    if world == 1 and not args.no_dftmma:
+        dmm = run_dftmma_sample(args, qbgpu, flush)
     sur = None
     if world == 1 and not args.no_surrogate:
         sur = run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value)
@@ -325,6 +328,8 @@ def run_ours(args):
         line["config2_sample"] = big
     if big3 is not None:
         line["config3_sample"] = big3
+    if dmm is not None:
+        line["dftmma_sample"] = dmm
     if sur is not None:
         line["surrogate"] = sur
     if sur64 is not None:
@@ -494,6 +499,58 @@ def run_precision_form(args, wl, qbgpu, q, B, Wall, flush, value64):
                                 "Cd_l1": rel(cd32, cd64, 1), f"W_l1_after_{args.steps}_steps": rel(b, a, 1),
                                 f"W_l1_after_{long_steps}_steps_first_{long_cells}_cells": rel(b8, a8, 1)},
             "bound": 1e-5}
+
+
+def run_dftmma_sample(args, qbgpu, flush, cells=64, N=16, J=16, M=16, L=6.0, R=3.75):
+    """The I3 sums of the FP32 form at N = 16 two ways: the FFT kernels
+    (k_i3, 4-CTA clusters) and DFT-GEMMs on the tensor cores (k_i3_mma32:
+    tcgen05.mma kind::tf32, TF32 hi/lo split); C[W] of `cells` cells per
+    evaluation, both against the FP64 operator.  Tensor-pipe work: every
+    1-D pass is a 128 x 64 x 64 real GEMM per 4 grids, 3 products (hi/lo)."""
+    import torch
+    import ctypes
+    L_ = qbgpu.lib()
+    q = qbgpu.Quad(N, J, M, L, R)
+    W = qbgpu.to_fourier(torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=5, ncells=cells)).cuda())
+    ws64 = qbgpu.Workspace(N)
+    cc64, cd64 = qbgpu.collision_operators(ws64, q, W)
+
+    def rel(a, b):
+        return float(torch.linalg.norm((a - b).flatten()) / torch.linalg.norm(b.flatten()))
+    out = {"workload": f"N={N} (padded {2 * N}), J={J}, M={M}, L={L}, R={R}, {cells} cells, FP32 form, C[W] of every cell "
+                       f"per evaluation; {args.steps} timed evaluations after {args.warmup} warm-up per variant, L2 flushed",
+           "unit": UNIT}
+    for var, name in ((0, "fft_kernels"), (1, "tensor_core_dft_gemm")):
+        ws = qbgpu.Workspace(N, precision=32)
+        ws.set_i3_variant(var)
+        for _ in range(args.warmup):
+            qbgpu.collision_operators(ws, q, W)
+        torch.cuda.synchronize()
+        L_.qb_profile_reset()
+        L_.qb_profile_enable(1)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record()
+            cc, cd = qbgpu.collision_operators(ws, q, W)
+            evs[k][1].record()
+        torch.cuda.synchronize()
+        L_.qb_profile_enable(0)
+        ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        kms, kn = ctypes.c_double(), ctypes.c_long()
+        L_.qb_profile_read(b"i3_cluster", ctypes.byref(kms), ctypes.byref(kn))
+        i3_ms = kms.value / max(1, kn.value)
+        entry = {"value": round(cells / (ms * 1e-3), 3), "ms_per_eval": round(ms, 4), "i3_kernel_ms": round(i3_ms, 4),
+                 "rel_l2_vs_fp64": {"Cc": rel(cc, cc64), "Cd": rel(cd, cd64)}, "device_errors": ws.device_errors()}
+        if var == 1:
+            passes = 2 + 4 * 4                                  # per (cell, term): spectra tile + 4 chain tiles x 4 passes
+            flops = cells * J * M * passes * 3 * 2 * 128 * 64 * 64
+            entry["tensor_flops_per_launch"] = flops
+            entry["tensor_tflops"] = round(flops / (i3_ms * 1e-3) / 1e12, 3)
+            entry["kernel"] = "k_i3_mma32 (tcgen05.mma kind::tf32, M128 N64 K8, accumulators in tensor memory)"
+        out[name] = entry
+    out["tensor_core_vs_fft_i3_kernel"] = round(out["fft_kernels"]["i3_kernel_ms"] / out["tensor_core_dft_gemm"]["i3_kernel_ms"], 4)
+    return out
 
 
 def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samples=3, iters=8000, lr=5e-3):
@@ -745,11 +802,19 @@ def main():
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
     ap.add_argument("--surrogate-n64", action="store_true", help="add the learned operator at N = 64 (about two minutes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-dftmma", action="store_true", help="skip the tensor-core DFT-GEMM sample (N = 16)")
+    ap.add_argument("--dftmma-only", action="store_true",
+                    help="run only the tensor-core DFT-GEMM sample and print its JSON block (for profiling)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
         run_reference(args)
+    elif args.dftmma_only:
+        import torch
+        qbgpu = _import("qbgpu", os.path.join(PKG, "qbgpu.py"))
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        print(json.dumps(run_dftmma_sample(args, qbgpu, flush)), flush=True)
     else:
         run_ours(args)
 

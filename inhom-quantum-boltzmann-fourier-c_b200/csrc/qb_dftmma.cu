@@ -99,11 +99,14 @@ constexpr size_t kSelftestSmem = 128 * 64 * 4 + 64 * 64 * 4 + 1024;
 // Between passes each thread reads its row of D from tensor memory and
 // writes the next A tile: its own row (a pass along the same axis) or, for
 // a pass along the other axis, one column of the next tile (the transpose).
-// Per term:
-//   P_c = FFT2(Pad(psi1_t . W_c))   warpgroup 0, tile rows (c, l)
-//   for combos c = wg, wg + 2:      tile rows (r, l) of outputs r = 0..3
-//     a = G_g . P_r -> IFFT along k -> IFFT along l -> x psi2_t
-//       -> FFT along l -> FFT along k -> X_r += coef P_a . (result)
+// The cell's four spectra G_g (32 KB) come into shared memory once, by a
+// bulk (TMA) copy.  Per term:
+//   P_c = FFT2(Pad(psi1_t . W_c))   warpgroup 0, tile rows (c, k)
+//   for combos c = wg, wg + 2:      tile rows (r, k) of outputs r = 0..3
+//     a = G_g . P_r -> IFFT along l -> IFFT along k -> x psi2_t
+//       -> FFT along k -> FFT along l -> X_r += coef P_a . (result)
+// (a thread holds a column of the grid on the passes along l, a row on the
+// passes along k, so every shared-memory access of a warp is conflict-free)
 // with IFFT = conj . FFT . conj, so one DFT matrix serves every pass.  The
 // sums X of a warpgroup live in tensor memory beside its D (row (r, l) of
 // X_r: real parts in 32 columns, imaginary parts in the next 32); the two
@@ -116,41 +119,47 @@ constexpr uint32_t kBmat = K2 * K2 * 4;            // the DFT matrix (16 KB)
 constexpr int kPitch = P + 1;                      // P grids in shared memory (complex pitch)
 constexpr uint32_t oBhi = 0, oBlo = kBmat, oA = 2 * kBmat;
 constexpr uint32_t oP = oA + 4 * kTile;            // A tiles: [warpgroup][hi, lo]
-constexpr uint32_t kSmem = oP + 4 * P * kPitch * 8 + 1024;
+constexpr uint32_t oG = oP + 4 * P * kPitch * 8;   // the cell's spectra G (4 grids, natural order)
+constexpr uint32_t kGBytes = 4 * P * P * 8;
+constexpr uint32_t kSmem = oG + kGBytes + 1024;
+static_assert(oG % 16 == 0 && kGBytes % 16 == 0, "bulk copies move 16-byte aligned multiples of 16 bytes");
+static_assert(kSmem <= 232448, "dynamic shared memory of one CTA");
 constexpr uint32_t kCols = 256;                    // tensor memory: per warpgroup a 64-column D and its 64-column sums X
 }  // namespace dm
+
+// the pointer, as a value the compiler cannot follow: per-thread addresses
+// derived from it are recomputed where they are used instead of being
+// hoisted out of the term and chain loops into (scarce) registers
+template <class T> __device__ __forceinline__ T *opaque(T *p) {
+	asm volatile("" : "+l"(p));
+	return p;
+}
 
 __device__ __forceinline__ int pad_src(int p) { return p < dm::N / 2 ? p : (p >= 3 * dm::N / 2 ? p - dm::N : -1); }
 
 __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(128) : "memory"); }
 
-// this thread's row r of the hi and lo tiles: values v[0..63] (real parts, then imaginary parts)
-__device__ __forceinline__ void put_row(unsigned char *hi, unsigned char *lo, int r, const float (&v)[64]) {
-#pragma unroll
-	for (int k = 0; k < 64; k += 4) {
-		float4 h, l;
-		h.x = umma::tf32_round(v[k]);     l.x = umma::tf32_round(v[k] - h.x);
-		h.y = umma::tf32_round(v[k + 1]); l.y = umma::tf32_round(v[k + 1] - h.y);
-		h.z = umma::tf32_round(v[k + 2]); l.z = umma::tf32_round(v[k + 2] - h.z);
-		h.w = umma::tf32_round(v[k + 3]); l.w = umma::tf32_round(v[k + 3] - h.w);
-		const uint32_t o = umma::kmajor_off(128, r, k);
-		*reinterpret_cast<float4 *>(hi + o) = h;
-		*reinterpret_cast<float4 *>(lo + o) = l;
-	}
-}
-
-// the transpose: row j of this thread's D (values d[j], d[32 + j]) becomes
-// column `col` (real) and 32 + col (imaginary) of row r0 + j of the next tile
-__device__ __forceinline__ void put_col(unsigned char *hi, unsigned char *lo, int r0, int col, const float (&d)[64]) {
-#pragma unroll
-	for (int j = 0; j < 32; j++) {
-		const float hr = umma::tf32_round(d[j]), hi_ = umma::tf32_round(d[32 + j]);
-		const uint32_t o0 = umma::kmajor_off(128, r0 + j, col), o1 = umma::kmajor_off(128, r0 + j, 32 + col);
-		*reinterpret_cast<float *>(hi + o0) = hr;
-		*reinterpret_cast<float *>(lo + o0) = umma::tf32_round(d[j] - hr);
-		*reinterpret_cast<float *>(hi + o1) = hi_;
-		*reinterpret_cast<float *>(lo + o1) = umma::tf32_round(d[32 + j] - hi_);
-	}
+// 4 consecutive complex values x[0..3] at columns k0 .. k0 + 3 (real parts)
+// and 32 + k0 .. (imaginary parts, conjugated when `conj`) of row r
+__device__ __forceinline__ void put_row4(unsigned char *hi, unsigned char *lo, int r, int k0, const float2 (&x)[4], bool conj) {
+	hi = opaque(hi);
+	lo = opaque(lo);
+	const float s = conj ? -1.0f : 1.0f;
+	float4 h, l;
+	h.x = umma::tf32_round(x[0].x); l.x = umma::tf32_round(x[0].x - h.x);
+	h.y = umma::tf32_round(x[1].x); l.y = umma::tf32_round(x[1].x - h.y);
+	h.z = umma::tf32_round(x[2].x); l.z = umma::tf32_round(x[2].x - h.z);
+	h.w = umma::tf32_round(x[3].x); l.w = umma::tf32_round(x[3].x - h.w);
+	uint32_t o = umma::kmajor_off(128, r, k0);
+	*reinterpret_cast<float4 *>(hi + o) = h;
+	*reinterpret_cast<float4 *>(lo + o) = l;
+	h.x = umma::tf32_round(s * x[0].y); l.x = umma::tf32_round(s * x[0].y - h.x);
+	h.y = umma::tf32_round(s * x[1].y); l.y = umma::tf32_round(s * x[1].y - h.y);
+	h.z = umma::tf32_round(s * x[2].y); l.z = umma::tf32_round(s * x[2].y - h.z);
+	h.w = umma::tf32_round(s * x[3].y); l.w = umma::tf32_round(s * x[3].y - h.w);
+	o = umma::kmajor_off(128, r, 32 + k0);
+	*reinterpret_cast<float4 *>(hi + o) = h;
+	*reinterpret_cast<float4 *>(lo + o) = l;
 }
 
 // D = A_lo B_hi + A_hi B_lo + A_hi B_hi over K = 64 (8 steps of 8), issued by one thread
@@ -179,10 +188,12 @@ struct MmaCtx {
 	unsigned phase;
 };
 
-// one pass: the staged A tile times the DFT matrix into D; on return d[] is
-// this thread's row of D.  A wait that runs out marks the warpgroup aborted;
-// later passes then issue and wait for nothing (every barrier still runs).
-__device__ __forceinline__ void mma_pass(MmaCtx &c, float (&d)[64]) {
+// one pass: the staged A tile times the DFT matrix into D.  A wait that runs
+// out marks the warpgroup aborted; later passes then issue and wait for
+// nothing (every barrier still runs).  Threads then read their row of D from
+// tensor memory, 16 columns at a time (real parts at columns 0..31,
+// imaginary parts at 32..63).
+__device__ __forceinline__ void mma_pass(MmaCtx &c) {
 	umma::fence_async_smem();
 	tmem_fence_before();
 	wg_sync(c.wg);
@@ -198,13 +209,35 @@ __device__ __forceinline__ void mma_pass(MmaCtx &c, float (&d)[64]) {
 		c.phase ^= 1u;
 		tmem_fence_after();
 	}
+}
+
+// values h*16 .. h*16 + 15 of this thread's row of D: re[i] = Re, im[i] = Im
+__device__ __forceinline__ void d_half(const MmaCtx &c, int h, float (&re)[16], float (&im)[16]) {
+	umma::tmem_ld16(c.trow + 16 * h, re);
+	umma::tmem_ld16(c.trow + 32 + 16 * h, im);
+	tmem_wait_ld();
+}
+
+// the transpose, streamed from tensor memory: value j of this thread's row of
+// D becomes column `col` (real) and 32 + col (imaginary) of row r0 + j of the
+// next A tile
+__device__ __forceinline__ void put_col_d(const MmaCtx &c, unsigned char *hi, unsigned char *lo, int r0, int col) {
 #pragma unroll
-	for (int q = 0; q < 4; q++) {
-		float v[16];
-		umma::tmem_ld16(c.trow + 16 * q, v);
-		tmem_wait_ld();
+	for (int h = 0; h < 2; h++) {
+		float re[16], im[16];
+		d_half(c, h, re, im);
+		hi = opaque(hi);
+		lo = opaque(lo);
 #pragma unroll
-		for (int i = 0; i < 16; i++) d[16 * q + i] = v[i];
+		for (int i = 0; i < 16; i++) {
+			const int j = 16 * h + i;
+			const float hr = umma::tf32_round(re[i]), hm = umma::tf32_round(im[i]);
+			const uint32_t o0 = umma::kmajor_off(128, r0 + j, col), o1 = umma::kmajor_off(128, r0 + j, 32 + col);
+			*reinterpret_cast<float *>(hi + o0) = hr;
+			*reinterpret_cast<float *>(lo + o0) = umma::tf32_round(re[i] - hr);
+			*reinterpret_cast<float *>(hi + o1) = hm;
+			*reinterpret_cast<float *>(lo + o1) = umma::tf32_round(im[i] - hm);
+		}
 	}
 }
 
@@ -212,7 +245,7 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 	using namespace dm;
 	extern __shared__ unsigned char smem_raw[];
 	unsigned char *base = align1024(smem_raw);
-	__shared__ uint64_t mbar[2];
+	__shared__ uint64_t mbar[3];                                // [0], [1]: MMA completion per warpgroup; [2]: the G copy
 	__shared__ uint32_t tslot;
 	__shared__ int abort_flag[2];
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, wg = warp >> 2, q = warp & 3;
@@ -222,6 +255,16 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
 	unsigned char *Ahi = base + oA + wg * 2 * kTile, *Alo = Ahi + kTile;
 	float2 *Pg = reinterpret_cast<float2 *>(base + oP);       // [4][P][kPitch], P_c[l][k] natural
+	const float2 *Gs = reinterpret_cast<const float2 *>(base + oG);   // the cell's 4 spectra G_g, natural [4][P][P]
+	if (tid == 0) {
+		umma::mbar_init(&mbar[0], 1);
+		umma::mbar_init(&mbar[1], 1);
+		umma::mbar_init(&mbar[2], 1);
+		fence_mbar_init();
+		abort_flag[0] = abort_flag[1] = 0;
+		// the cell's spectra G (32 KB, contiguous) into shared memory by one bulk copy
+		umma::bulk_g2s(base + oG, p.Ghat + cell * p.g_cell, kGBytes, &mbar[2]);
+	}
 	// the real-ified DFT matrix B (K x N) as its transpose, row n = column n of B, split hi / lo
 	for (int i = tid; i < K2 * K2; i += kThreads) {
 		const int n = i / K2, k = i % K2;
@@ -235,12 +278,6 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 		const uint32_t o = umma::kmajor_off(64, n, k);
 		*reinterpret_cast<float *>(base + oBhi + o) = h;
 		*reinterpret_cast<float *>(base + oBlo + o) = l;
-	}
-	if (tid == 0) {
-		umma::mbar_init(&mbar[0], 1);
-		umma::mbar_init(&mbar[1], 1);
-		fence_mbar_init();
-		abort_flag[0] = abort_flag[1] = 0;
 	}
 	if (warp == 0) tmem_alloc(&tslot, kCols);
 	umma::fence_async_smem();
@@ -257,6 +294,7 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 	mc.mbar = &mbar[wg];
 	mc.abort = &abort_flag[wg];
 	mc.phase = 0;
+	if (!umma::mbar_wait(&mbar[2], 0, kWaitPolls)) abort_flag[wg] = 1;    // G in shared memory
 	const int row = 32 * q + lane;
 	const uint32_t xrow = mc.trow + 128;                       // this thread's row of X (sums)
 	int ncmax = 0;
@@ -269,79 +307,94 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 		for (int c = 0; c < 64; c += 16) umma::tmem_st16(xrow + c, z);
 		tmem_wait_st();
 	}
-	float d[64];                                            // this thread's row: operand in, result out
 #pragma unroll 1
 	for (int t = t0; t < t1; t++) {
 		if (wg == 0) {
-			// P_q = FFT2(Pad(psi1_t . W_q)): row l = lane of the padded grid, along k, then along l
+			// P_q = FFT2(Pad(psi1_t . W_q)): tile row (q, k = lane) holds column k of the padded
+			// grid; the pass along l, then (transposed) along k leaves row (q, l) of P_q
 			const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[q] * N * N;
 			const float2 *ps1 = p.psi1 + (long)t * N * N;
-			const int ls = pad_src(lane);
+			const int ks = pad_src(lane);
+#pragma unroll 1
+			for (int l0 = 0; l0 < P; l0 += 4) {
+				float2 x[4];
 #pragma unroll
-			for (int k = 0; k < P; k++) {
-				const int ks = pad_src(k);
-				float2 x = make_float2(0.0f, 0.0f);
-				if (ls >= 0 && ks >= 0) {
-					const double2 w = src[ks + N * ls];
-					x = cmul(ps1[ks + N * ls], make_float2((float)w.x, (float)w.y));
+				for (int i = 0; i < 4; i++) {
+					const int ls = pad_src(l0 + i);
+					x[i] = make_float2(0.0f, 0.0f);
+					if (ls >= 0 && ks >= 0) {
+						const double2 w = src[ks + N * ls];
+						x[i] = cmul(ps1[ks + N * ls], make_float2((float)w.x, (float)w.y));
+					}
 				}
-				d[k] = x.x;
-				d[32 + k] = x.y;
+				put_row4(Ahi, Alo, row, l0, x, false);
 			}
-			put_row(Ahi, Alo, row, d);
-			mma_pass(mc, d);
-			put_col(Ahi, Alo, 32 * q, lane, d);
-			mma_pass(mc, d);                                    // row (q, k = lane): P_q[l][k] over l
+			mma_pass(mc);                                       // along l: row (q, k)
+			put_col_d(mc, Ahi, Alo, 32 * q, lane);
+			mma_pass(mc);                                       // along k: row (q, l = lane) of P_q over k
 #pragma unroll
-			for (int l = 0; l < P; l++) Pg[(q * P + l) * kPitch + lane] = make_float2(d[l], d[32 + l]);
+			for (int h = 0; h < 2; h++) {
+				float re[16], im[16];
+				d_half(mc, h, re, im);
+				float2 *pr = opaque(Pg + (q * P + lane) * kPitch + 16 * h);
+#pragma unroll
+				for (int i = 0; i < 16; i++) pr[i] = make_float2(re[i], im[i]);
+			}
 		}
 		__syncthreads();                                        // P grids of the term are in place
-		const float *ps2 = p.psi2T + (long)p.psi2_idx[t] * P * P + lane * P;    // psi2[l][k = lane] at ps2[l]
+		const float *ps2 = opaque(p.psi2T + (long)p.psi2_idx[t] * P * P + lane);   // psi2[l = lane][k] at ps2[k * P]
 		const float sc = (float)p.psi2_scale[t];
 #pragma unroll 1
 		for (int c = wg; c < ncmax; c += 2) {
 			const bool act = c < p.ncombo[q];
-			// a = G_g . P_q on row l = lane, conjugated (inverse transforms as conj . FFT . conj)
-			if (act) {
-				const float2 *Gg = p.Ghat + cell * p.g_cell + (long)p.cgi[q][c] * P * P + lane * P;
-				const float2 *Pq = Pg + (q * P + lane) * kPitch;
+			// column k = lane of a = G_g . P_q, conjugated (inverse transforms as conj . FFT . conj)
+			{
+				const float2 *Gg = opaque(Gs + (act ? p.cgi[q][c] : 0) * P * P + lane);
+				const float2 *Pq = opaque(Pg + q * P * kPitch + lane);
+#pragma unroll 1
+				for (int l0 = 0; l0 < P; l0 += 4) {
+					float2 x[4];
 #pragma unroll
-				for (int k = 0; k < P; k++) {
-					const float2 a = cmul(Gg[k], Pq[k]);
-					d[k] = a.x;
-					d[32 + k] = -a.y;
+					for (int i = 0; i < 4; i++) x[i] = act ? cmul(Gg[(l0 + i) * P], Pq[(l0 + i) * kPitch]) : make_float2(0.0f, 0.0f);
+					put_row4(Ahi, Alo, row, l0, x, true);
 				}
-			} else {
-#pragma unroll
-				for (int k = 0; k < 64; k++) d[k] = 0.0f;
 			}
-			put_row(Ahi, Alo, row, d);
-			mma_pass(mc, d);                                    // along k
-			put_col(Ahi, Alo, 32 * q, lane, d);
-			mma_pass(mc, d);                                    // along l: row (q, k = lane), conj IFFT2(a) over l
+			mma_pass(mc);                                       // along l: row (q, k)
+			put_col_d(mc, Ahi, Alo, 32 * q, lane);
+			mma_pass(mc);                                       // along k: row (q, l = lane), conj IFFT2(a) over k
+			// IFFT2(a) . psi2_t (the conjugate of D), as the operand of the forward pass along k
 #pragma unroll
-			for (int l = 0; l < P; l++) {
-				const float f = sc * ps2[l];
-				d[l] = d[l] * f;
-				d[32 + l] = -d[32 + l] * f;
+			for (int h = 0; h < 2; h++) {
+				float re[16], im[16];
+				d_half(mc, h, re, im);
+#pragma unroll
+				for (int i0 = 0; i0 < 16; i0 += 4) {
+					float2 x[4];
+#pragma unroll
+					for (int i = 0; i < 4; i++) {
+						const float f = sc * ps2[(16 * h + i0 + i) * P];
+						x[i] = make_float2(re[i0 + i] * f, im[i0 + i] * f);
+					}
+					put_row4(Ahi, Alo, row, 16 * h + i0, x, true);
+				}
 			}
-			put_row(Ahi, Alo, row, d);
-			mma_pass(mc, d);                                    // FFT along l
-			put_col(Ahi, Alo, 32 * q, lane, d);
-			mma_pass(mc, d);                                    // FFT along k: row (q, l = lane) over k
+			mma_pass(mc);                                       // FFT along k: row (q, l)
+			put_col_d(mc, Ahi, Alo, 32 * q, lane);
+			mma_pass(mc);                                       // FFT along l: row (q, k = lane) over l
 			if (act) {
-				const float2 *Pa = Pg + (p.ca[q][c] * P + lane) * kPitch;
+				const float2 *Pa = opaque(Pg + p.ca[q][c] * P * kPitch + lane);
 				const float coef = (float)p.ccoef[q][c];
 #pragma unroll
-				for (int h = 0; h < 2; h++) {                    // k = 16 h .. 16 h + 15
-					float xr[16], xi[16];
+				for (int h = 0; h < 2; h++) {                    // l = 16 h .. 16 h + 15
+					float xr[16], xi[16], re[16], im[16];
+					d_half(mc, h, re, im);
 					umma::tmem_ld16(xrow + 16 * h, xr);
 					umma::tmem_ld16(xrow + 32 + 16 * h, xi);
 					tmem_wait_ld();
 #pragma unroll
 					for (int i = 0; i < 16; i++) {
-						const int k = 16 * h + i;
-						const float2 y = cmul(Pa[k], make_float2(d[k], d[32 + k]));
+						const int l = 16 * h + i;
+						const float2 y = cmul(Pa[l * kPitch], make_float2(re[i], im[i]));
 						xr[i] += coef * y.x;
 						xi[i] += coef * y.y;
 					}
@@ -353,28 +406,35 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 		}
 		__syncthreads();                                        // every chain of the term is done with Pg
 	}
-	// the two warpgroups' sums, added in a fixed order (0 + 1), to the partial-sum slot
-#pragma unroll
-	for (int c = 0; c < 64; c += 16) {
-		float x[16];
-		umma::tmem_ld16(xrow + c, x);
-		tmem_wait_ld();
-#pragma unroll
-		for (int i = 0; i < 16; i++) d[c + i] = x[i];
-	}
+	// the two warpgroups' sums (column k = lane of X_q), added in a fixed order (0 + 1)
 	float *red = reinterpret_cast<float *>(base + oA);          // the operand tiles are free now
 	if (wg == 1) {
 #pragma unroll
-		for (int i = 0; i < 64; i++) red[i * 128 + row] = d[i];
+		for (int c = 0; c < 64; c += 16) {
+			float x[16];
+			umma::tmem_ld16(xrow + c, x);
+			tmem_wait_ld();
+#pragma unroll
+			for (int i = 0; i < 16; i++) red[(c + i) * 128 + row] = x[i];
+		}
 	}
 	__syncthreads();
 	const bool failed = abort_flag[0] != 0 || abort_flag[1] != 0;
 	if (wg == 0) {
-		float2 *o = p.out + ((cell * p.nchunk + chunk) * 4 + q) * (long)P * P + lane * P;
+		float2 *o = p.out + ((cell * p.nchunk + chunk) * 4 + q) * (long)P * P + lane;
 		const float nanv = __int_as_float(0x7fc00000);
 #pragma unroll
-		for (int k = 0; k < P; k++)
-			o[k] = failed ? make_float2(nanv, nanv) : make_float2(d[k] + red[k * 128 + row], d[32 + k] + red[(32 + k) * 128 + row]);
+		for (int h = 0; h < 2; h++) {
+			float xr[16], xi[16];
+			umma::tmem_ld16(xrow + 16 * h, xr);
+			umma::tmem_ld16(xrow + 32 + 16 * h, xi);
+			tmem_wait_ld();
+#pragma unroll
+			for (int i = 0; i < 16; i++) {
+				const int l = 16 * h + i;
+				o[l * P] = failed ? make_float2(nanv, nanv) : make_float2(xr[i] + red[l * 128 + row], xi[i] + red[(32 + l) * 128 + row]);
+			}
+		}
 	}
 	if (failed) {
 		if (tid == 0) atomicExch(err, 1);

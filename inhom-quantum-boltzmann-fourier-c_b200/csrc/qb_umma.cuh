@@ -76,6 +76,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, unsigned parity, unsig
 	return false;
 }
 
+// bulk copy (TMA, no tensor map) of `bytes` from global to this CTA's shared
+// memory, completing on `mbar` (which expects these bytes and one arrival);
+// both addresses 16-byte aligned, bytes a multiple of 16; one thread issues
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_global, uint32_t bytes, uint64_t *mbar) {
+	const uint32_t mb = smem_u32(mbar);
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst_smem)),
+	             "l"(src_global), "r"(bytes), "r"(mb)
+	             : "memory");
+}
+
 // generic-proxy shared-memory writes -> visible to the tensor core
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 

@@ -400,7 +400,55 @@ def run_config2_sample(args, qbgpu, flush, cells=64, steps=2, warmup=1):
         a, b = a.cpu().numpy().ravel(), b.cpu().numpy().ravel()
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
     out["rel_err_f32_vs_f64"] = {"Cc_l2": rel(cc32, cc64), "Cd_l2": rel(cd32, cd64)}
+    if args.config2_long_steps > 0:
+        out["long_run"] = config2_long_run(qbgpu, q, W0, h, dt, args.config2_long_cells, args.config2_long_steps)
     return out
+
+
+def config2_long_run(qbgpu, q, W0, h, dt, cells, steps):
+    """The FP32 form against FP64 after `steps` Strang steps on the first
+    `cells` x-cells of the sample (a periodic line of those cells, h and dt of
+    the 1024-cell domain): relative error of W and of Cc, Cd on the final FP64
+    state; and, with the conservation correction on, the relative drift of the
+    total mass, momentum and energy of the FP32 run."""
+    import torch
+    N = q.N
+    L = 6.0
+    Ws = W0[:cells].contiguous()
+    B = torch.zeros((cells, 3), dtype=torch.float64, device="cuda")
+    runs = {}
+    for name, prec, cons in (("f64", 64, False), ("f32", 32, False), ("f32_conserving", 32, True)):
+        ws = qbgpu.Workspace(N, precision=prec, conserve=cons)
+        a, b = Ws.clone(), torch.empty_like(Ws)
+        for _ in range(steps):
+            qbgpu.inhom_step(ws, q, a, h, dt, B, out=b)
+            a, b = b, a
+        torch.cuda.synchronize()
+        runs[name] = a
+
+    def rel(x, y, o):
+        x, y = x.cpu().numpy().ravel(), y.cpu().numpy().ravel()
+        return float(np.linalg.norm(x - y, o) / np.linalg.norm(y, o))
+
+    def totals(W):
+        d = qbgpu.diagnostics(W, L).cpu().numpy()       # the library's moment kernel (FP64)
+        mass = d[:, 0]
+        mom = mass[:, None] * d[:, 4:6]
+        energy = mass * (d[:, 6] + 0.5 * (d[:, 4] ** 2 + d[:, 5] ** 2))
+        return mass.sum(), mom.sum(axis=0), energy.sum()
+    m0, p0, e0 = totals(Ws)
+    m1, p1, e1 = totals(runs["f32_conserving"])
+    Wf = qbgpu.to_fourier(runs["f64"])
+    ws64, ws32 = qbgpu.Workspace(N), qbgpu.Workspace(N, precision=32)
+    cc64, cd64 = qbgpu.collision_operators(ws64, q, Wf)
+    cc32, cd32 = qbgpu.collision_operators(ws32, q, Wf)
+    return {"what": f"{steps} Strang steps of the first {cells} x-cells (a periodic line of them, h = 1/1024), FP32 form against FP64",
+            "W_rel_l1": rel(runs["f32"], runs["f64"], 1), "W_rel_l2": rel(runs["f32"], runs["f64"], 2),
+            "Cc_rel_l2_on_final_state": rel(cc32, cc64, 2), "Cd_rel_l2_on_final_state": rel(cd32, cd64, 2),
+            "conserving_f32_drift": {"mass": abs(m1 - m0) / abs(m0),
+                                     "momentum": float(np.linalg.norm(p1 - p0) / max(np.linalg.norm(p0), abs(m0))),
+                                     "energy": abs(e1 - e0) / abs(e0)},
+            "bounds": {"C": 1e-5, "drift": 1e-9}}
 
 
 def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
@@ -798,6 +846,9 @@ def main():
     ap.add_argument("--no-precision-form", action="store_true", help="skip the FP32-form measurement")
     ap.add_argument("--no-config2", action="store_true", help="skip the N = 64 precision-form sample")
     ap.add_argument("--config2-cells", type=int, default=64, help="x-cells of the N = 64 sample (of its 1024)")
+    ap.add_argument("--config2-long-steps", type=int, default=1000,
+                    help="Strang steps of the N = 64 FP32-against-FP64 long run (0 skips it)")
+    ap.add_argument("--config2-long-cells", type=int, default=2, help="x-cells of the N = 64 long run")
     ap.add_argument("--no-config3", action="store_true", help="skip the mixed-size batch sample")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
     ap.add_argument("--surrogate-n64", action="store_true", help="add the learned operator at N = 64 (about two minutes)")

@@ -213,14 +213,12 @@ def run_ours(args):
         def step(Win, Wout):
             qbgpu.inhom_step(ws, q, Win, wl["h"], wl["dt"], B, out=Wout)
     else:
-        def transport(ext):
-            return qbgpu.transport(ext, wl["L"], wl["h"], 0.5 * wl["dt"])
-
-        def collision(Wt):
-            return qbgpu.fourier_collision(ws, q, Wt, wl["dt"], B)
+        sharded = qd.ShardedStrang(cells, (4, N, N), torch.float64, W0.device,
+                                   lambda ext, out: qbgpu.transport(ext, wl["L"], wl["h"], 0.5 * wl["dt"], out=out),
+                                   lambda c, i: qbgpu.fourier_collision(ws, q, c, wl["dt"], B[i:i + c.shape[0]]))
 
         def step(Win, Wout):
-            Wout.copy_(qd.sharded_strang_step(Win, transport, collision))
+            sharded.step(Win, out=Wout)
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MB > 126 MB L2
     for i in range(args.warmup):
@@ -769,12 +767,11 @@ def run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall):
     hin = torch.from_numpy(Wall[rank * cells:(rank + 1) * cells].copy()).pin_memory()
     hout = torch.empty_like(hin).pin_memory()
 
-    def transport(ext):
-        return qbgpu.transport(ext, wl["L"], wl["h"], 0.5 * wl["dt"])
-
-    def collision(Wt):
-        return qbgpu.fourier_collision(ws, q, Wt, wl["dt"], B)
-
+    sharded = None
+    if world > 1:
+        sharded = qd.ShardedStrang(cells, (4, N, N), torch.float64, "cuda",
+                                   lambda ext, out: qbgpu.transport(ext, wl["L"], wl["h"], 0.5 * wl["dt"], out=out),
+                                   lambda c, i: qbgpu.fourier_collision(ws, q, c, wl["dt"], B[i:i + c.shape[0]]))
     import torch.distributed as dist
     torch.cuda.synchronize()
     if world > 1:
@@ -784,7 +781,7 @@ def run_e2e(args, wl, qbgpu, qd, world, rank, q, ws, B, Wall):
     for _ in range(steps):
         Wd = hin.cuda(non_blocking=True)
         if world > 1:
-            Wn = qd.sharded_strang_step(Wd, transport, collision)
+            Wn = sharded.step(Wd)
         else:
             Wn = qbgpu.inhom_step(ws, q, Wd, wl["h"], wl["dt"], B)
         hout.copy_(Wn, non_blocking=True)

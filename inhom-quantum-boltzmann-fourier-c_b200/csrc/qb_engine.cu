@@ -301,6 +301,27 @@ inline bool use_real_form() {
 	static const bool on = use_full128() && strcmp(i3_kernel_env(), "complex") != 0;
 	return on;
 }
+// The FP64 I3 sums at N = 32 run as one contiguous range of the (cell, term)
+// work per resident cluster (QB_I3_RANGES=0: the (cell, chunk) grid instead,
+// for comparisons): every cluster has the same number of terms, and a cell's
+// partial sums are one per cluster that touches it instead of one per chunk.
+inline bool term_ranges_enabled() {
+	static const bool on = [] { const char *e = getenv("QB_I3_RANGES"); return e == nullptr || strcmp(e, "0") != 0; }();
+	return on;
+}
+inline TermRanges term_ranges(int slots, int nterms, int ncells) {
+	TermRanges g;
+	g.nslots = slots;
+	g.nterms = nterms;
+	g.total = (long)ncells * nterms;
+	g.maxc = 1;
+	for (int k = 0; k < slots; k++) {
+		const long a = g.start(k), b = g.start(k + 1);
+		if (b > a) g.maxc = std::max(g.maxc, (int)((b - 1) / nterms - a / nterms + 1));
+	}
+	return g;
+}
+
 constexpr double kRealFormBound = 1e-6;
 // The real forms pack the combos of an output in pairs.  Both callers of the
 // I3 sums (the Cd assembly and the single-integral path) set 4 combos per
@@ -512,10 +533,16 @@ template <int P, class C> struct Rhs {
 		launch_i2<P>(p, (long)ncells * 4 * nchunk, s);
 	}
 
-	static void i3_sums(Workspace &ws, const DevI3 &t, int ncells, const double2 *W, int nchunk, cudaStream_t s) {
-		ws.i3p.ensure(sizeof(C) * ncells * nchunk * 4 * PP);
+	static void i3_sums(Workspace &ws, const DevI3 &t, int ncells, const double2 *W, const Chunks &ch, cudaStream_t s) {
+		const int nchunk = ch.i3;
 		I3ParamsT<C> p{};
 		p.nchunk = nchunk; p.nterms = t.nterms;
+		if (ch.i3_slots > 0) {
+			p.rg = term_ranges(ch.i3_slots, t.nterms, ncells);
+			ws.i3p.ensure(sizeof(C) * (size_t)p.rg.nslots * p.rg.maxc * 4 * PP);
+		} else {
+			ws.i3p.ensure(sizeof(C) * ncells * nchunk * 4 * PP);
+		}
 		p.src = W; p.src_cell = 4 * NN;
 		for (int r = 0; r < 4; r++) p.src_comp[r] = r;
 		p.Ghat = ws.What.as<C>(); p.g_cell = 4 * PP;
@@ -538,7 +565,7 @@ template <int P, class C> struct Rhs {
 					return;
 				}
 			}
-			launch_i3p<C>(p, (long)ncells * nchunk, nullptr, s);
+			launch_i3p<C>(p, p.rg.nslots > 0 ? (long)p.rg.nslots : (long)ncells * nchunk, nullptr, s);
 		} else {
 			if constexpr (P == 32 && sizeof(C) == 8) {
 				if (ws.i3_variant == 1) {
@@ -557,22 +584,27 @@ template <int P, class C> struct Rhs {
 			check_tmem_coresidency();
 			ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), num_sms(), 256, 0.15);      // one CTA per SM
 		}
+		// FP64 at N = 32: every resident cluster of k_i3p takes one contiguous range
+		// of the (cell, term) work, one partial per cell it touches
+		if (P == 64 && sizeof(C) == 16 && q.i3 && q.i3->nterms > 0 && term_ranges_enabled())
+			ch.i3_slots = (int)std::min<long>(active_i3p_clusters<C>(), (long)ncells * q.i3->nterms);
 		spectra(ws, ncells, W, s);
 		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
 		if (parts & RHS_CD) {
 			i1_sums(ws, *q.i4, ncells, W, false, ws.i1i4, ws.fs4, ch.i1, s);
 			i2_sums(ws, *q.i2, ncells, W, ch.i2, s);
-			i3_sums(ws, *q.i3, ncells, W, ch.i3, s);
+			i3_sums(ws, *q.i3, ncells, W, ch, s);
 		}
 	}
 
-	static AsmParamsT<C> asm_params(Workspace &ws, int parts, const Chunks &ch) {
+	static AsmParamsT<C> asm_params(Workspace &ws, int parts, const Chunks &ch, const QuadSet &q, int ncells) {
 		AsmParamsT<C> a{};
 		a.What = ws.What.as<C>();
 		a.FS = (parts & RHS_CC) ? ws.fs.as<C>() : nullptr;
 		a.FS4 = (parts & RHS_CD) ? ws.fs4.as<C>() : nullptr;
 		a.Qp = (parts & RHS_CD) ? ws.i2p.as<C>() : nullptr; a.nq = ch.i2;
 		a.Xp = (parts & RHS_CD) ? ws.i3p.as<C>() : nullptr; a.nx = ch.i3;
+		if (ch.i3_slots > 0 && (parts & RHS_CD)) a.xrg = term_ranges(ch.i3_slots, q.i3->nterms, ncells);
 		a.s2 = 1.0 / (double)PP;
 		a.s1 = a.s2 * a.s2;
 		return a;
@@ -581,7 +613,7 @@ template <int P, class C> struct Rhs {
 	static void operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
 		Chunks ch;
 		prepare(ws, q, ncells, W, parts, ch, s);
-		AsmParamsT<C> a = asm_params(ws, parts, ch);
+		AsmParamsT<C> a = asm_params(ws, parts, ch, q, ncells);
 		a.mode = 0; a.out_cc = cc; a.out_cd = cd;
 		launch_assemble<P>(a, ncells, s);
 	}
@@ -589,7 +621,7 @@ template <int P, class C> struct Rhs {
 	static void update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
 		Chunks ch;
 		prepare(ws, q, ncells, wcur, RHS_ALL, ch, s);
-		AsmParamsT<C> a = asm_params(ws, RHS_ALL, ch);
+		AsmParamsT<C> a = asm_params(ws, RHS_ALL, ch, q, ncells);
 		a.mode = 1; a.base = base; a.wcur = wcur; a.B = B; a.dtc = dtc; a.out = out;
 		launch_assemble<P>(a, ncells, s);
 	}
@@ -910,13 +942,14 @@ template <class C> struct Rhs<128, C> {
 		}
 	}
 
-	static AsmParamsT<C> asm_params(Workspace &ws, int parts, const Chunks &ch) {
+	static AsmParamsT<C> asm_params(Workspace &ws, int parts, const Chunks &ch, const QuadSet &q, int ncells) {
 		AsmParamsT<C> a{};
 		a.What = ws.What.as<C>();
 		a.FS = (parts & RHS_CC) ? ws.fs.as<C>() : nullptr;
 		a.FS4 = (parts & RHS_CD) ? ws.fs4.as<C>() : nullptr;
 		a.Qp = (parts & RHS_CD) ? ws.i2p.as<C>() : nullptr; a.nq = ch.i2;
 		a.Xp = (parts & RHS_CD) ? ws.i3p.as<C>() : nullptr; a.nx = ch.i3;
+		if (ch.i3_slots > 0 && (parts & RHS_CD)) a.xrg = term_ranges(ch.i3_slots, q.i3->nterms, ncells);
 		a.s2 = 1.0 / (double)PP;
 		a.s1 = a.s2 * a.s2;
 		return a;
@@ -925,7 +958,7 @@ template <class C> struct Rhs<128, C> {
 	static void operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
 		Chunks ch;
 		prepare(ws, q, ncells, W, parts, ch, s);
-		AsmParamsT<C> a = asm_params(ws, parts, ch);
+		AsmParamsT<C> a = asm_params(ws, parts, ch, q, ncells);
 		a.mode = 0; a.out_cc = cc; a.out_cd = cd;
 		launch_assemble128(a, ncells, s);
 	}
@@ -933,7 +966,7 @@ template <class C> struct Rhs<128, C> {
 	static void update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
 		Chunks ch;
 		prepare(ws, q, ncells, wcur, RHS_ALL, ch, s);
-		AsmParamsT<C> a = asm_params(ws, RHS_ALL, ch);
+		AsmParamsT<C> a = asm_params(ws, RHS_ALL, ch, q, ncells);
 		a.mode = 1; a.base = base; a.wcur = wcur; a.B = B; a.dtc = dtc; a.out = out;
 		launch_assemble128(a, ncells, s);
 	}

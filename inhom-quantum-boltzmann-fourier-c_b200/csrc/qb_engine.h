@@ -119,7 +119,10 @@ struct TmemKernel { const void *fn; size_t dyn_smem; int threads; int cols; cons
 std::vector<TmemKernel> dftmma_tmem_kernels();
 
 // chunking of the quadrature-term sums over CTAs (picked per launch shape)
-struct Chunks { int i1 = 1, i2 = 1, i3 = 1; };
+struct Chunks {
+	int i1 = 1, i2 = 1, i3 = 1;
+	int i3_slots = 0;                        // > 0: the I3 sums run as that many contiguous (cell, term) ranges instead of chunks
+};
 Chunks pick_chunks(int N, int ncells, const QuadSet &q, int prec);
 
 // ---- operators (device pointers, stream-ordered) ------------------------------

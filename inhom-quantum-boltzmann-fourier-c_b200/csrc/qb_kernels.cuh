@@ -296,9 +296,24 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_i2_terms(const I2ParamsT<C> p) {
 // into its shared memory; the other CTAs read it through distributed shared
 // memory.  For each of its combos (a, g, coef) it accumulates
 //   X_r += coef * P_a . FFT2(psi2_t . IFFT2(G_g . P_r)).
+// Contiguous ranges of the flattened (cell, term) work of the I3 sums, one per
+// cluster: cluster k takes u in [start(k), start(k + 1)) of total = ncells x
+// nterms, u = cell x nterms + term, and writes one partial per cell it
+// touches to slot k x maxc + (cell - first_cell(k)).  Cell c's partials are
+// those of clusters cluster_of(c nterms) .. cluster_of((c + 1) nterms - 1),
+// summed in that order.  nslots = 0: the (cell, chunk) grid instead.
+struct TermRanges {
+	int nslots = 0, nterms = 0, maxc = 0;
+	long total = 0;
+	__host__ __device__ long start(int k) const { return (long)k * total / nslots; }
+	__host__ __device__ int cluster_of(long u) const { return (int)(((u + 1) * nslots - 1) / total); }
+	__host__ __device__ long first_cell(int k) const { return start(k) / nterms; }
+};
+
 template <class C> struct I3ParamsT {
 	using R = typename CT<C>::R;
 	int nchunk, nterms;
+	TermRanges rg;                                        // nslots > 0: one term range per cluster (k_i3p)
 	const double2 *src; long src_cell; int src_comp[4];   // N x N grids (FP64 state)
 	const C *Ghat; long g_cell;                           // P x P grids, G_g at Ghat + cell*g_cell + g*P*P
 	int ncombo[4]; int ca[4][4], cgi[4][4]; double ccoef[4][4];
@@ -605,9 +620,18 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 	cg::cluster_group cluster = cg::this_cluster();
 	const int rank = (int)cluster.block_rank();
 	const long cid = blockIdx.x / 2;
-	const int chunk = (int)(cid % p.nchunk);
-	const long cell = cid / p.nchunk;
-	if (kind != nullptr && kind[cell] != 1) return;     // both CTAs of the cluster leave before any barrier
+	// work of this cluster: terms [u, u1) of the flattened (cell, term) order
+	long u, u1;
+	if (p.rg.nslots > 0) {
+		u = p.rg.start((int)cid);
+		u1 = p.rg.start((int)cid + 1);
+	} else {
+		const int chunk = (int)(cid % p.nchunk);
+		const long cell = cid / p.nchunk;
+		if (kind != nullptr && kind[cell] != 1) return;     // both CTAs of the cluster leave before any barrier
+		u = cell * p.nterms + (long)chunk * p.nterms / p.nchunk;
+		u1 = cell * p.nterms + (long)(chunk + 1) * p.nterms / p.nchunk;
+	}
 	const int warp = threadIdx.x >> 5;
 	if (warp == 0) tmem_alloc(&tmem_slot, TM::ALLOC);
 	init_twiddles<P>(tw);
@@ -627,14 +651,20 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 		for (int q = 0; q < 4; q++) a[q] = tw[(tau * (q + 1)) & (P - 1)];
 		tmem_st4(twaddr, a);
 	}
+	C *Ppeer = cluster.map_shared_rank(Pq, rank ^ 1);
+	// one segment per cell of the range (the (cell, chunk) grid has one)
+#pragma unroll 1
+	while (u < u1) {
+	const long cell = u / p.nterms;
+	const int t0 = (int)(u % p.nterms);
+	const int t1 = (int)min((long)p.nterms, t0 + (u1 - u));
+	u += t1 - t0;
 #pragma unroll
 	for (int q = 0; q < 2; q++)
 #pragma unroll
 		for (int e = 0; e < 8; e++) tmem_st(TM::addr(tbase, q, e), czero<C>());
 	tmem_wait_st();
 	const C *Gcell = p.Ghat + cell * p.g_cell;
-	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
-	C *Ppeer = cluster.map_shared_rank(Pq, rank ^ 1);
 	for (int t = t0; t < t1; t++) {
 #pragma unroll 1
 		for (int q = 0; q < 2; q++) {
@@ -735,14 +765,18 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 		}
 		cluster.sync();
 	}
+	// partial sums of this segment: slot (cluster, cell) of the ranges, or (cell, chunk)
+	const long slot = p.rg.nslots > 0 ? cid * p.rg.maxc + (cell - p.rg.first_cell((int)cid))
+	                                  : cell * p.nchunk + (int)(cid % p.nchunk);
 #pragma unroll 1
 	for (int q = 0; q < 2; q++) {
 		C acc[8];
 		tmem_ld8(TM::addr(tbase, q, 0), acc);
 		tmem_wait_ld();
-		C *o = p.out + ((cell * p.nchunk + chunk) * 4 + 2 * rank + q) * (long)P * P + line * P;
+		C *o = p.out + (slot * 4 + 2 * rank + q) * (long)P * P + line * P;
 #pragma unroll
 		for (int e = 0; e < 8; e++) o[Lp::out_pos(tau, e)] = acc[e];
+	}
 	}
 	tmem_fence_before();
 	__syncthreads();
@@ -951,6 +985,7 @@ template <class C> struct AsmParamsT {
 	const C *FS4;                     // [cell][4][P*P]  FFT2 of the I4 sums, or null
 	const C *Qp; int nq;              // [cell][4][nq][P*P] I2 partials, or null
 	const C *Xp; int nx;              // [cell][nx][4][P*P] I3 partials, or null
+	TermRanges xrg;                   // xrg.nslots > 0: Xp holds [slot][4][P*P] partials of term ranges
 	double s1, s2;
 	int mode;
 	double2 *out_cc, *out_cd;         // mode 0: [cell][4][N*N] (either may be null)
@@ -1017,7 +1052,14 @@ __global__ void __launch_bounds__(Geo<P>::NT) k_assemble(const AsmParamsT<C> p) 
 			}
 			if (p.Xp != nullptr) {
 				C s = czero<C>();
-				for (int k = 0; k < p.nx; k++) s = cadd(s, p.Xp[((cell * p.nx + k) * 4 + j) * (long)PP + i]);
+				if (p.xrg.nslots > 0) {
+					const TermRanges &g = p.xrg;
+					const int k0 = g.cluster_of(cell * (long)g.nterms), k1 = g.cluster_of((cell + 1) * (long)g.nterms - 1);
+					for (int k = k0; k <= k1; k++)
+						s = cadd(s, p.Xp[(((long)k * g.maxc + (cell - g.first_cell(k))) * 4 + j) * (long)PP + i]);
+				} else {
+					for (int k = 0; k < p.nx; k++) s = cadd(s, p.Xp[((cell * p.nx + k) * 4 + j) * (long)PP + i]);
+				}
 				z.x -= eta2[j] * s1 * s.x; z.y -= eta2[j] * s1 * s.y;
 			}
 			if (p.FS4 != nullptr) {

@@ -484,6 +484,25 @@ def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
         final[prec] = torch.cat([x.reshape(-1) for x in states]).cpu().numpy()
     out["speedup_f32_vs_f64"] = round(out["f32"]["value"] / out["f64"]["value"], 4)
     out["rel_l2_f32_vs_f64_final_states"] = float(np.linalg.norm(final[32] - final[64]) / np.linalg.norm(final[64]))
+    if args.config3_big > 0:
+        # the configuration's instance count in the FP32 form: sizes of this build, weights renormalised
+        nbig = args.config3_big
+        sizes_b = rng.choice([16, 32, 64], size=nbig, p=w / w.sum())
+        states = [qbgpu.to_fourier(torch.from_numpy(qbgpu.gaussian_mixture_state(int(n), L, seed=9000 + i, ncells=1)).cuda())[0].contiguous()
+                  for i, n in enumerate(sizes_b)]
+        qbgpu.homogeneous_batch(states, dt, 1, rk4=True, J=J, M=M, L=L, R=R, precision=32)     # tuning and sizing
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        e0.record()
+        qbgpu.homogeneous_batch(states, dt, 4, rk4=True, J=J, M=M, L=L, R=R, precision=32)     # 2 direct steps, then a 2-step graph
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 4
+        out["f32_all_instances"] = {"instances": nbig, "instances_per_N": {str(k): int((sizes_b == k).sum()) for k in (16, 32, 64)},
+                                    "value": round(nbig / (ms * 1e-3), 3), "ms_per_step": round(ms, 3),
+                                    "timed": "4 RK4 steps in one call (two direct, then one two-step CUDA graph replay)"}
+    out["schedules"] = [s_ for s_ in qbgpu.batch_schedules() if s_["J"] == J and s_["M"] == M]
     return out
 
 
@@ -847,6 +866,8 @@ def main():
                     help="Strang steps of the N = 64 FP32-against-FP64 long run (0 skips it)")
     ap.add_argument("--config2-long-cells", type=int, default=2, help="x-cells of the N = 64 long run")
     ap.add_argument("--no-config3", action="store_true", help="skip the mixed-size batch sample")
+    ap.add_argument("--config3-big", type=int, default=4096,
+                    help="instances of the FP32 mixed-size batch at the configuration's count (0 skips it)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
     ap.add_argument("--surrogate-n64", action="store_true", help="add the learned operator at N = 64 (about two minutes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

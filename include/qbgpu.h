@@ -110,6 +110,18 @@ int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *
 int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
                             int precision, int J, int M, double L, double R, void *stream);
 
+/* The schedules the batch calls above have tuned so far (no upstream
+ * counterpart), as a JSON array: per (device, N, precision, instance count,
+ * method, J, M) the chosen multipliers of the heuristic chunk counts, the I3
+ * schedule and variant, and the measured step time.  Writes at most len - 1
+ * characters and a terminating zero; returns the full length.  The first batch
+ * call for such a key times the candidates on the device (synchronising);
+ * QB_BATCH_TUNE=0 keeps the defaults.  All groups of a call advance
+ * concurrently on their own streams.  Within a call, once two direct steps
+ * have reallocated no buffer, two steps at a time replay a CUDA graph of all
+ * groups (QB_CUDA_GRAPHS=0: direct launches only). */
+int qb_batch_schedules(char *buf, int len);
+
 /* one Strang step of InhomStepPeriodic (bc = 0) / InhomStepDirichlet (bc = 1)
  * (upstream src/simulation.c:307-830) over ncells velocity-space cells with
  * box half-width L; Bext = 3 doubles per cell (NULL: no field).  Wnext must

@@ -3,20 +3,38 @@
 // SimulationHomogeneous, src/simulation.c:1219-1281, run on many instances
 // at once).
 //
-// Instances of equal grid size are gathered into one contiguous batch and
-// advanced together: one batched launch sequence per grid size and step, so
-// a batch of thousands of small instances costs a few launches per size
-// instead of a few per instance.  The quadrature tables and workspaces are
-// built once per (grid size, J, M, L, R) and kept for later calls.
+// Instances of equal grid size are gathered into one contiguous group and
+// advanced together: one batched launch sequence per group and step, so a
+// batch of thousands of small instances costs a few launches per size
+// instead of a few per instance.  On top of that:
+//   - every group runs on its own stream, forked from and joined to the
+//     caller's stream with events, so the groups of different sizes overlap
+//     on the GPU;
+//   - the first call for a (device, size, instance count, precision, method,
+//     tables) tunes the group's schedule by timing candidate settings on the
+//     device -- multipliers of the heuristic chunk counts of the quadrature
+//     sums, and where they exist the alternative I3 schedules (the term ranges
+//     or the (cell, chunk) grid of the FP64 sums at N = 32; the FFT kernels or
+//     the tensor-core DFT-GEMMs of the FP32 form at N = 16) -- and keeps the
+//     fastest;
+//   - the steps of all groups are captured once into a CUDA graph of two
+//     steps (state a -> b -> a), which is then relaunched.
+// The quadrature tables, workspaces, group buffers, schedules and the graph
+// are kept for later calls.
 #include "qb_engine.h"
 
 extern "C" {
 #include "qbgpu.h"
 }
 
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -42,8 +60,120 @@ std::map<std::tuple<int, int, int>, std::unique_ptr<qb::Workspace>> g_ws;   // (
 
 struct Group {
 	qb::DevBuf ptrs, state_a, state_b, bfield;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t done = nullptr;
+	~Group() {
+		if (done) cudaEventDestroy(done);
+		if (stream) cudaStreamDestroy(stream);
+	}
 };
-std::map<std::pair<int, int>, std::unique_ptr<Group>> g_groups;      // (device, N)
+std::map<std::tuple<int, int, int>, std::unique_ptr<Group>> g_groups;      // (device, N, precision)
+
+// a group's schedule: the workspace knobs (qb::Workspace) and its measured step time
+struct Sched {
+	float s12 = 1.0f, s3 = 1.0f;
+	int ranges = -1, variant = 0;
+	double ms = 0.0;
+};
+// (device, N, precision, instances, rk4, J, M, L, R)
+using SchedKey = std::tuple<int, int, int, int, int, int, int, double, double>;
+std::map<SchedKey, Sched> g_sched;
+
+struct BatchGraph {
+	std::vector<double> key;
+	cudaGraphExec_t exec = nullptr;
+	unsigned long long generation = 0;   // buffer_generation() at capture
+};
+std::map<int, BatchGraph> g_graph;                 // per device: the graph of the last batch layout
+// per device: the fork event of the groups' streams, and the stream the graph
+// is captured and launched on (the caller's stream may be the legacy default
+// stream, which cannot be captured) with the events that order it after and
+// before the caller's stream
+struct DevSync {
+	cudaEvent_t fork = nullptr, in = nullptr, out = nullptr;
+	cudaStream_t cap = nullptr;
+};
+std::map<int, DevSync> g_sync;
+
+bool env_on(const char *name) {
+	const char *e = getenv(name);
+	return e == nullptr || strcmp(e, "0") != 0;
+}
+
+void apply(qb::Workspace &ws, const Sched &sc) {
+	ws.chunk_scale12 = sc.s12;
+	ws.chunk_scale3 = sc.s3;
+	ws.i3_ranges = sc.ranges;
+	ws.i3_variant = sc.variant;
+}
+
+void step_one(qb::Workspace &ws, const qb::Quad &q, int g, const double2 *in, const double *B, double dt, double2 *out, int rk4,
+              cudaStream_t s) {
+	if (rk4) qb::collision_step_rk4(ws, q.set(), g, in, B, dt, out, s);
+	else qb::collision_step(ws, q.set(), g, in, B, dt, out, s);
+}
+
+// time the candidate schedules of one group on its stream: one warm-up step
+// with the default schedule, then one timed step per candidate (input a,
+// output b: the state is not advanced); the fastest is applied and returned.
+// A group whose default step takes longer than kTuneLimitMs already fills
+// the GPU with work units: it keeps the default without trying the others.
+constexpr double kTuneLimitMs = 500.0;
+Sched autotune(qb::Workspace &ws, const qb::Quad &q, int N, int prec, int g, const double2 *a, double2 *b, const double *B,
+               double dt, int rk4, cudaStream_t s) {
+	std::vector<Sched> cand(5);
+	cand[1].s12 = 0.5f;
+	cand[2].s12 = 2.0f;
+	cand[3].s3 = 0.5f;
+	cand[4].s3 = 2.0f;
+	if (N == 32 && prec == 64) { Sched c; c.ranges = 0; cand.push_back(c); }
+	if (N == 16 && prec == 32) { Sched c; c.variant = 1; cand.push_back(c); }
+	cudaEvent_t e0, e1;
+	QB_CUDA(cudaEventCreate(&e0));
+	QB_CUDA(cudaEventCreate(&e1));
+	apply(ws, cand[0]);
+	step_one(ws, q, g, a, B, dt, b, rk4, s);
+	Sched best;
+	best.ms = 1e300;
+	for (Sched &c : cand) {
+		apply(ws, c);
+		if (&c != &cand[0]) step_one(ws, q, g, a, B, dt, b, rk4, s);     // sizes the buffers of this schedule
+		QB_CUDA(cudaEventRecord(e0, s));
+		step_one(ws, q, g, a, B, dt, b, rk4, s);
+		QB_CUDA(cudaEventRecord(e1, s));
+		QB_CUDA(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		QB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+		c.ms = ms;
+		if (c.ms < best.ms) best = c;
+		if (&c == &cand[0] && c.ms > kTuneLimitMs) break;
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	apply(ws, best);
+	return best;
+}
+
+struct Live {             // one group of this call
+	int N, g;
+	long per;
+	qb::Workspace *ws;
+	qb::Quad *quad;
+	Group *grp;
+	double2 *cur, *nxt;
+};
+
+// one step of every group, each on its own stream between a fork and a join on s
+void step_all(std::vector<Live> &lv, double dt, int rk4, cudaEvent_t fork, cudaStream_t s) {
+	QB_CUDA(cudaEventRecord(fork, s));
+	for (Live &l : lv) {
+		QB_CUDA(cudaStreamWaitEvent(l.grp->stream, fork, 0));
+		step_one(*l.ws, *l.quad, l.g, l.cur, l.grp->bfield.as<double>(), dt, l.nxt, rk4, l.grp->stream);
+		QB_CUDA(cudaEventRecord(l.grp->done, l.grp->stream));
+		std::swap(l.cur, l.nxt);
+	}
+	for (Live &l : lv) QB_CUDA(cudaStreamWaitEvent(s, l.grp->done, 0));
+}
 
 }  // namespace
 
@@ -63,6 +193,8 @@ extern "C" int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, 
 			if (W[i] == nullptr) QB_FAIL("qb_homogeneous_batch: null state of instance " + std::to_string(i));
 			by_n[n[i]].push_back(i);
 		}
+		const bool tune = env_on("QB_BATCH_TUNE");
+		std::vector<Live> lv;
 		for (auto &kv : by_n) {
 			const int N = kv.first;
 			const std::vector<int> &idx = kv.second;
@@ -75,8 +207,12 @@ extern "C" int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, 
 				ws = std::make_unique<qb::Workspace>(N);
 				ws->prec = precision;
 			}
-			auto &grp = g_groups[{ dev, N }];
-			if (!grp) grp = std::make_unique<Group>();
+			auto &grp = g_groups[std::make_tuple(dev, N, precision)];
+			if (!grp) {
+				grp = std::make_unique<Group>();
+				QB_CUDA(cudaStreamCreateWithFlags(&grp->stream, cudaStreamNonBlocking));
+				QB_CUDA(cudaEventCreateWithFlags(&grp->done, cudaEventDisableTiming));
+			}
 			std::vector<const double2 *> src(g);
 			std::vector<double> bh(3L * g, 0.0);
 			for (int k = 0; k < g; k++) {
@@ -93,18 +229,83 @@ extern "C" int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, 
 			const unsigned nb = (unsigned)std::min<long>((per * g + 255) / 256, 148L * 16);
 			k_gather<<<nb, 256, 0, s>>>(grp->ptrs.as<const double2 *const>(), per, g, grp->state_a.as<double2>());
 			QB_CUDA(cudaGetLastError());
-			double2 *cur = grp->state_a.as<double2>(), *nxt = grp->state_b.as<double2>();
-			for (unsigned st = 0; st < steps; st++) {
-				if (rk4) qb::collision_step_rk4(*ws, quad->set(), g, cur, grp->bfield.as<double>(), dt, nxt, s);
-				else qb::collision_step(*ws, quad->set(), g, cur, grp->bfield.as<double>(), dt, nxt, s);
-				std::swap(cur, nxt);
+			const SchedKey sk(dev, N, precision, g, rk4 ? 1 : 0, J, M, L, R);
+			auto it = g_sched.find(sk);
+			if (it != g_sched.end()) {
+				apply(*ws, it->second);
+			} else if (tune) {
+				g_sched[sk] = autotune(*ws, *quad, N, precision, g, grp->state_a.as<double2>(), grp->state_b.as<double2>(),
+				                       grp->bfield.as<double>(), dt, rk4, s);
+			} else {
+				apply(*ws, Sched{});
 			}
-			k_scatter<<<nb, 256, 0, s>>>(cur, per, g, grp->ptrs.as<double2 *const>());
-			QB_CUDA(cudaGetLastError());
-			// the host vectors above are read by the asynchronous copies only
-			// until they return (pageable memory is staged); the device
-			// buffers of this group are reused by the next call on `s`
+			lv.push_back(Live{ N, g, per, ws.get(), quad.get(), grp.get(), grp->state_a.as<double2>(), grp->state_b.as<double2>() });
 		}
+		DevSync &ds = g_sync[dev];
+		if (ds.fork == nullptr) {
+			QB_CUDA(cudaEventCreateWithFlags(&ds.fork, cudaEventDisableTiming));
+			QB_CUDA(cudaEventCreateWithFlags(&ds.in, cudaEventDisableTiming));
+			QB_CUDA(cudaEventCreateWithFlags(&ds.out, cudaEventDisableTiming));
+			QB_CUDA(cudaStreamCreateWithFlags(&ds.cap, cudaStreamNonBlocking));
+		}
+		unsigned done = 0;
+		if (steps >= 2 && env_on("QB_CUDA_GRAPHS")) {
+			// the layout and parameters the graph is captured for
+			std::vector<double> key = { dt, (double)rk4, (double)precision, (double)J, (double)M, L, R };
+			for (const Live &l : lv) {
+				key.push_back((double)l.N);
+				key.push_back((double)l.g);
+				key.push_back((double)(uintptr_t)l.cur);
+				key.push_back((double)(uintptr_t)l.nxt);
+				key.push_back((double)(uintptr_t)l.grp->bfield.p);
+			}
+			BatchGraph &bg = g_graph[dev];
+			if (bg.key != key || bg.generation != qb::buffer_generation()) {
+				if (bg.exec) { cudaGraphExecDestroy(bg.exec); bg.exec = nullptr; }
+				bg.key = key;
+			}
+			// two steps run directly until none of them reallocated a buffer (the
+			// first steps of a layout size the buffers of its schedules); then two
+			// steps are captured (a -> b -> a) on the capture stream and relaunched
+			while (done + 2 <= steps && bg.exec == nullptr) {
+				const unsigned long long gen0 = qb::buffer_generation();
+				step_all(lv, dt, rk4, ds.fork, s);
+				step_all(lv, dt, rk4, ds.fork, s);
+				done += 2;
+				if (qb::buffer_generation() == gen0) {
+					cudaGraph_t gr = nullptr;
+					QB_CUDA(cudaStreamBeginCapture(ds.cap, cudaStreamCaptureModeThreadLocal));
+					step_all(lv, dt, rk4, ds.fork, ds.cap);
+					step_all(lv, dt, rk4, ds.fork, ds.cap);
+					QB_CUDA(cudaStreamEndCapture(ds.cap, &gr));
+					QB_CUDA(cudaGraphInstantiate(&bg.exec, gr, 0));
+					cudaGraphDestroy(gr);
+					bg.generation = qb::buffer_generation();
+				}
+			}
+			if (bg.exec != nullptr && done + 2 <= steps) {
+				QB_CUDA(cudaEventRecord(ds.in, s));
+				QB_CUDA(cudaStreamWaitEvent(ds.cap, ds.in, 0));
+				while (done + 2 <= steps) {
+					QB_CUDA(cudaGraphLaunch(bg.exec, ds.cap));
+					done += 2;
+				}
+				QB_CUDA(cudaEventRecord(ds.out, ds.cap));
+				QB_CUDA(cudaStreamWaitEvent(s, ds.out, 0));
+			}
+		}
+		while (done < steps) {
+			step_all(lv, dt, rk4, ds.fork, s);
+			done++;
+		}
+		for (const Live &l : lv) {
+			const unsigned nb = (unsigned)std::min<long>((l.per * l.g + 255) / 256, 148L * 16);
+			k_scatter<<<nb, 256, 0, s>>>(l.cur, l.per, l.g, l.grp->ptrs.as<double2 *const>());
+			QB_CUDA(cudaGetLastError());
+		}
+		// the host vectors above are read by the asynchronous copies only until
+		// they return (pageable memory is staged); the device buffers of the
+		// groups are reused by the next call on `s`
 		return 0;
 	} catch (const std::exception &) {
 		return -1;
@@ -114,4 +315,26 @@ extern "C" int qb_homogeneous_batch_ex(int ninst, const int *n, void *const *W, 
 extern "C" int qb_homogeneous_batch(int ninst, const int *n, void *const *W, const double *B, double dt, unsigned steps, int rk4,
                                     int J, int M, double L, double R, void *stream) {
 	return qb_homogeneous_batch_ex(ninst, n, W, B, dt, steps, rk4, 64, J, M, L, R, stream);
+}
+
+extern "C" int qb_batch_schedules(char *buf, int len) {
+	std::lock_guard<std::mutex> lk(g_mu);
+	std::string out = "[";
+	for (const auto &kv : g_sched) {
+		const SchedKey &k = kv.first;
+		const Sched &c = kv.second;
+		char line[320];
+		snprintf(line, sizeof(line),
+		         "%s{\"device\": %d, \"N\": %d, \"precision\": %d, \"instances\": %d, \"rk4\": %d, \"J\": %d, \"M\": %d, "
+		         "\"chunk_scale_i1_i2_i4\": %g, \"chunk_scale_i3\": %g, \"i3_ranges\": %d, \"i3_variant\": %d, \"step_ms\": %.4f}",
+		         out.size() > 1 ? ", " : "", std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), std::get<4>(k),
+		         std::get<5>(k), std::get<6>(k), c.s12, c.s3, c.ranges, c.variant, c.ms);
+		out += line;
+	}
+	out += "]";
+	if (buf != nullptr && len > 0) {
+		strncpy(buf, out.c_str(), (size_t)len - 1);
+		buf[len - 1] = 0;
+	}
+	return (int)out.size();
 }

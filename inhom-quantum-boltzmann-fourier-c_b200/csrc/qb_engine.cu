@@ -322,6 +322,19 @@ inline TermRanges term_ranges(int slots, int nterms, int ncells) {
 	return g;
 }
 
+// the workspace's chunk multipliers applied to heuristic chunk counts
+inline void scale_chunks(const Workspace &ws, const QuadSet &q, Chunks &ch) {
+	auto sc = [](int c, float f, int nterms, int cap) {
+		const int v = (int)std::lround((double)c * f);
+		return std::max(1, std::min(std::min(v, std::max(1, nterms)), cap));
+	};
+	if (ws.chunk_scale12 != 1.0f) {
+		if (q.i1) ch.i1 = sc(ch.i1, ws.chunk_scale12, q.i1->nterms, 64);
+		if (q.i2) ch.i2 = sc(ch.i2, ws.chunk_scale12, q.i2->nterms, 64);
+	}
+	if (ws.chunk_scale3 != 1.0f && q.i3) ch.i3 = sc(ch.i3, ws.chunk_scale3, q.i3->nterms, 256);
+}
+
 constexpr double kRealFormBound = 1e-6;
 // The real forms pack the combos of an output in pairs.  Both callers of the
 // I3 sums (the Cd assembly and the single-integral path) set 4 combos per
@@ -584,9 +597,11 @@ template <int P, class C> struct Rhs {
 			check_tmem_coresidency();
 			ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), num_sms(), 256, 0.15);      // one CTA per SM
 		}
+		scale_chunks(ws, q, ch);
 		// FP64 at N = 32: every resident cluster of k_i3p takes one contiguous range
 		// of the (cell, term) work, one partial per cell it touches
-		if (P == 64 && sizeof(C) == 16 && q.i3 && q.i3->nterms > 0 && term_ranges_enabled())
+		const bool ranges = ws.i3_ranges >= 0 ? ws.i3_ranges == 1 : term_ranges_enabled();
+		if (P == 64 && sizeof(C) == 16 && q.i3 && q.i3->nterms > 0 && ranges)
 			ch.i3_slots = (int)std::min<long>(active_i3p_clusters<C>(), (long)ncells * q.i3->nterms);
 		spectra(ws, ncells, W, s);
 		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
@@ -933,6 +948,7 @@ template <class C> struct Rhs<128, C> {
 			const int act = (sizeof(C) == 8 && use_full128()) ? active_i3_full128_clusters() : active_i3_clusters128<C>();
 			ch.i3 = best_chunks((long)ncells, std::max(1, q.i3->nterms), act, 256, 0.15);
 		}
+		scale_chunks(ws, q, ch);
 		spectra(ws, ncells, W, s);
 		if (parts & RHS_CC) i1_sums(ws, *q.i1, ncells, W, true, ws.i1cc, ws.fs, ch.i1, s);
 		if (parts & RHS_CD) {

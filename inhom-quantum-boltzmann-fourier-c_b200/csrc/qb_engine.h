@@ -94,6 +94,11 @@ struct Workspace {
 	DevBuf i3stats;                          // N = 64, FP32: cells evaluated by the real form, by either form (2 x u64)
 	DevBuf kerr;                             // device error word of kernels with bounded waits (nonzero: a wait ran out)
 	int i3_variant = 0;                      // I3 sums: 0 the FFT kernels, 1 DFT-GEMMs on the tensor cores (FP32 form, N = 16)
+	// schedule knobs (set by the batch autotuner): multipliers of the heuristic
+	// chunk counts of the I1/I2/I4 sums and of the I3 sums, and the FP64 I3
+	// schedule at N = 32 (-1: the default, 0: (cell, chunk) grid, 1: term ranges)
+	float chunk_scale12 = 1.0f, chunk_scale3 = 1.0f;
+	int i3_ranges = -1;
 	double tables_L = -1.0;                  // box half-width the velocity tables in `vgrid` were built for
 	// replay of repeated Strang steps (batched API): the launch sequence of a
 	// (pointers, parameters) key is captured on its second call and relaunched

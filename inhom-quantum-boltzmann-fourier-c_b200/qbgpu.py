@@ -71,6 +71,7 @@ def lib(n_grid=N_GRID):
     L.qb_workspace_set_i3_variant.argtypes = [_vp, C.c_int]
     L.qb_workspace_device_errors.argtypes = [_vp]
     L.qb_umma_selftest.argtypes = [_vp, _vp, _vp, _vp]
+    L.qb_batch_schedules.argtypes = [C.c_char_p, C.c_int]
     L.qb_fp64_peak_tflops.restype = C.c_double
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]
@@ -230,6 +231,15 @@ def inhom_step(ws, q, W, h, dt, Bext=None, bc="periodic", out=None):
     _check(lib().qb_inhom_step(ws.h, q.h, n, _ptr(W), _ptr(out), h, dt, _ptr(Bext), 0 if bc == "periodic" else 1, _stream()),
            "qb_inhom_step")
     return out
+
+
+def batch_schedules():
+    """the schedules tuned so far by homogeneous_batch (list of dicts)"""
+    import json
+    n = lib().qb_batch_schedules(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().qb_batch_schedules(buf, n + 1)
+    return json.loads(buf.value.decode())
 
 
 def homogeneous_batch(states, dt, steps, B=None, rk4=True, J=16, M=16, L=6.0, R=3.75, precision=64):

@@ -55,3 +55,32 @@ def test_fp32_batch_tracks_fp64_batch():
         assert 0 < e <= 1e-5, (sizes[i], e)
     with pytest.raises(RuntimeError):
         qbgpu.homogeneous_batch([torch.from_numpy(Wf[0].copy()).cuda()], 0.01, 1, precision=16)
+
+
+def test_batch_graph_replay_and_tuned_schedules(monkeypatch):
+    """a batch call of 7 steps: the groups' schedules are tuned on the first
+    call, two direct steps size the buffers, then two-step CUDA graphs of all
+    groups (each size on its own stream) are replayed; the result equals the
+    same call with direct launches bit for bit, and the oracle within 1e-12"""
+    sizes = [16, 8, 16, 32, 8]
+    rng = np.random.default_rng(21)
+    Wf = [orc.to_fourier(qbgpu.gaussian_mixture_state(n, L, seed=500 + i, ncells=1))[0] for i, n in enumerate(sizes)]
+    B = rng.standard_normal((len(sizes), 3)) * 0.1
+    dt, steps = 0.01, 7
+    graphed = [torch.from_numpy(w.copy()).cuda() for w in Wf]
+    qbgpu.homogeneous_batch(graphed, dt, steps, B=B, rk4=True, J=J, M=M, L=L, R=R)
+    monkeypatch.setenv("QB_CUDA_GRAPHS", "0")
+    direct = [torch.from_numpy(w.copy()).cuda() for w in Wf]
+    qbgpu.homogeneous_batch(direct, dt, steps, B=B, rk4=True, J=J, M=M, L=L, R=R)
+    torch.cuda.synchronize()
+    for a, b in zip(graphed, direct):
+        assert torch.equal(a, b)
+    oracles = {n: orc.Oracle(n, J, M, L, R) for n in set(sizes)}
+    for i, n in enumerate(sizes):
+        ref = Wf[i]
+        for _ in range(steps):
+            ref = oracles[n].collision_step(ref, dt, B[i], rk4=True)
+        assert rel_l1(graphed[i].cpu().numpy(), ref) < TOL, (i, n)
+    tuned = [s for s in qbgpu.batch_schedules() if s["J"] == J and s["M"] == M and s["rk4"] == 1]
+    assert {(s["N"], s["instances"]) for s in tuned} >= {(8, 2), (16, 2), (32, 1)}
+    assert all(s["step_ms"] > 0 for s in tuned)

@@ -672,10 +672,13 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samp
     for _ in range(args.warmup + args.steps):
         a = qbgpu.inhom_step(ws, q, a, wl["h"], wl["dt"], B)
     torch.cuda.synchronize()
+    long_run = surrogate_long_run(qbgpu, net, q, W0, wl, args.surrogate_long_steps, args.surrogate_long_cells) \
+        if args.surrogate_long_steps > 0 else None
     return {"what": f"Strang steps with the collision half from a Fourier neural operator (FP32), exact FP64 operator as judge "
                     f"every {every}th step and per-cell fallback above a relative L1 difference {tol} of the collision increment; "
                     f"the checking steps are inside "
                     f"the timed region",
+            "long_run": long_run,
             "value": round(value, 3), "unit": UNIT, "ms_per_step": round(ms / args.steps, 4),
             "speedup_vs_fp64": round(value / value64, 4),
             "training": {"pairs": nseeds * samples, "iterations": iters, "batch": 64, "lr": lr, "spin_rotations": True, "final_loss": loss,
@@ -683,6 +686,41 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samp
             "C_rel_l1_on_initial_state": round(c_err, 5),
             "cell_steps": {"surrogate": ns, "exact": ne}, "last_max_residual": round(res, 5),
             f"W_rel_l1_vs_fp64_after_{args.warmup + args.steps}_steps": rel(bufs[cur], a)}
+
+
+def surrogate_long_run(qbgpu, net, q, W0, wl, steps, cells, tols=(0.5, 0.1, 0.02, 1e-5), every=10):
+    """The surrogate's trajectory against the FP64 one over `steps` Strang
+    steps of the first `cells` x-cells (a periodic line of them, the workload's
+    h and dt), for judge tolerances `tols` (relative L1 of the collision
+    increment; 1e-5 is the configuration's residual bound): deviation of W,
+    cell-steps per operator, and the time per step against the FP64 step."""
+    import torch
+    N = wl["N"]
+    Ws = W0[:cells].contiguous()
+    B = torch.zeros((cells, 3), dtype=torch.float64, device="cuda")
+    ws = qbgpu.Workspace(N)
+
+    def run(step):
+        a, b = Ws.clone(), torch.empty_like(Ws)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            step(a, b)
+            a, b = b, a
+        e1.record()
+        torch.cuda.synchronize()
+        return a, e0.elapsed_time(e1) / steps
+    ref, ms64 = run(lambda a, b: qbgpu.inhom_step(ws, q, a, wl["h"], wl["dt"], B, out=b))
+    out = {"what": f"{steps} Strang steps of the first {cells} x-cells (a periodic line of them), judge every {every} steps",
+           "fp64_ms_per_step": round(ms64, 4), "by_tolerance": []}
+    for tol in tols:
+        sur = qbgpu.Surrogate(net, tol=tol, check_every=every)
+        Wn, ms = run(lambda a, b: sur.step(ws, q, a, wl["h"], wl["dt"], B, out=b))
+        ns, ne, _ = sur.stats()
+        out["by_tolerance"].append({"tol": tol, "W_rel_l1_vs_fp64": float((Wn - ref).abs().sum() / ref.abs().sum()),
+                                    "cell_steps": {"surrogate": ns, "exact": ne}, "ms_per_step": round(ms, 4),
+                                    "speedup_vs_fp64": round(ms64 / ms, 4)})
+    return out
 
 
 def run_surrogate64(args, qbgpu, flush, cells=64, nseeds=1024, samples=3, iters=8000, lr=5e-3, steps=10, warmup=3):
@@ -870,6 +908,9 @@ def main():
                     help="instances of the FP32 mixed-size batch at the configuration's count (0 skips it)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-operator measurement")
     ap.add_argument("--surrogate-n64", action="store_true", help="add the learned operator at N = 64 (about two minutes)")
+    ap.add_argument("--surrogate-long-steps", type=int, default=1000,
+                    help="Strang steps of the surrogate-against-FP64 long run (0 skips it)")
+    ap.add_argument("--surrogate-long-cells", type=int, default=16, help="x-cells of the surrogate long run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dftmma", action="store_true", help="skip the tensor-core DFT-GEMM sample (N = 16)")
     ap.add_argument("--dftmma-only", action="store_true",

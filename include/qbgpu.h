@@ -139,6 +139,25 @@ int qb_inhom_step_maxwell(qb_workspace *ws, const qb_quad *q, int ncells, const 
                           double h, double dt, double lambda, const double *WL, const double *WR,
                           const double *Bext, void *stream);
 
+/* One Strang step of this rank's block of a sharded periodic domain, for
+ * hosts that distribute the x-cells themselves (MPI ranks, or NCCL from C);
+ * it replaces upstream's MPI path of InhomStepPeriodic (src/simulation.c:
+ * 316-418).  ext_a and ext_b are device buffers of ncells + 4 velocity-space
+ * cells each, the haloed line [2 | local | 2]: the rank's cells start in
+ * ext_a[2 .. ncells + 1], and there the step leaves them.  exchange(ext,
+ * ncells, stream, user) must fill the halo cells 0, 1 and ncells + 2,
+ * ncells + 3 of `ext` with the last two cells of the left neighbour and the
+ * first two of the right neighbour on the periodic ring (ext's cells 2 ..
+ * ncells + 1 are this rank's), ordered on `stream` (e.g. ncclSend/ncclRecv
+ * there) or complete on return; it returns 0 on success.  It is called twice
+ * per step: before the first half step of transport, and after the collision
+ * of the two edge cells on each side, while the interior cells collide on
+ * the workspace's own stream (ncells >= 6; fewer cells collide all first).
+ * Bext: 3 doubles per local cell, or NULL. */
+typedef int (*qb_halo_exchange_fn)(double *ext, int ncells, void *stream, void *user);
+int qb_sharded_step(qb_workspace *ws, const qb_quad *q, int ncells, double *ext_a, double *ext_b, double h, double dt,
+                    const double *Bext, qb_halo_exchange_fn exchange, void *user, void *stream);
+
 /* velocity space <-> Fourier space for ngrids N x N components
  * (upstream src/simulation.c:224-283) */
 int qb_to_fourier(int N, int ngrids, const double *Wv, void *Wf, void *stream);

@@ -140,6 +140,8 @@ Workspace::~Workspace() {
 		if (g.exec) cudaGraphExecDestroy(g.exec);
 	if (ev_in) cudaEventDestroy(ev_in);
 	if (ev_out) cudaEventDestroy(ev_out);
+	if (ev_t) cudaEventDestroy(ev_t);
+	if (ev_i) cudaEventDestroy(ev_i);
 	if (stream) cudaStreamDestroy(stream);
 }
 

@@ -115,6 +115,10 @@ struct Workspace {
 	unsigned long long graph_clock = 0;
 	long graph_replays = 0;                  // launches served by an instantiated graph
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+	// the sharded step (qb_sharded_step): a second workspace for the edge cells,
+	// which collide on the caller's stream while the interior collides on `stream`
+	std::unique_ptr<Workspace> edge;
+	cudaEvent_t ev_t = nullptr, ev_i = nullptr;
 	explicit Workspace(int N);
 	~Workspace();
 };

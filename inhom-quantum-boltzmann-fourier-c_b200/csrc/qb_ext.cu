@@ -311,6 +311,47 @@ int qb_fourier_collision(qb_workspace *ws, const qb_quad *q, int ncells, double 
 	});
 }
 
+int qb_sharded_step(qb_workspace *ws, const qb_quad *q, int ncells, double *ext_a, double *ext_b, double h, double dt,
+                    const double *Bext, qb_halo_exchange_fn exchange, void *user, void *stream) {
+	return guarded([&] {
+		check(ws, q);
+		if (ncells < 2) QB_FAIL("qb_sharded_step: every rank needs at least two cells (upstream src/simulation.c:317)");
+		if (ext_a == nullptr || ext_b == nullptr || exchange == nullptr) QB_FAIL("qb_sharded_step: null buffer or exchange function");
+		if (ext_a == ext_b) QB_FAIL("qb_sharded_step: ext_a and ext_b must be distinct");
+		cudaStream_t s = pick(ws, stream);
+		const long NN = (long)ws->N * ws->N, cell = 4 * NN;
+		const double *A = velocity_tables(ws, q->q->L, s);
+		const int n = ncells;
+		if (exchange(ext_a, n, stream, user) != 0) QB_FAIL("qb_sharded_step: the halo exchange of the first half step failed");
+		qb::transport(4 * (int)NN, n + 4, ext_a, ext_b, A, h, 0.5 * dt, 0, s);
+		double *loc = ext_b + 2 * cell;                          // local cells of the half-stepped line
+		if (n >= 6) {
+			if (!ws->edge) ws->edge = std::make_unique<qb::Workspace>(ws->N);
+			qb::Workspace &ew = *ws->edge;
+			ew.prec = ws->prec;
+			ew.conserve = ws->conserve;
+			if (ws->ev_t == nullptr) {
+				QB_CUDA(cudaEventCreateWithFlags(&ws->ev_t, cudaEventDisableTiming));
+				QB_CUDA(cudaEventCreateWithFlags(&ws->ev_i, cudaEventDisableTiming));
+			}
+			// interior cells (local 2 .. n - 3) on the workspace stream, after the transport
+			QB_CUDA(cudaEventRecord(ws->ev_t, s));
+			QB_CUDA(cudaStreamWaitEvent(ws->stream, ws->ev_t, 0));
+			qb::fourier_collision(*ws, q->q->set(), n - 4, loc + 2 * cell, Bext ? Bext + 6 : nullptr, dt, ws->stream);
+			QB_CUDA(cudaEventRecord(ws->ev_i, ws->stream));
+			// edge cells on the caller's stream, then their halos leave while the interior collides
+			qb::fourier_collision(ew, q->q->set(), 2, loc, Bext, dt, s);
+			qb::fourier_collision(ew, q->q->set(), 2, loc + (long)(n - 2) * cell, Bext ? Bext + 3L * (n - 2) : nullptr, dt, s);
+			if (exchange(ext_b, n, stream, user) != 0) QB_FAIL("qb_sharded_step: the halo exchange of the second half step failed");
+			QB_CUDA(cudaStreamWaitEvent(s, ws->ev_i, 0));
+		} else {
+			qb::fourier_collision(*ws, q->q->set(), n, loc, Bext, dt, s);
+			if (exchange(ext_b, n, stream, user) != 0) QB_FAIL("qb_sharded_step: the halo exchange of the second half step failed");
+		}
+		qb::transport(4 * (int)NN, n + 4, ext_b, ext_a, A, h, 0.5 * dt, 0, s);
+	});
+}
+
 long qb_simulate_record(qb_workspace *ws, const qb_quad *q, int ncells, const double *W0, double h, double dt, unsigned numsteps,
                         const double *Bext, int bc, unsigned record_every, const char *path, double *final_out) {
 	long frames = 0;

@@ -37,6 +37,10 @@ def library_path(n_grid=N_GRID):
 _libs = {}
 
 
+# int exchange(double *ext, int ncells, void *stream, void *user) of qb_sharded_step
+HALO_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p)
+
+
 def lib(n_grid=N_GRID):
     """Load libqbgpu (raises if it has not been built)."""
     if n_grid in _libs:
@@ -72,6 +76,7 @@ def lib(n_grid=N_GRID):
     L.qb_workspace_device_errors.argtypes = [_vp]
     L.qb_umma_selftest.argtypes = [_vp, _vp, _vp, _vp]
     L.qb_batch_schedules.argtypes = [C.c_char_p, C.c_int]
+    L.qb_sharded_step.argtypes = [_vp, _vp, C.c_int, _vp, _vp, C.c_double, C.c_double, _vp, HALO_FN, _vp, _vp]
     L.qb_fp64_peak_tflops.restype = C.c_double
     L.qb_simulate_record.restype = C.c_long
     L.qb_simulate_record.argtypes = [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_uint, _vp, C.c_int, C.c_uint, C.c_char_p, _vp]

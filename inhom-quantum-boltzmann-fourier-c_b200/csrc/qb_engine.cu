@@ -670,17 +670,19 @@ template <class K> void set_smem_once(K kern, size_t bytes, DeviceFlag &done) {
 
 // I3 kernel of the collision operator at N = 64: 4 components on 2 CTA pairs
 constexpr int kI3Pairs128 = 2;
+// its dynamic shared memory: FP64 adds the landing buffer of the bulk-copy exchange
+template <class C> constexpr size_t smem_i3_128() { return smem128<C>() + (sizeof(C) == 16 ? kLbBytes : 0); }
 
 // active clusters of the 128 I3 kernel (occupancy query, cached per C)
 template <class C> int active_i3_clusters128() {
 	static DeviceInt cached{-1};
 	if (cached < 0) {
 		auto kern = k_i3_128<4, kI3Pairs128, C>;
-		set_smem(kern, smem128<C>());
+		set_smem(kern, smem_i3_128<C>());
 		cudaLaunchConfig_t cfg = {};
 		cfg.gridDim = dim3(2 * kI3Pairs128);
 		cfg.blockDim = dim3(G128::NT);
-		cfg.dynamicSmemBytes = smem128<C>();
+		cfg.dynamicSmemBytes = smem_i3_128<C>();
 		cudaLaunchAttribute attr;
 		attr.id = cudaLaunchAttributeClusterDimension;
 		attr.val.clusterDim.x = 2 * kI3Pairs128; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
@@ -718,18 +720,18 @@ template <class C> void launch_i2_128(const I2ParamsT<C> &p, long units, C *tmp,
 }
 // The tensor-memory allocation of k_i3_128 never waits as long as no more
 // CTAs share an SM than its 512 columns hold; checked before the first launch.
-template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, cudaStream_t s) {
+template <int CS, int NPAIR, class C> void launch_i3_128(const I3ParamsT<C> &p, long nclusters, C *pscr, int *err, cudaStream_t s) {
 	static DeviceFlag init;
 	if (!init) {
 		check_tmem_coresidency();
-		set_smem(k_i3_128<CS, NPAIR, C>, smem128<C>());
+		set_smem(k_i3_128<CS, NPAIR, C>, smem_i3_128<C>());
 		int per_sm = 0;
-		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_i3_128<CS, NPAIR, C>, G128::NT, smem128<C>()));
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_i3_128<CS, NPAIR, C>, G128::NT, smem_i3_128<C>()));
 		if (per_sm * (int)I3Tmem128<C, CS / NPAIR>::NCOLS > 512)
 			QB_FAIL("k_i3_128: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
 		init = true;
 	}
-	launch128(k_i3_128<CS, NPAIR, C>, "i3_cluster", nclusters * 2 * NPAIR, 2 * NPAIR, smem128<C>(), s, p, pscr);
+	launch128(k_i3_128<CS, NPAIR, C>, "i3_cluster", nclusters * 2 * NPAIR, 2 * NPAIR, smem_i3_128<C>(), s, p, pscr, err);
 }
 constexpr size_t kFull128Smem = sizeof(float2) * ((size_t)F128::GRID + 128 + 64);
 
@@ -807,11 +809,11 @@ void check_tmem_coresidency() {
 		{ (const void *)k_i3p<64, double2>, i3p_smem<double2>(), Geo<64>::NT, (int)I3Tmem<double2>::ALLOC, "k_i3p<f64>" },
 		{ (const void *)k_i3p<64, float2>, i3p_smem<float2>(), Geo<64>::NT, (int)I3Tmem<float2>::ALLOC, "k_i3p<f32>" },
 		{ (const void *)k_i3pr<64>, i3p_smem<float2>(), Geo<64>::NT, (int)I3TmemR::ALLOC, "k_i3pr" },
-		{ (const void *)k_i3_128<4, kI3Pairs128, double2>, smem128<double2>(), G128::NT,
+		{ (const void *)k_i3_128<4, kI3Pairs128, double2>, smem_i3_128<double2>(), G128::NT,
 		  (int)I3Tmem128<double2, 4 / kI3Pairs128>::NCOLS, "k_i3_128<f64>" },
-		{ (const void *)k_i3_128<4, kI3Pairs128, float2>, smem128<float2>(), G128::NT,
+		{ (const void *)k_i3_128<4, kI3Pairs128, float2>, smem_i3_128<float2>(), G128::NT,
 		  (int)I3Tmem128<float2, 4 / kI3Pairs128>::NCOLS, "k_i3_128<f32>" },
-		{ (const void *)k_i3_128<2, 1, double2>, smem128<double2>(), G128::NT, (int)I3Tmem128<double2, 2>::NCOLS,
+		{ (const void *)k_i3_128<2, 1, double2>, smem_i3_128<double2>(), G128::NT, (int)I3Tmem128<double2, 2>::NCOLS,
 		  "k_i3_128<f64, single integral>" },
 		{ (const void *)k_i3_full128<float2>, kFull128Smem, F128::NT, (int)F128Tmem::NCOLS, "k_i3_full128" },
 		{ (const void *)k_i3_full128r, kFull128Smem, F128::NT, (int)F128TmemR::NCOLS, "k_i3_full128r" },
@@ -938,7 +940,7 @@ template <class C> struct Rhs<128, C> {
 				return;
 			}
 		}
-		launch_i3_128<4, kI3Pairs128>(p, ncl, ws.scr128a.as<C>(), s);
+		launch_i3_128<4, kI3Pairs128>(p, ncl, ws.scr128a.as<C>(), ws.kerr.as<int>(), s);
 	}
 
 	static void prepare(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, Chunks &ch, cudaStream_t s) {
@@ -1294,7 +1296,7 @@ template <> struct I3S<128> {
 		p.psi1 = t.psi1.as<double2>(); p.psi2T = t.psi2T.as<double>();
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<double2>();
-		launch_i3_128<2, 1>(p, nchunk, ws.scr128a.as<double2>(), s);
+		launch_i3_128<2, 1>(p, nchunk, ws.scr128a.as<double2>(), ws.kerr.as<int>(), s);
 		ws.fs.ensure(sizeof(double2) * PP);
 		mul_sum(PP, nullptr, ws.i3p.as<double2>(), nchunk, 2 * PP, ws.fs.as<double2>(), s);
 		const double s2 = 1.0 / (double)PP;

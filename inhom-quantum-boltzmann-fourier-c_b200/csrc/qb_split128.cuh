@@ -245,6 +245,83 @@ __device__ __forceinline__ void pair_exchange(C *S, const C *peer, cg::cluster_g
 	__syncthreads();
 }
 
+// The same exchange for FP64 with the partner's half brought in by bulk
+// copies (the tensor-memory-access engine, cp.async.bulk between the
+// shared memories of the pair) instead of per-thread loads from distributed
+// shared memory.  A round covers columns 64 round .. 64 round + 63 of the 64
+// local rows: 64 threads each push one 1 KB row segment of their CTA's half
+// into the partner's landing buffer Lb (row pitch 65 values: the column
+// reads of the op are conflict-free), completing on the partner's mbarrier;
+// each CTA waits for its own incoming 64 KB, computes, waits until its
+// outgoing copies have read their source, then overwrites its half.  One
+// cluster barrier per round keeps the landing buffers free.  A wait that runs
+// out sets *abort (the kernel then stops waiting) and the error word.
+constexpr int kLbPitch = 65;
+constexpr size_t kLbBytes = sizeof(double2) * 64 * kLbPitch;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t map_peer(uint32_t local, int rank) {
+	uint32_t r;
+	asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+	return r;
+}
+__device__ __forceinline__ bool mbar_wait_parity(uint32_t mb, unsigned parity, unsigned limit) {
+	for (unsigned i = 0; i < limit; i++) {
+		uint32_t done = 0;
+		asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+		             : "=r"(done) : "r"(mb), "r"(parity) : "memory");
+		if (done) return true;
+	}
+	return false;
+}
+
+template <class Op>
+__device__ __forceinline__ void pair_exchange_bulk(double2 *S, double2 *Lb, uint64_t *mbar, unsigned &phase, int prank,
+                                                   cg::cluster_group &cl, volatile int *abort, int *err, const Op &op) {
+	using G = G128;
+	const int tid = (int)threadIdx.x;
+	const uint32_t mb = smem_addr(mbar);
+	const uint32_t lb_remote = map_peer(smem_addr(Lb), prank), mb_remote = map_peer(mb, prank);
+#pragma unroll 1
+	for (int round = 0; round < 2; round++) {
+		// this thread's writes of the half (and reads of the landing buffer) are ordered before the
+		// bulk copies, which go through the async proxy
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+		cl.sync();                                   // both halves final, the partner's landing buffer free
+		const bool skip = *abort != 0;
+		if (tid == 0)
+			asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(64u * 64u * 16u) : "memory");
+		if (tid < 64) {
+			const uint32_t src = smem_addr(S + tid * G::LDP + 64 * round);
+			const uint32_t dst = lb_remote + (uint32_t)(tid * kLbPitch * sizeof(double2));
+			asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+			             ::"r"(dst), "r"(src), "r"(1024u), "r"(mb_remote) : "memory");
+			asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+		}
+		if (!skip && !mbar_wait_parity(mb, phase, 1u << 24)) {
+			*abort = 1;
+			atomicExch(err, 1);
+		}
+		phase ^= 1u;
+		double2 res[8];
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			const int idx = i * 512 + tid;
+			const int l = idx & 63, kk = idx >> 6, k = 64 * round + kk;
+			res[i] = op(S[l * G::LDP + k], Lb[l * kLbPitch + kk], l, k);
+		}
+		if (tid < 64) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+		__syncthreads();
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			const int idx = i * 512 + tid;
+			const int l = idx & 63, k = 64 * round + (idx >> 6);
+			S[l * G::LDP + k] = res[i];
+		}
+	}
+	__syncthreads();
+}
+
 // value of the inverse (decimation-in-time) butterfly at row l' of half h:
 // CTA 0 holds E (even spectral rows), CTA 1 holds O; y[l'] = E + w'^l' O,
 // y[l' + 64] = E - w'^l' O with w' = exp(+2 pi i / 128)
@@ -417,17 +494,27 @@ template <class C, int CPP> struct I3Tmem128 {
 // with one pair exchange each (inverse butterfly, psi2, forward butterfly).
 // Components with fewer combos than the largest count run the barriers only.
 template <int CS, int NPAIR, class C>
-__global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr) {
+__global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr, int *err) {
 	using G = G128;
 	using R = typename CT<C>::R;
 	constexpr int CPP = CS / NPAIR;             // components per pair
 	static_assert(CS % NPAIR == 0, "components must divide over the pairs");
+	constexpr bool kBulk = sizeof(C) == 16;     // FP64: the exchange by bulk copies (landing buffer after the twiddles)
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *S = reinterpret_cast<C *>(smem_raw), *tw128 = S + G::GRID_H, *tw64 = tw128 + 128;
+	double2 *Lb = reinterpret_cast<double2 *>(tw64 + 64);
+	__shared__ __align__(8) uint64_t xmbar;
+	__shared__ int xabort;
+	unsigned xphase = 0;
 	cg::cluster_group cl = cg::this_cluster();
 	const int rank = (int)cl.block_rank();
 	const int pair = rank >> 1, h = rank & 1;
 	const C *peer = cl.map_shared_rank(S, rank ^ 1);
+	if (kBulk && threadIdx.x == 0) {
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&xmbar)) : "memory");
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		xabort = 0;
+	}
 	const long cid = blockIdx.x / (2 * NPAIR);
 	const int chunk = (int)(cid % p.nchunk);
 	const long cell = cid / p.nchunk;
@@ -491,7 +578,7 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 					col_pass<+1>(S, tw64, ColFromS<C>{S});
 				}
 				// inverse butterfly -> psi2 -> forward butterfly, one exchange
-				pair_exchange<true>(S, peer, cl, [&](C own, C oth, int l, int k) {
+				auto xop = [&](C own, C oth, int l, int k) {
 					if (!act) return own;
 					const C E = h ? oth : own, O = h ? own : oth;
 					const C w = tw128[l];
@@ -499,7 +586,9 @@ __global__ void __launch_bounds__(512, 1) k_i3_128(const I3ParamsT<C> p, C *pscr
 					const R f0 = sc * psi2[(long)k * G::P + l], f1 = sc * psi2[(long)k * G::P + l + 64];
 					const C z0 = cscale(cadd(E, wo), f0), z1 = cscale(csub(E, wo), f1);
 					return h ? cmul(csub(z0, z1), w) : cadd(z0, z1);
-				});
+				};
+				if constexpr (kBulk) pair_exchange_bulk(S, Lb, &xmbar, xphase, rank ^ 1, cl, &xabort, err, xop);
+				else pair_exchange<true>(S, peer, cl, xop);
 				if (act) {
 					col_pass<-1>(S, tw64, ColFromS<C>{S});
 					__syncthreads();

@@ -358,7 +358,12 @@ void launch_nyquist_kind(int N, int ncells, const double2 *W, double bound, int 
 // I3Tmem<C>::NCOLS columns never waits as long as no more CTAs share an SM
 // than its 512 columns hold; the shared-memory (FP64) or register (FP32)
 // footprint keeps it at one CTA per SM, checked here before the first launch.
-template <class C> size_t i3p_smem() { return sizeof(C) * ((size_t)3 * Geo<64, C>::GRID + 64); }
+// three grids and the twiddles; in FP32 two more grids receive the partner's P grids
+template <class C> size_t i3p_smem() {
+	return sizeof(C) * ((size_t)(sizeof(C) == 8 ? 5 : 3) * Geo<64, C>::GRID + 64);
+}
+// the real form receives the partner's packed P grid in its second grid slot
+inline size_t i3pr_smem() { return sizeof(float2) * ((size_t)3 * Geo<64, float2>::GRID + 64); }
 
 template <class C> int active_i3p_clusters() {
 	static DeviceInt cached{-1};
@@ -412,9 +417,9 @@ void launch_i3pr(const I3ParamsT<float2> &p, long nclusters, const int *kind, cu
 	auto kern = k_i3pr<64>;
 	if (!init) {
 		check_tmem_coresidency();
-		set_smem(kern, i3p_smem<float2>());
+		set_smem(kern, i3pr_smem());
 		int per_sm = 0;
-		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Geo<64>::NT, i3p_smem<float2>()));
+		QB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Geo<64>::NT, i3pr_smem()));
 		if (per_sm * (int)I3TmemR::ALLOC > 512)
 			QB_FAIL("k_i3pr: " + std::to_string(per_sm) + " CTAs per SM would oversubscribe tensor memory");
 		init = true;
@@ -422,7 +427,7 @@ void launch_i3pr(const I3ParamsT<float2> &p, long nclusters, const int *kind, cu
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3((unsigned)(nclusters * 2));
 	cfg.blockDim = dim3(Geo<64>::NT);
-	cfg.dynamicSmemBytes = i3p_smem<float2>();
+	cfg.dynamicSmemBytes = i3pr_smem();
 	cfg.stream = s;
 	cudaLaunchAttribute attr;
 	attr.id = cudaLaunchAttributeClusterDimension;
@@ -569,6 +574,7 @@ template <int P, class C> struct Rhs {
 		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
+		p.err = ws.kerr.as<int>();
 		if constexpr (P == 64) {
 			if constexpr (sizeof(C) == 8) {
 				if (use_real_form() && even_combos(p)) {
@@ -808,7 +814,7 @@ void check_tmem_coresidency() {
 	std::vector<TmemKernel> ks = {
 		{ (const void *)k_i3p<64, double2>, i3p_smem<double2>(), Geo<64>::NT, (int)I3Tmem<double2>::ALLOC, "k_i3p<f64>" },
 		{ (const void *)k_i3p<64, float2>, i3p_smem<float2>(), Geo<64>::NT, (int)I3Tmem<float2>::ALLOC, "k_i3p<f32>" },
-		{ (const void *)k_i3pr<64>, i3p_smem<float2>(), Geo<64>::NT, (int)I3TmemR::ALLOC, "k_i3pr" },
+		{ (const void *)k_i3pr<64>, i3pr_smem(), Geo<64>::NT, (int)I3TmemR::ALLOC, "k_i3pr" },
 		{ (const void *)k_i3_128<4, kI3Pairs128, double2>, smem_i3_128<double2>(), G128::NT,
 		  (int)I3Tmem128<double2, 4 / kI3Pairs128>::NCOLS, "k_i3_128<f64>" },
 		{ (const void *)k_i3_128<4, kI3Pairs128, float2>, smem_i3_128<float2>(), G128::NT,
@@ -926,6 +932,7 @@ template <class C> struct Rhs<128, C> {
 		p.psi1 = T::i3_psi1(t); p.psi2T = T::i3_psi2T(t);
 		p.psi2_idx = t.idx.as<int>(); p.psi2_scale = t.scale.as<double>();
 		p.out = ws.i3p.as<C>();
+		p.err = ws.kerr.as<int>();
 		if constexpr (sizeof(C) == 8) {
 			if (use_full128()) {
 				if (use_real_form() && even_combos(p)) {

@@ -321,6 +321,7 @@ template <class C> struct I3ParamsT {
 	const R *psi2T;                                       // transposed P x P tables
 	const int *psi2_idx; const double *psi2_scale;        // per term
 	C *out;                                               // [cell][chunk][CS][P*P]
+	int *err;                                             // error word of bounded waits (may be null)
 };
 using I3Params = I3ParamsT<double2>;
 
@@ -589,6 +590,55 @@ template <class C> struct I3Tmem {
 	__device__ __forceinline__ static unsigned twaddr(unsigned base) { return base + lanes() + NCOLS + 4 * (PSI + PJ) + slot() * 16u; }
 };
 
+// FP32 at P = 64: each CTA of the pair pushes its P grids of the term into the
+// partner's shared memory by bulk copies (cp.async.bulk between the pair's
+// shared memories, completing on the partner's mbarrier), so that every P_a
+// of the chains is read from local shared memory.  push_issue sends `bytes`
+// of the own grids at `own` to `peer_copy` in the partner, after the CTA
+// barrier that follows the grid's transform (the partner has finished reading
+// its copy of the previous term: a cluster barrier ends every term).
+// push_wait waits for the partner's copies before the chains (bounded: a wait
+// that runs out sets the error word).  push_release keeps the copies' sources
+// until they have been read, before the next term overwrites them.
+__device__ __forceinline__ uint32_t smem_u32a(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// `expect` > 0: this CTA's arrival on its own mbarrier for the term, expecting
+// that many bytes from the partner (the first of the term's copies)
+__device__ __forceinline__ void push_issue(const void *own, void *peer_copy, uint32_t bytes, uint64_t *mbar, int prank,
+                                           uint32_t expect) {
+	if (threadIdx.x == 0) {
+		const uint32_t mb = smem_u32a(mbar);
+		uint32_t dst, mbr;
+		asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(dst) : "r"(smem_u32a(peer_copy)), "r"(prank));
+		asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(mbr) : "r"(mb), "r"(prank));
+		if (expect > 0) asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(expect) : "memory");
+		asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+		             "r"(smem_u32a(own)), "r"(bytes), "r"(mbr) : "memory");
+		asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+	}
+}
+__device__ __forceinline__ void push_wait(uint64_t *mbar, unsigned &phase, int *err) {
+	const uint32_t mb = smem_u32a(mbar);
+	bool ok = false;
+	for (unsigned i = 0; i < (1u << 24) && !ok; i++) {
+		uint32_t done = 0;
+		asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+		             : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+		ok = done != 0;
+	}
+	if (!ok && err != nullptr && (threadIdx.x & 31) == 0) atomicExch(err, 1);
+	phase ^= 1u;
+}
+__device__ __forceinline__ void push_release() {
+	if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void push_init(uint64_t *mbar) {
+	if (threadIdx.x == 0) {
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32a(mbar)) : "memory");
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+}
+__device__ __forceinline__ void fence_async_smem_a() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // K4p: the I3 sums of the collision operator on a cluster of 2 CTAs, CTA r
 // holding components 2r and 2r + 1: per term it computes both spectra
@@ -613,10 +663,14 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 	using Lp = Len<P>;
 	using R = typename CT<C>::R;
 	using TM = I3Tmem<C>;
+	constexpr bool kPush = sizeof(C) == 8;                   // FP32: the partner's P grids copied in (Pr)
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ unsigned tmem_slot;
+	__shared__ __align__(8) uint64_t pmbar;
+	unsigned pphase = 0;
 	C *Pq = reinterpret_cast<C *>(smem_raw);                 // P of components 2r, 2r + 1 (2 grids)
 	C *Ug = Pq + 2 * G::GRID, *tw = Pq + 3 * G::GRID;
+	C *Pr = tw + P;                                          // FP32: the partner's 2 P grids
 	cg::cluster_group cluster = cg::this_cluster();
 	const int rank = (int)cluster.block_rank();
 	const long cid = blockIdx.x / 2;
@@ -652,6 +706,10 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 		tmem_st4(twaddr, a);
 	}
 	C *Ppeer = cluster.map_shared_rank(Pq, rank ^ 1);
+	if constexpr (kPush) {
+		push_init(&pmbar);
+		cluster.sync();                                      // the partner's mbarrier is initialised
+	}
 	// one segment per cell of the range (the (cell, chunk) grid has one)
 #pragma unroll 1
 	while (u < u1) {
@@ -670,8 +728,16 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 		for (int q = 0; q < 2; q++) {
 			const double2 *src = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank + q] * G::N * G::N;
 			fft2_pad<P, -1>(Pq + q * G::GRID, tw, src, MulCplx<C>{p.psi1 + (long)t * G::N * G::N});
+			if constexpr (kPush) {
+				// FP32: each grid goes to the partner as soon as it is complete, the
+				// first copy overlapping the second transform
+				fence_async_smem_a();
+				__syncthreads();
+				push_issue(Pq + q * G::GRID, Pr + q * G::GRID, (uint32_t)(G::GRID * sizeof(C)), &pmbar, rank ^ 1,
+				           q == 0 ? (uint32_t)(2 * G::GRID * sizeof(C)) : 0u);
+			}
 		}
-		cluster.sync();
+		if constexpr (!kPush) cluster.sync();
 		const R *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
 		const R sc = (R)p.psi2_scale[t];
 		{
@@ -684,6 +750,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 			tmem_st8r(TM::psiaddr(tbase), f);
 			tmem_wait_st();
 		}
+		if constexpr (kPush) push_wait(&pmbar, pphase, p.err);
 #pragma unroll 1
 		for (int q = 0; q < 2; q++) {
 			const int j = 2 * rank + q;
@@ -737,7 +804,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
 				fft1d_lane<P, -1>(x, tau, G::row(Ug, line), wp, twaddr);
 				const int a = p.ca[j][c];
-				const C *Pa = ((a >> 1) == rank ? Pq : Ppeer) + (a & 1) * G::GRID;
+				const C *Pa = ((a >> 1) == rank ? Pq : (kPush ? Pr : Ppeer)) + (a & 1) * G::GRID;
 				const R coef = (R)p.ccoef[j][c];
 				C acc[8];
 				if constexpr (sizeof(C) == 16) tmem_ld8(TM::addr(tbase, q, 0), acc);   // one load (FP64); FP32 per value measured faster
@@ -763,6 +830,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3p(const I3ParamsT<C> p, con
 				// column pass waits behind the next pair's first barrier
 			}
 		}
+		if constexpr (kPush) push_release();              // the own P grids are read by the copy before they change
 		cluster.sync();
 	}
 	// partial sums of this segment: slot (cluster, cell) of the ranges, or (cell, chunk)
@@ -811,6 +879,9 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3pr(const I3ParamsT<float2> 
 	__shared__ unsigned tmem_slot;
 	C *Pq = reinterpret_cast<C *>(smem_raw);                 // P_2r + i P_2r+1
 	C *Ug = Pq + 2 * G::GRID, *tw = Pq + 3 * G::GRID;
+	C *Pr = Pq + G::GRID;                                    // the partner's packed P grid, copied in
+	__shared__ __align__(8) uint64_t pmbar;
+	unsigned pphase = 0;
 	cg::cluster_group cluster = cg::this_cluster();
 	const int rank = (int)cluster.block_rank();
 	const long cid = blockIdx.x / 2;
@@ -836,14 +907,17 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3pr(const I3ParamsT<float2> 
 	}
 	const C *Gcell = p.Ghat + cell * p.g_cell;
 	const int t0 = (int)((long)chunk * p.nterms / p.nchunk), t1 = (int)((long)(chunk + 1) * p.nterms / p.nchunk);
-	const C *Ppeer = cluster.map_shared_rank(Pq, rank ^ 1);
+	push_init(&pmbar);
+	cluster.sync();                                          // the partner's mbarrier is initialised
 	for (int t = t0; t < t1; t++) {
 		{
 			const double2 *sa = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank] * G::N * G::N;
 			const double2 *sb = p.src + cell * p.src_cell + (long)p.src_comp[2 * rank + 1] * G::N * G::N;
 			fft2_pad<P, -1>(Pq, tw, sa, MulCplxPair<C>{p.psi1 + (long)t * G::N * G::N, sb});
 		}
-		cluster.sync();
+		fence_async_smem_a();
+		__syncthreads();                                     // no distributed-shared-memory reads: a CTA barrier
+		push_issue(Pq, Pr, (uint32_t)(G::GRID * sizeof(C)), &pmbar, rank ^ 1, (uint32_t)(G::GRID * sizeof(C)));
 		const float *psi2 = p.psi2T + (long)p.psi2_idx[t] * P * P;
 		const float sc = (float)p.psi2_scale[t];
 		{
@@ -853,6 +927,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3pr(const I3ParamsT<float2> 
 			tmem_st8r(TM::psiaddr(tbase), f);
 			tmem_wait_st();
 		}
+		push_wait(&pmbar, pphase, p.err);
 #pragma unroll 1
 		for (int q = 0; q < 2; q++) {
 			const int j = 2 * rank + q;
@@ -909,7 +984,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3pr(const I3ParamsT<float2> 
 				for (int r = 0; r < 8; r++) x[r] = Ug[G::at(line, tau + G::T * r)];
 				fft1d_lane<P, -1>(x, tau, G::row(Ug, line), wp, 0u);
 				const int a0 = p.ca[j][c], a1 = p.ca[j][c + 1];
-				const C *Pa0 = ((a0 >> 1) == rank ? Pq : Ppeer), *Pa1 = ((a1 >> 1) == rank ? Pq : Ppeer);
+				const C *Pa0 = ((a0 >> 1) == rank ? Pq : Pr), *Pa1 = ((a1 >> 1) == rank ? Pq : Pr);
 				const float c0 = (float)p.ccoef[j][c], c1 = (float)p.ccoef[j][c + 1];
 				float acc[8];
 				tmem_ld8r(TM::addr(tbase, q), acc);
@@ -926,6 +1001,7 @@ __global__ void __launch_bounds__(Geo<P>::NT, 1) k_i3pr(const I3ParamsT<float2> 
 				// no barrier here, as in k_i3p
 			}
 		}
+		push_release();                                      // the own P grid is read by the copy before it changes
 		cluster.sync();
 	}
 #pragma unroll 1

@@ -25,7 +25,7 @@ INC = os.path.join(REPO, "include")
 LIB = os.path.join(HERE, "lib")
 OBJ = os.path.join(HERE, "_build")
 
-SOURCES = ["qb_engine.cu", "qb_tables.cu", "qb_abi.cu", "qb_fftw.cu", "qb_ext.cu", "qb_noalloc.cu", "qb_diag.cu", "qb_batch.cu",
+SOURCES = ["qb_engine.cu", "qb_anyn.cu", "qb_tables.cu", "qb_abi.cu", "qb_fftw.cu", "qb_ext.cu", "qb_noalloc.cu", "qb_diag.cu", "qb_batch.cu",
            "qb_fno.cu", "qb_surrogate.cu", "qb_dftmma.cu"]
 # sources that depend on N_GRID (the upstream ABI); the others are grid-size independent
 NGRID_SOURCES = {"qb_abi.cu", "qb_ext.cu"}

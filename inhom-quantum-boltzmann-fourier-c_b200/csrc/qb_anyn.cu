@@ -1,0 +1,964 @@
+// qb_anyn.cu — the collision operator at grid sizes that have no fixed-size
+// kernels: N with 2N = 2^a 3^b up to N = 128, i.e. N = 24, 48, 96 (radix-3
+// transforms) and N = 128 (256 x 256 padded grids), in FP64 or the FP32 form.
+//
+// The sums are those of the fixed-size engine (qb_kernels.cuh), factored the
+// same way:
+//   spectra  W^_c  = FFT2(Pad(W_c))
+//   I1 / I4  S_g   = sum_t phi_t . IFFT2(F . FFT2(Pad(psi2_t . g)))       F = fa W^_f + fb
+//   I2       Q_i   = sum_t FFT2(Pad(psi1_t . W_i)) . FFT2(Pad(psi2_t . W_i))
+//   I3       X_j   = sum_t sum_i eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j)),  P_j = FFT2(Pad(psi1_t . W_j))
+//   assembly Cc_j, Cd_j = Extract(IFFT2(Z_j)) of the pointwise combinations Z_j
+// (upstream src/integrals.c:90-133, :211-251, :332-379 and
+// src/collision.c:74-168, :209-254).
+//
+// Layout and passes.  The padded P x P grids (P = 2N) live in global memory,
+// dense and row-major; at these sizes a grid (18 KB to 1 MB) no longer fits a
+// CTA's shared memory next to the others a term needs.  Every 2-D transform is
+// a row pass and a column pass.  A pass kernel stages a tile of `nl` lines
+// (rows, or columns read as row segments of nl consecutive elements) of one
+// grid in shared memory, transforms them with a mixed-radix Stockham FFT
+// (radices 8, 4, 3, 2 in the order of a plan, ping-ponging between two
+// buffers, the twiddles from a table of the L-th roots of unity), and fuses
+// the pointwise products of the sums into the load and the store of the tile.
+// The quadrature terms run in waves of nt terms for all cells of the batch:
+// one wave is a handful of launches over (cell, term, grid) units, and the
+// sums accumulate in global memory.  Every element of a sum has one owner per
+// launch (the CTA holding its line), which adds the wave's terms in order, and
+// the waves follow one another on the stream, so the result is deterministic.
+#include "qb_engine.h"
+#include "qb_fft.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <set>
+#include <tuple>
+
+namespace qb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxStages = 8;
+constexpr size_t kMaxSmem = 200 * 1024;
+
+// radix schedule of one transform length: radices 2, 3, 4, 8 whose product is L
+struct Plan {
+	int L = 0, nst = 0;
+	int r[kMaxStages] = {};
+};
+
+__device__ __forceinline__ int src_idx(int p, int N) {         // padded index -> N-grid index, or -1 (zero band)
+	return p < N / 2 ? p : (p >= 3 * N / 2 ? p - N : -1);
+}
+
+template <int DIR, class C> __device__ __forceinline__ void dft3(C &x0, C &x1, C &x2) {
+	using R = typename CT<C>::R;
+	const C t1 = cadd(x1, x2);
+	const C m = csub(x0, cscale(t1, (R)0.5));
+	const C d = mul_i<DIR>(cscale(csub(x1, x2), (R)0.86602540378443864676));   // sin(2 pi / 3)
+	x0 = cadd(x0, t1);
+	x1 = cadd(m, d);
+	x2 = csub(m, d);
+}
+
+template <int RAD, int DIR, class C> __device__ __forceinline__ void dft_r(C (&v)[RAD]) {
+	if constexpr (RAD == 8) dft8<DIR>(v);
+	else if constexpr (RAD == 4) dft4<DIR>(v[0], v[1], v[2], v[3]);
+	else if constexpr (RAD == 3) dft3<DIR>(v[0], v[1], v[2]);
+	else dft2(v[0], v[1]);
+}
+
+// one Stockham stage of radix RAD over nl lines of length L (sub-transforms of
+// length Ns done): butterfly j of a line reads x[j + r L/RAD], twiddles by
+// w^(r (j mod Ns)) with w = exp(DIR 2 pi i / (Ns RAD)), and writes its outputs
+// to (j / Ns) Ns RAD + (j mod Ns) + r Ns.  tw[m] = exp(-2 pi i m / L).
+template <int RAD, int DIR, class C>
+__device__ __forceinline__ void stage(const C *in, C *out, int nl, int pitch, int L, int Ns, const C *tw) {
+	const int m = L / RAD, tstep = L / (Ns * RAD);
+	for (int b = threadIdx.x; b < nl * m; b += blockDim.x) {
+		const int line = b / m, j = b - line * m;
+		const int k = j % Ns;
+		const C *src = in + line * pitch + j;
+		C v[RAD];
+#pragma unroll
+		for (int r = 0; r < RAD; r++) v[r] = src[r * m];
+		if (Ns > 1) {
+#pragma unroll
+			for (int r = 1; r < RAD; r++) {
+				C w = tw[r * k * tstep];                        // r k tstep < L
+				if (DIR > 0) w.y = -w.y;
+				v[r] = cmul(v[r], w);
+			}
+		}
+		dft_r<RAD, DIR>(v);
+		C *dst = out + line * pitch + (j / Ns) * Ns * RAD + k;
+#pragma unroll
+		for (int r = 0; r < RAD; r++) dst[r * Ns] = v[r];
+	}
+}
+
+// transforms the nl lines at `a` (line stride `pitch`) in the direction DIR,
+// with `b` as the second buffer; returns the buffer that holds the result.
+// Starts and ends with the CTA synchronised.
+template <int DIR, class C> __device__ C *fft_lines(C *a, C *b, int nl, int pitch, const Plan &pl, const C *tw) {
+	int Ns = 1;
+	for (int s = 0; s < pl.nst; s++) {
+		const int R = pl.r[s];
+		if (R == 8) stage<8, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
+		else if (R == 4) stage<4, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
+		else if (R == 3) stage<3, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
+		else stage<2, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
+		__syncthreads();
+		C *t = a; a = b; b = t;
+		Ns *= R;
+	}
+	return a;
+}
+
+// the twiddle table tw[m] = exp(-2 pi i m / L), then a CTA barrier
+template <class C> __device__ void init_tw(C *tw, int L) {
+	for (int m = threadIdx.x; m < L; m += blockDim.x) {
+		double s, c;
+		sincospi(2.0 * m / L, &s, &c);
+		tw[m] = mk<C>(c, -s);
+	}
+	__syncthreads();
+}
+
+// shared-memory layout of a pass: the twiddles, then two buffers of nl lines
+template <class C> struct Tile {
+	C *tw, *a, *b;
+	int pitch;
+	__device__ Tile(unsigned char *sm, int L, int nl) {
+		pitch = L + 1;
+		tw = reinterpret_cast<C *>(sm);
+		a = tw + L;
+		b = a + (long)nl * pitch;
+	}
+};
+template <class C> size_t tile_bytes(int L, int nl) { return sizeof(C) * ((size_t)L + 2 * (size_t)nl * (L + 1)); }
+
+// ---------------------------------------------------------------------------
+// passes
+
+// rows of Pad(mult . W_comp) for unit u = (cell nt + tt) nsub + sub, forward
+// transform: out[u] (row pass of the spectra, of P_j and of the first
+// transforms of the I1 / I2 terms).  psel: 0 no factor, 1 / 2 real table A / B
+// of term t0 + tt, 3 the complex table.
+template <class C> struct PadRowsP {
+	using R = typename CT<C>::R;
+	const double2 *W; long w_cell;
+	int N, nl, nt, t0, nsub;
+	int comp[8], psel[8];
+	const R *psiA, *psiB;                 // real N x N tables, one per term
+	const C *psiC;                        // complex N x N tables, one per term
+	C *out;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(const PadRowsP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int N = p.N, P = 2 * N, nl = p.nl;
+	const long NN = (long)N * N, PP = (long)P * P;
+	Tile<C> T(sm, P, nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long u = blockIdx.x / bpg;
+	const int l0 = (int)(blockIdx.x % bpg) * nl;
+	const int sub = (int)(u % p.nsub);
+	const long ct = u / p.nsub;
+	const int t = p.t0 + (int)(ct % p.nt);
+	const long cell = ct / p.nt;
+	const double2 *w = p.W + cell * p.w_cell + (long)p.comp[sub] * NN;
+	const int ps = p.psel[sub];
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int li = i / P, k = i - li * P;
+		const int ls = src_idx(l0 + li, N), ks = src_idx(k, N);
+		C v = czero<C>();
+		if (ls >= 0 && ks >= 0) {
+			const long q = (long)ls * N + ks;
+			const double2 x = w[q];
+			if (ps == 0) v = mk<C>(x.x, x.y);
+			else if (ps == 3) v = cmul(p.psiC[t * NN + q], mk<C>(x.x, x.y));
+			else {
+				const R f = (ps == 1 ? p.psiA : p.psiB)[t * NN + q];
+				v = mk<C>(0.0, 0.0);
+				v.x = f * (R)x.x;
+				v.y = f * (R)x.y;
+			}
+		}
+		T.a[li * T.pitch + k] = v;
+	}
+	__syncthreads();
+	const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	C *o = p.out + u * PP + (long)l0 * P;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int li = i / P, k = i - li * P;
+		o[(long)li * P + k] = r[li * T.pitch + k];
+	}
+}
+
+// in-place row or column transforms of L x L grids g[u] (spectra, FS, the
+// Fourier representation)
+template <class C> struct PlainP {
+	C *g; int L, nl;
+	Plan pl;
+};
+template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThreads) k_any_plain(const PlainP<C> p) {
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int L = p.L, nl = p.nl;
+	Tile<C> T(sm, L, nl);
+	init_tw(T.tw, L);
+	const int bpg = L / nl;
+	const long u = blockIdx.x / bpg;
+	const int x0 = (int)(blockIdx.x % bpg) * nl;
+	C *g = p.g + u * (long)L * L;
+	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+		if (COLS) { const int kk = i % nl, l = i / nl; T.a[kk * T.pitch + l] = g[(long)l * L + x0 + kk]; }
+		else { const int li = i / L, k = i - li * L; T.a[li * T.pitch + k] = g[(long)(x0 + li) * L + k]; }
+	}
+	__syncthreads();
+	const C *r = fft_lines<DIR>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+		if (COLS) { const int kk = i % nl, l = i / nl; g[(long)l * L + x0 + kk] = r[kk * T.pitch + l]; }
+		else { const int li = i / L, k = i - li * L; g[(long)(x0 + li) * L + k] = r[li * T.pitch + k]; }
+	}
+}
+
+// I1 / I4 columns of unit u = (cell nt + tt) nsub + sub: forward transform,
+// times F = fa W^_f + fb, inverse transform, in place
+template <class C> struct I1ColsP {
+	C *g; const C *What; int N, nl, nt, nsub, fcomp;
+	double fa, fb;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(const I1ColsP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long u = blockIdx.x / bpg;
+	const int k0 = (int)(blockIdx.x % bpg) * nl;
+	const long cell = u / ((long)p.nsub * p.nt);
+	C *g = p.g + u * PP;
+	const C *F = p.What + (cell * 4 + p.fcomp) * PP;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		T.a[kk * T.pitch + l] = g[(long)l * P + k0 + kk];
+	}
+	__syncthreads();
+	C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	const R fa = (R)p.fa, fb = (R)p.fb;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		const C w = F[(long)l * P + k0 + kk];
+		C f; f.x = fa * w.x + fb; f.y = fa * w.y;
+		r[kk * T.pitch + l] = cmul(f, r[kk * T.pitch + l]);
+	}
+	__syncthreads();
+	const C *r2 = fft_lines<+1>(r, r == T.a ? T.b : T.a, nl, T.pitch, p.pl, T.tw);
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		g[(long)l * P + k0 + kk] = r2[kk * T.pitch + l];
+	}
+}
+
+// I1 / I4 rows, inverse transform, S[cell][sub] += phi_t . row, for the wave's
+// terms in order (one CTA per (cell, sub, row block))
+template <class C> struct I1RowsP {
+	using R = typename CT<C>::R;
+	const C *g; C *S; const R *phi; int N, nl, nt, t0, nsub;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(const I1RowsP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long cs = blockIdx.x / bpg;             // cell nsub + sub
+	const int l0 = (int)(blockIdx.x % bpg) * nl;
+	const long cell = cs / p.nsub;
+	const int sub = (int)(cs % p.nsub);
+	C *S = p.S + cs * PP + (long)l0 * P;
+	for (int tt = 0; tt < p.nt; tt++) {
+		const C *g = p.g + ((cell * p.nt + tt) * p.nsub + sub) * PP + (long)l0 * P;
+		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+			const int li = i / P, k = i - li * P;
+			T.a[li * T.pitch + k] = g[(long)li * P + k];
+		}
+		__syncthreads();
+		const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+		const R *phi = p.phi + (long)(p.t0 + tt) * PP + (long)l0 * P;
+		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+			const int li = i / P, k = i - li * P;
+			const R f = phi[(long)li * P + k];
+			const C x = r[li * T.pitch + k];
+			C s = S[(long)li * P + k];
+			s.x += f * x.x;
+			s.y += f * x.y;
+			S[(long)li * P + k] = s;
+		}
+		__syncthreads();
+	}
+}
+
+// I2 columns: forward transforms of A = g[(cell nt + tt) 8 + 2i] and
+// B = g[... + 2i + 1], Q[cell][i] += A . B over the wave's terms in order
+template <class C> struct I2ColsP {
+	const C *g; C *Q; int N, nl, nt;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(const I2ColsP<C> p) {
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, 2 * nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long ci = blockIdx.x / bpg;             // cell 4 + i
+	const int k0 = (int)(blockIdx.x % bpg) * nl;
+	const long cell = ci / 4;
+	const int ii = (int)(ci % 4);
+	C *Q = p.Q + ci * PP;
+	for (int tt = 0; tt < p.nt; tt++) {
+		const C *ga = p.g + ((cell * p.nt + tt) * 8 + 2 * ii) * PP;
+		for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
+			const int h = i / (nl * P), rem = i - h * nl * P, kk = rem % nl, l = rem / nl;
+			T.a[(h * nl + kk) * T.pitch + l] = ga[h * PP + (long)l * P + k0 + kk];
+		}
+		__syncthreads();
+		const C *r = fft_lines<-1>(T.a, T.b, 2 * nl, T.pitch, p.pl, T.tw);
+		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+			const int kk = i % nl, l = i / nl;
+			const long o = (long)l * P + k0 + kk;
+			Q[o] = cfma(r[kk * T.pitch + l], r[(nl + kk) * T.pitch + l], Q[o]);
+		}
+		__syncthreads();
+	}
+}
+
+// I3 chain, first rows: unit u = ((cell nt + tt) 4 + j) 4 + i, inverse
+// transform of the rows of W^_i . P_j into Y[u]
+template <class C> struct I3RowsAP {
+	const C *What, *Pg; C *Y; int N, nl, nt;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long u = blockIdx.x / bpg;
+	const int l0 = (int)(blockIdx.x % bpg) * nl;
+	const int i3 = (int)(u % 4), j3 = (int)((u / 4) % 4);
+	const long ct = u / 16, cell = ct / p.nt;
+	const C *G = p.What + (cell * 4 + i3) * PP + (long)l0 * P;
+	const C *Pj = p.Pg + (ct * 4 + j3) * PP + (long)l0 * P;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int li = i / P, k = i - li * P;
+		T.a[li * T.pitch + k] = cmul(G[(long)li * P + k], Pj[(long)li * P + k]);
+	}
+	__syncthreads();
+	const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	C *o = p.Y + u * PP + (long)l0 * P;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int li = i / P, k = i - li * P;
+		o[(long)li * P + k] = r[li * T.pitch + k];
+	}
+}
+
+// I3 chain, columns of Y[u]: inverse transform, times psi2_t (element (l, k)
+// = scale[t] ST[idx[t]][k P + l]), forward transform, in place
+template <class C> struct I3ColsP {
+	using R = typename CT<C>::R;
+	C *Y; const R *psi2T; const int *idx; const double *scale; int N, nl, nt, t0;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_cols(const I3ColsP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long u = blockIdx.x / bpg;
+	const int k0 = (int)(blockIdx.x % bpg) * nl;
+	const int t = p.t0 + (int)((u / 16) % p.nt);
+	C *g = p.Y + u * PP;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		T.a[kk * T.pitch + l] = g[(long)l * P + k0 + kk];
+	}
+	__syncthreads();
+	C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	const R sc = (R)p.scale[t];
+	const R *ps = p.psi2T + (long)p.idx[t] * PP;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		const R f = sc * ps[(long)(k0 + kk) * P + l];
+		C x = r[kk * T.pitch + l];
+		x.x *= f;
+		x.y *= f;
+		r[kk * T.pitch + l] = x;
+	}
+	__syncthreads();
+	const C *r2 = fft_lines<-1>(r, r == T.a ? T.b : T.a, nl, T.pitch, p.pl, T.tw);
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		g[(long)l * P + k0 + kk] = r2[kk * T.pitch + l];
+	}
+}
+
+// I3 chain, last rows: forward transforms of Y[((cell nt + tt) 4 + j) 4 + i],
+// i = 0..3, and X[cell][j] += sum_i eta_i P_i . row, over the wave's terms in
+// order (one CTA per (cell, j, row block))
+template <class C> struct I3RowsBP {
+	const C *Y, *Pg; C *X; int N, nl, nt;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, 4 * nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long cj = blockIdx.x / bpg;             // cell 4 + j
+	const int l0 = (int)(blockIdx.x % bpg) * nl;
+	const long cell = cj / 4;
+	const int j3 = (int)(cj % 4);
+	const R eta[4] = { (R)1, (R)-1, (R)-1, (R)-1 };
+	C *X = p.X + cj * PP + (long)l0 * P;
+	for (int tt = 0; tt < p.nt; tt++) {
+		const long ct = cell * p.nt + tt;
+		const C *y = p.Y + ((ct * 4 + j3) * 4) * PP + (long)l0 * P;
+		for (int i = threadIdx.x; i < 4 * nl * P; i += blockDim.x) {
+			const int h = i / (nl * P), rem = i - h * nl * P, li = rem / P, k = rem - li * P;
+			T.a[(h * nl + li) * T.pitch + k] = y[h * PP + (long)li * P + k];
+		}
+		__syncthreads();
+		const C *r = fft_lines<-1>(T.a, T.b, 4 * nl, T.pitch, p.pl, T.tw);
+		const C *Pa = p.Pg + ct * 4 * PP + (long)l0 * P;
+		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+			const int li = i / P, k = i - li * P;
+			const long o = (long)li * P + k;
+			C acc = X[o];
+#pragma unroll
+			for (int h = 0; h < 4; h++) {
+				const C v = cmul(Pa[h * PP + o], r[(h * nl + li) * T.pitch + k]);
+				acc.x += eta[h] * v.x;
+				acc.y += eta[h] * v.y;
+			}
+			X[o] = acc;
+		}
+		__syncthreads();
+	}
+}
+
+// assembly rows: Zcc_j and Zcd_j (the combinations of k_assemble) for unit
+// (cell, j), inverse row transforms into Z[(cell 4 + j) 2 + {0, 1}]
+template <class C> struct AsmP {
+	const C *What, *FS, *FS4, *Q, *X;    // FS [cell][3], FS4 / Q / X [cell][4] (null: part absent)
+	C *Z; int N, nl;
+	double s1, s2;
+	int mode;
+	double2 *out_cc, *out_cd;
+	const double2 *base, *wcur; const double *B; double dtc; double2 *out;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(const AsmP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, nl = p.nl;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, 2 * nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long cj = blockIdx.x / bpg;
+	const int l0 = (int)(blockIdx.x % bpg) * nl;
+	const long cell = cj / 4;
+	const int j = (int)(cj % 4);
+	const R eta2[4] = { 2, -2, -2, -2 };
+	const R s1 = (R)p.s1, s2 = (R)p.s2;
+	const C *Wh = p.What + cell * 4 * PP;
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int li = i / P, k = i - li * P;
+		const long e = (long)(l0 + li) * P + k;
+		C zc = czero<C>(), zd = czero<C>();
+		if (p.FS != nullptr && j > 0) {
+			const int gi = (j % 3) + 1, hi = ((j + 1) % 3) + 1;
+			const C *FS = p.FS + cell * 3 * PP;
+			zc = csub(cmul(Wh[hi * PP + e], FS[(gi - 1) * PP + e]), cmul(Wh[gi * PP + e], FS[(hi - 1) * PP + e]));
+		}
+		if (p.Q != nullptr) {
+			C q = czero<C>();
+			for (int ii = 0; ii < 4; ii++) {
+				const C s = p.Q[(cell * 4 + ii) * PP + e];
+				q.x += eta2[ii] * s.x;
+				q.y += eta2[ii] * s.y;
+			}
+			C h; h.x = -Wh[j * PP + e].x; h.y = -Wh[j * PP + e].y;
+			if (j == 0) h.x += (R)1.0;
+			const C v = cmul(h, q);
+			zd.x += s2 * v.x;
+			zd.y += s2 * v.y;
+		}
+		if (p.X != nullptr) {
+			const C s = p.X[(cell * 4 + j) * PP + e];
+			zd.x -= eta2[j] * s1 * s.x;
+			zd.y -= eta2[j] * s1 * s.y;
+		}
+		if (p.FS4 != nullptr) {
+			const C *F4 = p.FS4 + cell * 4 * PP;
+			C v = cadd(cscale(cmul(Wh[e], F4[j * PP + e]), eta2[j]), cscale(cmul(Wh[j * PP + e], F4[e]), (R)2.0));
+			if (j == 0) {
+				C s = czero<C>();
+				for (int c = 0; c < 4; c++) s = cadd(s, cmul(Wh[c * PP + e], F4[c * PP + e]));
+				v = csub(v, cscale(s, (R)2.0));
+			}
+			zd.x += s1 * v.x;
+			zd.y += s1 * v.y;
+		}
+		T.a[li * T.pitch + k] = zc;
+		T.a[(nl + li) * T.pitch + k] = zd;
+	}
+	__syncthreads();
+	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, p.pl, T.tw);
+	C *z = p.Z + cj * 2 * PP + (long)l0 * P;
+	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
+		const int h = i / (nl * P), rem = i - h * nl * P, li = rem / P, k = rem - li * P;
+		z[h * PP + (long)li * P + k] = r[(h * nl + li) * T.pitch + k];
+	}
+}
+
+// assembly columns: inverse column transforms of Zcc_j, Zcd_j, Extract, and
+// the outputs (mode 0: Cc = s1 Zcc, Cd = Zcd; mode 1: base + dtc (Cc + Cd + CB))
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(const AsmP<C> p) {
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int N = p.N, P = 2 * N, nl = p.nl;
+	const long PP = (long)P * P, NN = (long)N * N;
+	Tile<C> T(sm, P, 2 * nl);
+	init_tw(T.tw, P);
+	const int bpg = P / nl;
+	const long cj = blockIdx.x / bpg;
+	const int k0 = (int)(blockIdx.x % bpg) * nl;
+	const long cell = cj / 4;
+	const int j = (int)(cj % 4);
+	const C *z = p.Z + cj * 2 * PP;
+	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
+		const int h = i / (nl * P), rem = i - h * nl * P, kk = rem % nl, l = rem / nl;
+		T.a[(h * nl + kk) * T.pitch + l] = z[h * PP + (long)l * P + k0 + kk];
+	}
+	__syncthreads();
+	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, p.pl, T.tw);
+	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
+		const int kk = i % nl, l = i / nl;
+		const int ls = src_idx(l, N), ks = src_idx(k0 + kk, N);
+		if (ls < 0 || ks < 0) continue;
+		const C zc = r[kk * T.pitch + l], zd = r[(nl + kk) * T.pitch + l];
+		const double2 cc = make_double2(p.s1 * (double)zc.x, p.s1 * (double)zc.y);
+		const double2 cd = make_double2((double)zd.x, (double)zd.y);
+		const long q = (long)ls * N + ks, o = cj * NN + q;
+		if (p.mode == 0) {
+			if (p.out_cc) p.out_cc[o] = cc;
+			if (p.out_cd) p.out_cd[o] = cd;
+		} else {
+			const double2 *w = p.wcur + cell * 4 * NN + q;
+			double2 cb = make_double2(0.0, 0.0);         // -i [B, W] = 2 (B x w) . sigma
+			if (p.B != nullptr) {
+				const double *B = p.B + cell * 3;
+				if (j == 1) cb = make_double2(2 * (B[1] * w[3 * NN].x - B[2] * w[2 * NN].x), 2 * (B[1] * w[3 * NN].y - B[2] * w[2 * NN].y));
+				if (j == 2) cb = make_double2(2 * (B[2] * w[1 * NN].x - B[0] * w[3 * NN].x), 2 * (B[2] * w[1 * NN].y - B[0] * w[3 * NN].y));
+				if (j == 3) cb = make_double2(2 * (B[0] * w[2 * NN].x - B[1] * w[1 * NN].x), 2 * (B[0] * w[2 * NN].y - B[1] * w[1 * NN].y));
+			}
+			const double2 b = p.base ? p.base[o] : make_double2(0.0, 0.0);
+			p.out[o] = make_double2(b.x + p.dtc * ((cc.x + cd.x) + cb.x), b.y + p.dtc * ((cc.y + cd.y) + cb.y));
+		}
+	}
+}
+
+// the Fourier representation (upstream simulation.c:224-283): real N x N
+// components -> complex grids, and the Hermitian completion of the forward
+// transform scaled by 1 / N^2
+__global__ void k_any_real_to_cplx(long n, const double *__restrict__ v, double2 *__restrict__ c) {
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) c[i] = make_double2(v[i], 0.0);
+}
+__global__ void k_any_hermitian(int N, long ngrids, const double2 *__restrict__ a, double2 *__restrict__ f) {
+	const long NN = (long)N * N, n = ngrids * NN;
+	const double sc = 1.0 / ((double)N * N);
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+		const long g = i / NN;
+		const int l = (int)((i % NN) / N), k = (int)(i % N);
+		double2 z;
+		if (k <= N / 2) {
+			z = a[i];
+		} else {
+			const int lc = (N - l) % N, kc = N - k;
+			z = a[g * NN + (long)lc * N + kc];
+			z.y = -z.y;
+		}
+		f[i] = make_double2(z.x * sc, z.y * sc);
+	}
+}
+__global__ void k_any_real_part(long n, const double2 *__restrict__ c, double *__restrict__ v) {
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[i] = c[i].x;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+bool smooth23(int L) {
+	if (L < 2) return false;
+	while (L % 2 == 0) L /= 2;
+	while (L % 3 == 0) L /= 3;
+	return L == 1;
+}
+
+// radix plans of a length: variant 0 takes radix 8 first, then 4, 3, 2;
+// variant 1 the radix-3 stages first; variant 2 radix 4 instead of 8
+Plan make_plan(int L, int variant) {
+	Plan p;
+	p.L = L;
+	int a = 0, b = 0, m = L;
+	while (m % 2 == 0) { m /= 2; a++; }
+	while (m % 3 == 0) { m /= 3; b++; }
+	if (m != 1) QB_FAIL("transform length " + std::to_string(L) + " is not of the form 2^a 3^b");
+	int rad[kMaxStages], n = 0;
+	auto push = [&](int r) {
+		if (n >= kMaxStages) QB_FAIL("transform length " + std::to_string(L) + " needs too many stages");
+		rad[n++] = r;
+	};
+	if (variant == 1) for (int i = 0; i < b; i++) push(3);
+	int e = a;
+	if (variant != 2) while (e >= 3) { push(8); e -= 3; }
+	while (e >= 2) { push(4); e -= 2; }
+	if (e == 1) push(2);
+	if (variant != 1) for (int i = 0; i < b; i++) push(3);
+	p.nst = n;
+	for (int i = 0; i < n; i++) p.r[i] = rad[i];
+	return p;
+}
+
+// lines per tile: the largest of the candidates that divides L and fits
+int pick_lines(int L, int want, int tiles, size_t elem) {
+	for (int nl = want; nl >= 1; nl--) {
+		if (L % nl) continue;
+		if (elem * ((size_t)L + 2 * (size_t)tiles * nl * (L + 1)) <= kMaxSmem) return nl;
+	}
+	return 1;
+}
+
+template <class K> void smem_attr(K kern, size_t bytes) {
+	static std::mutex mu;
+	static std::set<std::tuple<int, const void *>> done;
+	int dev = 0;
+	QB_CUDA(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lk(mu);
+	if (done.insert(std::make_tuple(dev, (const void *)kern)).second)
+		QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+	(void)bytes;
+}
+
+template <class K, class Prm> void launch(K kern, const char *name, long blocks, size_t smem, cudaStream_t s, const Prm &p) {
+	if (blocks <= 0) return;
+	smem_attr(kern, smem);
+	ProfScope ps(name, s);
+	kern<<<(unsigned)blocks, kThreads, smem, s>>>(p);
+	QB_CUDA(cudaGetLastError());
+}
+
+template <class C> struct Tabs;
+template <> struct Tabs<double2> {
+	static const double *i1_psi2(const DevI1 &t) { return t.psi2.as<double>(); }
+	static const double *i1_phi(const DevI1 &t) { return t.phi.as<double>(); }
+	static const double *i2_psi1(const DevI2 &t) { return t.psi1.as<double>(); }
+	static const double *i2_psi2(const DevI2 &t) { return t.psi2.as<double>(); }
+	static const double2 *i3_psi1(const DevI3 &t) { return t.psi1.as<double2>(); }
+	static const double *i3_psi2T(const DevI3 &t) { return t.psi2T.as<double>(); }
+};
+template <> struct Tabs<float2> {
+	static const float *i1_psi2(const DevI1 &t) { return t.psi2f.as<float>(); }
+	static const float *i1_phi(const DevI1 &t) { return t.phif.as<float>(); }
+	static const float *i2_psi1(const DevI2 &t) { return t.psi1f.as<float>(); }
+	static const float *i2_psi2(const DevI2 &t) { return t.psi2f.as<float>(); }
+	static const float2 *i3_psi1(const DevI3 &t) { return t.psi1f.as<float2>(); }
+	static const float *i3_psi2T(const DevI3 &t) { return t.psi2Tf.as<float>(); }
+};
+
+template <class C> struct AnyRhs {
+	using R = typename CT<C>::R;
+	Workspace &ws;
+	const QuadSet &q;
+	int N, P, ncells;
+	long PP;
+	Plan pl;
+	int nl1;              // lines per tile of the single-tile passes
+	cudaStream_t s;
+
+	AnyRhs(Workspace &w, const QuadSet &qs, int nc, cudaStream_t st) : ws(w), q(qs), N(w.N), P(2 * w.N), ncells(nc), s(st) {
+		PP = (long)P * P;
+		pl = make_plan(P, ws.anyn_plan);
+		nl1 = pick_lines(P, ws.anyn_lines > 0 ? ws.anyn_lines : std::max(1, 2048 / P), 1, sizeof(C));
+	}
+	size_t smem(int nl, int tiles) const { return tile_bytes<C>(P, nl * tiles); }
+	long blocks(long units, int nl) const { return units * (P / nl); }
+
+	// terms per wave: the wave's scratch of `per_term` grids per cell within the budget
+	int wave(int nterms, int per_term) const {
+		const double mb = ws.anyn_wave_mb > 0 ? ws.anyn_wave_mb : 96.0;
+		const double per = (double)per_term * ncells * PP * sizeof(C);
+		const int nt = (int)std::max(1.0, std::floor(mb * 1048576.0 / per));
+		return std::min(nt, std::max(1, nterms));
+	}
+
+	void plain(C *g, long ngrids, int dir, bool cols) {
+		PlainP<C> p{};
+		p.g = g; p.L = P; p.nl = nl1; p.pl = pl;
+		const long nb = blocks(ngrids, nl1);
+		const size_t sm = smem(nl1, 1);
+		if (dir < 0) {
+			if (cols) launch(k_any_plain<C, -1, true>, "any_cols", nb, sm, s, p);
+			else launch(k_any_plain<C, -1, false>, "any_rows", nb, sm, s, p);
+		} else {
+			if (cols) launch(k_any_plain<C, +1, true>, "any_cols", nb, sm, s, p);
+			else launch(k_any_plain<C, +1, false>, "any_rows", nb, sm, s, p);
+		}
+	}
+
+	PadRowsP<C> pad_params(const double2 *W, int nt, int t0, int nsub, C *out) const {
+		PadRowsP<C> p{};
+		p.W = W; p.w_cell = 4L * N * N; p.N = N; p.nl = nl1; p.nt = nt; p.t0 = t0; p.nsub = nsub; p.out = out; p.pl = pl;
+		return p;
+	}
+	void pad_rows(const PadRowsP<C> &p) {
+		launch(k_any_pad_rows<C>, "any_pad_rows", blocks((long)ncells * p.nt * p.nsub, nl1), smem(nl1, 1), s, p);
+	}
+
+	void spectra(const double2 *W) {
+		ws.What.ensure(sizeof(C) * 4 * ncells * PP);
+		PadRowsP<C> p = pad_params(W, 1, 0, 4, ws.What.as<C>());
+		for (int c = 0; c < 4; c++) { p.comp[c] = c; p.psel[c] = 0; }
+		pad_rows(p);
+		plain(ws.What.as<C>(), 4L * ncells, -1, true);
+	}
+
+	// I1-type sums into S [cell][ntask] and their forward transforms into FS
+	void i1_sums(const DevI1 &t, const double2 *W, bool cc, DevBuf &Sbuf, DevBuf &FSbuf) {
+		const int ntask = cc ? 3 : 4;
+		Sbuf.ensure(sizeof(C) * ncells * ntask * PP);
+		QB_CUDA(cudaMemsetAsync(Sbuf.p, 0, sizeof(C) * ncells * ntask * PP, s));
+		const int nt = wave(t.nterms, ntask);
+		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * ntask * PP);
+		C *G = ws.wave1.as<C>();
+		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+			const int n = std::min(nt, t.nterms - t0);
+			PadRowsP<C> p = pad_params(W, n, t0, ntask, G);
+			for (int k = 0; k < ntask; k++) { p.comp[k] = cc ? std::min(k + 1, 3) : k; p.psel[k] = 1; }
+			p.psiA = Tabs<C>::i1_psi2(t);
+			pad_rows(p);
+			I1ColsP<C> c{};
+			c.g = G; c.What = ws.What.as<C>(); c.N = N; c.nl = nl1; c.nt = n; c.nsub = ntask; c.fcomp = 0;
+			c.fa = cc ? -4.0 : 2.0; c.fb = cc ? 2.0 : -1.0; c.pl = pl;
+			launch(k_any_i1_cols<C>, "any_i1_cols", blocks((long)ncells * n * ntask, nl1), smem(nl1, 1), s, c);
+			I1RowsP<C> r{};
+			r.g = G; r.S = Sbuf.as<C>(); r.phi = Tabs<C>::i1_phi(t); r.N = N; r.nl = nl1; r.nt = n; r.t0 = t0; r.nsub = ntask; r.pl = pl;
+			launch(k_any_i1_rows<C>, "any_i1_rows", blocks((long)ncells * ntask, nl1), smem(nl1, 1), s, r);
+		}
+		FSbuf.ensure(sizeof(C) * ncells * ntask * PP);
+		QB_CUDA(cudaMemcpyAsync(FSbuf.p, Sbuf.p, sizeof(C) * ncells * ntask * PP, cudaMemcpyDeviceToDevice, s));
+		plain(FSbuf.as<C>(), (long)ncells * ntask, -1, false);
+		plain(FSbuf.as<C>(), (long)ncells * ntask, -1, true);
+	}
+
+	void i2_sums(const DevI2 &t, const double2 *W) {
+		ws.i2p.ensure(sizeof(C) * ncells * 4 * PP);
+		QB_CUDA(cudaMemsetAsync(ws.i2p.p, 0, sizeof(C) * ncells * 4 * PP, s));
+		const int nt = wave(t.nterms, 8);
+		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 8 * PP);
+		C *G = ws.wave1.as<C>();
+		const int nl2 = pick_lines(P, nl1, 2, sizeof(C));
+		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+			const int n = std::min(nt, t.nterms - t0);
+			PadRowsP<C> p = pad_params(W, n, t0, 8, G);
+			for (int i = 0; i < 4; i++) { p.comp[2 * i] = i; p.psel[2 * i] = 1; p.comp[2 * i + 1] = i; p.psel[2 * i + 1] = 2; }
+			p.psiA = Tabs<C>::i2_psi1(t); p.psiB = Tabs<C>::i2_psi2(t);
+			pad_rows(p);
+			I2ColsP<C> c{};
+			c.g = G; c.Q = ws.i2p.as<C>(); c.N = N; c.nl = nl2; c.nt = n; c.pl = pl;
+			launch(k_any_i2_cols<C>, "any_i2_cols", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, c);
+		}
+	}
+
+	void i3_sums(const DevI3 &t, const double2 *W) {
+		ws.i3p.ensure(sizeof(C) * ncells * 4 * PP);
+		QB_CUDA(cudaMemsetAsync(ws.i3p.p, 0, sizeof(C) * ncells * 4 * PP, s));
+		const int nt = wave(t.nterms, 20);
+		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
+		ws.wave2.ensure(sizeof(C) * (size_t)ncells * nt * 16 * PP);      // chains
+		C *Pg = ws.wave1.as<C>(), *Y = ws.wave2.as<C>();
+		const int nl4 = pick_lines(P, nl1, 4, sizeof(C));
+		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+			const int n = std::min(nt, t.nterms - t0);
+			PadRowsP<C> p = pad_params(W, n, t0, 4, Pg);
+			for (int j = 0; j < 4; j++) { p.comp[j] = j; p.psel[j] = 3; }
+			p.psiC = Tabs<C>::i3_psi1(t);
+			pad_rows(p);
+			plain(Pg, (long)ncells * n * 4, -1, true);
+			I3RowsAP<C> a{};
+			a.What = ws.What.as<C>(); a.Pg = Pg; a.Y = Y; a.N = N; a.nl = nl1; a.nt = n; a.pl = pl;
+			launch(k_any_i3_rows_a<C>, "any_i3_rows_a", blocks((long)ncells * n * 16, nl1), smem(nl1, 1), s, a);
+			I3ColsP<C> c{};
+			c.Y = Y; c.psi2T = Tabs<C>::i3_psi2T(t); c.idx = t.idx.as<int>(); c.scale = t.scale.as<double>();
+			c.N = N; c.nl = nl1; c.nt = n; c.t0 = t0; c.pl = pl;
+			launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)ncells * n * 16, nl1), smem(nl1, 1), s, c);
+			I3RowsBP<C> b{};
+			b.Y = Y; b.Pg = Pg; b.X = ws.i3p.as<C>(); b.N = N; b.nl = nl4; b.nt = n; b.pl = pl;
+			launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)ncells * 4, nl4), smem(nl4, 4), s, b);
+		}
+	}
+
+	AsmP<C> prepare(const double2 *W, int parts) {
+		if (sizeof(C) == 8) prepare_f32_tables(q, s);
+		spectra(W);
+		AsmP<C> a{};
+		a.What = ws.What.as<C>();
+		if ((parts & RHS_CC) && q.i1) { i1_sums(*q.i1, W, true, ws.i1cc, ws.fs); a.FS = ws.fs.as<C>(); }
+		if (parts & RHS_CD) {
+			if (q.i4) { i1_sums(*q.i4, W, false, ws.i1i4, ws.fs4); a.FS4 = ws.fs4.as<C>(); }
+			if (q.i2) { i2_sums(*q.i2, W); a.Q = ws.i2p.as<C>(); }
+			if (q.i3) { i3_sums(*q.i3, W); a.X = ws.i3p.as<C>(); }
+		}
+		a.N = N;
+		a.s2 = 1.0 / (double)PP;
+		a.s1 = a.s2 * a.s2;
+		a.pl = pl;
+		return a;
+	}
+
+	void assemble(AsmP<C> &a) {
+		const int nl2 = pick_lines(P, nl1, 2, sizeof(C));
+		a.nl = nl2;
+		ws.wave1.ensure(sizeof(C) * (size_t)ncells * 8 * PP);
+		a.Z = ws.wave1.as<C>();
+		launch(k_any_asm_rows<C>, "any_asm_rows", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, a);
+		launch(k_any_asm_cols<C>, "any_asm_cols", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, a);
+	}
+};
+
+template <class C>
+void any_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
+	AnyRhs<C> r(ws, q, ncells, s);
+	AsmP<C> a = r.prepare(W, parts);
+	a.mode = 0; a.out_cc = cc; a.out_cd = cd;
+	r.assemble(a);
+}
+
+template <class C>
+void any_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc,
+                double2 *out, cudaStream_t s) {
+	AnyRhs<C> r(ws, q, ncells, s);
+	AsmP<C> a = r.prepare(wcur, RHS_ALL);
+	a.mode = 1; a.base = base; a.wcur = wcur; a.B = B; a.dtc = dtc; a.out = out;
+	r.assemble(a);
+}
+
+unsigned grid1d(long n) { return (unsigned)std::min<long>((n + 255) / 256, 148L * 16); }
+
+}  // namespace
+
+bool anyn_supported(int N) {
+	return N >= 4 && N <= 128 && N % 2 == 0 && smooth23(N);
+}
+
+bool anyn_route(int N) {
+	if (N == 8 || N == 16 || N == 32 || N == 64) {
+		const char *e = getenv("QB_ANYN");
+		return e != nullptr && strcmp(e, "1") == 0;
+	}
+	return anyn_supported(N);
+}
+
+void anyn_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *cc, double2 *cd, cudaStream_t s) {
+	if (ncells <= 0) return;
+	if (ws.prec == 32) any_operators<float2>(ws, q, ncells, W, parts, cc, cd, s);
+	else any_operators<double2>(ws, q, ncells, W, parts, cc, cd, s);
+}
+
+void anyn_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc,
+                 double2 *out, cudaStream_t s) {
+	if (ncells <= 0) return;
+	if (ws.prec == 32) any_update<float2>(ws, q, ncells, base, wcur, B, dtc, out, s);
+	else any_update<double2>(ws, q, ncells, base, wcur, B, dtc, out, s);
+}
+
+// the Fourier representation at any supported N, through the same passes
+// (length-N transforms, FP64), with a scratch grid set kept per device
+namespace {
+double2 *repr_scratch(long n) {
+	static std::mutex mu;
+	static DevBuf bufs[64];
+	int dev = 0;
+	QB_CUDA(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lk(mu);
+	DevBuf &b = bufs[dev & 63];
+	if (b.bytes < sizeof(double2) * (size_t)n) b.ensure(sizeof(double2) * (size_t)n);
+	return b.as<double2>();
+}
+void repr_passes(int N, int ngrids, double2 *a, int dir, cudaStream_t s) {
+	PlainP<double2> p{};
+	p.g = a; p.L = N; p.nl = pick_lines(N, 8, 1, sizeof(double2)); p.pl = make_plan(N, 0);
+	const size_t sm = tile_bytes<double2>(N, p.nl);
+	const long nb = (long)ngrids * (N / p.nl);
+	if (dir < 0) {
+		launch(k_any_plain<double2, -1, false>, "any_rows", nb, sm, s, p);
+		launch(k_any_plain<double2, -1, true>, "any_cols", nb, sm, s, p);
+	} else {
+		launch(k_any_plain<double2, +1, false>, "any_rows", nb, sm, s, p);
+		launch(k_any_plain<double2, +1, true>, "any_cols", nb, sm, s, p);
+	}
+}
+}  // namespace
+
+void anyn_to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s) {
+	const long n = (long)ngrids * N * N;
+	double2 *a = repr_scratch(n);
+	{
+		ProfScope ps("any_repr", s);
+		k_any_real_to_cplx<<<grid1d(n), 256, 0, s>>>(n, Wv, a);
+	}
+	QB_CUDA(cudaGetLastError());
+	repr_passes(N, ngrids, a, -1, s);
+	{
+		ProfScope ps("any_repr", s);
+		k_any_hermitian<<<grid1d(n), 256, 0, s>>>(N, ngrids, a, Wf);
+	}
+	QB_CUDA(cudaGetLastError());
+}
+
+void anyn_from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t s) {
+	const long n = (long)ngrids * N * N;
+	double2 *a = repr_scratch(n);
+	QB_CUDA(cudaMemcpyAsync(a, Wf, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+	repr_passes(N, ngrids, a, +1, s);
+	{
+		ProfScope ps("any_repr", s);
+		k_any_real_part<<<grid1d(n), 256, 0, s>>>(n, a, Wv);
+	}
+	QB_CUDA(cudaGetLastError());
+}
+
+}  // namespace qb

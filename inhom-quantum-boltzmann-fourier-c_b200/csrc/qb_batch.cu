@@ -15,8 +15,9 @@
 //     device -- multipliers of the heuristic chunk counts of the quadrature
 //     sums, and where they exist the alternative I3 schedules (the term ranges
 //     or the (cell, chunk) grid of the FP64 sums at N = 32; the FFT kernels or
-//     the tensor-core DFT-GEMMs of the FP32 form at N = 16) -- and keeps the
-//     fastest;
+//     the tensor-core DFT-GEMMs of the FP32 form at N = 16), or for the sizes
+//     of the any-N engine its radix schedules, tile heights and wave budgets
+//     -- and keeps the fastest;
 //   - the steps of all groups are captured once into a CUDA graph of two
 //     steps (state a -> b -> a), which is then relaunched.
 // The quadrature tables, workspaces, group buffers, schedules and the graph
@@ -27,6 +28,7 @@ extern "C" {
 #include "qbgpu.h"
 }
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -73,6 +75,8 @@ std::map<std::tuple<int, int, int>, std::unique_ptr<Group>> g_groups;      // (d
 struct Sched {
 	float s12 = 1.0f, s3 = 1.0f;
 	int ranges = -1, variant = 0;
+	int plan = 0, lines = 0;          // any-N engine: radix-plan variant, lines per tile (0: default)
+	float wave_mb = 0.0f;             // any-N engine: wave budget (0: default)
 	double ms = 0.0;
 };
 // (device, N, precision, instances, rk4, J, M, L, R)
@@ -105,6 +109,9 @@ void apply(qb::Workspace &ws, const Sched &sc) {
 	ws.chunk_scale3 = sc.s3;
 	ws.i3_ranges = sc.ranges;
 	ws.i3_variant = sc.variant;
+	ws.anyn_plan = sc.plan;
+	ws.anyn_lines = sc.lines;
+	ws.anyn_wave_mb = sc.wave_mb;
 }
 
 void step_one(qb::Workspace &ws, const qb::Quad &q, int g, const double2 *in, const double *B, double dt, double2 *out, int rk4,
@@ -121,13 +128,23 @@ void step_one(qb::Workspace &ws, const qb::Quad &q, int g, const double2 *in, co
 constexpr double kTuneLimitMs = 500.0;
 Sched autotune(qb::Workspace &ws, const qb::Quad &q, int N, int prec, int g, const double2 *a, double2 *b, const double *B,
                double dt, int rk4, cudaStream_t s) {
-	std::vector<Sched> cand(5);
-	cand[1].s12 = 0.5f;
-	cand[2].s12 = 2.0f;
-	cand[3].s3 = 0.5f;
-	cand[4].s3 = 2.0f;
-	if (N == 32 && prec == 64) { Sched c; c.ranges = 0; cand.push_back(c); }
-	if (N == 16 && prec == 32) { Sched c; c.variant = 1; cand.push_back(c); }
+	std::vector<Sched> cand(1);
+	if (qb::anyn_route(N)) {
+		// the any-N engine: radix schedules (radix 8 first, radix 3 first, radix 4
+		// only), tile heights (lines per tile) and wave budgets
+		const int P = 2 * N, dl = std::max(1, 2048 / P);
+		for (int v : { 1, 2 }) { Sched c; c.plan = v; cand.push_back(c); }
+		for (int nl : { dl / 2, 2 * dl }) if (nl >= 1 && nl <= P) { Sched c; c.lines = nl; cand.push_back(c); }
+		for (float mb : { 24.0f, 384.0f }) { Sched c; c.wave_mb = mb; cand.push_back(c); }
+	} else {
+		cand.resize(5);
+		cand[1].s12 = 0.5f;
+		cand[2].s12 = 2.0f;
+		cand[3].s3 = 0.5f;
+		cand[4].s3 = 2.0f;
+		if (N == 32 && prec == 64) { Sched c; c.ranges = 0; cand.push_back(c); }
+		if (N == 16 && prec == 32) { Sched c; c.variant = 1; cand.push_back(c); }
+	}
 	cudaEvent_t e0, e1;
 	QB_CUDA(cudaEventCreate(&e0));
 	QB_CUDA(cudaEventCreate(&e1));
@@ -323,12 +340,13 @@ extern "C" int qb_batch_schedules(char *buf, int len) {
 	for (const auto &kv : g_sched) {
 		const SchedKey &k = kv.first;
 		const Sched &c = kv.second;
-		char line[320];
+		char line[448];
 		snprintf(line, sizeof(line),
 		         "%s{\"device\": %d, \"N\": %d, \"precision\": %d, \"instances\": %d, \"rk4\": %d, \"J\": %d, \"M\": %d, "
-		         "\"chunk_scale_i1_i2_i4\": %g, \"chunk_scale_i3\": %g, \"i3_ranges\": %d, \"i3_variant\": %d, \"step_ms\": %.4f}",
+		         "\"chunk_scale_i1_i2_i4\": %g, \"chunk_scale_i3\": %g, \"i3_ranges\": %d, \"i3_variant\": %d, "
+		         "\"anyn_plan\": %d, \"anyn_lines\": %d, \"anyn_wave_mb\": %g, \"step_ms\": %.4f}",
 		         out.size() > 1 ? ", " : "", std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), std::get<4>(k),
-		         std::get<5>(k), std::get<6>(k), c.s12, c.s3, c.ranges, c.variant, c.ms);
+		         std::get<5>(k), std::get<6>(k), c.s12, c.s3, c.ranges, c.variant, c.plan, c.lines, c.wave_mb, c.ms);
 		out += line;
 	}
 	out += "]";

@@ -37,7 +37,7 @@ std::string last_error() {
 	return g_last_error;
 }
 
-bool supported_n(int N) { return N == 8 || N == 16 || N == 32 || N == 64; }
+bool supported_n(int N) { return N == 8 || N == 16 || N == 32 || N == 64 || anyn_supported(N); }
 
 // ---------------------------------------------------------------------------
 // launch accounting
@@ -1059,12 +1059,16 @@ Chunks pick_chunks(int N, int ncells, const QuadSet &q, int prec) {
 	return c;
 }
 
+void prepare_f32_tables(const QuadSet &q, cudaStream_t s) { Tab<float2>::prepare(q, s); }
+
 void collision_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *out_cc, double2 *out_cd, cudaStream_t s) {
+	if (anyn_route(ws.N)) { anyn_operators(ws, q, ncells, W, parts, out_cc, out_cd, s); return; }
 	if (ws.prec == 32) by_n<OpsRun<float2>::F>(ws.N, ws, q, ncells, W, parts, out_cc, out_cd, s);
 	else by_n<OpsRun<double2>::F>(ws.N, ws, q, ncells, W, parts, out_cc, out_cd, s);
 }
 
 void collision_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc, double2 *out, cudaStream_t s) {
+	if (anyn_route(ws.N)) { anyn_update(ws, q, ncells, base, wcur, B, dtc, out, s); return; }
 	if (ws.prec == 32) by_n<UpdRun<float2>::F>(ws.N, ws, q, ncells, base, wcur, B, dtc, out, s);
 	else by_n<UpdRun<double2>::F>(ws.N, ws, q, ncells, base, wcur, B, dtc, out, s);
 }
@@ -1350,7 +1354,9 @@ void to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s
 	case 16: launch_to_fourier<16>(ngrids, Wv, Wf, s); break;
 	case 32: launch_to_fourier<32>(ngrids, Wv, Wf, s); break;
 	case 64: launch_to_fourier<64>(ngrids, Wv, Wf, s); break;
-	default: QB_FAIL("to_fourier: unsupported N");
+	default:
+		if (!anyn_supported(N)) QB_FAIL("to_fourier: unsupported N");
+		anyn_to_fourier(N, ngrids, Wv, Wf, s);
 	}
 }
 
@@ -1361,7 +1367,9 @@ void from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t
 	case 16: launch_from_fourier<16>(ngrids, Wf, Wv, s); break;
 	case 32: launch_from_fourier<32>(ngrids, Wf, Wv, s); break;
 	case 64: launch_from_fourier<64>(ngrids, Wf, Wv, s); break;
-	default: QB_FAIL("from_fourier: unsupported N");
+	default:
+		if (!anyn_supported(N)) QB_FAIL("from_fourier: unsupported N");
+		anyn_from_fourier(N, ngrids, Wf, Wv, s);
 	}
 }
 

@@ -21,7 +21,7 @@ namespace qb {
 void fail(const char *file, int line, const std::string &msg);
 #define QB_FAIL(msg) ::qb::fail(__FILE__, __LINE__, (msg))
 #define QB_CUDA(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) ::qb::fail(__FILE__, __LINE__, std::string(#call) + ": " + cudaGetErrorString(e_)); } while (0)
-bool supported_n(int N);      // grid sizes with compiled kernels
+bool supported_n(int N);      // grid sizes with kernels: the fixed sizes 8, 16, 32, 64 and the any-N engine's
 
 // ---- device buffers ---------------------------------------------------------
 // Process-wide count of device-buffer reallocations and releases: a captured
@@ -93,6 +93,10 @@ struct Workspace {
 	DevBuf i3kind;                           // N = 64, FP32: per-cell I3 kernel (0 real form, 1 complex)
 	DevBuf i3stats;                          // N = 64, FP32: cells evaluated by the real form, by either form (2 x u64)
 	DevBuf kerr;                             // device error word of kernels with bounded waits (nonzero: a wait ran out)
+	DevBuf wave1, wave2;                     // any-N engine: per-wave scratch of the quadrature sums, assembly scratch
+	// any-N engine knobs (0: default): radix-plan variant, lines per tile, wave budget in MB
+	int anyn_plan = 0, anyn_lines = 0;
+	float anyn_wave_mb = 0.0f;
 	int i3_variant = 0;                      // I3 sums: 0 the FFT kernels, 1 DFT-GEMMs on the tensor cores (FP32 form, N = 16)
 	// schedule knobs (set by the batch autotuner): multipliers of the heuristic
 	// chunk counts of the I1/I2/I4 sums and of the I3 sums, and the FP64 I3
@@ -155,6 +159,19 @@ void collision_step_rk4(Workspace &ws, const QuadSet &q, int ncells, const doubl
 void integral_i1(Workspace &ws, const DevI1 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s);
 void integral_i2(Workspace &ws, const DevI2 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s);
 void integral_i3(Workspace &ws, const DevI3 &t, const double2 *f, const double2 *g, const double2 *h, double2 *out, cudaStream_t s);
+
+// the any-N engine (qb_anyn.cu): grid sizes N with 2N = 2^a 3^b up to 128
+// that have no fixed-size kernels (N = 24, 48, 96, 128, ...); QB_ANYN=1
+// routes the fixed sizes through it too (a cross-check of the two engines)
+bool anyn_supported(int N);
+bool anyn_route(int N);
+void anyn_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *out_cc, double2 *out_cd, cudaStream_t s);
+void anyn_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc,
+                 double2 *out, cudaStream_t s);
+void anyn_to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s);
+void anyn_from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t s);
+// FP32 roundings of a table set (made once, on the caller's stream, which is then synchronised)
+void prepare_f32_tables(const QuadSet &q, cudaStream_t s);
 
 void to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s);
 void from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t s);

@@ -1,0 +1,134 @@
+"""The any-N engine (grid sizes without fixed-size kernels: N = 24, 48, 96 with
+radix-3 transforms, N = 128 with 256 x 256 padded grids) against the oracle,
+which restates upstream with N as a run-time parameter and a mixed-radix
+(2, 3) FFT.  FP64 within 1e-12 relative L1, the FP32 form within 1e-5.
+QB_ANYN=1 routes the fixed sizes through the same engine: a cross-check of the
+two engines on identical inputs."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "inhom-quantum-boltzmann-fourier-c_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+pytestmark = pytest.mark.gpu
+
+L, R = 6.0, 3.75
+
+
+def rel_l1(a, b):
+    return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+
+@pytest.fixture(scope="module")
+def mods():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    import qbgpu
+    import orc
+    return torch, qbgpu, orc
+
+
+def _states(qbgpu, orc, N, ncells, seed):
+    Wv = qbgpu.gaussian_mixture_state(N, L, seed=seed, ncells=ncells)
+    return Wv, orc.to_fourier(Wv)
+
+
+@pytest.mark.parametrize("N,J,M", [(24, 4, 3), (48, 4, 2), (12, 2, 3)])
+def test_operators_fp64_vs_oracle(mods, N, J, M):
+    torch, qbgpu, orc = mods
+    ws, q = qbgpu.Workspace(N), qbgpu.Quad(N, J, M, L, R)
+    o = orc.Oracle(N, J, M, L, R)
+    _, WF = _states(qbgpu, orc, N, 3, 70 + N)
+    cc, cd = qbgpu.collision_operators(ws, q, torch.from_numpy(WF).cuda())
+    cc, cd = cc.cpu().numpy(), cd.cpu().numpy()
+    for i in range(3):
+        assert rel_l1(cc[i], o.cc(WF[i])) < 1e-12
+        assert rel_l1(cd[i], o.cd(WF[i])) < 1e-12
+
+
+@pytest.mark.parametrize("N,J,M", [(24, 4, 3), (96, 2, 2)])
+def test_operators_fp32_vs_oracle(mods, N, J, M):
+    torch, qbgpu, orc = mods
+    ws, q = qbgpu.Workspace(N, precision=32), qbgpu.Quad(N, J, M, L, R)
+    o = orc.Oracle(N, J, M, L, R)
+    _, WF = _states(qbgpu, orc, N, 2, 90 + N)
+    cc, cd = qbgpu.collision_operators(ws, q, torch.from_numpy(WF).cuda())
+    cc, cd = cc.cpu().numpy(), cd.cpu().numpy()
+    for i in range(2):
+        assert rel_l1(cc[i], o.cc(WF[i])) < 1e-5
+        assert rel_l1(cd[i], o.cd(WF[i])) < 1e-5
+
+
+def test_n128_fp64_collision_step_vs_oracle(mods):
+    torch, qbgpu, orc = mods
+    N, J, M = 128, 2, 2
+    ws, q = qbgpu.Workspace(N), qbgpu.Quad(N, J, M, L, R)
+    o = orc.Oracle(N, J, M, L, R)
+    _, WF = _states(qbgpu, orc, N, 1, 128)
+    B = np.array([[0.2, -0.1, 0.3]])
+    out = qbgpu.collision_step(ws, q, torch.from_numpy(WF).cuda(), 0.01, torch.from_numpy(B).cuda(), rk4=True).cpu().numpy()
+    assert rel_l1(out[0], o.collision_step(WF[0], 0.01, B[0], rk4=True)) < 1e-12
+
+
+@pytest.mark.parametrize("N", [24, 48, 96])
+def test_transforms_vs_oracle(mods, N):
+    torch, qbgpu, orc = mods
+    Wv = qbgpu.gaussian_mixture_state(N, L, seed=5, ncells=2)
+    WF = qbgpu.to_fourier(torch.from_numpy(Wv).cuda()).cpu().numpy()
+    assert rel_l1(WF, orc.to_fourier(Wv)) < 1e-14
+    back = qbgpu.from_fourier(torch.from_numpy(WF).cuda()).cpu().numpy()
+    assert rel_l1(back, orc.from_fourier(WF)) < 1e-14
+    assert rel_l1(back, Wv) < 1e-14
+
+
+def test_mixed_size_batch_rk4_vs_oracle(mods):
+    """A batch of homogeneous instances of the configuration's sizes N = 16,
+    24, 32, 48 (fixed-size and any-N groups side by side), RK4 steps, against
+    the oracle's RK4 per instance."""
+    torch, qbgpu, orc = mods
+    J, M, dt, steps = 4, 3, 0.01, 2
+    sizes = [24, 16, 48, 24, 32]
+    W0 = [orc.to_fourier(qbgpu.gaussian_mixture_state(n, L, seed=400 + i, ncells=1))[0] for i, n in enumerate(sizes)]
+    states = [torch.from_numpy(w.copy()).cuda() for w in W0]
+    qbgpu.homogeneous_batch(states, dt, steps, rk4=True, J=J, M=M, L=L, R=R, precision=64)
+    for i, n in enumerate(sizes):
+        o = orc.Oracle(n, J, M, L, R)
+        w = W0[i]
+        for _ in range(steps):
+            w = o.collision_step(w, dt, rk4=True)
+        assert rel_l1(states[i].cpu().numpy(), w) < 1e-12, n
+
+
+def test_fixed_sizes_through_the_any_n_engine():
+    """QB_ANYN=1 (read per call) sends N = 16 and 32 through the any-N engine;
+    both engines agree within FP64 rounding (run in a child process so the
+    switch does not leak into other tests)."""
+    code = r"""
+import os, sys, numpy as np, torch
+sys.path.insert(0, %r); sys.path.insert(0, %r)
+import qbgpu, orc
+for N in (16, 32):
+    q = qbgpu.Quad(N, 4, 3, 6.0, 3.75)
+    WF = orc.to_fourier(qbgpu.gaussian_mixture_state(N, 6.0, seed=9, ncells=2))
+    W = torch.from_numpy(WF).cuda()
+    os.environ["QB_ANYN"] = "0"
+    a = [x.cpu().numpy() for x in qbgpu.collision_operators(qbgpu.Workspace(N), q, W)]
+    os.environ["QB_ANYN"] = "1"
+    b = [x.cpu().numpy() for x in qbgpu.collision_operators(qbgpu.Workspace(N), q, W)]
+    for x, y in zip(a, b):
+        r = np.abs(x - y).sum() / np.abs(x).sum()
+        assert r < 1e-12, (N, r)
+print("ok")
+""" % (os.path.join(ROOT, "inhom-quantum-boltzmann-fourier-c_b200"), os.path.join(ROOT, "oracle"))
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr

@@ -451,21 +451,25 @@ def config2_long_run(qbgpu, q, W0, h, dt, cells, steps):
 
 def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
     """A sample of the mixed-size batch configuration: `ninst` independent
-    homogeneous instances with N drawn from the configuration's sizes this
-    build supports (16, 32, 64, weights 0.1, 0.25, 0.2 renormalised), seeded
-    Gaussian mixtures, RK4 steps of dt = 0.01 (J = M = 16), FP64 and the FP32
-    form timed alike (CUDA events, L2 flushed before every step), with the
-    FP32 form's deviation from FP64 on the final states."""
+    homogeneous instances with N drawn from the configuration's sizes (16, 24,
+    32, 48, 64, 96, 128 with weights 0.1, 0.1, 0.25, 0.2, 0.2, 0.1, 0.05;
+    N = 24, 48, 96, 128 run on the any-N engine), seeded Gaussian mixtures, RK4
+    steps of dt = 0.01 (J = M = 16), FP64 and the FP32 form timed alike (CUDA
+    events, L2 flushed before every step), with the FP32 form's deviation from
+    FP64 on the final states; then all `config3_big` instances in the FP32
+    form."""
     import torch
     L, R, J, M, dt = 6.0, 3.75, 16, 16, 0.01
     rng = np.random.default_rng(3)
-    w = np.array([0.1, 0.25, 0.2])
-    sizes = rng.choice([16, 32, 64], size=ninst, p=w / w.sum())
+    sizes_all = [16, 24, 32, 48, 64, 96, 128]
+    w = np.array([0.1, 0.1, 0.25, 0.2, 0.2, 0.1, 0.05])
+    sizes = rng.choice(sizes_all, size=ninst, p=w / w.sum())
     Wf = [qbgpu.to_fourier(torch.from_numpy(qbgpu.gaussian_mixture_state(int(n), L, seed=3000 + i, ncells=1)).cuda())[0].contiguous()
           for i, n in enumerate(sizes)]
-    out = {"workload": f"{ninst} homogeneous instances, N in (16, 32, 64) with weights (0.1, 0.25, 0.2) renormalised, "
-                       f"J={J}, M={M}, RK4 dt={dt}, {steps} timed steps after {warmup} warm-up per precision",
-           "unit": "instance-steps/s", "instances_per_N": {str(k): int((sizes == k).sum()) for k in (16, 32, 64)}}
+    out = {"workload": f"{ninst} homogeneous instances, N in (16, 24, 32, 48, 64, 96, 128) with weights "
+                       f"(0.1, 0.1, 0.25, 0.2, 0.2, 0.1, 0.05), J={J}, M={M}, RK4 dt={dt}, {steps} timed steps after {warmup} "
+                       "warm-up per precision",
+           "unit": "instance-steps/s", "instances_per_N": {str(k): int((sizes == k).sum()) for k in sizes_all}}
     final = {}
     for prec in (64, 32):
         states = [x.clone() for x in Wf]
@@ -485,9 +489,9 @@ def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
     out["speedup_f32_vs_f64"] = round(out["f32"]["value"] / out["f64"]["value"], 4)
     out["rel_l2_f32_vs_f64_final_states"] = float(np.linalg.norm(final[32] - final[64]) / np.linalg.norm(final[64]))
     if args.config3_big > 0:
-        # the configuration's instance count in the FP32 form: sizes of this build, weights renormalised
+        # the configuration's instance count in the FP32 form
         nbig = args.config3_big
-        sizes_b = rng.choice([16, 32, 64], size=nbig, p=w / w.sum())
+        sizes_b = rng.choice(sizes_all, size=nbig, p=w / w.sum())
         states = [qbgpu.to_fourier(torch.from_numpy(qbgpu.gaussian_mixture_state(int(n), L, seed=9000 + i, ncells=1)).cuda())[0].contiguous()
                   for i, n in enumerate(sizes_b)]
         qbgpu.homogeneous_batch(states, dt, 1, rk4=True, J=J, M=M, L=L, R=R, precision=32)     # tuning and sizing
@@ -499,7 +503,7 @@ def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / 4
-        out["f32_all_instances"] = {"instances": nbig, "instances_per_N": {str(k): int((sizes_b == k).sum()) for k in (16, 32, 64)},
+        out["f32_all_instances"] = {"instances": nbig, "instances_per_N": {str(k): int((sizes_b == k).sum()) for k in sizes_all},
                                     "value": round(nbig / (ms * 1e-3), 3), "ms_per_step": round(ms, 3),
                                     "timed": "4 RK4 steps in one call (two direct, then one two-step CUDA graph replay)"}
     out["schedules"] = [s_ for s_ in qbgpu.batch_schedules() if s_["J"] == J and s_["M"] == M]

@@ -76,16 +76,27 @@ template <int RAD, int DIR, class C> __device__ __forceinline__ void dft_r(C (&v
 // length Ns done): butterfly j of a line reads x[j + r L/RAD], twiddles by
 // w^(r (j mod Ns)) with w = exp(DIR 2 pi i / (Ns RAD)), and writes its outputs
 // to (j / Ns) Ns RAD + (j mod Ns) + r Ns.  tw[m] = exp(-2 pi i m / L).
+// shared-memory slot of tile element i: one pad element every 16 spreads the
+// strided accesses of the Stockham stages over the banks
+__device__ __forceinline__ int sw(int i) { return i + (i >> 4); }
+
+// x / d for x, d < 2^16 as a high multiply by floor(2^32 / d) + 1: the error
+// x (d - 2^32 mod d) / (d 2^32) stays below 1/d, so the quotient is exact;
+// d = 1 (whose multiplier does not fit 32 bits) is marked by 0
+__device__ __forceinline__ unsigned magic_div(unsigned d) { return d == 1u ? 0u : 0xffffffffu / d + 1u; }
+__device__ __forceinline__ int fdiv(int x, unsigned mg) { return mg ? (int)__umulhi((unsigned)x, mg) : x; }
+
 template <int RAD, int DIR, class C>
-__device__ __forceinline__ void stage(const C *in, C *out, int nl, int pitch, int L, int Ns, const C *tw) {
+__device__ __forceinline__ void stage(const C *in, C *out, int nl, int ls, int es, int L, int Ns, const C *tw) {
 	const int m = L / RAD, tstep = L / (Ns * RAD);
+	const unsigned mg_m = magic_div((unsigned)m), mg_ns = magic_div((unsigned)Ns);
 	for (int b = threadIdx.x; b < nl * m; b += blockDim.x) {
-		const int line = b / m, j = b - line * m;
-		const int k = j % Ns;
-		const C *src = in + line * pitch + j;
+		const int line = fdiv(b, mg_m), j = b - line * m;
+		const int jq = fdiv(j, mg_ns), k = j - jq * Ns;
+		const int base = line * ls + j * es;
 		C v[RAD];
 #pragma unroll
-		for (int r = 0; r < RAD; r++) v[r] = src[r * m];
+		for (int r = 0; r < RAD; r++) v[r] = in[sw(base + r * m * es)];
 		if (Ns > 1) {
 #pragma unroll
 			for (int r = 1; r < RAD; r++) {
@@ -95,23 +106,24 @@ __device__ __forceinline__ void stage(const C *in, C *out, int nl, int pitch, in
 			}
 		}
 		dft_r<RAD, DIR>(v);
-		C *dst = out + line * pitch + (j / Ns) * Ns * RAD + k;
+		const int ob = line * ls + (jq * Ns * RAD + k) * es;
 #pragma unroll
-		for (int r = 0; r < RAD; r++) dst[r * Ns] = v[r];
+		for (int r = 0; r < RAD; r++) out[sw(ob + r * Ns * es)] = v[r];
 	}
 }
 
-// transforms the nl lines at `a` (line stride `pitch`) in the direction DIR,
-// with `b` as the second buffer; returns the buffer that holds the result.
-// Starts and ends with the CTA synchronised.
-template <int DIR, class C> __device__ C *fft_lines(C *a, C *b, int nl, int pitch, const Plan &pl, const C *tw) {
+// transforms the nl lines at `a` (line stride ls, element stride es; rows of
+// a tile: (pitch, 1), its columns: (1, pitch)) in the direction DIR, with `b`
+// as the second buffer; returns the buffer that holds the result.  Starts and
+// ends with the CTA synchronised.
+template <int DIR, class C> __device__ C *fft_lines(C *a, C *b, int nl, int ls, int es, const Plan &pl, const C *tw) {
 	int Ns = 1;
 	for (int s = 0; s < pl.nst; s++) {
 		const int R = pl.r[s];
-		if (R == 8) stage<8, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
-		else if (R == 4) stage<4, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
-		else if (R == 3) stage<3, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
-		else stage<2, DIR>(a, b, nl, pitch, pl.L, Ns, tw);
+		if (R == 8) stage<8, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		else if (R == 4) stage<4, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		else if (R == 3) stage<3, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		else stage<2, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
 		__syncthreads();
 		C *t = a; a = b; b = t;
 		Ns *= R;
@@ -137,13 +149,38 @@ template <class C> struct Tile {
 		pitch = L + 1;
 		tw = reinterpret_cast<C *>(sm);
 		a = tw + L;
-		b = a + (long)nl * pitch;
+		const int n = nl * pitch;
+		b = a + n + (n >> 4) + 1;
 	}
 };
-template <class C> size_t tile_bytes(int L, int nl) { return sizeof(C) * ((size_t)L + 2 * (size_t)nl * (L + 1)); }
+// the twiddles and two buffers of nl lines of pitch L + 1, with the pads of sw()
+template <class C> size_t tile_bytes(int L, int nl) {
+	const size_t n = (size_t)nl * (L + 1);
+	return sizeof(C) * ((size_t)L + 2 * (n + (n >> 4) + 1));
+}
 
 // ---------------------------------------------------------------------------
 // passes
+
+// element loop of a tile with kBatch global loads in flight per thread:
+// v = ld(i) for i = tid + u kThreads (u < kBatch), then st(i, v)
+constexpr int kBatch = 8;
+template <class V, class Ld, class St> __device__ __forceinline__ void batched(int n, const Ld &ld, const St &st) {
+	for (int i0 = threadIdx.x; i0 < n; i0 += kBatch * kThreads) {
+		V v[kBatch];
+#pragma unroll
+		for (int u = 0; u < kBatch; u++) {
+			const int i = i0 + u * kThreads;
+			if (i < n) v[u] = ld(i);
+		}
+#pragma unroll
+		for (int u = 0; u < kBatch; u++) {
+			const int i = i0 + u * kThreads;
+			if (i < n) st(i, v[u]);
+		}
+	}
+}
+template <class C> struct Two { C a, b; };
 
 // rows of Pad(mult . W_comp) for unit u = (cell nt + tt) nsub + sub, forward
 // transform: out[u] (row pass of the spectra, of P_j and of the first
@@ -165,6 +202,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 	const int N = p.N, P = 2 * N, nl = p.nl;
 	const long NN = (long)N * N, PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
@@ -175,8 +213,8 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 	const long cell = ct / p.nt;
 	const double2 *w = p.W + cell * p.w_cell + (long)p.comp[sub] * NN;
 	const int ps = p.psel[sub];
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = i / P, k = i - li * P;
+	batched<C>(nl * P, [&](int i) {
+		const int li = fdiv(i, mgP), k = i - li * P;
 		const int ls = src_idx(l0 + li, N), ks = src_idx(k, N);
 		C v = czero<C>();
 		if (ls >= 0 && ks >= 0) {
@@ -186,19 +224,21 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 			else if (ps == 3) v = cmul(p.psiC[t * NN + q], mk<C>(x.x, x.y));
 			else {
 				const R f = (ps == 1 ? p.psiA : p.psiB)[t * NN + q];
-				v = mk<C>(0.0, 0.0);
 				v.x = f * (R)x.x;
 				v.y = f * (R)x.y;
 			}
 		}
-		T.a[li * T.pitch + k] = v;
-	}
+		return v;
+	}, [&](int i, const C &v) {
+		const int li = fdiv(i, mgP), k = i - li * P;
+		T.a[sw(li * T.pitch + k)] = v;
+	});
 	__syncthreads();
-	const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	C *o = p.out + u * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = i / P, k = i - li * P;
-		o[(long)li * P + k] = r[li * T.pitch + k];
+		const int li = fdiv(i, mgP), k = i - li * P;
+		o[(long)li * P + k] = r[sw(li * T.pitch + k)];
 	}
 }
 
@@ -212,20 +252,25 @@ template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThread
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int L = p.L, nl = p.nl;
 	Tile<C> T(sm, L, nl);
+	const unsigned mgP = magic_div((unsigned)L), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, L);
 	const int bpg = L / nl;
 	const long u = blockIdx.x / bpg;
 	const int x0 = (int)(blockIdx.x % bpg) * nl;
 	C *g = p.g + u * (long)L * L;
-	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-		if (COLS) { const int kk = i % nl, l = i / nl; T.a[kk * T.pitch + l] = g[(long)l * L + x0 + kk]; }
-		else { const int li = i / L, k = i - li * L; T.a[li * T.pitch + k] = g[(long)(x0 + li) * L + k]; }
-	}
+	batched<C>(nl * L, [&](int i) {
+		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; return g[(long)l * L + x0 + kk]; }
+		const int li = fdiv(i, mgP), k = i - li * L;
+		return g[(long)(x0 + li) * L + k];
+	}, [&](int i, const C &v) {
+		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; T.a[sw(kk * T.pitch + l)] = v; }
+		else { const int li = fdiv(i, mgP), k = i - li * L; T.a[sw(li * T.pitch + k)] = v; }
+	});
 	__syncthreads();
-	const C *r = fft_lines<DIR>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	const C *r = fft_lines<DIR>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-		if (COLS) { const int kk = i % nl, l = i / nl; g[(long)l * L + x0 + kk] = r[kk * T.pitch + l]; }
-		else { const int li = i / L, k = i - li * L; g[(long)(x0 + li) * L + k] = r[li * T.pitch + k]; }
+		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; g[(long)l * L + x0 + kk] = r[sw(kk * T.pitch + l)]; }
+		else { const int li = fdiv(i, mgP), k = i - li * L; g[(long)(x0 + li) * L + k] = r[sw(li * T.pitch + k)]; }
 	}
 }
 
@@ -242,6 +287,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(con
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
@@ -249,24 +295,29 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(con
 	const long cell = u / ((long)p.nsub * p.nt);
 	C *g = p.g + u * PP;
 	const C *F = p.What + (cell * 4 + p.fcomp) * PP;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
-		T.a[kk * T.pitch + l] = g[(long)l * P + k0 + kk];
-	}
+	batched<C>(nl * P, [&](int i) {
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		return g[(long)l * P + k0 + kk];
+	}, [&](int i, const C &v) {
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		T.a[sw(kk * T.pitch + l)] = v;
+	});
 	__syncthreads();
-	C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	const R fa = (R)p.fa, fb = (R)p.fb;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
-		const C w = F[(long)l * P + k0 + kk];
+	batched<C>(nl * P, [&](int i) {
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		return F[(long)l * P + k0 + kk];
+	}, [&](int i, const C &w) {
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		C f; f.x = fa * w.x + fb; f.y = fa * w.y;
-		r[kk * T.pitch + l] = cmul(f, r[kk * T.pitch + l]);
-	}
+		r[sw(kk * T.pitch + l)] = cmul(f, r[sw(kk * T.pitch + l)]);
+	});
 	__syncthreads();
-	const C *r2 = fft_lines<+1>(r, r == T.a ? T.b : T.a, nl, T.pitch, p.pl, T.tw);
+	const C *r2 = fft_lines<+1>(r, r == T.a ? T.b : T.a, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
-		g[(long)l * P + k0 + kk] = r2[kk * T.pitch + l];
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		g[(long)l * P + k0 + kk] = r2[sw(kk * T.pitch + l)];
 	}
 }
 
@@ -283,6 +334,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(con
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long cs = blockIdx.x / bpg;             // cell nsub + sub
@@ -292,22 +344,27 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(con
 	C *S = p.S + cs * PP + (long)l0 * P;
 	for (int tt = 0; tt < p.nt; tt++) {
 		const C *g = p.g + ((cell * p.nt + tt) * p.nsub + sub) * PP + (long)l0 * P;
-		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-			const int li = i / P, k = i - li * P;
-			T.a[li * T.pitch + k] = g[(long)li * P + k];
-		}
+		batched<C>(nl * P, [&](int i) { return g[i]; }, [&](int i, const C &v) {
+			const int li = fdiv(i, mgP), k = i - li * P;
+			T.a[sw(li * T.pitch + k)] = v;
+		});
 		__syncthreads();
-		const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+		const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 		const R *phi = p.phi + (long)(p.t0 + tt) * PP + (long)l0 * P;
-		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-			const int li = i / P, k = i - li * P;
-			const R f = phi[(long)li * P + k];
-			const C x = r[li * T.pitch + k];
-			C s = S[(long)li * P + k];
+		batched<Two<C>>(nl * P, [&](int i) {
+			Two<C> v;
+			v.a = S[i];
+			v.b.x = phi[i];
+			return v;
+		}, [&](int i, const Two<C> &v) {
+			const int li = fdiv(i, mgP), k = i - li * P;
+			const R f = v.b.x;
+			const C x = r[sw(li * T.pitch + k)];
+			C s = v.a;
 			s.x += f * x.x;
 			s.y += f * x.y;
-			S[(long)li * P + k] = s;
-		}
+			S[i] = s;
+		});
 		__syncthreads();
 	}
 }
@@ -323,6 +380,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, 2 * nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long ci = blockIdx.x / bpg;             // cell 4 + i
@@ -332,17 +390,22 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 	C *Q = p.Q + ci * PP;
 	for (int tt = 0; tt < p.nt; tt++) {
 		const C *ga = p.g + ((cell * p.nt + tt) * 8 + 2 * ii) * PP;
-		for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
-			const int h = i / (nl * P), rem = i - h * nl * P, kk = rem % nl, l = rem / nl;
-			T.a[(h * nl + kk) * T.pitch + l] = ga[h * PP + (long)l * P + k0 + kk];
-		}
+		batched<C>(2 * nl * P, [&](int i) {
+			const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
+			return ga[h * PP + (long)l * P + k0 + kk];
+		}, [&](int i, const C &v) {
+			const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
+			T.a[sw((h * nl + kk) * T.pitch + l)] = v;
+		});
 		__syncthreads();
-		const C *r = fft_lines<-1>(T.a, T.b, 2 * nl, T.pitch, p.pl, T.tw);
-		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-			const int kk = i % nl, l = i / nl;
-			const long o = (long)l * P + k0 + kk;
-			Q[o] = cfma(r[kk * T.pitch + l], r[(nl + kk) * T.pitch + l], Q[o]);
-		}
+		const C *r = fft_lines<-1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
+		batched<C>(nl * P, [&](int i) {
+			const int l = fdiv(i, mgnl), kk = i - l * nl;
+			return Q[(long)l * P + k0 + kk];
+		}, [&](int i, const C &q) {
+			const int l = fdiv(i, mgnl), kk = i - l * nl;
+			Q[(long)l * P + k0 + kk] = cfma(r[sw(kk * T.pitch + l)], r[sw((nl + kk) * T.pitch + l)], q);
+		});
 		__syncthreads();
 	}
 }
@@ -358,6 +421,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(c
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
@@ -366,16 +430,21 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(c
 	const long ct = u / 16, cell = ct / p.nt;
 	const C *G = p.What + (cell * 4 + i3) * PP + (long)l0 * P;
 	const C *Pj = p.Pg + (ct * 4 + j3) * PP + (long)l0 * P;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = i / P, k = i - li * P;
-		T.a[li * T.pitch + k] = cmul(G[(long)li * P + k], Pj[(long)li * P + k]);
-	}
+	batched<Two<C>>(nl * P, [&](int i) {
+		Two<C> v;
+		v.a = G[i];
+		v.b = Pj[i];
+		return v;
+	}, [&](int i, const Two<C> &v) {
+		const int li = fdiv(i, mgP), k = i - li * P;
+		T.a[sw(li * T.pitch + k)] = cmul(v.a, v.b);
+	});
 	__syncthreads();
-	const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	C *o = p.Y + u * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = i / P, k = i - li * P;
-		o[(long)li * P + k] = r[li * T.pitch + k];
+		const int li = fdiv(i, mgP), k = i - li * P;
+		o[(long)li * P + k] = r[sw(li * T.pitch + k)];
 	}
 }
 
@@ -392,39 +461,45 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_cols(con
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
 	const int t = p.t0 + (int)((u / 16) % p.nt);
 	C *g = p.Y + u * PP;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
-		T.a[kk * T.pitch + l] = g[(long)l * P + k0 + kk];
-	}
+	batched<C>(nl * P, [&](int i) {
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		return g[(long)l * P + k0 + kk];
+	}, [&](int i, const C &v) {
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		T.a[sw(kk * T.pitch + l)] = v;
+	});
 	__syncthreads();
-	C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, p.pl, T.tw);
+	C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	const R sc = (R)p.scale[t];
-	const R *ps = p.psi2T + (long)p.idx[t] * PP;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
-		const R f = sc * ps[(long)(k0 + kk) * P + l];
-		C x = r[kk * T.pitch + l];
+	const R *ps = p.psi2T + (long)p.idx[t] * PP + (long)k0 * P;       // rows k0.. of the transposed table: contiguous
+	batched<R>(nl * P, [&](int i) { return ps[i]; }, [&](int i, const R &f0) {
+		const int kk = fdiv(i, mgP), l = i - kk * P;                   // table element (k0 + kk, l)
+		const R f = sc * f0;
+		C x = r[sw(kk * T.pitch + l)];
 		x.x *= f;
 		x.y *= f;
-		r[kk * T.pitch + l] = x;
-	}
+		r[sw(kk * T.pitch + l)] = x;
+	});
 	__syncthreads();
-	const C *r2 = fft_lines<-1>(r, r == T.a ? T.b : T.a, nl, T.pitch, p.pl, T.tw);
+	const C *r2 = fft_lines<-1>(r, r == T.a ? T.b : T.a, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
-		g[(long)l * P + k0 + kk] = r2[kk * T.pitch + l];
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
+		g[(long)l * P + k0 + kk] = r2[sw(kk * T.pitch + l)];
 	}
 }
 
 // I3 chain, last rows: forward transforms of Y[((cell nt + tt) 4 + j) 4 + i],
-// i = 0..3, and X[cell][j] += sum_i eta_i P_i . row, over the wave's terms in
-// order (one CTA per (cell, j, row block))
+// one tile at a time, and X[cell][j] += sum_i eta_i P_i . row, over the
+// wave's terms and i in order, in registers (one CTA per (cell, j, row block);
+// a thread owns the tile elements tid + e kThreads, e < own_of<C>())
+template <class C> __host__ __device__ constexpr int own_of() { return sizeof(C) == 16 ? 8 : 16; }   // nl P <= own_of<C>() kThreads
 template <class C> struct I3RowsBP {
 	const C *Y, *Pg; C *X; int N, nl, nt;
 	Plan pl;
@@ -432,40 +507,127 @@ template <class C> struct I3RowsBP {
 template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
-	const int P = 2 * p.N, nl = p.nl;
+	const int P = 2 * p.N, nl = p.nl, ne = nl * P;
 	const long PP = (long)P * P;
-	Tile<C> T(sm, P, 4 * nl);
+	Tile<C> T(sm, P, nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long cj = blockIdx.x / bpg;             // cell 4 + j
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
 	const long cell = cj / 4;
 	const int j3 = (int)(cj % 4);
-	const R eta[4] = { (R)1, (R)-1, (R)-1, (R)-1 };
 	C *X = p.X + cj * PP + (long)l0 * P;
+	constexpr int kOwn = own_of<C>();
+	C acc[kOwn];
+#pragma unroll
+	for (int e = 0; e < kOwn; e++) {
+		const int i = threadIdx.x + e * kThreads;
+		acc[e] = i < ne ? X[i] : czero<C>();       // rows l0.. of X are contiguous: element i at X[i]
+	}
 	for (int tt = 0; tt < p.nt; tt++) {
 		const long ct = cell * p.nt + tt;
-		const C *y = p.Y + ((ct * 4 + j3) * 4) * PP + (long)l0 * P;
-		for (int i = threadIdx.x; i < 4 * nl * P; i += blockDim.x) {
-			const int h = i / (nl * P), rem = i - h * nl * P, li = rem / P, k = rem - li * P;
-			T.a[(h * nl + li) * T.pitch + k] = y[h * PP + (long)li * P + k];
-		}
-		__syncthreads();
-		const C *r = fft_lines<-1>(T.a, T.b, 4 * nl, T.pitch, p.pl, T.tw);
-		const C *Pa = p.Pg + ct * 4 * PP + (long)l0 * P;
-		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-			const int li = i / P, k = i - li * P;
-			const long o = (long)li * P + k;
-			C acc = X[o];
+		for (int h = 0; h < 4; h++) {
+			const C *y = p.Y + ((ct * 4 + j3) * 4 + h) * PP + (long)l0 * P;
+			batched<C>(ne, [&](int i) { return y[i]; }, [&](int i, const C &v) {
+				const int li = fdiv(i, mgP), k = i - li * P;
+				T.a[sw(li * T.pitch + k)] = v;
+			});
+			__syncthreads();
+			const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+			const C *Pa = p.Pg + (ct * 4 + h) * PP + (long)l0 * P;
+			const R eta = h == 0 ? (R)1 : (R)-1;
 #pragma unroll
-			for (int h = 0; h < 4; h++) {
-				const C v = cmul(Pa[h * PP + o], r[(h * nl + li) * T.pitch + k]);
-				acc.x += eta[h] * v.x;
-				acc.y += eta[h] * v.y;
+			for (int e = 0; e < kOwn; e++) {
+				const int i = threadIdx.x + e * kThreads;
+				if (i < ne) {
+					const int li = fdiv(i, mgP), k = i - li * P;
+					const C v = cmul(Pa[i], r[sw(li * T.pitch + k)]);
+					acc[e].x += eta * v.x;
+					acc[e].y += eta * v.y;
+				}
 			}
-			X[o] = acc;
+			__syncthreads();
 		}
-		__syncthreads();
+	}
+#pragma unroll
+	for (int e = 0; e < kOwn; e++) {
+		const int i = threadIdx.x + e * kThreads;
+		if (i < ne) X[i] = acc[e];
+	}
+}
+
+// The I3 chains with the whole P x P grid in shared memory (P = 48 and 96 in
+// FP32, P = 48 in FP64): one CTA per (cell, j) runs the wave's terms and
+// i = 0..3 in order, X[cell][j] += eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j)),
+// each chain one load of W^_i . P_j, four in-place 2-D passes over the tile
+// and one update of X (in L2) instead of three global passes.
+template <class C> struct I3FusedP {
+	using R = typename CT<C>::R;
+	const C *What, *Pg; C *X; const R *psi2T; const int *idx; const double *scale;
+	int N, nt, t0;
+	Plan pl;
+};
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(const I3FusedP<C> p) {
+	using R = typename CT<C>::R;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const int P = 2 * p.N, PPi = P * P;
+	const long PP = (long)P * P;
+	Tile<C> T(sm, P, P);
+	const unsigned mgP = magic_div((unsigned)P);
+	init_tw(T.tw, P);
+	const long cj = blockIdx.x;                   // cell 4 + j
+	const long cell = cj / 4;
+	const int j3 = (int)(cj % 4);
+	C *X = p.X + cj * PP;
+	for (int tt = 0; tt < p.nt; tt++) {
+		const long ct = cell * p.nt + tt;
+		const int t = p.t0 + tt;
+		const R sc = (R)p.scale[t];
+		const R *ps = p.psi2T + (long)p.idx[t] * PP;
+		const C *Pj = p.Pg + (ct * 4 + j3) * PP;
+		for (int h = 0; h < 4; h++) {
+			const C *G = p.What + (cell * 4 + h) * PP;
+			batched<Two<C>>(PPi, [&](int i) {
+				Two<C> v;
+				v.a = G[i];
+				v.b = Pj[i];
+				return v;
+			}, [&](int i, const Two<C> &v) {
+				const int l = fdiv(i, mgP), k = i - l * P;
+				T.a[sw(l * T.pitch + k)] = cmul(v.a, v.b);
+			});
+			__syncthreads();
+			C *r = fft_lines<+1>(T.a, T.b, P, T.pitch, 1, p.pl, T.tw);               // rows
+			r = fft_lines<+1>(r, r == T.a ? T.b : T.a, P, 1, T.pitch, p.pl, T.tw);     // columns
+			batched<R>(PPi, [&](int i) { return ps[i]; }, [&](int i, const R &f0) {
+				const int k = fdiv(i, mgP), l = i - k * P;                   // transposed table: element (l, k)
+				const R f = sc * f0;
+				C x = r[sw(l * T.pitch + k)];
+				x.x *= f;
+				x.y *= f;
+				r[sw(l * T.pitch + k)] = x;
+			});
+			__syncthreads();
+			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, 1, T.pitch, p.pl, T.tw);     // columns
+			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, T.pitch, 1, p.pl, T.tw);     // rows
+			const C *Pa = p.Pg + (ct * 4 + h) * PP;
+			const R eta = h == 0 ? (R)1 : (R)-1;
+			batched<Two<C>>(PPi, [&](int i) {
+				Two<C> v;
+				v.a = Pa[i];
+				v.b = X[i];
+				return v;
+			}, [&](int i, const Two<C> &v) {
+				const int l = fdiv(i, mgP), k = i - l * P;
+				const C y = cmul(v.a, r[sw(l * T.pitch + k)]);
+				C x = v.b;
+				x.x += eta * y.x;
+				x.y += eta * y.y;
+				X[i] = x;
+			});
+			__syncthreads();
+		}
 	}
 }
 
@@ -486,6 +648,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, 2 * nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long cj = blockIdx.x / bpg;
@@ -496,7 +659,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 	const R s1 = (R)p.s1, s2 = (R)p.s2;
 	const C *Wh = p.What + cell * 4 * PP;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = i / P, k = i - li * P;
+		const int li = fdiv(i, mgP), k = i - li * P;
 		const long e = (long)(l0 + li) * P + k;
 		C zc = czero<C>(), zd = czero<C>();
 		if (p.FS != nullptr && j > 0) {
@@ -533,15 +696,15 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 			zd.x += s1 * v.x;
 			zd.y += s1 * v.y;
 		}
-		T.a[li * T.pitch + k] = zc;
-		T.a[(nl + li) * T.pitch + k] = zd;
+		T.a[sw(li * T.pitch + k)] = zc;
+		T.a[sw((nl + li) * T.pitch + k)] = zd;
 	}
 	__syncthreads();
-	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, p.pl, T.tw);
+	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
 	C *z = p.Z + cj * 2 * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
-		const int h = i / (nl * P), rem = i - h * nl * P, li = rem / P, k = rem - li * P;
-		z[h * PP + (long)li * P + k] = r[(h * nl + li) * T.pitch + k];
+		const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, li = fdiv(rem, mgP), k = rem - li * P;
+		z[h * PP + (long)li * P + k] = r[sw((h * nl + li) * T.pitch + k)];
 	}
 }
 
@@ -552,6 +715,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(co
 	const int N = p.N, P = 2 * N, nl = p.nl;
 	const long PP = (long)P * P, NN = (long)N * N;
 	Tile<C> T(sm, P, 2 * nl);
+	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long cj = blockIdx.x / bpg;
@@ -560,16 +724,16 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(co
 	const int j = (int)(cj % 4);
 	const C *z = p.Z + cj * 2 * PP;
 	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
-		const int h = i / (nl * P), rem = i - h * nl * P, kk = rem % nl, l = rem / nl;
-		T.a[(h * nl + kk) * T.pitch + l] = z[h * PP + (long)l * P + k0 + kk];
+		const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
+		T.a[sw((h * nl + kk) * T.pitch + l)] = z[h * PP + (long)l * P + k0 + kk];
 	}
 	__syncthreads();
-	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, p.pl, T.tw);
+	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int kk = i % nl, l = i / nl;
+		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		const int ls = src_idx(l, N), ks = src_idx(k0 + kk, N);
 		if (ls < 0 || ks < 0) continue;
-		const C zc = r[kk * T.pitch + l], zd = r[(nl + kk) * T.pitch + l];
+		const C zc = r[sw(kk * T.pitch + l)], zd = r[sw((nl + kk) * T.pitch + l)];
 		const double2 cc = make_double2(p.s1 * (double)zc.x, p.s1 * (double)zc.y);
 		const double2 cd = make_double2((double)zd.x, (double)zd.y);
 		const long q = (long)ls * N + ks, o = cj * NN + q;
@@ -657,7 +821,8 @@ Plan make_plan(int L, int variant) {
 int pick_lines(int L, int want, int tiles, size_t elem) {
 	for (int nl = want; nl >= 1; nl--) {
 		if (L % nl) continue;
-		if (elem * ((size_t)L + 2 * (size_t)tiles * nl * (L + 1)) <= kMaxSmem) return nl;
+		const size_t n = (size_t)tiles * nl * (L + 1);
+		if (elem * ((size_t)L + 2 * (n + (n >> 4) + 1)) <= kMaxSmem) return nl;
 	}
 	return 1;
 }
@@ -668,8 +833,11 @@ template <class K> void smem_attr(K kern, size_t bytes) {
 	int dev = 0;
 	QB_CUDA(cudaGetDevice(&dev));
 	std::lock_guard<std::mutex> lk(mu);
-	if (done.insert(std::make_tuple(dev, (const void *)kern)).second)
+	if (done.insert(std::make_tuple(dev, (const void *)kern)).second) {
 		QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+		// occupancy is bound by shared memory, not by L1 hits (the tiles are read once)
+		QB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+	}
 	(void)bytes;
 }
 
@@ -719,7 +887,7 @@ template <class C> struct AnyRhs {
 
 	// terms per wave: the wave's scratch of `per_term` grids per cell within the budget
 	int wave(int nterms, int per_term) const {
-		const double mb = ws.anyn_wave_mb > 0 ? ws.anyn_wave_mb : 96.0;
+		const double mb = ws.anyn_wave_mb > 0 ? ws.anyn_wave_mb : 32.0;      // the wave's scratch stays in L2
 		const double per = (double)per_term * ncells * PP * sizeof(C);
 		const int nt = (int)std::max(1.0, std::floor(mb * 1048576.0 / per));
 		return std::min(nt, std::max(1, nterms));
@@ -803,14 +971,42 @@ template <class C> struct AnyRhs {
 		}
 	}
 
+	// whole-grid chains when the tile fits (QB_ANYN_FUSED=0 or the knob turns them off)
+	bool fused_i3() const {
+		if (ws.anyn_fused == 0) return false;
+		const char *e = getenv("QB_ANYN_FUSED");
+		if (e != nullptr && strcmp(e, "0") == 0) return false;
+		return tile_bytes<C>(P, P) <= kMaxSmem;
+	}
+
 	void i3_sums(const DevI3 &t, const double2 *W) {
 		ws.i3p.ensure(sizeof(C) * ncells * 4 * PP);
 		QB_CUDA(cudaMemsetAsync(ws.i3p.p, 0, sizeof(C) * ncells * 4 * PP, s));
+		if (fused_i3()) {
+			const int nt = wave(t.nterms, 4);
+			ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
+			C *Pg = ws.wave1.as<C>();
+			for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+				const int n = std::min(nt, t.nterms - t0);
+				PadRowsP<C> p = pad_params(W, n, t0, 4, Pg);
+				for (int j = 0; j < 4; j++) { p.comp[j] = j; p.psel[j] = 3; }
+				p.psiC = Tabs<C>::i3_psi1(t);
+				pad_rows(p);
+				plain(Pg, (long)ncells * n * 4, -1, true);
+				I3FusedP<C> f{};
+				f.What = ws.What.as<C>(); f.Pg = Pg; f.X = ws.i3p.as<C>();
+				f.psi2T = Tabs<C>::i3_psi2T(t); f.idx = t.idx.as<int>(); f.scale = t.scale.as<double>();
+				f.N = N; f.nt = n; f.t0 = t0; f.pl = pl;
+				launch(k_any_i3_fused<C>, "any_i3_fused", (long)ncells * 4, tile_bytes<C>(P, P), s, f);
+			}
+			return;
+		}
 		const int nt = wave(t.nterms, 20);
 		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
 		ws.wave2.ensure(sizeof(C) * (size_t)ncells * nt * 16 * PP);      // chains
 		C *Pg = ws.wave1.as<C>(), *Y = ws.wave2.as<C>();
-		const int nl4 = pick_lines(P, nl1, 4, sizeof(C));
+		int nl4 = nl1;                                      // one tile, at most kOwn elements a thread
+		while (nl4 > 1 && (nl4 * P > own_of<C>() * kThreads || P % nl4)) nl4--;
 		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
 			const int n = std::min(nt, t.nterms - t0);
 			PadRowsP<C> p = pad_params(W, n, t0, 4, Pg);
@@ -827,7 +1023,7 @@ template <class C> struct AnyRhs {
 			launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)ncells * n * 16, nl1), smem(nl1, 1), s, c);
 			I3RowsBP<C> b{};
 			b.Y = Y; b.Pg = Pg; b.X = ws.i3p.as<C>(); b.N = N; b.nl = nl4; b.nt = n; b.pl = pl;
-			launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)ncells * 4, nl4), smem(nl4, 4), s, b);
+			launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)ncells * 4, nl4), smem(nl4, 1), s, b);
 		}
 	}
 

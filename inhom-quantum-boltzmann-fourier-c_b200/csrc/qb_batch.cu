@@ -76,6 +76,7 @@ struct Sched {
 	float s12 = 1.0f, s3 = 1.0f;
 	int ranges = -1, variant = 0;
 	int plan = 0, lines = 0;          // any-N engine: radix-plan variant, lines per tile (0: default)
+	int fused = 1;                    // any-N engine: whole-grid I3 chains where a grid fits shared memory
 	float wave_mb = 0.0f;             // any-N engine: wave budget (0: default)
 	double ms = 0.0;
 };
@@ -112,6 +113,7 @@ void apply(qb::Workspace &ws, const Sched &sc) {
 	ws.anyn_plan = sc.plan;
 	ws.anyn_lines = sc.lines;
 	ws.anyn_wave_mb = sc.wave_mb;
+	ws.anyn_fused = sc.fused;
 }
 
 void step_one(qb::Workspace &ws, const qb::Quad &q, int g, const double2 *in, const double *B, double dt, double2 *out, int rk4,
@@ -131,11 +133,13 @@ Sched autotune(qb::Workspace &ws, const qb::Quad &q, int N, int prec, int g, con
 	std::vector<Sched> cand(1);
 	if (qb::anyn_route(N)) {
 		// the any-N engine: radix schedules (radix 8 first, radix 3 first, radix 4
-		// only), tile heights (lines per tile) and wave budgets
+		// only), tile heights (lines per tile), wave budgets, and the global-pass
+		// I3 chains against the whole-grid ones
 		const int P = 2 * N, dl = std::max(1, 2048 / P);
 		for (int v : { 1, 2 }) { Sched c; c.plan = v; cand.push_back(c); }
 		for (int nl : { dl / 2, 2 * dl }) if (nl >= 1 && nl <= P) { Sched c; c.lines = nl; cand.push_back(c); }
-		for (float mb : { 24.0f, 384.0f }) { Sched c; c.wave_mb = mb; cand.push_back(c); }
+		for (float mb : { 12.0f, 96.0f }) { Sched c; c.wave_mb = mb; cand.push_back(c); }
+		{ Sched c; c.fused = 0; cand.push_back(c); }
 	} else {
 		cand.resize(5);
 		cand[1].s12 = 0.5f;
@@ -344,9 +348,9 @@ extern "C" int qb_batch_schedules(char *buf, int len) {
 		snprintf(line, sizeof(line),
 		         "%s{\"device\": %d, \"N\": %d, \"precision\": %d, \"instances\": %d, \"rk4\": %d, \"J\": %d, \"M\": %d, "
 		         "\"chunk_scale_i1_i2_i4\": %g, \"chunk_scale_i3\": %g, \"i3_ranges\": %d, \"i3_variant\": %d, "
-		         "\"anyn_plan\": %d, \"anyn_lines\": %d, \"anyn_wave_mb\": %g, \"step_ms\": %.4f}",
+		         "\"anyn_plan\": %d, \"anyn_lines\": %d, \"anyn_wave_mb\": %g, \"anyn_fused\": %d, \"step_ms\": %.4f}",
 		         out.size() > 1 ? ", " : "", std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), std::get<4>(k),
-		         std::get<5>(k), std::get<6>(k), c.s12, c.s3, c.ranges, c.variant, c.plan, c.lines, c.wave_mb, c.ms);
+		         std::get<5>(k), std::get<6>(k), c.s12, c.s3, c.ranges, c.variant, c.plan, c.lines, c.wave_mb, c.fused, c.ms);
 		out += line;
 	}
 	out += "]";

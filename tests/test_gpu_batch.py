@@ -33,8 +33,9 @@ def test_mixed_size_batch_matches_oracle(rk4):
 
 
 def test_batch_rejects_unsupported_size():
-    bad = [torch.zeros((4, 24, 24), dtype=torch.complex128, device="cuda")]
-    with pytest.raises(RuntimeError, match="N=24"):
+    """N = 20 (2N = 40 has the factor 5: neither a fixed-size nor an any-N size)"""
+    bad = [torch.zeros((4, 20, 20), dtype=torch.complex128, device="cuda")]
+    with pytest.raises(RuntimeError, match="N=20"):
         qbgpu.homogeneous_batch(bad, 0.01, 1, J=J, M=M, L=L, R=R)
 
 

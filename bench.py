@@ -303,7 +303,7 @@ def run_ours(args):
         big = run_config2_sample(args, qbgpu, flush, cells=args.config2_cells)
     big3 = None
     if world == 1 and not args.no_config3:
-        big3 = run_config3_sample(args, qbgpu, flush)
+        big3 = run_config3_sample(args, qbgpu, flush, ninst=args.config3_ninst)
     dmm = None
     if world == 1 and not args.no_dftmma:
         dmm = run_dftmma_sample(args, qbgpu, flush)
@@ -917,6 +917,9 @@ def main():
     ap.add_argument("--surrogate-long-cells", type=int, default=16, help="x-cells of the surrogate long run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dftmma", action="store_true", help="skip the tensor-core DFT-GEMM sample (N = 16)")
+    ap.add_argument("--config3-only", action="store_true",
+                    help="print only the mixed-size batch sample (a small case for profiling, with --config3-ninst)")
+    ap.add_argument("--config3-ninst", type=int, default=256, help="instances of the mixed-size batch sample")
     ap.add_argument("--dftmma-only", action="store_true",
                     help="run only the tensor-core DFT-GEMM sample and print its JSON block (for profiling)")
     args = ap.parse_args()
@@ -929,6 +932,11 @@ def main():
         qbgpu = _import("qbgpu", os.path.join(PKG, "qbgpu.py"))
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
         print(json.dumps(run_dftmma_sample(args, qbgpu, flush)), flush=True)
+    elif args.config3_only:
+        import torch
+        qbgpu = _import("qbgpu", os.path.join(PKG, "qbgpu.py"))
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        print(json.dumps(run_config3_sample(args, qbgpu, flush, ninst=args.config3_ninst)), flush=True)
     else:
         run_ours(args)
 

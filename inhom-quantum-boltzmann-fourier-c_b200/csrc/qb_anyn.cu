@@ -558,10 +558,11 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(c
 }
 
 // The I3 chains with the whole P x P grid in shared memory (P = 48 and 96 in
-// FP32, P = 48 in FP64): one CTA per (cell, j) runs the wave's terms and
-// i = 0..3 in order, X[cell][j] += eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j)),
-// each chain one load of W^_i . P_j, four in-place 2-D passes over the tile
-// and one update of X (in L2) instead of three global passes.
+// FP32, P = 48 in FP64): one CTA per (cell, j, i) runs the wave's terms in
+// order, X[cell][j][i] += eta_i P_i . FFT2(psi2_t . IFFT2(W^_i . P_j)), each
+// chain one load of W^_i . P_j, four in-place 2-D passes over the tile and one
+// update of the partial X[cell][j][i] (in L2) instead of three global passes;
+// the assembly adds the four partials of (cell, j) in the order i = 0..3.
 template <class C> struct I3FusedP {
 	using R = typename CT<C>::R;
 	const C *What, *Pg; C *X; const R *psi2T; const int *idx; const double *scale;
@@ -576,18 +577,18 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(co
 	Tile<C> T(sm, P, P);
 	const unsigned mgP = magic_div((unsigned)P);
 	init_tw(T.tw, P);
-	const long cj = blockIdx.x;                   // cell 4 + j
-	const long cell = cj / 4;
-	const int j3 = (int)(cj % 4);
-	C *X = p.X + cj * PP;
+	const long cji = blockIdx.x;                  // (cell 4 + j) 4 + i
+	const long cell = cji / 16;
+	const int j3 = (int)((cji / 4) % 4), h = (int)(cji % 4);
+	C *X = p.X + cji * PP;
+	const C *G = p.What + (cell * 4 + h) * PP;
 	for (int tt = 0; tt < p.nt; tt++) {
 		const long ct = cell * p.nt + tt;
 		const int t = p.t0 + tt;
 		const R sc = (R)p.scale[t];
 		const R *ps = p.psi2T + (long)p.idx[t] * PP;
 		const C *Pj = p.Pg + (ct * 4 + j3) * PP;
-		for (int h = 0; h < 4; h++) {
-			const C *G = p.What + (cell * 4 + h) * PP;
+		{
 			batched<Two<C>>(PPi, [&](int i) {
 				Two<C> v;
 				v.a = G[i];
@@ -634,7 +635,8 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(co
 // assembly rows: Zcc_j and Zcd_j (the combinations of k_assemble) for unit
 // (cell, j), inverse row transforms into Z[(cell 4 + j) 2 + {0, 1}]
 template <class C> struct AsmP {
-	const C *What, *FS, *FS4, *Q, *X;    // FS [cell][3], FS4 / Q / X [cell][4] (null: part absent)
+	const C *What, *FS, *FS4, *Q, *X;    // FS [cell][3], FS4 / Q [cell][4], X [cell][4][nxp] (null: part absent)
+	int nxp;                             // partials of X per (cell, j), added in order
 	C *Z; int N, nl;
 	double s1, s2;
 	int mode;
@@ -681,7 +683,8 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 			zd.y += s2 * v.y;
 		}
 		if (p.X != nullptr) {
-			const C s = p.X[(cell * 4 + j) * PP + e];
+			C s = p.X[(cell * 4 + j) * p.nxp * PP + e];
+			for (int k = 1; k < p.nxp; k++) s = cadd(s, p.X[((cell * 4 + j) * p.nxp + k) * PP + e]);
 			zd.x -= eta2[j] * s1 * s.x;
 			zd.y -= eta2[j] * s1 * s.y;
 		}
@@ -979,10 +982,12 @@ template <class C> struct AnyRhs {
 		return tile_bytes<C>(P, P) <= kMaxSmem;
 	}
 
-	void i3_sums(const DevI3 &t, const double2 *W) {
-		ws.i3p.ensure(sizeof(C) * ncells * 4 * PP);
-		QB_CUDA(cudaMemsetAsync(ws.i3p.p, 0, sizeof(C) * ncells * 4 * PP, s));
-		if (fused_i3()) {
+	// returns the partials of X per (cell, j)
+	int i3_sums(const DevI3 &t, const double2 *W) {
+		const int nxp = fused_i3() ? 4 : 1;
+		ws.i3p.ensure(sizeof(C) * ncells * 4 * nxp * PP);
+		QB_CUDA(cudaMemsetAsync(ws.i3p.p, 0, sizeof(C) * ncells * 4 * nxp * PP, s));
+		if (nxp == 4) {
 			const int nt = wave(t.nterms, 4);
 			ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
 			C *Pg = ws.wave1.as<C>();
@@ -997,9 +1002,9 @@ template <class C> struct AnyRhs {
 				f.What = ws.What.as<C>(); f.Pg = Pg; f.X = ws.i3p.as<C>();
 				f.psi2T = Tabs<C>::i3_psi2T(t); f.idx = t.idx.as<int>(); f.scale = t.scale.as<double>();
 				f.N = N; f.nt = n; f.t0 = t0; f.pl = pl;
-				launch(k_any_i3_fused<C>, "any_i3_fused", (long)ncells * 4, tile_bytes<C>(P, P), s, f);
+				launch(k_any_i3_fused<C>, "any_i3_fused", (long)ncells * 16, tile_bytes<C>(P, P), s, f);
 			}
-			return;
+			return nxp;
 		}
 		const int nt = wave(t.nterms, 20);
 		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
@@ -1025,6 +1030,7 @@ template <class C> struct AnyRhs {
 			b.Y = Y; b.Pg = Pg; b.X = ws.i3p.as<C>(); b.N = N; b.nl = nl4; b.nt = n; b.pl = pl;
 			launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)ncells * 4, nl4), smem(nl4, 1), s, b);
 		}
+		return nxp;
 	}
 
 	AsmP<C> prepare(const double2 *W, int parts) {
@@ -1036,7 +1042,7 @@ template <class C> struct AnyRhs {
 		if (parts & RHS_CD) {
 			if (q.i4) { i1_sums(*q.i4, W, false, ws.i1i4, ws.fs4); a.FS4 = ws.fs4.as<C>(); }
 			if (q.i2) { i2_sums(*q.i2, W); a.Q = ws.i2p.as<C>(); }
-			if (q.i3) { i3_sums(*q.i3, W); a.X = ws.i3p.as<C>(); }
+			if (q.i3) { a.nxp = i3_sums(*q.i3, W); a.X = ws.i3p.as<C>(); }
 		}
 		a.N = N;
 		a.s2 = 1.0 / (double)PP;

@@ -12,6 +12,9 @@
 #include "qb_kernels.cuh"
 #include "qb_umma.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <mutex>
 #include <vector>
 
 extern "C" {
@@ -122,7 +125,7 @@ constexpr uint32_t oP = oA + 4 * kTile;            // A tiles: [warpgroup][hi, l
 constexpr uint32_t oG = oP + 4 * P * kPitch * 8;   // the cell's spectra G (4 grids, natural order)
 constexpr uint32_t kGBytes = 4 * P * P * 8;
 constexpr uint32_t kSmem = oG + kGBytes + 1024;
-static_assert(oG % 16 == 0 && kGBytes % 16 == 0, "bulk copies move 16-byte aligned multiples of 16 bytes");
+static_assert(oG % 128 == 0 && kGBytes % 16 == 0, "the TMA tile lands 128-byte aligned");
 static_assert(kSmem <= 232448, "dynamic shared memory of one CTA");
 constexpr uint32_t kCols = 256;                    // tensor memory: per warpgroup a 64-column D and its 64-column sums X
 }  // namespace dm
@@ -241,7 +244,7 @@ __device__ __forceinline__ void put_col_d(const MmaCtx &c, unsigned char *hi, un
 	}
 }
 
-__global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<float2> p, int *err) {
+__global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<float2> p, int *err, const __grid_constant__ CUtensorMap tmG) {
 	using namespace dm;
 	extern __shared__ unsigned char smem_raw[];
 	unsigned char *base = align1024(smem_raw);
@@ -262,8 +265,9 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 		umma::mbar_init(&mbar[2], 1);
 		fence_mbar_init();
 		abort_flag[0] = abort_flag[1] = 0;
-		// the cell's spectra G (32 KB, contiguous) into shared memory by one bulk copy
-		umma::bulk_g2s(base + oG, p.Ghat + cell * p.g_cell, kGBytes, &mbar[2]);
+		// the cell's spectra G: a 128-row tile of the spectra tensor (rows of 32
+		// complex values, 4 grids a cell) into shared memory by one TMA copy
+		umma::tma_load_2d(base + oG, &tmG, 0, (int)(cell * 4 * P), &mbar[2], kGBytes);
 	}
 	// the real-ified DFT matrix B (K x N) as its transpose, row n = column n of B, split hi / lo
 	for (int i = tid; i < K2 * K2; i += kThreads) {
@@ -449,6 +453,37 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_i3_mma32(const I3ParamsT<fl
 
 }  // namespace
 
+// the driver's tensor-map encoder, through the runtime's entry-point query
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+	static std::mutex mu;
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	std::lock_guard<std::mutex> lk(mu);
+	if (fn == nullptr) {
+		void *f = nullptr;
+		cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+		QB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+		if (f == nullptr || q != cudaDriverEntryPointSuccess) QB_FAIL("cuTensorMapEncodeTiled is not available");
+		fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+	}
+	return fn;
+}
+
+// the spectra of ncells cells ([cell][4][P][P] complex FP32) as a 2-D tensor
+// of FP32 values: rows of 2P floats, 4P rows a cell; the box is one cell
+CUtensorMap spectra_map(const float2 *G, long ncells) {
+	using namespace dm;
+	CUtensorMap m;
+	const cuuint64_t dims[2] = { (cuuint64_t)(2 * P), (cuuint64_t)(ncells * 4 * P) };
+	const cuuint64_t strides[1] = { (cuuint64_t)(2 * P * sizeof(float)) };
+	const cuuint32_t box[2] = { (cuuint32_t)(2 * P), (cuuint32_t)(4 * P) };
+	const cuuint32_t estr[2] = { 1, 1 };
+	const CUresult r = tmap_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2 *>(G), dims, strides, box, estr,
+	                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+	                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS) QB_FAIL("cuTensorMapEncodeTiled failed for the spectra map (" + std::to_string((int)r) + ")");
+	return m;
+}
+
 // launcher (engine): ncl = cells x chunks CTAs
 void launch_i3_mma32(const I3ParamsT<float2> &p, long ncl, int *err, cudaStream_t s) {
 	static bool attr_done[64] = {};
@@ -458,8 +493,10 @@ void launch_i3_mma32(const I3ParamsT<float2> &p, long ncl, int *err, cudaStream_
 		QB_CUDA(cudaFuncSetAttribute(k_i3_mma32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::kSmem));
 		attr_done[dev & 63] = true;
 	}
+	if (p.g_cell != 4L * dm::P * dm::P) QB_FAIL("k_i3_mma32: the spectra must be [cell][4][P][P]");
+	const CUtensorMap tmG = spectra_map(p.Ghat, ncl / p.nchunk);
 	ProfScope ps("i3_cluster", s);
-	k_i3_mma32<<<(unsigned)ncl, dm::kThreads, dm::kSmem, s>>>(p, err);
+	k_i3_mma32<<<(unsigned)ncl, dm::kThreads, dm::kSmem, s>>>(p, err, tmG);
 	QB_CUDA(cudaGetLastError());
 }
 

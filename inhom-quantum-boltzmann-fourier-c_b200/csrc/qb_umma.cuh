@@ -87,6 +87,18 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_global,
 	             : "memory");
 }
 
+// a 2-D tile of a tensor map (TMA, no multicast) into shared memory, completing
+// on `mbar` (which expects `bytes`); the map lives in kernel parameter space
+// (__grid_constant__).  The innermost coordinate x times the element size is
+// a multiple of 16 bytes, and the destination is 128-byte aligned.
+__device__ __forceinline__ void tma_load_2d(void *dst_smem, const void *tmap, int x, int y, uint64_t *mbar, uint32_t bytes) {
+	const uint32_t mb = smem_u32(mbar);
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+	             ::"r"(smem_u32(dst_smem)), "l"(tmap), "r"(x), "r"(y), "r"(mb)
+	             : "memory");
+}
+
 // generic-proxy shared-memory writes -> visible to the tensor core
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 

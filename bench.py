@@ -463,6 +463,10 @@ def run_config3_sample(args, qbgpu, flush, ninst=256, steps=2, warmup=1):
     rng = np.random.default_rng(3)
     sizes_all = [16, 24, 32, 48, 64, 96, 128]
     w = np.array([0.1, 0.1, 0.25, 0.2, 0.2, 0.1, 0.05])
+    if args.config3_sizes:                 # a subset of the sizes (profiling), weights renormalised
+        keep = [int(x) for x in args.config3_sizes.split(",")]
+        w = np.array([wi for n, wi in zip(sizes_all, w) if n in keep])
+        sizes_all = [n for n in sizes_all if n in keep]
     sizes = rng.choice(sizes_all, size=ninst, p=w / w.sum())
     Wf = [qbgpu.to_fourier(torch.from_numpy(qbgpu.gaussian_mixture_state(int(n), L, seed=3000 + i, ncells=1)).cuda())[0].contiguous()
           for i, n in enumerate(sizes)]
@@ -920,6 +924,7 @@ def main():
     ap.add_argument("--config3-only", action="store_true",
                     help="print only the mixed-size batch sample (a small case for profiling, with --config3-ninst)")
     ap.add_argument("--config3-ninst", type=int, default=256, help="instances of the mixed-size batch sample")
+    ap.add_argument("--config3-sizes", default="", help="comma-separated subset of the sizes of the batch sample")
     ap.add_argument("--dftmma-only", action="store_true",
                     help="run only the tensor-core DFT-GEMM sample and print its JSON block (for profiling)")
     args = ap.parse_args()

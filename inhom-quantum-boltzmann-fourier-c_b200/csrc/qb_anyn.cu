@@ -45,7 +45,7 @@ constexpr int kThreads = 256;
 constexpr int kMaxStages = 8;
 constexpr size_t kMaxSmem = 200 * 1024;
 
-// radix schedule of one transform length: radices 2, 3, 4, 8 whose product is L
+// radix schedule of one transform length: radices 2, 3, 4, 6, 8, 12, 16 whose product is L
 struct Plan {
 	int L = 0, nst = 0;
 	int r[kMaxStages] = {};
@@ -65,11 +65,78 @@ template <int DIR, class C> __device__ __forceinline__ void dft3(C &x0, C &x1, C
 	x2 = csub(m, d);
 }
 
+// cos and sin of 2 pi m / R for R = 6, 12, 16 (the twiddles of the composite
+// register DFTs; folded to constants when m is known at compile time)
+__host__ __device__ constexpr double cos_r(int R, int m) {
+	constexpr double h = 0.5, c3 = 0.86602540378443864676, c8 = 0.70710678118654752440;
+	constexpr double a = 0.92387953251128675613, b = 0.38268343236508977173;
+	if (R == 16) {
+		const double t[16] = { 1, a, c8, b, 0, -b, -c8, -a, -1, -a, -c8, -b, 0, b, c8, a };
+		return t[m];
+	}
+	if (R == 12) {
+		const double t[12] = { 1, c3, h, 0, -h, -c3, -1, -c3, -h, 0, h, c3 };
+		return t[m];
+	}
+	const double t[6] = { 1, h, -h, -1, -h, h };
+	return t[m];
+}
+__host__ __device__ constexpr double sin_r(int R, int m) {
+	if (R == 6) {
+		constexpr double c3 = 0.86602540378443864676;
+		const double t[6] = { 0, c3, c3, 0, -c3, -c3 };
+		return t[m];
+	}
+	return cos_r(R, (m + 3 * R / 4) % R);     // sin x = cos(x - pi/2); R = 12, 16 are multiples of 4
+}
+
+template <int R1, int R2, int DIR, class C> __device__ __forceinline__ void dft_ct(C (&x)[R1 * R2]);
+
 template <int RAD, int DIR, class C> __device__ __forceinline__ void dft_r(C (&v)[RAD]) {
-	if constexpr (RAD == 8) dft8<DIR>(v);
+	if constexpr (RAD == 16) dft_ct<4, 4, DIR>(v);
+	else if constexpr (RAD == 12) dft_ct<4, 3, DIR>(v);
+	else if constexpr (RAD == 8) dft8<DIR>(v);
+	else if constexpr (RAD == 6) dft_ct<2, 3, DIR>(v);
 	else if constexpr (RAD == 4) dft4<DIR>(v[0], v[1], v[2], v[3]);
 	else if constexpr (RAD == 3) dft3<DIR>(v[0], v[1], v[2]);
 	else dft2(v[0], v[1]);
+}
+
+// an R1 R2-point DFT in registers, natural order in and out: R2 DFTs of R1
+// points (stride R2), twiddles w_R^(n2 k1), R1 DFTs of R2 points; output
+// k1 + R1 k2
+template <int R1, int R2, int DIR, class C> __device__ __forceinline__ void dft_ct(C (&x)[R1 * R2]) {
+	using R = typename CT<C>::R;
+	constexpr int RR = R1 * R2;
+	C a[RR];
+#pragma unroll
+	for (int n2 = 0; n2 < R2; n2++) {
+		C v[R1];
+#pragma unroll
+		for (int n1 = 0; n1 < R1; n1++) v[n1] = x[n2 + R2 * n1];
+		dft_r<R1, DIR>(v);
+#pragma unroll
+		for (int k1 = 0; k1 < R1; k1++) {
+			const int m = (n2 * k1) % RR;
+			if (m == 0) {
+				a[n2 * R1 + k1] = v[k1];
+			} else {
+				C w;
+				w.x = (R)cos_r(RR, m);
+				w.y = (R)(DIR < 0 ? -sin_r(RR, m) : sin_r(RR, m));
+				a[n2 * R1 + k1] = cmul(v[k1], w);
+			}
+		}
+	}
+#pragma unroll
+	for (int k1 = 0; k1 < R1; k1++) {
+		C v[R2];
+#pragma unroll
+		for (int n2 = 0; n2 < R2; n2++) v[n2] = a[n2 * R1 + k1];
+		dft_r<R2, DIR>(v);
+#pragma unroll
+		for (int k2 = 0; k2 < R2; k2++) x[k1 + R1 * k2] = v[k2];
+	}
 }
 
 // one Stockham stage of radix RAD over nl lines of length L (sub-transforms of
@@ -120,7 +187,10 @@ template <int DIR, class C> __device__ C *fft_lines(C *a, C *b, int nl, int ls, 
 	int Ns = 1;
 	for (int s = 0; s < pl.nst; s++) {
 		const int R = pl.r[s];
-		if (R == 8) stage<8, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		if (R == 16) stage<16, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		else if (R == 12) stage<12, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		else if (R == 8) stage<8, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
+		else if (R == 6) stage<6, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
 		else if (R == 4) stage<4, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
 		else if (R == 3) stage<3, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
 		else stage<2, DIR>(a, b, nl, ls, es, pl.L, Ns, tw);
@@ -795,8 +865,10 @@ bool smooth23(int L) {
 	return L == 1;
 }
 
-// radix plans of a length: variant 0 takes radix 8 first, then 4, 3, 2;
-// variant 1 the radix-3 stages first; variant 2 radix 4 instead of 8
+// radix plans of a length: variant 0 the fewest stages (the largest of 16,
+// 12, 8, 6, 4, 3, 2 that divides what is left, first: 48 = 16 3, 96 = 16 6,
+// 192 = 16 12, 256 = 16 16); variant 1 radix 8 first, then 4, 2, 3; variant 2
+// the radix-3 stages first; variant 3 radix 4 instead of 8
 Plan make_plan(int L, int variant) {
 	Plan p;
 	p.L = L;
@@ -809,12 +881,20 @@ Plan make_plan(int L, int variant) {
 		if (n >= kMaxStages) QB_FAIL("transform length " + std::to_string(L) + " needs too many stages");
 		rad[n++] = r;
 	};
-	if (variant == 1) for (int i = 0; i < b; i++) push(3);
-	int e = a;
-	if (variant != 2) while (e >= 3) { push(8); e -= 3; }
-	while (e >= 2) { push(4); e -= 2; }
-	if (e == 1) push(2);
-	if (variant != 1) for (int i = 0; i < b; i++) push(3);
+	if (variant == 0) {
+		int left = L;
+		while (left > 1) {
+			for (int r : { 16, 12, 8, 6, 4, 3, 2 })
+				if (left % r == 0) { push(r); left /= r; break; }
+		}
+	} else {
+		if (variant == 2) for (int i = 0; i < b; i++) push(3);
+		int e = a;
+		if (variant != 3) while (e >= 3) { push(8); e -= 3; }
+		while (e >= 2) { push(4); e -= 2; }
+		if (e == 1) push(2);
+		if (variant != 2) for (int i = 0; i < b; i++) push(3);
+	}
 	p.nst = n;
 	for (int i = 0; i < n; i++) p.r[i] = rad[i];
 	return p;

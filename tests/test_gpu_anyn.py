@@ -132,3 +132,49 @@ print("ok")
         pytest.skip("no GPU")
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("bc", ["periodic", "dirichlet"])
+def test_inhomogeneous_strang_step_n24_vs_oracle(mods, bc):
+    """The inhomogeneous Strang step (transport, Fourier representation,
+    collision step, back, transport) at N = 24 through the any-N engine."""
+    torch, qbgpu, orc = mods
+    N, J, M, cells = 24, 4, 3, 5
+    ws, q = qbgpu.Workspace(N), qbgpu.Quad(N, J, M, L, R)
+    o = orc.Oracle(N, J, M, L, R)
+    Wv = qbgpu.gaussian_mixture_state(N, L, seed=240, ncells=cells)
+    Bext = np.random.default_rng(24).standard_normal((cells, 3)) * 0.2
+    h, dt = 1.0 / cells, 0.4 / cells / L
+    out = qbgpu.inhom_step(ws, q, torch.from_numpy(Wv).cuda(), h, dt, torch.from_numpy(Bext).cuda(), bc=bc).cpu().numpy()
+    want = o.inhom_step(Wv, h, dt, Bext, bc=bc)
+    assert rel_l1(out, want) < 1e-12
+
+
+def test_inhomogeneous_graph_replay_n48(mods):
+    """Strang steps at N = 48 that alternate two buffers replay their CUDA
+    graphs from the third call of each direction on, bit-identical to
+    kernel-by-kernel launches (profiling on)."""
+    torch, qbgpu, orc = mods
+    N, J, M, cells = 48, 4, 2, 3
+    q = qbgpu.Quad(N, J, M, L, R)
+    W0 = torch.from_numpy(qbgpu.gaussian_mixture_state(N, L, seed=48, ncells=cells)).cuda()
+    B = torch.zeros((cells, 3), dtype=torch.float64, device="cuda")
+    h, dt, steps = 1.0 / cells, 0.4 / cells / L, 8
+    ws = qbgpu.Workspace(N)
+    bufs = [W0.clone(), torch.empty_like(W0)]
+    for k in range(steps):
+        qbgpu.inhom_step(ws, q, bufs[k % 2], h, dt, B, out=bufs[(k + 1) % 2])
+    torch.cuda.synchronize()
+    assert ws.graph_replays == steps - 4
+    L_ = qbgpu.lib()
+    ref, wsd = W0.clone(), qbgpu.Workspace(N)
+    L_.qb_profile_enable(1)
+    try:
+        for k in range(steps):
+            ref = qbgpu.inhom_step(wsd, q, ref, h, dt, B)
+        torch.cuda.synchronize()
+    finally:
+        L_.qb_profile_enable(0)
+        L_.qb_profile_reset()
+    assert wsd.graph_replays == 0
+    assert torch.equal(bufs[steps % 2], ref)

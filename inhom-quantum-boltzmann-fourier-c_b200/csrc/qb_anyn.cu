@@ -102,13 +102,13 @@ template <int RAD, int DIR, class C> __device__ __forceinline__ void dft_r(C (&v
 	else dft2(v[0], v[1]);
 }
 
-// an R1 R2-point DFT in registers, natural order in and out: R2 DFTs of R1
-// points (stride R2), twiddles w_R^(n2 k1), R1 DFTs of R2 points; output
-// k1 + R1 k2
+// an R1 R2-point DFT in registers, in place: R2 DFTs of R1 points (stride
+// R2), twiddles w_R^(n2 k1), R1 DFTs of R2 points.  Input in natural order;
+// output frequency k1 + R1 k2 lands in slot k1 R2 + k2 (freq_of gives the
+// frequency of a slot), so no second array of R values is live
 template <int R1, int R2, int DIR, class C> __device__ __forceinline__ void dft_ct(C (&x)[R1 * R2]) {
 	using R = typename CT<C>::R;
 	constexpr int RR = R1 * R2;
-	C a[RR];
 #pragma unroll
 	for (int n2 = 0; n2 < R2; n2++) {
 		C v[R1];
@@ -119,12 +119,12 @@ template <int R1, int R2, int DIR, class C> __device__ __forceinline__ void dft_
 		for (int k1 = 0; k1 < R1; k1++) {
 			const int m = (n2 * k1) % RR;
 			if (m == 0) {
-				a[n2 * R1 + k1] = v[k1];
+				x[n2 + R2 * k1] = v[k1];
 			} else {
 				C w;
 				w.x = (R)cos_r(RR, m);
 				w.y = (R)(DIR < 0 ? -sin_r(RR, m) : sin_r(RR, m));
-				a[n2 * R1 + k1] = cmul(v[k1], w);
+				x[n2 + R2 * k1] = cmul(v[k1], w);
 			}
 		}
 	}
@@ -132,11 +132,20 @@ template <int R1, int R2, int DIR, class C> __device__ __forceinline__ void dft_
 	for (int k1 = 0; k1 < R1; k1++) {
 		C v[R2];
 #pragma unroll
-		for (int n2 = 0; n2 < R2; n2++) v[n2] = a[n2 * R1 + k1];
+		for (int n2 = 0; n2 < R2; n2++) v[n2] = x[k1 * R2 + n2];
 		dft_r<R2, DIR>(v);
 #pragma unroll
-		for (int k2 = 0; k2 < R2; k2++) x[k1 + R1 * k2] = v[k2];
+		for (int k2 = 0; k2 < R2; k2++) x[k1 * R2 + k2] = v[k2];
 	}
+}
+
+// frequency held in slot s after dft_r<RAD> (the composite radices leave
+// their output permuted; 2, 3, 4, 8 and the sub-DFTs are in natural order)
+template <int RAD> __host__ __device__ constexpr int freq_of(int s) {
+	if (RAD == 16) return s / 4 + 4 * (s % 4);
+	if (RAD == 12) return s / 3 + 4 * (s % 3);
+	if (RAD == 6) return s / 3 + 2 * (s % 3);
+	return s;
 }
 
 // one Stockham stage of radix RAD over nl lines of length L (sub-transforms of
@@ -175,7 +184,7 @@ __device__ __forceinline__ void stage(const C *in, C *out, int nl, int ls, int e
 		dft_r<RAD, DIR>(v);
 		const int ob = line * ls + (jq * Ns * RAD + k) * es;
 #pragma unroll
-		for (int r = 0; r < RAD; r++) out[sw(ob + r * Ns * es)] = v[r];
+		for (int r = 0; r < RAD; r++) out[sw(ob + freq_of<RAD>(r) * Ns * es)] = v[r];
 	}
 }
 
@@ -1081,7 +1090,10 @@ template <class C> struct AnyRhs {
 				I3FusedP<C> f{};
 				f.What = ws.What.as<C>(); f.Pg = Pg; f.X = ws.i3p.as<C>();
 				f.psi2T = Tabs<C>::i3_psi2T(t); f.idx = t.idx.as<int>(); f.scale = t.scale.as<double>();
-				f.N = N; f.nt = n; f.t0 = t0; f.pl = pl;
+				f.N = N; f.nt = n; f.t0 = t0;
+				// FP32 default: radix-8 stages (the radix-16 register DFTs push this
+				// kernel to 173 registers, one CTA an SM); FP64 runs one CTA an SM anyway
+				f.pl = (ws.anyn_plan == 0 && sizeof(C) == 8) ? make_plan(P, 1) : pl;
 				launch(k_any_i3_fused<C>, "any_i3_fused", (long)ncells * 16, tile_bytes<C>(P, P), s, f);
 			}
 			return nxp;

@@ -286,6 +286,15 @@ int qb_fno_get_params(const qb_fno *net, float *host);
 int qb_fno_set_params(qb_fno *net, const float *host);
 int qb_fno_set_scale(qb_fno *net, const double *scale);          /* 4 output scales (> 0) */
 int qb_fno_set_input_scale(qb_fno *net, const double *scale);    /* 14 input scales (> 0) */
+/* Extension, no counterpart in the reference: on != 0 runs the pointwise
+ * channel maps (the lift, each layer's W, the projection, and their
+ * transposes in the backward pass) on the tensor cores with BF16 operands and
+ * FP32 accumulation (tcgen05.mma, accumulator in tensor memory); the spectral
+ * parts and the weight gradients stay FP32.  Off by default. */
+int qb_fno_set_tensor_cores(qb_fno *net, int on);
+/* nonzero when a tensor-core MMA of the network did not complete within its
+ * poll limit (its outputs are then undefined); 0 otherwise */
+int qb_fno_device_errors(const qb_fno *net);
 /* C[b] ~ C[W[b]] for `batch` cells */
 int qb_fno_forward(qb_fno *net, int batch, const double *W, double *C, void *stream);
 /* loss = mean over all outputs of (y - target / scale)^2 (y: the unscaled

@@ -825,6 +825,7 @@ void check_tmem_coresidency() {
 		{ (const void *)k_i3_full128r, kFull128Smem, F128::NT, (int)F128TmemR::NCOLS, "k_i3_full128r" },
 	};
 	for (const TmemKernel &k : dftmma_tmem_kernels()) ks.push_back(k);
+	for (const TmemKernel &k : fno_tmem_kernels()) ks.push_back(k);
 	const int n = (int)ks.size();
 	int dev = 0, sm_smem = 0, sm_regs = 0, sm_threads = 0, sm_blocks = 0, reserved = 0;
 	QB_CUDA(cudaGetDevice(&dev));
@@ -866,6 +867,10 @@ void check_tmem_coresidency() {
 	dfs.go(0, 0, 0, 0, 0, 0);
 	done = true;
 }
+
+}  // namespace
+void ensure_tmem_coresidency() { check_tmem_coresidency(); }
+namespace {
 
 template <class C> void launch_assemble128(const AsmParamsT<C> &p, long ncells, cudaStream_t s) {
 	static DeviceFlag init;

@@ -131,6 +131,10 @@ struct Workspace {
 // a kernel that allocates tensor memory, for the co-residency check
 struct TmemKernel { const void *fn; size_t dyn_smem; int threads; int cols; const char *name; };
 std::vector<TmemKernel> dftmma_tmem_kernels();
+std::vector<TmemKernel> fno_tmem_kernels();
+// before the first launch of a tensor-memory kernel on a device: no set of
+// tensor-memory kernels that can share an SM asks for more than 512 columns
+void ensure_tmem_coresidency();
 
 // chunking of the quadrature-term sums over CTAs (picked per launch shape)
 struct Chunks {

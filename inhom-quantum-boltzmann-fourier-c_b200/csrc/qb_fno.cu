@@ -20,6 +20,10 @@
 // 1/N^2).  Every reduction (loss, weight gradients) is a fixed-order tree or
 // a per-chunk partial sum reduced in order: results are deterministic.
 #include "qb_engine.h"
+#include "qb_kernels.cuh"
+#include "qb_umma.cuh"
+
+#include <cuda_bf16.h>
 
 extern "C" {
 #include "qbgpu.h"
@@ -324,7 +328,150 @@ __global__ void k_fno_adam(long n, float *__restrict__ w, const float *__restric
 	}
 }
 
+// ---------------------------------------------------------------------------
+// The pointwise channel maps on the tensor cores (BF16 operands, FP32
+// accumulation): for the points of a tile of 128 (rows of the flattened
+// (b, p) index) D[row][n] = sum_k X[row][k] Wt[n][k] with one tcgen05.mma
+// of M = 128, N = npad, K = 16 per step.
+//   trans = 0 (forward map): X = in[b][k][p] (k < kin = cin), Wt[n][k] = M[n cin + k],
+//            out = D + bias (+ add); act: uout = u, hout = gelu(u), else hout = u;
+//   trans = 1 (its transpose, backward): X = in[b][k][p] (k < kin = cout),
+//            Wt[n][k] = M[k cin + n] (n < nout = cin), hout = D.
+// A (128 x 64 BF16) and B (npad x 64 BF16) are K-major with the 128-byte
+// swizzle; D is 64 FP32 columns of tensor memory, row r in lane r, read back
+// by the thread of that row.  Persistent CTAs of 128 threads stride over the
+// tiles.  The MMA completion wait is bounded; a wait that runs out sets the
+// error word and leaves the outputs of that tile undefined.
+namespace fnomma {
+constexpr int kThreads = 128, kRows = 128, kMaxK = 64, kCols = 64;
+constexpr uint32_t oA = 0, oB = kRows * 128, kUsed = oB + kMaxK * 128;
+// dynamic shared memory: the operands, 1024-byte alignment slack, and enough
+// more that at most 7 CTAs share an SM (7 x 64 tensor-memory columns <= 512)
+constexpr uint32_t kSmem = 33 * 1024;
+static_assert(kUsed + 1024 <= kSmem, "operand tiles fit");
+constexpr unsigned kPolls = 1u << 24;
+}  // namespace fnomma
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+	__nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+	return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__global__ void __launch_bounds__(fnomma::kThreads) k_fno_pointwise_mma(int B, int P, int cin, int cout, int trans,
+                                                                         const float *__restrict__ in, const float *__restrict__ M,
+                                                                         const float *__restrict__ bias, const float *__restrict__ add,
+                                                                         float *__restrict__ uout, float *__restrict__ hout, int act,
+                                                                         int *err) {
+	using namespace fnomma;
+	using namespace qb;
+	extern __shared__ unsigned char smem_raw[];
+	unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+	__shared__ uint64_t mbar;
+	__shared__ uint32_t tslot;
+	__shared__ int abort_flag;
+	const int tid = threadIdx.x, warp = tid >> 5;
+	const int kin = trans ? cout : cin, nout = trans ? cin : cout;
+	const int kpad = (kin + 15) & ~15, npad = (nout + 15) & ~15;
+	// B: the weights as Wt[n][k], BF16, zero beyond (nout, kin)
+	for (int i = tid; i < kMaxK * (kMaxK / 2); i += kThreads) {
+		const int n = i / (kMaxK / 2), k = 2 * (i % (kMaxK / 2));
+		float w0 = 0.0f, w1 = 0.0f;
+		if (n < nout) {
+			if (k < kin) w0 = trans ? M[k * cin + n] : M[n * cin + k];
+			if (k + 1 < kin) w1 = trans ? M[(k + 1) * cin + n] : M[n * cin + k + 1];
+		}
+		*reinterpret_cast<uint32_t *>(base + oB + umma::kmajor_off16(n, k)) = pack_bf16x2(w0, w1);
+	}
+	if (tid == 0) {
+		umma::mbar_init(&mbar, 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		abort_flag = 0;
+	}
+	if (warp == 0) tmem_alloc(&tslot, kCols);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const uint32_t tmem = tslot;
+	const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);      // this warp's 32 lanes
+	uint32_t idesc = 0;
+	switch (npad) {
+	case 16: idesc = umma::idesc_bf16<128, 16>(); break;
+	case 32: idesc = umma::idesc_bf16<128, 32>(); break;
+	case 48: idesc = umma::idesc_bf16<128, 48>(); break;
+	default: idesc = umma::idesc_bf16<128, 64>(); break;
+	}
+	const long rows = (long)B * P, ntiles = (rows + kRows - 1) / kRows;
+	unsigned phase = 0;
+	for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+		const long row = tile * kRows + tid;
+		const bool live = row < rows;
+		const long b = live ? row / P : 0, p = live ? row % P : 0;
+		// A: this thread's row (its point), BF16, zero beyond kin
+		const float *x = in + b * (long)kin * P + p;
+#pragma unroll 4
+		for (int k = 0; k < kMaxK; k += 2) {
+			const float x0 = (live && k < kin) ? x[(long)k * P] : 0.0f;
+			const float x1 = (live && k + 1 < kin) ? x[(long)(k + 1) * P] : 0.0f;
+			*reinterpret_cast<uint32_t *>(base + oA + umma::kmajor_off16(tid, k)) = pack_bf16x2(x0, x1);
+		}
+		umma::fence_async_smem();
+		tmem_fence_before();
+		__syncthreads();
+		tmem_fence_after();
+		if (tid == 0) {
+			const uint32_t a0 = umma::smem_u32(base + oA), b0 = umma::smem_u32(base + oB);
+			for (int k = 0; k < kpad; k += 16)
+				umma::mma_f16(tmem, umma::desc_sw128(a0 + 2 * k, 16, 1024), umma::desc_sw128(b0 + 2 * k, 16, 1024), idesc, k > 0 ? 1u : 0u);
+			umma::commit(&mbar);
+		}
+		if (!abort_flag && !umma::mbar_wait(&mbar, phase, kPolls)) {
+			abort_flag = 1;
+			if (err) atomicExch(err, 1);
+		}
+		phase ^= 1u;
+		tmem_fence_after();
+		// epilogue: this thread's row of D, 16 columns at a time
+		for (int n0 = 0; n0 < npad; n0 += 16) {
+			float d[16];
+			umma::tmem_ld16(trow + (uint32_t)n0, d);
+			asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+			if (!live) continue;
+#pragma unroll
+			for (int j = 0; j < 16; j++) {
+				const int n = n0 + j;
+				if (n >= nout) break;
+				const long oi = (b * nout + n) * (long)P + p;
+				float v = d[j];
+				if (!trans) {
+					if (bias) v += bias[n];
+					if (add) v += add[oi];
+					if (uout) uout[oi] = v;
+					hout[oi] = act ? gelu_f(v) : v;
+				} else {
+					hout[oi] = v;
+				}
+			}
+		}
+		tmem_fence_before();
+		__syncthreads();                      // D read and A free before the next tile's MMA
+		tmem_fence_after();
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tmem, kCols);
+}
+
 unsigned grid_for(long n) { return (unsigned)std::max<long>(1, std::min<long>((n + 255) / 256, 148L * 32)); }
+
+}  // namespace
+
+// the tensor-memory kernel of this file, for the engine's co-residency check
+std::vector<qb::TmemKernel> qb::fno_tmem_kernels() {
+	return { { (const void *)k_fno_pointwise_mma, fnomma::kSmem, fnomma::kThreads, fnomma::kCols, "k_fno_pointwise_mma" } };
+}
+
+namespace {
 
 // every launch is counted (and timed while profiling is on) under its kernel's name
 template <class... P, class... A>
@@ -347,8 +494,41 @@ struct qb_fno {
 	qb::DevBuf x, y, dy, dh, tmp, lossp, partial;
 	std::vector<qb::DevBuf> h, u, H;             // h[0..L], u[0..L-1], H[0..L-1]
 	qb::DevBuf GO, GH;
+	int use_tc = 0;                               // pointwise maps on the tensor cores (BF16, FP32 accumulation)
+	qb::DevBuf kerr;                              // error word of the bounded MMA waits
 
 	float *P_(long o) { return params.as<float>() + o; }
+
+	// out = M in + bias (+ add), gelu when act (uout keeps the pre-activation)
+	void pointwise(int B, int cin, int cout, const float *in, const float *M, const float *bias, const float *add, float *uout,
+	               float *hout, int act, cudaStream_t s) {
+		if (use_tc) pointwise_mma(B, cin, cout, 0, in, M, bias, add, uout, hout, act, s);
+		else launch("fno_pointwise", k_fno_pointwise, grid_for((long)B * P), 256, 0, s, B, P, cin, cout, in, M, bias, add, uout, hout, act);
+	}
+	// out = M^T in (the backward of a pointwise map)
+	void pointwise_t(int B, int cin, int cout, const float *in, const float *M, float *out, cudaStream_t s) {
+		if (use_tc) pointwise_mma(B, cin, cout, 1, in, M, nullptr, nullptr, nullptr, out, 0, s);
+		else launch("fno_pointwise_t", k_fno_pointwise_t, grid_for((long)B * P), 256, 0, s, B, P, cin, cout, in, M, out);
+	}
+	void pointwise_mma(int B, int cin, int cout, int trans, const float *in, const float *M, const float *bias, const float *add,
+	                   float *uout, float *hout, int act, cudaStream_t s) {
+		static int attr_done[64] = {};
+		int dev = 0;
+		QB_CUDA(cudaGetDevice(&dev));
+		if (!attr_done[dev & 63]) {
+			qb::ensure_tmem_coresidency();
+			QB_CUDA(cudaFuncSetAttribute(k_fno_pointwise_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fnomma::kSmem));
+			attr_done[dev & 63] = 1;
+		}
+		if (kerr.p == nullptr) {
+			kerr.ensure(sizeof(int));
+			QB_CUDA(cudaMemsetAsync(kerr.p, 0, sizeof(int), s));
+		}
+		const long tiles = ((long)B * P + fnomma::kRows - 1) / fnomma::kRows;
+		const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(tiles, 148L * 7));
+		launch("fno_pointwise_mma", k_fno_pointwise_mma, grid, fnomma::kThreads, (size_t)fnomma::kSmem, s, B, P, cin, cout, trans, in, M,
+		       bias, add, uout, hout, act, kerr.as<int>());
+	}
 	float *G_(long o) { return grads.as<float>() + o; }
 
 	void reserve(int B) {
@@ -378,15 +558,15 @@ struct qb_fno {
 	void forward(int B, const double *W, cudaStream_t s) {
 		reserve(B);
 		launch("fno_in", k_fno_in, grid_for((long)B * P), 256, 0, s, B, P, W, inscale, x.as<float>());
-		launch("fno_pointwise", k_fno_pointwise, grid_for((long)B * P), 256, 0, s, B, P, kFnoIn, w, x.as<float>(), P_(off.A), P_(off.a), nullptr, nullptr, h[0].as<float>(), 0);
+		pointwise(B, kFnoIn, w, x.as<float>(), P_(off.A), P_(off.a), nullptr, nullptr, h[0].as<float>(), 0, s);
 		for (int l = 0; l < L; l++) {
 			launch("fno_dft", k_fno_dft, (unsigned)(B * w), 256, dft_smem(), s, N, m, h[l].as<float>(), H[l].as<float2>(), 1.0f);
 			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, H[l].as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GO.as<float2>(), 0);
 			launch("fno_idft", k_fno_idft, (unsigned)(B * w), 256, idft_smem(), s, N, m, GO.as<float2>(), tmp.as<float>(), 1.0f / (float)P, 0);
-			launch("fno_pointwise", k_fno_pointwise, grid_for((long)B * P), 256, 0, s, B, P, w, w, h[l].as<float>(), P_(off.W[l]), P_(off.b[l]), tmp.as<float>(),
-			                                                      u[l].as<float>(), h[l + 1].as<float>(), l < L - 1 ? 1 : 0);
+			pointwise(B, w, w, h[l].as<float>(), P_(off.W[l]), P_(off.b[l]), tmp.as<float>(), u[l].as<float>(), h[l + 1].as<float>(),
+			          l < L - 1 ? 1 : 0, s);
 		}
-		launch("fno_pointwise", k_fno_pointwise, grid_for((long)B * P), 256, 0, s, B, P, w, 4, h[L].as<float>(), P_(off.Q), P_(off.q), nullptr, nullptr, y.as<float>(), 0);
+		pointwise(B, w, 4, h[L].as<float>(), P_(off.Q), P_(off.q), nullptr, nullptr, y.as<float>(), 0, s);
 		QB_CUDA(cudaGetLastError());
 	}
 
@@ -406,7 +586,7 @@ struct qb_fno {
 		launch("fno_loss", k_fno_loss, lb, 256, 0, s, B, P, y.as<float>(), target, scale[0], scale[1], scale[2], scale[3], dy.as<float>(), lossp.as<double>());
 		// projection
 		pw_grads(B, w, 4, h[L].as<float>(), dy.as<float>(), off.Q, off.q, s);
-		launch("fno_pointwise_t", k_fno_pointwise_t, grid_for((long)B * P), 256, 0, s, B, P, w, 4, dy.as<float>(), P_(off.Q), dh.as<float>());
+		pointwise_t(B, w, 4, dy.as<float>(), P_(off.Q), dh.as<float>(), s);
 		for (int l = L - 1; l >= 0; l--) {
 			if (l < L - 1) launch("fno_gelu_bwd", k_fno_gelu_bwd, grid_for(nw), 256, 0, s, nw, u[l].as<float>(), dh.as<float>());
 			// dh now holds du
@@ -414,7 +594,7 @@ struct qb_fno {
 			launch("fno_dft", k_fno_dft, (unsigned)(B * w), 256, dft_smem(), s, N, m, dh.as<float>(), GO.as<float2>(), 1.0f / (float)P);
 			launch("fno_rgrad", k_fno_rgrad, grid_for((long)w * w * K), 256, 0, s, B, w, K, GO.as<float2>(), H[l].as<float2>(), G_(off.Rr[l]), G_(off.Ri[l]));
 			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, GO.as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GH.as<float2>(), 1);
-			launch("fno_pointwise_t", k_fno_pointwise_t, grid_for((long)B * P), 256, 0, s, B, P, w, w, dh.as<float>(), P_(off.W[l]), tmp.as<float>());
+			pointwise_t(B, w, w, dh.as<float>(), P_(off.W[l]), tmp.as<float>(), s);
 			launch("fno_idft", k_fno_idft, (unsigned)(B * w), 256, idft_smem(), s, N, m, GH.as<float2>(), tmp.as<float>(), 1.0f, 1);
 			std::swap(dh, tmp);
 		}
@@ -528,6 +708,20 @@ int qb_fno_set_input_scale(qb_fno *net, const double *scale) {
 			net->inscale.s[f] = scale[f];
 		}
 	});
+}
+
+int qb_fno_set_tensor_cores(qb_fno *net, int on) {
+	return fno_guard([&] {
+		if (net == nullptr) QB_FAIL("qb_fno_set_tensor_cores: null network");
+		net->use_tc = on ? 1 : 0;
+	});
+}
+
+int qb_fno_device_errors(const qb_fno *net) {
+	int h = 0;
+	if (net == nullptr || net->kerr.p == nullptr) return 0;
+	if (cudaMemcpy(&h, net->kerr.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+	return h;
 }
 
 int qb_fno_forward(qb_fno *net, int batch, const double *W, double *C, void *stream) {

@@ -38,6 +38,33 @@ __host__ __device__ constexpr uint32_t idesc_tf32() {
 	return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// instruction descriptor of kind::f16 with BF16 operands and FP32
+// accumulation: D format F32 (bits 4-5 = 1), A and B format BF16 (bits 7-9,
+// 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+template <int M, int N>
+__host__ __device__ constexpr uint32_t idesc_bf16() {
+	static_assert(M == 128, "one-CTA M = 128 tiles (row m of D in tensor-memory lane m)");
+	static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N of a kind::f16 MMA with M = 128");
+	return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[desc] x B[desc], 16-bit operands (one K step: 16 elements); one thread issues
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, uint32_t accumulate) {
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "setp.ne.b32 p, %4, 0;\n\t"
+	    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+	    "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+	    : "memory");
+}
+
+// byte offset of 16-bit element (row r, k), k < 64, of a K-major 128B-swizzled
+// tile: row r at (r / 8) * 1024 + (r % 8) * 128, 16-byte chunk k / 8 at
+// ((k / 8) ^ (r % 8)) * 16; a K step of 16 elements starts 32 bytes further
+__host__ __device__ constexpr uint32_t kmajor_off16(int r, int k) {
+	return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) & 7) ^ (r & 7)) << 4) + (k & 7) * 2);
+}
+
 // D[tmem] (+)= A[desc] x B[desc]; issued by one thread
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, uint32_t accumulate) {
 	asm volatile(

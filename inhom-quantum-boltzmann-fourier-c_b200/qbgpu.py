@@ -97,6 +97,8 @@ def lib(n_grid=N_GRID):
     L.qb_fno_set_scale.argtypes = [_vp, _vp]
     L.qb_fno_set_input_scale.argtypes = [_vp, _vp]
     L.qb_fno_forward.argtypes = [_vp, C.c_int, _vp, _vp, _vp]
+    L.qb_fno_set_tensor_cores.argtypes = [_vp, C.c_int]
+    L.qb_fno_device_errors.argtypes = [_vp]
     L.qb_fno_gradients.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
     L.qb_fno_train_step.argtypes = [_vp, C.c_int, _vp, _vp, C.c_float, _vp, _vp]
     L.qb_surrogate_create.restype = _vp
@@ -352,6 +354,15 @@ class FNO:
         ry = np.sqrt(np.mean(np.asarray(Y, dtype=np.float64).reshape(Y.shape[0], 4, -1) ** 2, axis=(0, 2)))
         self.set_input_scale(1.0 / np.where(rx > 0, rx, 1.0))
         self.set_scale(np.where(ry > 0, ry, 1.0))
+
+    def set_tensor_cores(self, on=True):
+        """pointwise channel maps on the tensor cores (BF16 operands, FP32
+        accumulation) when on; FP32 on the CUDA cores otherwise (the default)"""
+        _check(lib().qb_fno_set_tensor_cores(self.h, 1 if on else 0), "qb_fno_set_tensor_cores")
+
+    def device_errors(self):
+        """nonzero when a tensor-core MMA did not complete within its poll limit"""
+        return int(lib().qb_fno_device_errors(self.h))
 
     def forward(self, W, out=None):
         """C~[W] for float64 CUDA states W (B, 4, N, N)"""

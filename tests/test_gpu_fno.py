@@ -69,6 +69,42 @@ def test_forward_and_gradients_match_oracle():
     assert not np.array_equal(net.get_params(), theta.astype(np.float32))
 
 
+@pytest.mark.parametrize("N,w,m,Ly,B", [(16, 8, 4, 3, 3), (32, 32, 12, 4, 5)])
+def test_tensor_core_pointwise_maps_against_oracle(N, w, m, Ly, B):
+    """The pointwise channel maps on the tensor cores (BF16 operands, FP32
+    accumulation): forward pass and weight gradients against the float64
+    restatement within BF16 accuracy (inputs and weights rounded to 8
+    significant bits), the MMA waits complete, and the FP32 path is untouched."""
+    net = qbgpu.FNO(N, width=w, modes=m, layers=Ly, seed=7)
+    W = mixture_states(N, B, seed=13)
+    rng = np.random.default_rng(9)
+    target = rng.standard_normal((B, 4, N, N)) * 0.1
+    inscale = np.linspace(0.5, 2.0, fno_ref.NFEAT)
+    scale = np.array([0.1, 0.2, 0.05, 0.3])
+    net.set_input_scale(inscale)
+    net.set_scale(scale)
+    theta = net.get_params().astype(np.float64)
+    x = fno_ref.features(W, inscale)
+    y_ref = fno_ref.forward(theta, x, N, w, m, Ly) * scale[None, :, None]
+    Wd = torch.from_numpy(W).cuda()
+    y32 = net.forward(Wd).cpu().numpy().reshape(B, 4, -1)
+    net.set_tensor_cores(True)
+    ytc = net.forward(Wd).cpu().numpy().reshape(B, 4, -1)
+    assert net.device_errors() == 0
+    e_tc, e_32 = rel_l2(ytc, y_ref), rel_l2(y32, y_ref)
+    assert e_32 < 1e-5
+    assert 1e-5 < e_tc < 2e-2, e_tc
+    loss, g = net.gradients(Wd, torch.from_numpy(target).cuda())
+    loss_ref, g_ref = fno_ref.loss_and_grads(theta, x, target, scale, N, w, m, Ly)
+    assert abs(loss - loss_ref) <= 3e-2 * loss_ref
+    gd, gr = fno_ref.unflatten(g.astype(np.float64), w, m, Ly), fno_ref.unflatten(g_ref, w, m, Ly)
+    for name in gr:
+        assert rel_l2(gd[name], gr[name]) < 5e-2, name
+    assert net.device_errors() == 0
+    net.set_tensor_cores(False)
+    assert np.array_equal(net.forward(Wd).cpu().numpy().reshape(B, 4, -1), y32)
+
+
 def test_parameters_roundtrip_and_bad_arguments():
     net = qbgpu.FNO(8, width=4, modes=2, layers=1, seed=1)
     p = net.get_params()

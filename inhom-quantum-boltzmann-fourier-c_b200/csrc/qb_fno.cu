@@ -462,13 +462,180 @@ __global__ void __launch_bounds__(fnomma::kThreads) k_fno_pointwise_mma(int B, i
 	if (warp == 0) tmem_dealloc(tmem, kCols);
 }
 
+// ---------------------------------------------------------------------------
+// A row GEMM on the tensor cores (BF16 operands, FP32 accumulation) for the
+// separable truncated DFTs: for 128-row tiles of `rows` rows,
+// D[row][n] = sum_k A[row][k] Bm[n][k], k < K <= 128, n < Nn <= 128, with A
+// read through the loader ld(row, k) and every row of D handed whole to the
+// epilogue ep(row, d).  Bm is an FP32 [Nn][K] matrix in global memory (the
+// twiddles).  Operands K-major with the 128-byte swizzle in two 64-element
+// atoms; D in 128 tensor-memory columns.  Persistent CTAs of 128 threads; the
+// MMA completion wait is bounded (a wait that runs out sets the error word).
+namespace fnotc {
+constexpr int kThreads = 128, kRows = 128, kMaxK = 128, kMaxN = 128, kCols = 128;
+constexpr uint32_t oA = 0, oB = kRows * kMaxK * 2, kUsed = oB + kMaxN * kMaxK * 2;
+// operands, alignment slack, and enough more that at most 3 CTAs share an SM (3 x 128 columns <= 512)
+constexpr uint32_t kSmem = 72 * 1024;
+static_assert(kUsed + 1024 <= kSmem, "operand tiles fit");
+constexpr unsigned kPolls = 1u << 24;
+__host__ __device__ constexpr uint32_t off(int R, int r, int k) {
+	return (uint32_t)((k >> 6) * R * 128) + qb::umma::kmajor_off16(r, k & 63);
+}
+}  // namespace fnotc
+
+template <class Ld, class Ep>
+__global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const Ep ep, long rows, int K, int Nn, const float *__restrict__ Bm,
+                                                             int *err) {
+	using namespace fnotc;
+	using namespace qb;
+	extern __shared__ unsigned char smem_raw[];
+	unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+	__shared__ uint64_t mbar;
+	__shared__ uint32_t tslot;
+	__shared__ int abort_flag;
+	const int tid = threadIdx.x, warp = tid >> 5;
+	const int kpad = (K + 15) & ~15, npad = (Nn + 15) & ~15;
+	for (int i = tid; i < npad * (kpad / 2); i += kThreads) {
+		const int n = i / (kpad / 2), k = 2 * (i % (kpad / 2));
+		const float b0 = (n < Nn && k < K) ? Bm[(long)n * K + k] : 0.0f;
+		const float b1 = (n < Nn && k + 1 < K) ? Bm[(long)n * K + k + 1] : 0.0f;
+		*reinterpret_cast<uint32_t *>(base + oB + off(npad, n, k)) = pack_bf16x2(b0, b1);
+	}
+	if (tid == 0) {
+		umma::mbar_init(&mbar, 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		abort_flag = 0;
+	}
+	if (warp == 0) tmem_alloc(&tslot, kCols);
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	const uint32_t tmem = tslot;
+	const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+	const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+	const long ntiles = (rows + kRows - 1) / kRows;
+	unsigned phase = 0;
+	for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+		const long row = tile * kRows + tid;
+		const bool live = row < rows;
+		for (int k = 0; k < kpad; k += 2) {
+			const float x0 = (live && k < K) ? ld(row, k) : 0.0f;
+			const float x1 = (live && k + 1 < K) ? ld(row, k + 1) : 0.0f;
+			*reinterpret_cast<uint32_t *>(base + oA + off(kRows, tid, k)) = pack_bf16x2(x0, x1);
+		}
+		umma::fence_async_smem();
+		tmem_fence_before();
+		__syncthreads();
+		tmem_fence_after();
+		if (tid == 0) {
+			const uint32_t a0 = umma::smem_u32(base + oA), b0 = umma::smem_u32(base + oB);
+			for (int k = 0; k < kpad; k += 16) {
+				const uint32_t ao = (uint32_t)((k >> 6) * kRows * 128 + (k & 63) * 2);
+				const uint32_t bo = (uint32_t)((k >> 6) * npad * 128 + (k & 63) * 2);
+				umma::mma_f16(tmem, umma::desc_sw128(a0 + ao, 16, 1024), umma::desc_sw128(b0 + bo, 16, 1024), idesc, k > 0 ? 1u : 0u);
+			}
+			umma::commit(&mbar);
+		}
+		if (!abort_flag && !umma::mbar_wait(&mbar, phase, kPolls)) {
+			abort_flag = 1;
+			if (err) atomicExch(err, 1);
+		}
+		phase ^= 1u;
+		tmem_fence_after();
+		float d[kMaxN];
+#pragma unroll
+		for (int c = 0; c < kMaxN / 16; c++) {
+			if (16 * c < npad) {
+				float v[16];
+				umma::tmem_ld16(trow + (uint32_t)(16 * c), v);
+				asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+				for (int j = 0; j < 16; j++) d[16 * c + j] = v[j];
+			}
+		}
+		if (live) ep(row, d);
+		tmem_fence_before();
+		__syncthreads();
+		tmem_fence_after();
+	}
+	tmem_fence_before();
+	__syncthreads();
+	tmem_fence_after();
+	if (warp == 0) tmem_dealloc(tmem, kCols);
+}
+
+// the truncated DFT of a field f (N x N real) to H (K complex, kx in [-m+1, m-1],
+// ky in [0, m)) as two row GEMMs:
+//   1. along kv: T[fld][ky][l] = sum_kv f[fld][l][kv] e^{-2 pi i ky kv / N}   (rows (fld, l), K = N, Nn = 2m)
+//   2. along l:  H[fld][kx][ky] = scale sum_l T[fld][ky][l] e^{-2 pi i kx l / N} (rows (fld, ky), K = 2N, Nn = 2(2m-1))
+// and its inverse out[fld][l][kv] (=, +=) scale Re sum_k O[fld][k] e^{+i theta}:
+//   A. along kx: U[fld][l][ky] = sum_kx O[fld][kx][ky] e^{+2 pi i kx l / N}      (rows (fld, ky), K = 2(2m-1), Nn = 2N)
+//   B. along ky: out = scale Re sum_ky U[fld][l][ky] e^{+2 pi i ky kv / N}        (rows (fld, l), K = 2m, Nn = N)
+struct LdDft1 { const float *f; int N; __device__ float operator()(long row, int k) const { return f[row * N + k]; } };
+struct EpDft1 {
+	float *T; int N, m;
+	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+		const long fld = row / N;
+		const int l = (int)(row % N);
+		for (int ky = 0; ky < m; ky++) {
+			float *t = T + (fld * m + ky) * 2L * N;
+			t[l] = d[ky];
+			t[N + l] = d[m + ky];
+		}
+	}
+};
+struct LdDft2 { const float *T; int N; __device__ float operator()(long row, int k) const { return T[row * 2L * N + k]; } };
+struct EpDft2 {
+	float2 *H; int m; float scale;
+	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+		const int K = (2 * m - 1) * m, nk = 2 * m - 1;
+		const long fld = row / m;
+		const int ky = (int)(row % m);
+		for (int kxi = 0; kxi < nk; kxi++) H[fld * K + kxi * m + ky] = make_float2(scale * d[kxi], scale * d[nk + kxi]);
+	}
+};
+struct LdIdftA {
+	const float2 *O; int m;
+	__device__ float operator()(long row, int k) const {
+		const int K = (2 * m - 1) * m, nk = 2 * m - 1;
+		const long fld = row / m;
+		const int ky = (int)(row % m);
+		const float2 o = O[fld * K + (k % nk) * m + ky];
+		return k < nk ? o.x : o.y;
+	}
+};
+struct EpIdftA {
+	float *U; int N, m;
+	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+		const long fld = row / m;
+		const int ky = (int)(row % m);
+		for (int l = 0; l < N; l++) {
+			float *u = U + (fld * N + l) * 2L * m;
+			u[ky] = d[l];
+			u[m + ky] = d[N + l];
+		}
+	}
+};
+struct LdIdftB { const float *U; int m; __device__ float operator()(long row, int k) const { return U[row * 2L * m + k]; } };
+struct EpIdftB {
+	float *out; int N; float scale; int accumulate;
+	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+		float *o = out + row * N;           // row = fld N + l: out[fld][l][kv]
+		for (int kv = 0; kv < N; kv++) o[kv] = accumulate ? o[kv] + scale * d[kv] : scale * d[kv];
+	}
+};
+
 unsigned grid_for(long n) { return (unsigned)std::max<long>(1, std::min<long>((n + 255) / 256, 148L * 32)); }
 
 }  // namespace
 
 // the tensor-memory kernel of this file, for the engine's co-residency check
 std::vector<qb::TmemKernel> qb::fno_tmem_kernels() {
-	return { { (const void *)k_fno_pointwise_mma, fnomma::kSmem, fnomma::kThreads, fnomma::kCols, "k_fno_pointwise_mma" } };
+	return { { (const void *)k_fno_pointwise_mma, fnomma::kSmem, fnomma::kThreads, fnomma::kCols, "k_fno_pointwise_mma" },
+	         { (const void *)k_fno_tc<LdDft1, EpDft1>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<dft 1>" },
+	         { (const void *)k_fno_tc<LdDft2, EpDft2>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<dft 2>" },
+	         { (const void *)k_fno_tc<LdIdftA, EpIdftA>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<idft A>" },
+	         { (const void *)k_fno_tc<LdIdftB, EpIdftB>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<idft B>" } };
 }
 
 namespace {
@@ -494,8 +661,85 @@ struct qb_fno {
 	qb::DevBuf x, y, dy, dh, tmp, lossp, partial;
 	std::vector<qb::DevBuf> h, u, H;             // h[0..L], u[0..L-1], H[0..L-1]
 	qb::DevBuf GO, GH;
-	int use_tc = 0;                               // pointwise maps on the tensor cores (BF16, FP32 accumulation)
+	int use_tc = 0;                               // pointwise maps and truncated DFTs on the tensor cores (BF16, FP32 accumulation)
 	qb::DevBuf kerr;                              // error word of the bounded MMA waits
+	qb::DevBuf twm, tscr, uscr;                   // tensor-core DFTs: the 4 twiddle matrices, stage scratch
+	const float *Bm1 = nullptr, *Bm2 = nullptr, *BmA = nullptr, *BmB = nullptr;
+
+	// the twiddle matrices of the two-stage DFT and inverse (FP32 [Nn][K], from FP64)
+	void build_twiddles(cudaStream_t s) {
+		if (twm.p != nullptr) return;
+		const int nk = 2 * m - 1;
+		const long n1 = 2L * m * N, n2 = 2L * nk * 2 * N, nA = 2L * N * 2 * nk, nB = (long)N * 2 * m;
+		std::vector<float> h(n1 + n2 + nA + nB);
+		auto c = [&](long a) { return (float)std::cos(2.0 * M_PI * (double)a / N); };
+		auto sn = [&](long a) { return (float)std::sin(2.0 * M_PI * (double)a / N); };
+		float *b1 = h.data(), *b2 = b1 + n1, *bA = b2 + n2, *bB = bA + nA;
+		for (int n = 0; n < m; n++)
+			for (int kv = 0; kv < N; kv++) { b1[n * N + kv] = c((long)n * kv); b1[(m + n) * N + kv] = -sn((long)n * kv); }
+		for (int kxi = 0; kxi < nk; kxi++) {
+			const int kx = kxi - (m - 1);
+			for (int l = 0; l < N; l++) {
+				const long a = (long)kx * l;
+				b2[kxi * 2L * N + l] = c(a);         b2[kxi * 2L * N + N + l] = sn(a);
+				b2[(nk + kxi) * 2L * N + l] = -sn(a); b2[(nk + kxi) * 2L * N + N + l] = c(a);
+				bA[l * 2L * nk + kxi] = c(a);        bA[l * 2L * nk + nk + kxi] = -sn(a);
+				bA[(N + l) * 2L * nk + kxi] = sn(a); bA[(N + l) * 2L * nk + nk + kxi] = c(a);
+			}
+		}
+		for (int kv = 0; kv < N; kv++)
+			for (int ky = 0; ky < m; ky++) { bB[kv * 2L * m + ky] = c((long)ky * kv); bB[kv * 2L * m + m + ky] = -sn((long)ky * kv); }
+		twm.ensure(sizeof(float) * h.size());
+		QB_CUDA(cudaMemcpyAsync(twm.p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, s));
+		QB_CUDA(cudaStreamSynchronize(s));
+		Bm1 = twm.as<float>(); Bm2 = Bm1 + n1; BmA = Bm2 + n2; BmB = BmA + nA;
+	}
+
+	template <class Ld, class Ep> void row_gemm(const char *name, const Ld &ld, const Ep &ep, long rows, int K, int Nn, const float *Bm,
+	                                            cudaStream_t s) {
+		static int attr_done[64] = {};
+		int dev = 0;
+		QB_CUDA(cudaGetDevice(&dev));
+		if (!attr_done[dev & 63]) {
+			qb::ensure_tmem_coresidency();
+			QB_CUDA(cudaFuncSetAttribute(k_fno_tc<Ld, Ep>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fnotc::kSmem));
+			attr_done[dev & 63] = 1;
+		}
+		const long tiles = (rows + fnotc::kRows - 1) / fnotc::kRows;
+		const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(tiles, 148L * 3));
+		launch(name, k_fno_tc<Ld, Ep>, grid, fnotc::kThreads, (size_t)fnotc::kSmem, s, ld, ep, rows, K, Nn, Bm, kerr.as<int>());
+	}
+
+	// H[fld] = scale DFT(f[fld]) for the B w fields
+	void dft(int B, const float *f, float2 *Hout, float scale, cudaStream_t s) {
+		if (!use_tc) {
+			launch("fno_dft", k_fno_dft, (unsigned)(B * w), 256, dft_smem(), s, N, m, f, Hout, scale);
+			return;
+		}
+		ensure_err(s);
+		build_twiddles(s);
+		const long nf = (long)B * w;
+		row_gemm("fno_dft_tc", LdDft1{ f, N }, EpDft1{ tscr.as<float>(), N, m }, nf * N, N, 2 * m, Bm1, s);
+		row_gemm("fno_dft_tc", LdDft2{ tscr.as<float>(), N }, EpDft2{ Hout, m, scale }, nf * m, 2 * N, 2 * (2 * m - 1), Bm2, s);
+	}
+	// out[fld] (=, +=) scale Re IDFT(O[fld])
+	void idft(int B, const float2 *O, float *out, float scale, int accumulate, cudaStream_t s) {
+		if (!use_tc) {
+			launch("fno_idft", k_fno_idft, (unsigned)(B * w), 256, idft_smem(), s, N, m, O, out, scale, accumulate);
+			return;
+		}
+		ensure_err(s);
+		build_twiddles(s);
+		const long nf = (long)B * w;
+		row_gemm("fno_idft_tc", LdIdftA{ O, m }, EpIdftA{ uscr.as<float>(), N, m }, nf * m, 2 * (2 * m - 1), 2 * N, BmA, s);
+		row_gemm("fno_idft_tc", LdIdftB{ uscr.as<float>(), m }, EpIdftB{ out, N, scale, accumulate }, nf * N, 2 * m, N, BmB, s);
+	}
+	void ensure_err(cudaStream_t s) {
+		if (kerr.p == nullptr) {
+			kerr.ensure(sizeof(int));
+			QB_CUDA(cudaMemsetAsync(kerr.p, 0, sizeof(int), s));
+		}
+	}
 
 	float *P_(long o) { return params.as<float>() + o; }
 
@@ -520,10 +764,7 @@ struct qb_fno {
 			QB_CUDA(cudaFuncSetAttribute(k_fno_pointwise_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fnomma::kSmem));
 			attr_done[dev & 63] = 1;
 		}
-		if (kerr.p == nullptr) {
-			kerr.ensure(sizeof(int));
-			QB_CUDA(cudaMemsetAsync(kerr.p, 0, sizeof(int), s));
-		}
+		ensure_err(s);
 		const long tiles = ((long)B * P + fnomma::kRows - 1) / fnomma::kRows;
 		const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(tiles, 148L * 7));
 		launch("fno_pointwise_mma", k_fno_pointwise_mma, grid, fnomma::kThreads, (size_t)fnomma::kSmem, s, B, P, cin, cout, trans, in, M,
@@ -546,6 +787,8 @@ struct qb_fno {
 		for (int l = 0; l < L; l++) { u[l].ensure(sizeof(float) * f); H[l].ensure(sizeof(float2) * (long)B * w * K); }
 		GO.ensure(sizeof(float2) * (long)B * w * K);
 		GH.ensure(sizeof(float2) * (long)B * w * K);
+		tscr.ensure(sizeof(float) * (long)B * w * m * 2 * N);
+		uscr.ensure(sizeof(float) * (long)B * w * N * 2 * m);
 		const long nchunk = ((long)B * P + kChunk - 1) / kChunk;
 		partial.ensure(sizeof(float) * nchunk * kFnoMaxWidth * kFnoMaxWidth);
 		lossp.ensure(sizeof(double) * 4096);
@@ -560,9 +803,9 @@ struct qb_fno {
 		launch("fno_in", k_fno_in, grid_for((long)B * P), 256, 0, s, B, P, W, inscale, x.as<float>());
 		pointwise(B, kFnoIn, w, x.as<float>(), P_(off.A), P_(off.a), nullptr, nullptr, h[0].as<float>(), 0, s);
 		for (int l = 0; l < L; l++) {
-			launch("fno_dft", k_fno_dft, (unsigned)(B * w), 256, dft_smem(), s, N, m, h[l].as<float>(), H[l].as<float2>(), 1.0f);
+			dft(B, h[l].as<float>(), H[l].as<float2>(), 1.0f, s);
 			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, H[l].as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GO.as<float2>(), 0);
-			launch("fno_idft", k_fno_idft, (unsigned)(B * w), 256, idft_smem(), s, N, m, GO.as<float2>(), tmp.as<float>(), 1.0f / (float)P, 0);
+			idft(B, GO.as<float2>(), tmp.as<float>(), 1.0f / (float)P, 0, s);
 			pointwise(B, w, w, h[l].as<float>(), P_(off.W[l]), P_(off.b[l]), tmp.as<float>(), u[l].as<float>(), h[l + 1].as<float>(),
 			          l < L - 1 ? 1 : 0, s);
 		}
@@ -591,11 +834,11 @@ struct qb_fno {
 			if (l < L - 1) launch("fno_gelu_bwd", k_fno_gelu_bwd, grid_for(nw), 256, 0, s, nw, u[l].as<float>(), dh.as<float>());
 			// dh now holds du
 			pw_grads(B, w, w, h[l].as<float>(), dh.as<float>(), off.W[l], off.b[l], s);
-			launch("fno_dft", k_fno_dft, (unsigned)(B * w), 256, dft_smem(), s, N, m, dh.as<float>(), GO.as<float2>(), 1.0f / (float)P);
+			dft(B, dh.as<float>(), GO.as<float2>(), 1.0f / (float)P, s);
 			launch("fno_rgrad", k_fno_rgrad, grid_for((long)w * w * K), 256, 0, s, B, w, K, GO.as<float2>(), H[l].as<float2>(), G_(off.Rr[l]), G_(off.Ri[l]));
 			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, GO.as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GH.as<float2>(), 1);
 			pointwise_t(B, w, w, dh.as<float>(), P_(off.W[l]), tmp.as<float>(), s);
-			launch("fno_idft", k_fno_idft, (unsigned)(B * w), 256, idft_smem(), s, N, m, GH.as<float2>(), tmp.as<float>(), 1.0f, 1);
+			idft(B, GH.as<float2>(), tmp.as<float>(), 1.0f, 1, s);
 			std::swap(dh, tmp);
 		}
 		// lift

@@ -682,6 +682,23 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samp
     torch.cuda.synchronize()
     long_run = surrogate_long_run(qbgpu, net, q, W0, wl, args.surrogate_long_steps, args.surrogate_long_cells) \
         if args.surrogate_long_steps > 0 else None
+    # the trained network's inference with the pointwise maps and DFTs on the tensor cores (BF16, FP32 accumulation)
+    infer = {}
+    for tc in (False, True):
+        net.set_tensor_cores(tc)
+        for _ in range(3):
+            yb = net.forward(W0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            yb = net.forward(W0)
+        e1.record()
+        torch.cuda.synchronize()
+        infer["tensor_cores" if tc else "fp32"] = {"cells_per_s": round(cells * 20 / (e0.elapsed_time(e1) * 1e-3), 1), "out": yb.clone()}
+    net.set_tensor_cores(False)
+    tc_vs_fp32 = rel(infer["tensor_cores"].pop("out"), infer["fp32"].pop("out"))
+    infer["rel_l1_tensor_cores_vs_fp32"] = round(tc_vs_fp32, 6)
+    infer["device_errors"] = net.device_errors()
     return {"what": f"Strang steps with the collision half from a Fourier neural operator (FP32), exact FP64 operator as judge "
                     f"every {every}th step and per-cell fallback above a relative L1 difference {tol} of the collision increment; "
                     f"the checking steps are inside "
@@ -693,7 +710,8 @@ def run_surrogate(args, wl, qbgpu, q, B, Wall, flush, value64, nseeds=1024, samp
                          "data_s": round(t_data, 2), "train_s": round(t_train, 2), "params": net.num_params},
             "C_rel_l1_on_initial_state": round(c_err, 5),
             "cell_steps": {"surrogate": ns, "exact": ne}, "last_max_residual": round(res, 5),
-            f"W_rel_l1_vs_fp64_after_{args.warmup + args.steps}_steps": rel(bufs[cur], a)}
+            f"W_rel_l1_vs_fp64_after_{args.warmup + args.steps}_steps": rel(bufs[cur], a),
+            "inference_forward": infer}
 
 
 def surrogate_long_run(qbgpu, net, q, W0, wl, steps, cells, tols=(0.5, 0.1, 0.02, 1e-5), every=10):

@@ -288,9 +288,10 @@ int qb_fno_set_scale(qb_fno *net, const double *scale);          /* 4 output sca
 int qb_fno_set_input_scale(qb_fno *net, const double *scale);    /* 14 input scales (> 0) */
 /* Extension, no counterpart in the reference: on != 0 runs the pointwise
  * channel maps (the lift, each layer's W, the projection, and their
- * transposes in the backward pass) on the tensor cores with BF16 operands and
- * FP32 accumulation (tcgen05.mma, accumulator in tensor memory); the spectral
- * parts and the weight gradients stay FP32.  Off by default. */
+ * transposes in the backward pass) and the truncated DFTs and their inverses
+ * on the tensor cores with BF16 operands and FP32 accumulation (tcgen05.mma,
+ * accumulator in tensor memory); the mode mixing and the weight gradients
+ * stay FP32.  Off by default. */
 int qb_fno_set_tensor_cores(qb_fno *net, int on);
 /* nonzero when a tensor-core MMA of the network did not complete within its
  * poll limit (its outputs are then undefined); 0 otherwise */

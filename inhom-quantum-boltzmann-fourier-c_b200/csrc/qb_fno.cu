@@ -1,6 +1,8 @@
 // qb_fno.cu — a Fourier-neural-operator surrogate of the collision operator
 // C[W] = Cc + Cd on one velocity-space cell, with hand-written forward,
-// backward and Adam kernels (FP32 arithmetic, FP64 inputs and outputs).
+// backward and Adam kernels (FP32 arithmetic, FP64 inputs and outputs; on
+// request the pointwise maps and the truncated DFTs run on the tensor cores
+// with BF16 operands and FP32 accumulation).
 //
 // Model (per cell; fields on the N x N velocity grid, point p = (l, k_v)):
 //   x        = the 4 Pauli components and their 10 pairwise products (the

@@ -465,14 +465,16 @@ __global__ void __launch_bounds__(fnomma::kThreads) k_fno_pointwise_mma(int B, i
 }
 
 // ---------------------------------------------------------------------------
-// A row GEMM on the tensor cores (BF16 operands, FP32 accumulation) for the
-// separable truncated DFTs: for 128-row tiles of `rows` rows,
-// D[row][n] = sum_k A[row][k] Bm[n][k], k < K <= 128, n < Nn <= 128, with A
-// read through the loader ld(row, k) and every row of D handed whole to the
-// epilogue ep(row, d).  Bm is an FP32 [Nn][K] matrix in global memory (the
-// twiddles).  Operands K-major with the 128-byte swizzle in two 64-element
-// atoms; D in 128 tensor-memory columns.  Persistent CTAs of 128 threads; the
-// MMA completion wait is bounded (a wait that runs out sets the error word).
+// A grouped row GEMM on the tensor cores (BF16 operands, FP32 accumulation)
+// for the separable truncated DFTs and the mode mixing: for each of the
+// bm.groups() groups and 128-row tiles of its bm.rows() rows,
+// D[row][n] = sum_k A[row][k] Bg[n][k], k < K <= 128, n < Nn <= 128, with A
+// read through the loader ld(g, row, k), Bg through bm(g, n, k) (rebuilt when a
+// CTA moves to another group), and every row of D handed whole to the
+// epilogue ep(g, row, d).  Operands K-major with the 128-byte swizzle in two
+// 64-element atoms; D in 128 tensor-memory columns.  Persistent CTAs of 128
+// threads; the MMA completion wait is bounded (a wait that runs out sets the
+// error word).
 namespace fnotc {
 constexpr int kThreads = 128, kRows = 128, kMaxK = 128, kMaxN = 128, kCols = 128;
 constexpr uint32_t oA = 0, oB = kRows * kMaxK * 2, kUsed = oB + kMaxN * kMaxK * 2;
@@ -485,9 +487,8 @@ __host__ __device__ constexpr uint32_t off(int R, int r, int k) {
 }
 }  // namespace fnotc
 
-template <class Ld, class Ep>
-__global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const Ep ep, long rows, int K, int Nn, const float *__restrict__ Bm,
-                                                             int *err) {
+template <class Ld, class Ep, class Bb>
+__global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const Ep ep, const Bb bm, int K, int Nn, int *err) {
 	using namespace fnotc;
 	using namespace qb;
 	extern __shared__ unsigned char smem_raw[];
@@ -497,12 +498,6 @@ __global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const E
 	__shared__ int abort_flag;
 	const int tid = threadIdx.x, warp = tid >> 5;
 	const int kpad = (K + 15) & ~15, npad = (Nn + 15) & ~15;
-	for (int i = tid; i < npad * (kpad / 2); i += kThreads) {
-		const int n = i / (kpad / 2), k = 2 * (i % (kpad / 2));
-		const float b0 = (n < Nn && k < K) ? Bm[(long)n * K + k] : 0.0f;
-		const float b1 = (n < Nn && k + 1 < K) ? Bm[(long)n * K + k + 1] : 0.0f;
-		*reinterpret_cast<uint32_t *>(base + oB + off(npad, n, k)) = pack_bf16x2(b0, b1);
-	}
 	if (tid == 0) {
 		umma::mbar_init(&mbar, 1);
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -515,14 +510,25 @@ __global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const E
 	const uint32_t tmem = tslot;
 	const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
 	const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-	const long ntiles = (rows + kRows - 1) / kRows;
+	const long rows = bm.rows(), tpg = (rows + kRows - 1) / kRows, ntiles = tpg * bm.groups();
 	unsigned phase = 0;
+	int cur_g = -1;
 	for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-		const long row = tile * kRows + tid;
+		const int g = (int)(tile / tpg);
+		const long row = (tile % tpg) * kRows + tid;
 		const bool live = row < rows;
+		if (g != cur_g) {                     // this group's B (the previous MMA has completed)
+			for (int i = tid; i < npad * (kpad / 2); i += kThreads) {
+				const int n = i / (kpad / 2), k = 2 * (i % (kpad / 2));
+				const float b0 = (n < Nn && k < K) ? bm(g, n, k) : 0.0f;
+				const float b1 = (n < Nn && k + 1 < K) ? bm(g, n, k + 1) : 0.0f;
+				*reinterpret_cast<uint32_t *>(base + oB + off(npad, n, k)) = pack_bf16x2(b0, b1);
+			}
+			cur_g = g;
+		}
 		for (int k = 0; k < kpad; k += 2) {
-			const float x0 = (live && k < K) ? ld(row, k) : 0.0f;
-			const float x1 = (live && k + 1 < K) ? ld(row, k + 1) : 0.0f;
+			const float x0 = (live && k < K) ? ld(g, row, k) : 0.0f;
+			const float x1 = (live && k + 1 < K) ? ld(g, row, k + 1) : 0.0f;
 			*reinterpret_cast<uint32_t *>(base + oA + off(kRows, tid, k)) = pack_bf16x2(x0, x1);
 		}
 		umma::fence_async_smem();
@@ -555,7 +561,7 @@ __global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const E
 				for (int j = 0; j < 16; j++) d[16 * c + j] = v[j];
 			}
 		}
-		if (live) ep(row, d);
+		if (live) ep(g, row, d);
 		tmem_fence_before();
 		__syncthreads();
 		tmem_fence_after();
@@ -573,10 +579,46 @@ __global__ void __launch_bounds__(fnotc::kThreads) k_fno_tc(const Ld ld, const E
 // and its inverse out[fld][l][kv] (=, +=) scale Re sum_k O[fld][k] e^{+i theta}:
 //   A. along kx: U[fld][l][ky] = sum_kx O[fld][kx][ky] e^{+2 pi i kx l / N}      (rows (fld, ky), K = 2(2m-1), Nn = 2N)
 //   B. along ky: out = scale Re sum_ky U[fld][l][ky] e^{+2 pi i ky kv / N}        (rows (fld, l), K = 2m, Nn = N)
-struct LdDft1 { const float *f; int N; __device__ float operator()(long row, int k) const { return f[row * N + k]; } };
+// one fixed FP32 [Nn][K] matrix in global memory (the twiddles) for `nrows` rows
+struct BMat {
+	const float *Bm; int K; long nrows;
+	__device__ long rows() const { return nrows; }
+	__device__ int groups() const { return 1; }
+	__device__ float operator()(int, int n, int k) const { return Bm[(long)n * K + k]; }
+};
+// mode mixing, one group per mode k: rows b (cells), A = [in_re | in_im] of the
+// summed channels, outputs [out_re | out_im]; forward out_o = sum_i R[i][o] in_i,
+// backward (conj) out_i = sum_o conj(R[i][o]) in_o (R[i][o][k] = Rr + i Ri)
+struct BMix {
+	const float *Rr, *Ri; int w, K, nb, conj;
+	__device__ long rows() const { return nb; }
+	__device__ int groups() const { return K; }
+	__device__ float operator()(int g, int n, int k) const {
+		const int c = n % w, j = k % w;           // output channel c, summed channel j
+		const long ri = conj ? ((long)c * w + j) * K + g : ((long)j * w + c) * K + g;
+		const float rr = Rr[ri], rim = conj ? -Ri[ri] : Ri[ri];
+		// out_re = sum rr in_re - rim in_im, out_im = sum rim in_re + rr in_im
+		if (n < w) return k < w ? rr : -rim;
+		return k < w ? rim : rr;
+	}
+};
+struct LdMix {
+	const float2 *in; int w, K;
+	__device__ float operator()(int g, long row, int k) const {
+		const float2 v = in[(row * w + (k % w)) * (long)K + g];
+		return k < w ? v.x : v.y;
+	}
+};
+struct EpMix {
+	float2 *out; int w, K;
+	__device__ void operator()(int g, long row, const float (&d)[fnotc::kMaxN]) const {
+		for (int c = 0; c < w; c++) out[(row * w + c) * (long)K + g] = make_float2(d[c], d[w + c]);
+	}
+};
+struct LdDft1 { const float *f; int N; __device__ float operator()(int, long row, int k) const { return f[row * N + k]; } };
 struct EpDft1 {
 	float *T; int N, m;
-	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+	__device__ void operator()(int, long row, const float (&d)[fnotc::kMaxN]) const {
 		const long fld = row / N;
 		const int l = (int)(row % N);
 		for (int ky = 0; ky < m; ky++) {
@@ -586,10 +628,10 @@ struct EpDft1 {
 		}
 	}
 };
-struct LdDft2 { const float *T; int N; __device__ float operator()(long row, int k) const { return T[row * 2L * N + k]; } };
+struct LdDft2 { const float *T; int N; __device__ float operator()(int, long row, int k) const { return T[row * 2L * N + k]; } };
 struct EpDft2 {
 	float2 *H; int m; float scale;
-	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+	__device__ void operator()(int, long row, const float (&d)[fnotc::kMaxN]) const {
 		const int K = (2 * m - 1) * m, nk = 2 * m - 1;
 		const long fld = row / m;
 		const int ky = (int)(row % m);
@@ -598,7 +640,7 @@ struct EpDft2 {
 };
 struct LdIdftA {
 	const float2 *O; int m;
-	__device__ float operator()(long row, int k) const {
+	__device__ float operator()(int, long row, int k) const {
 		const int K = (2 * m - 1) * m, nk = 2 * m - 1;
 		const long fld = row / m;
 		const int ky = (int)(row % m);
@@ -608,7 +650,7 @@ struct LdIdftA {
 };
 struct EpIdftA {
 	float *U; int N, m;
-	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+	__device__ void operator()(int, long row, const float (&d)[fnotc::kMaxN]) const {
 		const long fld = row / m;
 		const int ky = (int)(row % m);
 		for (int l = 0; l < N; l++) {
@@ -618,10 +660,10 @@ struct EpIdftA {
 		}
 	}
 };
-struct LdIdftB { const float *U; int m; __device__ float operator()(long row, int k) const { return U[row * 2L * m + k]; } };
+struct LdIdftB { const float *U; int m; __device__ float operator()(int, long row, int k) const { return U[row * 2L * m + k]; } };
 struct EpIdftB {
 	float *out; int N; float scale; int accumulate;
-	__device__ void operator()(long row, const float (&d)[fnotc::kMaxN]) const {
+	__device__ void operator()(int, long row, const float (&d)[fnotc::kMaxN]) const {
 		float *o = out + row * N;           // row = fld N + l: out[fld][l][kv]
 		for (int kv = 0; kv < N; kv++) o[kv] = accumulate ? o[kv] + scale * d[kv] : scale * d[kv];
 	}
@@ -634,10 +676,11 @@ unsigned grid_for(long n) { return (unsigned)std::max<long>(1, std::min<long>((n
 // the tensor-memory kernel of this file, for the engine's co-residency check
 std::vector<qb::TmemKernel> qb::fno_tmem_kernels() {
 	return { { (const void *)k_fno_pointwise_mma, fnomma::kSmem, fnomma::kThreads, fnomma::kCols, "k_fno_pointwise_mma" },
-	         { (const void *)k_fno_tc<LdDft1, EpDft1>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<dft 1>" },
-	         { (const void *)k_fno_tc<LdDft2, EpDft2>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<dft 2>" },
-	         { (const void *)k_fno_tc<LdIdftA, EpIdftA>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<idft A>" },
-	         { (const void *)k_fno_tc<LdIdftB, EpIdftB>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<idft B>" } };
+	         { (const void *)k_fno_tc<LdDft1, EpDft1, BMat>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<dft 1>" },
+	         { (const void *)k_fno_tc<LdDft2, EpDft2, BMat>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<dft 2>" },
+	         { (const void *)k_fno_tc<LdIdftA, EpIdftA, BMat>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<idft A>" },
+	         { (const void *)k_fno_tc<LdIdftB, EpIdftB, BMat>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<idft B>" },
+	         { (const void *)k_fno_tc<LdMix, EpMix, BMix>, fnotc::kSmem, fnotc::kThreads, fnotc::kCols, "k_fno_tc<mix>" } };
 }
 
 namespace {
@@ -697,19 +740,18 @@ struct qb_fno {
 		Bm1 = twm.as<float>(); Bm2 = Bm1 + n1; BmA = Bm2 + n2; BmB = BmA + nA;
 	}
 
-	template <class Ld, class Ep> void row_gemm(const char *name, const Ld &ld, const Ep &ep, long rows, int K, int Nn, const float *Bm,
-	                                            cudaStream_t s) {
+	template <class Ld, class Ep, class Bb> void row_gemm(const char *name, const Ld &ld, const Ep &ep, const Bb &bm, long tiles, int K, int Nn,
+	                                                      cudaStream_t s) {
 		static int attr_done[64] = {};
 		int dev = 0;
 		QB_CUDA(cudaGetDevice(&dev));
 		if (!attr_done[dev & 63]) {
 			qb::ensure_tmem_coresidency();
-			QB_CUDA(cudaFuncSetAttribute(k_fno_tc<Ld, Ep>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fnotc::kSmem));
+			QB_CUDA(cudaFuncSetAttribute(k_fno_tc<Ld, Ep, Bb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fnotc::kSmem));
 			attr_done[dev & 63] = 1;
 		}
-		const long tiles = (rows + fnotc::kRows - 1) / fnotc::kRows;
 		const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(tiles, 148L * 3));
-		launch(name, k_fno_tc<Ld, Ep>, grid, fnotc::kThreads, (size_t)fnotc::kSmem, s, ld, ep, rows, K, Nn, Bm, kerr.as<int>());
+		launch(name, k_fno_tc<Ld, Ep, Bb>, grid, fnotc::kThreads, (size_t)fnotc::kSmem, s, ld, ep, bm, K, Nn, kerr.as<int>());
 	}
 
 	// H[fld] = scale DFT(f[fld]) for the B w fields
@@ -721,8 +763,9 @@ struct qb_fno {
 		ensure_err(s);
 		build_twiddles(s);
 		const long nf = (long)B * w;
-		row_gemm("fno_dft_tc", LdDft1{ f, N }, EpDft1{ tscr.as<float>(), N, m }, nf * N, N, 2 * m, Bm1, s);
-		row_gemm("fno_dft_tc", LdDft2{ tscr.as<float>(), N }, EpDft2{ Hout, m, scale }, nf * m, 2 * N, 2 * (2 * m - 1), Bm2, s);
+		row_gemm("fno_dft_tc", LdDft1{ f, N }, EpDft1{ tscr.as<float>(), N, m }, BMat{ Bm1, N, nf * N }, (nf * N + 127) / 128, N, 2 * m, s);
+		row_gemm("fno_dft_tc", LdDft2{ tscr.as<float>(), N }, EpDft2{ Hout, m, scale }, BMat{ Bm2, 2 * N, nf * m }, (nf * m + 127) / 128,
+		         2 * N, 2 * (2 * m - 1), s);
 	}
 	// out[fld] (=, +=) scale Re IDFT(O[fld])
 	void idft(int B, const float2 *O, float *out, float scale, int accumulate, cudaStream_t s) {
@@ -733,8 +776,22 @@ struct qb_fno {
 		ensure_err(s);
 		build_twiddles(s);
 		const long nf = (long)B * w;
-		row_gemm("fno_idft_tc", LdIdftA{ O, m }, EpIdftA{ uscr.as<float>(), N, m }, nf * m, 2 * (2 * m - 1), 2 * N, BmA, s);
-		row_gemm("fno_idft_tc", LdIdftB{ uscr.as<float>(), m }, EpIdftB{ out, N, scale, accumulate }, nf * N, 2 * m, N, BmB, s);
+		row_gemm("fno_idft_tc", LdIdftA{ O, m }, EpIdftA{ uscr.as<float>(), N, m }, BMat{ BmA, 2 * (2 * m - 1), nf * m }, (nf * m + 127) / 128,
+		         2 * (2 * m - 1), 2 * N, s);
+		row_gemm("fno_idft_tc", LdIdftB{ uscr.as<float>(), m }, EpIdftB{ out, N, scale, accumulate }, BMat{ BmB, 2 * m, nf * N },
+		         (nf * N + 127) / 128, 2 * m, N, s);
+	}
+	// mode mixing: out[b][c][k] = sum over the other channel of R (or conj R, backward) times in.
+	// On the tensor cores a mode's B matrix is rebuilt per 128-cell tile, which
+	// pays only when the batch fills the tiles (at 64 cells the FP32 kernel is faster)
+	void mix(int B, const float2 *in, const float *Rr, const float *Ri, float2 *out, int conj, cudaStream_t s) {
+		if (!use_tc || B < 128) {
+			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, in, Rr, Ri, out, conj);
+			return;
+		}
+		ensure_err(s);
+		row_gemm("fno_mix_tc", LdMix{ in, w, K }, EpMix{ out, w, K }, BMix{ Rr, Ri, w, K, B, conj }, (long)K * ((B + 127) / 128), 2 * w,
+		         2 * w, s);
 	}
 	void ensure_err(cudaStream_t s) {
 		if (kerr.p == nullptr) {
@@ -806,7 +863,7 @@ struct qb_fno {
 		pointwise(B, kFnoIn, w, x.as<float>(), P_(off.A), P_(off.a), nullptr, nullptr, h[0].as<float>(), 0, s);
 		for (int l = 0; l < L; l++) {
 			dft(B, h[l].as<float>(), H[l].as<float2>(), 1.0f, s);
-			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, H[l].as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GO.as<float2>(), 0);
+			mix(B, H[l].as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GO.as<float2>(), 0, s);
 			idft(B, GO.as<float2>(), tmp.as<float>(), 1.0f / (float)P, 0, s);
 			pointwise(B, w, w, h[l].as<float>(), P_(off.W[l]), P_(off.b[l]), tmp.as<float>(), u[l].as<float>(), h[l + 1].as<float>(),
 			          l < L - 1 ? 1 : 0, s);
@@ -838,7 +895,7 @@ struct qb_fno {
 			pw_grads(B, w, w, h[l].as<float>(), dh.as<float>(), off.W[l], off.b[l], s);
 			dft(B, dh.as<float>(), GO.as<float2>(), 1.0f / (float)P, s);
 			launch("fno_rgrad", k_fno_rgrad, grid_for((long)w * w * K), 256, 0, s, B, w, K, GO.as<float2>(), H[l].as<float2>(), G_(off.Rr[l]), G_(off.Ri[l]));
-			launch("fno_mix", k_fno_mix, grid_for((long)B * w * K), 256, 0, s, B, w, K, GO.as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GH.as<float2>(), 1);
+			mix(B, GO.as<float2>(), P_(off.Rr[l]), P_(off.Ri[l]), GH.as<float2>(), 1, s);
 			pointwise_t(B, w, w, dh.as<float>(), P_(off.W[l]), tmp.as<float>(), s);
 			idft(B, GH.as<float2>(), tmp.as<float>(), 1.0f, 1, s);
 			std::swap(dh, tmp);

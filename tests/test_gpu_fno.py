@@ -69,12 +69,13 @@ def test_forward_and_gradients_match_oracle():
     assert not np.array_equal(net.get_params(), theta.astype(np.float32))
 
 
-@pytest.mark.parametrize("N,w,m,Ly,B", [(16, 8, 4, 3, 3), (32, 32, 12, 4, 5)])
-def test_tensor_core_pointwise_maps_against_oracle(N, w, m, Ly, B):
-    """The pointwise channel maps on the tensor cores (BF16 operands, FP32
-    accumulation): forward pass and weight gradients against the float64
-    restatement within BF16 accuracy (inputs and weights rounded to 8
-    significant bits), the MMA waits complete, and the FP32 path is untouched."""
+@pytest.mark.parametrize("N,w,m,Ly,B", [(16, 8, 4, 3, 3), (32, 32, 12, 4, 5), (16, 8, 4, 2, 130)])
+def test_tensor_core_stages_against_oracle(N, w, m, Ly, B):
+    """The pointwise channel maps, the truncated DFTs and (from 128 cells on)
+    the mode mixing on the tensor cores (BF16 operands, FP32 accumulation):
+    forward pass and weight gradients against the float64 restatement within
+    BF16 accuracy (inputs and weights rounded to 8 significant bits), the MMA
+    waits complete, and the FP32 path is untouched."""
     net = qbgpu.FNO(N, width=w, modes=m, layers=Ly, seed=7)
     W = mixture_states(N, B, seed=13)
     rng = np.random.default_rng(9)

@@ -70,9 +70,10 @@ int qb_workspace_device_errors(qb_workspace *ws);
  * upstream counterpart; off by default (the upstream step). */
 int qb_workspace_set_conservation(qb_workspace *ws, int on);
 
-/* N = 32 and 64 in the FP32 form: the I3 sums of a cell whose Fourier state
- * has a Nyquist content (sum of |W| on row and column N/2 over sum of |W|, the
- * 4 components) of at most 1e-6 run in real arithmetic, two quadrature chains
+/* The FP32 form (every N): the I3 sums of a cell whose Fourier state has a
+ * Nyquist content (sum of |W| on row and column N/2 over sum of |W|, the 4
+ * components) and an anti-Hermitian part of at most 1e-6 of the state run in
+ * real arithmetic, two quadrature chains
  * per complex transform (exact when that content is zero); the other cells
  * take the complex kernel.  Reports the cells evaluated so far through `ws`
  * by the real form and by either form (synchronises the device); reset != 0

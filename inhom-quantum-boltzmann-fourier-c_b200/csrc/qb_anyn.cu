@@ -49,6 +49,8 @@ constexpr size_t kMaxSmem = 200 * 1024;
 struct Plan {
 	int L = 0, nst = 0;
 	int r[kMaxStages] = {};
+	const double2 *twd = nullptr;        // the L-th roots of unity, built once per workspace (null: each CTA computes them)
+	const float2 *twf = nullptr;
 };
 
 __device__ __forceinline__ int src_idx(int p, int N) {         // padded index -> N-grid index, or -1 (zero band)
@@ -211,13 +213,42 @@ template <int DIR, class C> __device__ C *fft_lines(C *a, C *b, int nl, int ls, 
 }
 
 // the twiddle table tw[m] = exp(-2 pi i m / L), then a CTA barrier
-template <class C> __device__ void init_tw(C *tw, int L) {
+__device__ __forceinline__ const double2 *plan_tw(const Plan &pl, double2 *) { return pl.twd; }
+__device__ __forceinline__ const float2 *plan_tw(const Plan &pl, float2 *) { return pl.twf; }
+// exp(-2 pi i m / L), out of line: the kernels that read the table do not
+// carry its registers
+__device__ __noinline__ double2 root_of_unity(int m, int L) {
+	double s, c;
+	sincospi(2.0 * m / L, &s, &c);
+	return make_double2(c, -s);
+}
+// the table of the workspace (every pass of AnyRhs has one)
+template <class C> __device__ void load_tw(C *tw, int L, const Plan &pl) {
+	const C *g = plan_tw(pl, tw);
+	for (int m = threadIdx.x; m < L; m += blockDim.x) tw[m] = g[m];
+	__syncthreads();
+}
+// the table, or without one (the workspace-free transforms) computed per CTA
+template <class C> __device__ void init_tw(C *tw, int L, const Plan &pl) {
+	const C *g = plan_tw(pl, tw);
+	for (int m = threadIdx.x; m < L; m += blockDim.x) {
+		if (g != nullptr) {
+			tw[m] = g[m];
+		} else {
+			const double2 w = root_of_unity(m, L);
+			tw[m] = mk<C>(w.x, w.y);
+		}
+	}
+	__syncthreads();
+}
+// the table of init_tw for L = P, in both precisions
+__global__ void k_any_build_tw(int L, double2 *twd, float2 *twf) {
 	for (int m = threadIdx.x; m < L; m += blockDim.x) {
 		double s, c;
 		sincospi(2.0 * m / L, &s, &c);
-		tw[m] = mk<C>(c, -s);
+		twd[m] = make_double2(c, -s);
+		twf[m] = mk<float2>(c, -s);
 	}
-	__syncthreads();
 }
 
 // shared-memory layout of a pass: the twiddles, then two buffers of nl lines
@@ -269,10 +300,11 @@ template <class C> struct PadRowsP {
 	using R = typename CT<C>::R;
 	const double2 *W; long w_cell;
 	int N, nl, nt, t0, nsub;
-	int comp[8], psel[8];
+	int comp[8], psel[8], comp2[8];      // psel 4: psiC . (W_comp + i W_comp2)
 	const R *psiA, *psiB;                 // real N x N tables, one per term
 	const C *psiC;                        // complex N x N tables, one per term
 	C *out;
+	const int *kind; int want;            // kind != null: only the cells of kind `want`
 	Plan pl;
 };
 template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(const PadRowsP<C> p) {
@@ -282,7 +314,6 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 	const long NN = (long)N * N, PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
@@ -290,7 +321,10 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 	const long ct = u / p.nsub;
 	const int t = p.t0 + (int)(ct % p.nt);
 	const long cell = ct / p.nt;
+	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	load_tw(T.tw, P, p.pl);
 	const double2 *w = p.W + cell * p.w_cell + (long)p.comp[sub] * NN;
+	const double2 *w2 = p.W + cell * p.w_cell + (long)p.comp2[sub] * NN;
 	const int ps = p.psel[sub];
 	batched<C>(nl * P, [&](int i) {
 		const int li = fdiv(i, mgP), k = i - li * P;
@@ -301,6 +335,10 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 			const double2 x = w[q];
 			if (ps == 0) v = mk<C>(x.x, x.y);
 			else if (ps == 3) v = cmul(p.psiC[t * NN + q], mk<C>(x.x, x.y));
+			else if (ps == 4) {
+				const double2 y = w2[q];
+				v = cmul(p.psiC[t * NN + q], mk<C>(x.x - y.y, x.y + y.x));
+			}
 			else {
 				const R f = (ps == 1 ? p.psiA : p.psiB)[t * NN + q];
 				v.x = f * (R)x.x;
@@ -325,6 +363,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 // Fourier representation)
 template <class C> struct PlainP {
 	C *g; int L, nl;
+	const int *kind; int want; long gpc;  // kind != null: only the grids of cells of kind `want` (gpc grids a cell)
 	Plan pl;
 };
 template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThreads) k_any_plain(const PlainP<C> p) {
@@ -332,10 +371,11 @@ template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThread
 	const int L = p.L, nl = p.nl;
 	Tile<C> T(sm, L, nl);
 	const unsigned mgP = magic_div((unsigned)L), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, L);
 	const int bpg = L / nl;
 	const long u = blockIdx.x / bpg;
 	const int x0 = (int)(blockIdx.x % bpg) * nl;
+	if (p.kind != nullptr && p.kind[u / p.gpc] != p.want) return;
+	init_tw(T.tw, L, p.pl);
 	C *g = p.g + u * (long)L * L;
 	batched<C>(nl * L, [&](int i) {
 		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; return g[(long)l * L + x0 + kk]; }
@@ -367,7 +407,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(con
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
+	load_tw(T.tw, P, p.pl);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
@@ -414,7 +454,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(con
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
+	load_tw(T.tw, P, p.pl);
 	const int bpg = P / nl;
 	const long cs = blockIdx.x / bpg;             // cell nsub + sub
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
@@ -460,7 +500,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, 2 * nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
+	load_tw(T.tw, P, p.pl);
 	const int bpg = P / nl;
 	const long ci = blockIdx.x / bpg;             // cell 4 + i
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
@@ -490,34 +530,56 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 }
 
 // I3 chain, first rows: unit u = ((cell nt + tt) 4 + j) 4 + i, inverse
-// transform of the rows of W^_i . P_j into Y[u]
+// transform of the rows of W^_i . P_j into Y[u].  Real form (RF, FP32, cells
+// without Nyquist content, where W^ and P are real): u = ((cell nt + tt) 4 + j)
+// 2 + pr, one complex chain of P_j . (W^_2pr + i W^_2pr+1) for the two combos,
+// and Pg holds two grids per (cell, term), P_2s + i P_2s+1.
 template <class C> struct I3RowsAP {
 	const C *What, *Pg; C *Y; int N, nl, nt;
+	const int *kind; int want;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
+template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
-	const int i3 = (int)(u % 4), j3 = (int)((u / 4) % 4);
-	const long ct = u / 16, cell = ct / p.nt;
-	const C *G = p.What + (cell * 4 + i3) * PP + (long)l0 * P;
-	const C *Pj = p.Pg + (ct * 4 + j3) * PP + (long)l0 * P;
-	batched<Two<C>>(nl * P, [&](int i) {
-		Two<C> v;
-		v.a = G[i];
-		v.b = Pj[i];
-		return v;
-	}, [&](int i, const Two<C> &v) {
-		const int li = fdiv(i, mgP), k = i - li * P;
-		T.a[sw(li * T.pitch + k)] = cmul(v.a, v.b);
-	});
+	constexpr int kCpt = RF ? 8 : 16;             // chains per (cell, term)
+	const int i3 = (int)(u % (kCpt / 4)), j3 = (int)((u / (kCpt / 4)) % 4);
+	const long ct = u / kCpt, cell = ct / p.nt;
+	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	load_tw(T.tw, P, p.pl);
+	if constexpr (RF) {
+		const C *G0 = p.What + (cell * 4 + 2 * i3) * PP + (long)l0 * P, *G1 = G0 + PP;
+		const C *Pj = p.Pg + (ct * 2 + j3 / 2) * PP + (long)l0 * P;
+		const bool im = j3 & 1;
+		batched<Two<C>>(nl * P, [&](int i) {
+			Two<C> v;
+			v.a = mk<C>(G0[i].x, G1[i].x);
+			v.b = Pj[i];
+			return v;
+		}, [&](int i, const Two<C> &v) {
+			const int li = fdiv(i, mgP), k = i - li * P;
+			const typename CT<C>::R pj = im ? v.b.y : v.b.x;
+			T.a[sw(li * T.pitch + k)] = cscale(v.a, pj);
+		});
+	} else {
+		const C *G = p.What + (cell * 4 + i3) * PP + (long)l0 * P;
+		const C *Pj = p.Pg + (ct * 4 + j3) * PP + (long)l0 * P;
+		batched<Two<C>>(nl * P, [&](int i) {
+			Two<C> v;
+			v.a = G[i];
+			v.b = Pj[i];
+			return v;
+		}, [&](int i, const Two<C> &v) {
+			const int li = fdiv(i, mgP), k = i - li * P;
+			T.a[sw(li * T.pitch + k)] = cmul(v.a, v.b);
+		});
+	}
 	__syncthreads();
 	const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	C *o = p.Y + u * PP + (long)l0 * P;
@@ -532,20 +594,25 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(c
 template <class C> struct I3ColsP {
 	using R = typename CT<C>::R;
 	C *Y; const R *psi2T; const int *idx; const double *scale; int N, nl, nt, t0;
+	int cpt;                              // chains per (cell, term): 16, or 8 in the real form (no other value)
+	const int *kind; int want;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_cols(const I3ColsP<C> p) {
+// FP64: two CTAs an SM (at most 128 registers; the pass waits on global loads)
+template <class C> __global__ void __launch_bounds__(kThreads, sizeof(C) == 16 ? 2 : 0) k_any_i3_cols(const I3ColsP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
-	const int t = p.t0 + (int)((u / 16) % p.nt);
+	const int ct = (int)(p.cpt == 8 ? u >> 3 : u >> 4);            // (cell, term) of the wave: below 2^31
+	const int cell = ct / p.nt, t = p.t0 + (ct - cell * p.nt);
+	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	load_tw(T.tw, P, p.pl);
 	C *g = p.Y + u * PP;
 	batched<C>(nl * P, [&](int i) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
@@ -581,21 +648,25 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_cols(con
 template <class C> __host__ __device__ constexpr int own_of() { return sizeof(C) == 16 ? 8 : 16; }   // nl P <= own_of<C>() kThreads
 template <class C> struct I3RowsBP {
 	const C *Y, *Pg; C *X; int N, nl, nt;
+	const int *kind; int want;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
+// RF: Y holds the two packed chains of (cell, term, j); X[cell][j] (real) +=
+// eta_2pr P_2pr . Re(row) + eta_2pr+1 P_2pr+1 . Im(row)
+template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl, ne = nl * P;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
 	const int bpg = P / nl;
 	const long cj = blockIdx.x / bpg;             // cell 4 + j
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
 	const long cell = cj / 4;
 	const int j3 = (int)(cj % 4);
+	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	load_tw(T.tw, P, p.pl);
 	C *X = p.X + cj * PP + (long)l0 * P;
 	constexpr int kOwn = own_of<C>();
 	C acc[kOwn];
@@ -606,24 +677,39 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(c
 	}
 	for (int tt = 0; tt < p.nt; tt++) {
 		const long ct = cell * p.nt + tt;
-		for (int h = 0; h < 4; h++) {
-			const C *y = p.Y + ((ct * 4 + j3) * 4 + h) * PP + (long)l0 * P;
+		constexpr int kH = RF ? 2 : 4;
+		for (int h = 0; h < kH; h++) {
+			const C *y = p.Y + ((ct * 4 + j3) * kH + h) * PP + (long)l0 * P;
 			batched<C>(ne, [&](int i) { return y[i]; }, [&](int i, const C &v) {
 				const int li = fdiv(i, mgP), k = i - li * P;
 				T.a[sw(li * T.pitch + k)] = v;
 			});
 			__syncthreads();
 			const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
-			const C *Pa = p.Pg + (ct * 4 + h) * PP + (long)l0 * P;
-			const R eta = h == 0 ? (R)1 : (R)-1;
+			if constexpr (RF) {
+				const C *Pa = p.Pg + (ct * 2 + h) * PP + (long)l0 * P;      // P_2h + i P_2h+1
+				const R e0 = h == 0 ? (R)1 : (R)-1;                          // eta_2h; eta_2h+1 = -1
 #pragma unroll
-			for (int e = 0; e < kOwn; e++) {
-				const int i = threadIdx.x + e * kThreads;
-				if (i < ne) {
-					const int li = fdiv(i, mgP), k = i - li * P;
-					const C v = cmul(Pa[i], r[sw(li * T.pitch + k)]);
-					acc[e].x += eta * v.x;
-					acc[e].y += eta * v.y;
+				for (int e = 0; e < kOwn; e++) {
+					const int i = threadIdx.x + e * kThreads;
+					if (i < ne) {
+						const int li = fdiv(i, mgP), k = i - li * P;
+						const C pa = Pa[i], y = r[sw(li * T.pitch + k)];
+						acc[e].x += e0 * (pa.x * y.x) - pa.y * y.y;
+					}
+				}
+			} else {
+				const C *Pa = p.Pg + (ct * 4 + h) * PP + (long)l0 * P;
+				const R eta = h == 0 ? (R)1 : (R)-1;
+#pragma unroll
+				for (int e = 0; e < kOwn; e++) {
+					const int i = threadIdx.x + e * kThreads;
+					if (i < ne) {
+						const int li = fdiv(i, mgP), k = i - li * P;
+						const C v = cmul(Pa[i], r[sw(li * T.pitch + k)]);
+						acc[e].x += eta * v.x;
+						acc[e].y += eta * v.y;
+					}
 				}
 			}
 			__syncthreads();
@@ -646,36 +732,41 @@ template <class C> struct I3FusedP {
 	using R = typename CT<C>::R;
 	const C *What, *Pg; C *X; const R *psi2T; const int *idx; const double *scale;
 	int N, nt, t0;
+	const int *kind; int want;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(const I3FusedP<C> p) {
+// RF: one CTA per (cell, j, pr) runs the packed chain of the combos 2pr, 2pr + 1
+// into the real partial X[cell][j][pr] (partials 2, 3 stay zero)
+template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(const I3FusedP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, PPi = P * P;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, P);
 	const unsigned mgP = magic_div((unsigned)P);
-	init_tw(T.tw, P);
-	const long cji = blockIdx.x;                  // (cell 4 + j) 4 + i
-	const long cell = cji / 16;
-	const int j3 = (int)((cji / 4) % 4), h = (int)(cji % 4);
-	C *X = p.X + cji * PP;
-	const C *G = p.What + (cell * 4 + h) * PP;
+	constexpr int kPer = RF ? 2 : 4;              // CTAs per (cell, j)
+	const long cji = blockIdx.x;                  // (cell 4 + j) kPer + h
+	const long cell = cji / (4 * kPer);
+	const int j3 = (int)((cji / kPer) % 4), h = (int)(cji % kPer);
+	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	load_tw(T.tw, P, p.pl);
+	C *X = p.X + ((cell * 4 + j3) * 4 + h) * PP;
+	const C *G = p.What + (cell * 4 + (RF ? 2 * h : h)) * PP;
 	for (int tt = 0; tt < p.nt; tt++) {
 		const long ct = cell * p.nt + tt;
 		const int t = p.t0 + tt;
 		const R sc = (R)p.scale[t];
 		const R *ps = p.psi2T + (long)p.idx[t] * PP;
-		const C *Pj = p.Pg + (ct * 4 + j3) * PP;
+		const C *Pj = p.Pg + (RF ? ct * 2 + j3 / 2 : ct * 4 + j3) * PP;
 		{
 			batched<Two<C>>(PPi, [&](int i) {
 				Two<C> v;
-				v.a = G[i];
+				v.a = RF ? mk<C>(G[i].x, G[i + PP].x) : G[i];
 				v.b = Pj[i];
 				return v;
 			}, [&](int i, const Two<C> &v) {
 				const int l = fdiv(i, mgP), k = i - l * P;
-				T.a[sw(l * T.pitch + k)] = cmul(v.a, v.b);
+				T.a[sw(l * T.pitch + k)] = RF ? cscale(v.a, (j3 & 1) ? v.b.y : v.b.x) : cmul(v.a, v.b);
 			});
 			__syncthreads();
 			C *r = fft_lines<+1>(T.a, T.b, P, T.pitch, 1, p.pl, T.tw);               // rows
@@ -691,7 +782,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(co
 			__syncthreads();
 			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, 1, T.pitch, p.pl, T.tw);     // columns
 			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, T.pitch, 1, p.pl, T.tw);     // rows
-			const C *Pa = p.Pg + (ct * 4 + h) * PP;
+			const C *Pa = p.Pg + (RF ? ct * 2 + h : ct * 4 + h) * PP;
 			const R eta = h == 0 ? (R)1 : (R)-1;
 			batched<Two<C>>(PPi, [&](int i) {
 				Two<C> v;
@@ -700,10 +791,15 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(co
 				return v;
 			}, [&](int i, const Two<C> &v) {
 				const int l = fdiv(i, mgP), k = i - l * P;
-				const C y = cmul(v.a, r[sw(l * T.pitch + k)]);
 				C x = v.b;
-				x.x += eta * y.x;
-				x.y += eta * y.y;
+				const C y0 = r[sw(l * T.pitch + k)];
+				if (RF) {                                  // eta_2h P_2h Re + eta_2h+1 P_2h+1 Im (eta_2h+1 = -1)
+					x.x += eta * (v.a.x * y0.x) - v.a.y * y0.y;
+				} else {
+					const C y = cmul(v.a, y0);
+					x.x += eta * y.x;
+					x.y += eta * y.y;
+				}
 				X[i] = x;
 			});
 			__syncthreads();
@@ -730,7 +826,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, 2 * nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
+	load_tw(T.tw, P, p.pl);
 	const int bpg = P / nl;
 	const long cj = blockIdx.x / bpg;
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
@@ -798,7 +894,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(co
 	const long PP = (long)P * P, NN = (long)N * N;
 	Tile<C> T(sm, P, 2 * nl);
 	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
-	init_tw(T.tw, P);
+	load_tw(T.tw, P, p.pl);
 	const int bpg = P / nl;
 	const long cj = blockIdx.x / bpg;
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
@@ -971,23 +1067,53 @@ template <class C> struct AnyRhs {
 
 	AnyRhs(Workspace &w, const QuadSet &qs, int nc, cudaStream_t st) : ws(w), q(qs), N(w.N), P(2 * w.N), ncells(nc), s(st) {
 		PP = (long)P * P;
-		pl = make_plan(P, ws.anyn_plan);
+		pl = with_tw(make_plan(P, ws.anyn_plan));
 		nl1 = pick_lines(P, ws.anyn_lines > 0 ? ws.anyn_lines : std::max(1, 2048 / P), 1, sizeof(C));
+	}
+	Plan with_tw(Plan p) const {
+		p.twd = ws.anyn_tw.as<double2>();
+		p.twf = reinterpret_cast<const float2 *>(p.twd + P);
+		return p;
 	}
 	size_t smem(int nl, int tiles) const { return tile_bytes<C>(P, nl * tiles); }
 	long blocks(long units, int nl) const { return units * (P / nl); }
 
-	// terms per wave: the wave's scratch of `per_term` grids per cell within the budget
-	int wave(int nterms, int per_term) const {
-		const double mb = ws.anyn_wave_mb > 0 ? ws.anyn_wave_mb : 32.0;      // the wave's scratch stays in L2
-		const double per = (double)per_term * ncells * PP * sizeof(C);
-		const int nt = (int)std::max(1.0, std::floor(mb * 1048576.0 / per));
+	static double env_mb(const char *name) {
+		const char *e = getenv(name);
+		return e != nullptr ? atof(e) : 0.0;
+	}
+	// the wave's scratch in bytes, within L2: the workspace's knob, else
+	// QB_ANYN_WAVE_MB (read per call), else 32 MB
+	double wave_budget() const {
+		const double mb = ws.anyn_wave_mb > 0 ? ws.anyn_wave_mb : env_mb("QB_ANYN_WAVE_MB");
+		return (mb > 0 ? mb : 32.0) * 1048576.0;
+	}
+	// terms per wave: the wave's scratch of `per_term` grids per cell for nc cells within the budget
+	int wave(int nterms, int per_term, int nc = -1) const {
+		const double per = (double)per_term * (nc < 0 ? ncells : nc) * PP * sizeof(C);
+		const int nt = (int)std::max(1.0, std::floor(wave_budget() / per));
 		return std::min(nt, std::max(1, nterms));
 	}
+	// cells per wave: all of them, unless one term of the batch needs more
+	// scratch than the cap (QB_ANYN_SLICE_MB, read per call, else 4 GB); then
+	// equal slices of the batch within it.  Slices within the L2 budget were
+	// measured slower (N = 96 and 128: more, smaller launches cost more than
+	// the L2 misses they save), so the cap only bounds the scratch memory.
+	int wave_cells(int per_term) const {
+		const double mb = env_mb("QB_ANYN_SLICE_MB");
+		const double cap = (mb > 0 ? mb : 4096.0) * 1048576.0;
+		const double per = (double)per_term * PP * sizeof(C);
+		const int fit = (int)std::max(1.0, std::floor(cap / per));
+		if (fit >= ncells) return ncells;
+		const int nslices = (ncells + fit - 1) / fit;
+		return (ncells + nslices - 1) / nslices;
+	}
 
-	void plain(C *g, long ngrids, int dir, bool cols) {
+	// kind != null: only the grids of the cells of kind `want`, gpc grids a cell
+	void plain(C *g, long ngrids, int dir, bool cols, const int *kind = nullptr, int want = 0, long gpc = 1) {
 		PlainP<C> p{};
 		p.g = g; p.L = P; p.nl = nl1; p.pl = pl;
+		p.kind = kind; p.want = want; p.gpc = gpc;
 		const long nb = blocks(ngrids, nl1);
 		const size_t sm = smem(nl1, 1);
 		if (dir < 0) {
@@ -1004,8 +1130,8 @@ template <class C> struct AnyRhs {
 		p.W = W; p.w_cell = 4L * N * N; p.N = N; p.nl = nl1; p.nt = nt; p.t0 = t0; p.nsub = nsub; p.out = out; p.pl = pl;
 		return p;
 	}
-	void pad_rows(const PadRowsP<C> &p) {
-		launch(k_any_pad_rows<C>, "any_pad_rows", blocks((long)ncells * p.nt * p.nsub, nl1), smem(nl1, 1), s, p);
+	void pad_rows(const PadRowsP<C> &p, int nc = -1) {
+		launch(k_any_pad_rows<C>, "any_pad_rows", blocks((long)(nc < 0 ? ncells : nc) * p.nt * p.nsub, nl1), smem(nl1, 1), s, p);
 	}
 
 	void spectra(const double2 *W) {
@@ -1021,22 +1147,27 @@ template <class C> struct AnyRhs {
 		const int ntask = cc ? 3 : 4;
 		Sbuf.ensure(sizeof(C) * ncells * ntask * PP);
 		QB_CUDA(cudaMemsetAsync(Sbuf.p, 0, sizeof(C) * ncells * ntask * PP, s));
-		const int nt = wave(t.nterms, ntask);
-		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * ntask * PP);
+		const int cpw = wave_cells(ntask);                  // waves of terms and, if need be, slices of cells
+		const int nt = wave(t.nterms, ntask, cpw);
+		ws.wave1.ensure(sizeof(C) * (size_t)cpw * nt * ntask * PP);
 		C *G = ws.wave1.as<C>();
-		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
-			const int n = std::min(nt, t.nterms - t0);
-			PadRowsP<C> p = pad_params(W, n, t0, ntask, G);
-			for (int k = 0; k < ntask; k++) { p.comp[k] = cc ? std::min(k + 1, 3) : k; p.psel[k] = 1; }
-			p.psiA = Tabs<C>::i1_psi2(t);
-			pad_rows(p);
-			I1ColsP<C> c{};
-			c.g = G; c.What = ws.What.as<C>(); c.N = N; c.nl = nl1; c.nt = n; c.nsub = ntask; c.fcomp = 0;
-			c.fa = cc ? -4.0 : 2.0; c.fb = cc ? 2.0 : -1.0; c.pl = pl;
-			launch(k_any_i1_cols<C>, "any_i1_cols", blocks((long)ncells * n * ntask, nl1), smem(nl1, 1), s, c);
-			I1RowsP<C> r{};
-			r.g = G; r.S = Sbuf.as<C>(); r.phi = Tabs<C>::i1_phi(t); r.N = N; r.nl = nl1; r.nt = n; r.t0 = t0; r.nsub = ntask; r.pl = pl;
-			launch(k_any_i1_rows<C>, "any_i1_rows", blocks((long)ncells * ntask, nl1), smem(nl1, 1), s, r);
+		for (int c0 = 0; c0 < ncells; c0 += cpw) {
+			const int nc = std::min(cpw, ncells - c0);
+			for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+				const int n = std::min(nt, t.nterms - t0);
+				PadRowsP<C> p = pad_params(W + (long)c0 * 4 * N * N, n, t0, ntask, G);
+				for (int k = 0; k < ntask; k++) { p.comp[k] = cc ? std::min(k + 1, 3) : k; p.psel[k] = 1; }
+				p.psiA = Tabs<C>::i1_psi2(t);
+				pad_rows(p, nc);
+				I1ColsP<C> c{};
+				c.g = G; c.What = ws.What.as<C>() + (long)c0 * 4 * PP; c.N = N; c.nl = nl1; c.nt = n; c.nsub = ntask; c.fcomp = 0;
+				c.fa = cc ? -4.0 : 2.0; c.fb = cc ? 2.0 : -1.0; c.pl = pl;
+				launch(k_any_i1_cols<C>, "any_i1_cols", blocks((long)nc * n * ntask, nl1), smem(nl1, 1), s, c);
+				I1RowsP<C> r{};
+				r.g = G; r.S = Sbuf.as<C>() + (long)c0 * ntask * PP; r.phi = Tabs<C>::i1_phi(t); r.N = N; r.nl = nl1; r.nt = n; r.t0 = t0;
+				r.nsub = ntask; r.pl = pl;
+				launch(k_any_i1_rows<C>, "any_i1_rows", blocks((long)nc * ntask, nl1), smem(nl1, 1), s, r);
+			}
 		}
 		FSbuf.ensure(sizeof(C) * ncells * ntask * PP);
 		QB_CUDA(cudaMemcpyAsync(FSbuf.p, Sbuf.p, sizeof(C) * ncells * ntask * PP, cudaMemcpyDeviceToDevice, s));
@@ -1047,19 +1178,23 @@ template <class C> struct AnyRhs {
 	void i2_sums(const DevI2 &t, const double2 *W) {
 		ws.i2p.ensure(sizeof(C) * ncells * 4 * PP);
 		QB_CUDA(cudaMemsetAsync(ws.i2p.p, 0, sizeof(C) * ncells * 4 * PP, s));
-		const int nt = wave(t.nterms, 8);
-		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 8 * PP);
+		const int cpw = wave_cells(8);                      // waves of terms and, if need be, slices of cells
+		const int nt = wave(t.nterms, 8, cpw);
+		ws.wave1.ensure(sizeof(C) * (size_t)cpw * nt * 8 * PP);
 		C *G = ws.wave1.as<C>();
 		const int nl2 = pick_lines(P, nl1, 2, sizeof(C));
-		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
-			const int n = std::min(nt, t.nterms - t0);
-			PadRowsP<C> p = pad_params(W, n, t0, 8, G);
-			for (int i = 0; i < 4; i++) { p.comp[2 * i] = i; p.psel[2 * i] = 1; p.comp[2 * i + 1] = i; p.psel[2 * i + 1] = 2; }
-			p.psiA = Tabs<C>::i2_psi1(t); p.psiB = Tabs<C>::i2_psi2(t);
-			pad_rows(p);
-			I2ColsP<C> c{};
-			c.g = G; c.Q = ws.i2p.as<C>(); c.N = N; c.nl = nl2; c.nt = n; c.pl = pl;
-			launch(k_any_i2_cols<C>, "any_i2_cols", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, c);
+		for (int c0 = 0; c0 < ncells; c0 += cpw) {
+			const int nc = std::min(cpw, ncells - c0);
+			for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+				const int n = std::min(nt, t.nterms - t0);
+				PadRowsP<C> p = pad_params(W + (long)c0 * 4 * N * N, n, t0, 8, G);
+				for (int i = 0; i < 4; i++) { p.comp[2 * i] = i; p.psel[2 * i] = 1; p.comp[2 * i + 1] = i; p.psel[2 * i + 1] = 2; }
+				p.psiA = Tabs<C>::i2_psi1(t); p.psiB = Tabs<C>::i2_psi2(t);
+				pad_rows(p, nc);
+				I2ColsP<C> c{};
+				c.g = G; c.Q = ws.i2p.as<C>() + (long)c0 * 4 * PP; c.N = N; c.nl = nl2; c.nt = n; c.pl = pl;
+				launch(k_any_i2_cols<C>, "any_i2_cols", blocks((long)nc * 4, nl2), smem(nl2, 2), s, c);
+			}
 		}
 	}
 
@@ -1071,58 +1206,81 @@ template <class C> struct AnyRhs {
 		return tile_bytes<C>(P, P) <= kMaxSmem;
 	}
 
-	// returns the partials of X per (cell, j)
+	// returns the partials of X per (cell, j).  FP32: the cells of kind 0 (no
+	// Nyquist content, Hermitian state) take the real form, two chains packed
+	// in one complex transform; the others the complex chains.
 	int i3_sums(const DevI3 &t, const double2 *W) {
 		const int nxp = fused_i3() ? 4 : 1;
 		ws.i3p.ensure(sizeof(C) * ncells * 4 * nxp * PP);
 		QB_CUDA(cudaMemsetAsync(ws.i3p.p, 0, sizeof(C) * ncells * 4 * nxp * PP, s));
-		if (nxp == 4) {
-			const int nt = wave(t.nterms, 4);
-			ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
-			C *Pg = ws.wave1.as<C>();
-			for (int t0 = 0; t0 < t.nterms; t0 += nt) {
-				const int n = std::min(nt, t.nterms - t0);
-				PadRowsP<C> p = pad_params(W, n, t0, 4, Pg);
-				for (int j = 0; j < 4; j++) { p.comp[j] = j; p.psel[j] = 3; }
-				p.psiC = Tabs<C>::i3_psi1(t);
-				pad_rows(p);
-				plain(Pg, (long)ncells * n * 4, -1, true);
-				I3FusedP<C> f{};
-				f.What = ws.What.as<C>(); f.Pg = Pg; f.X = ws.i3p.as<C>();
-				f.psi2T = Tabs<C>::i3_psi2T(t); f.idx = t.idx.as<int>(); f.scale = t.scale.as<double>();
-				f.N = N; f.nt = n; f.t0 = t0;
-				// FP32 default: radix-8 stages (the radix-16 register DFTs push this
-				// kernel to 173 registers, one CTA an SM); FP64 runs one CTA an SM anyway
-				f.pl = (ws.anyn_plan == 0 && sizeof(C) == 8) ? make_plan(P, 1) : pl;
-				launch(k_any_i3_fused<C>, "any_i3_fused", (long)ncells * 16, tile_bytes<C>(P, P), s, f);
+		if constexpr (sizeof(typename CT<C>::R) == 4) {
+			if (real_form_enabled()) {
+				const int *kind = i3_form_kinds(ws, ncells, W, s);
+				i3_waves<true>(t, W, nxp, kind, 0);
+				i3_waves<false>(t, W, nxp, kind, 1);
+				return nxp;
 			}
-			return nxp;
 		}
-		const int nt = wave(t.nterms, 20);
-		ws.wave1.ensure(sizeof(C) * (size_t)ncells * nt * 4 * PP);       // P_j
-		ws.wave2.ensure(sizeof(C) * (size_t)ncells * nt * 16 * PP);      // chains
-		C *Pg = ws.wave1.as<C>(), *Y = ws.wave2.as<C>();
+		i3_waves<false>(t, W, nxp, nullptr, 0);
+		return nxp;
+	}
+
+	// the I3 chains in waves of terms and, where one term of the batch
+	// overflows the scratch cap, slices of cells; RF: the real form (Pg holds
+	// the packed pairs P_0 + i P_1, P_2 + i P_3, and 8 chains a (cell, term)).
+	// A cell's terms still run in order, so the sums do not depend on the waves.
+	template <bool RF> void i3_waves(const DevI3 &t, const double2 *W, int nxp, const int *kind, int want) {
+		constexpr int kGrids = RF ? 2 : 4, kChains = RF ? 8 : 16;
+		const bool fused = nxp == 4;
+		const int per_term = fused ? kGrids : kGrids + kChains;
+		const int cpw = wave_cells(per_term);
+		const int nt = wave(t.nterms, per_term, cpw);
+		ws.wave1.ensure(sizeof(C) * (size_t)cpw * nt * kGrids * PP);                // P_j
+		if (!fused) ws.wave2.ensure(sizeof(C) * (size_t)cpw * nt * kChains * PP);   // chains
+		C *Pg = ws.wave1.as<C>(), *Y = fused ? nullptr : ws.wave2.as<C>();
 		int nl4 = nl1;                                      // one tile, at most kOwn elements a thread
 		while (nl4 > 1 && (nl4 * P > own_of<C>() * kThreads || P % nl4)) nl4--;
-		for (int t0 = 0; t0 < t.nterms; t0 += nt) {
-			const int n = std::min(nt, t.nterms - t0);
-			PadRowsP<C> p = pad_params(W, n, t0, 4, Pg);
-			for (int j = 0; j < 4; j++) { p.comp[j] = j; p.psel[j] = 3; }
-			p.psiC = Tabs<C>::i3_psi1(t);
-			pad_rows(p);
-			plain(Pg, (long)ncells * n * 4, -1, true);
-			I3RowsAP<C> a{};
-			a.What = ws.What.as<C>(); a.Pg = Pg; a.Y = Y; a.N = N; a.nl = nl1; a.nt = n; a.pl = pl;
-			launch(k_any_i3_rows_a<C>, "any_i3_rows_a", blocks((long)ncells * n * 16, nl1), smem(nl1, 1), s, a);
-			I3ColsP<C> c{};
-			c.Y = Y; c.psi2T = Tabs<C>::i3_psi2T(t); c.idx = t.idx.as<int>(); c.scale = t.scale.as<double>();
-			c.N = N; c.nl = nl1; c.nt = n; c.t0 = t0; c.pl = pl;
-			launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)ncells * n * 16, nl1), smem(nl1, 1), s, c);
-			I3RowsBP<C> b{};
-			b.Y = Y; b.Pg = Pg; b.X = ws.i3p.as<C>(); b.N = N; b.nl = nl4; b.nt = n; b.pl = pl;
-			launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)ncells * 4, nl4), smem(nl4, 1), s, b);
+		for (int c0 = 0; c0 < ncells; c0 += cpw) {
+			const int nc = std::min(cpw, ncells - c0);
+			const double2 *Wc = W + (long)c0 * 4 * N * N;
+			const C *What = ws.What.as<C>() + (long)c0 * 4 * PP;
+			C *X = ws.i3p.as<C>() + (long)c0 * 4 * nxp * PP;
+			const int *kc = kind ? kind + c0 : nullptr;
+			for (int t0 = 0; t0 < t.nterms; t0 += nt) {
+				const int n = std::min(nt, t.nterms - t0);
+				PadRowsP<C> p = pad_params(Wc, n, t0, kGrids, Pg);
+				for (int g = 0; g < kGrids; g++) {
+					p.comp[g] = RF ? 2 * g : g;
+					p.comp2[g] = RF ? 2 * g + 1 : g;
+					p.psel[g] = RF ? 4 : 3;
+				}
+				p.psiC = Tabs<C>::i3_psi1(t);
+				p.kind = kc; p.want = want;
+				launch(k_any_pad_rows<C>, "any_pad_rows", blocks((long)nc * n * kGrids, nl1), smem(nl1, 1), s, p);
+				plain(Pg, (long)nc * n * kGrids, -1, true, kc, want, (long)n * kGrids);
+				if (fused) {
+					I3FusedP<C> f{};
+					f.What = What; f.Pg = Pg; f.X = X;
+					f.psi2T = Tabs<C>::i3_psi2T(t); f.idx = t.idx.as<int>(); f.scale = t.scale.as<double>();
+					f.N = N; f.nt = n; f.t0 = t0; f.kind = kc; f.want = want;
+					// FP32 default: radix-8 stages (the radix-16 register DFTs push this
+					// kernel to 173 registers, one CTA an SM); FP64 runs one CTA an SM anyway
+					f.pl = (ws.anyn_plan == 0 && sizeof(C) == 8) ? with_tw(make_plan(P, 1)) : pl;
+					launch(k_any_i3_fused<C, RF>, "any_i3_fused", (long)nc * kChains, tile_bytes<C>(P, P), s, f);
+					continue;
+				}
+				I3RowsAP<C> a{};
+				a.What = What; a.Pg = Pg; a.Y = Y; a.N = N; a.nl = nl1; a.nt = n; a.kind = kc; a.want = want; a.pl = pl;
+				launch(k_any_i3_rows_a<C, RF>, "any_i3_rows_a", blocks((long)nc * n * kChains, nl1), smem(nl1, 1), s, a);
+				I3ColsP<C> c{};
+				c.Y = Y; c.psi2T = Tabs<C>::i3_psi2T(t); c.idx = t.idx.as<int>(); c.scale = t.scale.as<double>();
+				c.N = N; c.nl = nl1; c.nt = n; c.t0 = t0; c.cpt = kChains; c.kind = kc; c.want = want; c.pl = pl;
+				launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)nc * n * kChains, nl1), smem(nl1, 1), s, c);
+				I3RowsBP<C> b{};
+				b.Y = Y; b.Pg = Pg; b.X = X; b.N = N; b.nl = nl4; b.nt = n; b.kind = kc; b.want = want; b.pl = pl;
+				launch(k_any_i3_rows_b<C, RF>, "any_i3_rows_b", blocks((long)nc * 4, nl4), smem(nl4, 1), s, b);
+			}
 		}
-		return nxp;
 	}
 
 	AsmP<C> prepare(const double2 *W, int parts) {
@@ -1176,6 +1334,15 @@ unsigned grid1d(long n) { return (unsigned)std::min<long>((n + 255) / 256, 148L 
 
 bool anyn_supported(int N) {
 	return N >= 4 && N <= 128 && N % 2 == 0 && smooth23(N);
+}
+
+void anyn_build_twiddles(Workspace &ws) {
+	const int P = 2 * ws.N;
+	ws.anyn_tw.ensure(P * (sizeof(double2) + sizeof(float2)));
+	double2 *twd = ws.anyn_tw.as<double2>();
+	k_any_build_tw<<<1, 256, 0, ws.stream>>>(P, twd, reinterpret_cast<float2 *>(twd + P));
+	QB_CUDA(cudaGetLastError());
+	QB_CUDA(cudaStreamSynchronize(ws.stream));
 }
 
 bool anyn_route(int N) {

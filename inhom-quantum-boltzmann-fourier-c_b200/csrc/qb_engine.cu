@@ -133,6 +133,7 @@ Workspace::Workspace(int n) : N(n) {
 	QB_CUDA(cudaMemset(i3stats.p, 0, 2 * sizeof(unsigned long long)));
 	kerr.ensure(sizeof(int));
 	QB_CUDA(cudaMemset(kerr.p, 0, sizeof(int)));
+	if (anyn_supported(N)) anyn_build_twiddles(*this);
 }
 
 Workspace::~Workspace() {
@@ -869,6 +870,16 @@ void check_tmem_coresidency() {
 }
 
 }  // namespace
+
+bool real_form_enabled() { return use_real_form(); }
+
+int *i3_form_kinds(Workspace &ws, int ncells, const double2 *W, cudaStream_t s) {
+	ws.i3kind.ensure(sizeof(int) * ncells);
+	int *kind = ws.i3kind.as<int>();
+	launch_nyquist_kind(ws.N, ncells, W, kRealFormBound, kind, ws.i3stats.as<unsigned long long>(), s);
+	return kind;
+}
+
 void ensure_tmem_coresidency() { check_tmem_coresidency(); }
 namespace {
 

@@ -90,14 +90,15 @@ struct Workspace {
 	DevBuf aux, aux2;
 	DevBuf inv;                              // per-cell collision invariants (conservation on)
 	DevBuf scr128a, scr128b;                 // N = 64: per-cluster spectra of the I3 terms, first I2 spectra
-	DevBuf i3kind;                           // N = 64, FP32: per-cell I3 kernel (0 real form, 1 complex)
-	DevBuf i3stats;                          // N = 64, FP32: cells evaluated by the real form, by either form (2 x u64)
+	DevBuf i3kind;                           // FP32 I3 sums: per-cell form (0 real, 1 complex)
+	DevBuf i3stats;                          // FP32 I3 sums: cells evaluated by the real form, by either form (2 x u64)
 	DevBuf kerr;                             // device error word of kernels with bounded waits (nonzero: a wait ran out)
 	DevBuf wave1, wave2;                     // any-N engine: per-wave scratch of the quadrature sums, assembly scratch
 	// any-N engine knobs (0: default): radix-plan variant, lines per tile, wave budget in MB
 	int anyn_plan = 0, anyn_lines = 0;
 	int anyn_fused = 1;                      // any-N engine: whole-grid I3 chains where a grid fits shared memory
 	float anyn_wave_mb = 0.0f;
+	DevBuf anyn_tw;                          // any-N engine: roots of unity of the padded grid (double2, then float2)
 	int i3_variant = 0;                      // I3 sums: 0 the FFT kernels, 1 DFT-GEMMs on the tensor cores (FP32 form, N = 16)
 	// schedule knobs (set by the batch autotuner): multipliers of the heuristic
 	// chunk counts of the I1/I2/I4 sums and of the I3 sums, and the FP64 I3
@@ -173,8 +174,17 @@ bool anyn_route(int N);
 void anyn_operators(Workspace &ws, const QuadSet &q, int ncells, const double2 *W, int parts, double2 *out_cc, double2 *out_cd, cudaStream_t s);
 void anyn_update(Workspace &ws, const QuadSet &q, int ncells, const double2 *base, const double2 *wcur, const double *B, double dtc,
                  double2 *out, cudaStream_t s);
+// the twiddle table ws.anyn_tw (made at construction, outside any graph capture)
+void anyn_build_twiddles(Workspace &ws);
 void anyn_to_fourier(int N, int ngrids, const double *Wv, double2 *Wf, cudaStream_t s);
 void anyn_from_fourier(int N, int ngrids, const double2 *Wf, double *Wv, cudaStream_t s);
+// The FP32 I3 sums take the real form for the cells whose Nyquist content and
+// anti-Hermitian part are at most 1e-6 of the state (QB_I3_KERNEL=complex or
+// pair: never).  i3_form_kinds writes the per-cell form (0 real, 1 complex) of
+// W [ncells][4][N*N] into ws.i3kind, counts the cells in ws.i3stats and
+// returns the device array.
+bool real_form_enabled();
+int *i3_form_kinds(Workspace &ws, int ncells, const double2 *W, cudaStream_t s);
 // FP32 roundings of a table set (made once, on the caller's stream, which is then synchronised)
 void prepare_f32_tables(const QuadSet &q, cudaStream_t s);
 

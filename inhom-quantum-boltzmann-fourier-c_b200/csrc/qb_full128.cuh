@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(kNyqThreads) k_nyquist_kind(int N, const doubl
 		if (k == N / 2 || l == N / 2) {
 			nyq += a;
 		} else {
-			const int kc = (N - k) & (N - 1), lc = (N - l) & (N - 1);      // N is a power of 2
+			const int kc = (N - k) % N, lc = (N - l) % N;
 			const double2 p = w[c * NN + kc + (long)N * lc];
 			anti += hypot(v.x - p.x, v.y + p.y);
 		}

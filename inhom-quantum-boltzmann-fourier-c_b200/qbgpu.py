@@ -182,7 +182,7 @@ class Workspace:
 
     def i3_forms(self, reset=False):
         """(cells whose I3 sums ran in the real form, all cells) evaluated so
-        far through this workspace at N = 32 or 64 in FP32 (zero otherwise)."""
+        far through this workspace in FP32 (zero in FP64)."""
         r, a = C.c_longlong(), C.c_longlong()
         _check(lib().qb_workspace_i3_forms(self.h, C.byref(r), C.byref(a), 1 if reset else 0), "qb_workspace_i3_forms")
         return r.value, a.value

@@ -178,3 +178,47 @@ def test_inhomogeneous_graph_replay_n48(mods):
         L_.qb_profile_reset()
     assert wsd.graph_replays == 0
     assert torch.equal(bufs[steps % 2], ref)
+
+
+def test_waves_do_not_change_the_sums():
+    """The I1-I4 sums run in waves of terms and, where one term of the batch
+    overflows the scratch cap, in slices of cells; every cell still adds its
+    terms in order.  A 1 MB wave budget and scratch cap (QB_ANYN_WAVE_MB,
+    QB_ANYN_SLICE_MB, read per call) cut the batch into slices of one cell
+    and one term a wave; Cc and Cd stay
+    bit-identical to the default waves, FP32 real and complex forms (N = 96,
+    three global passes), FP32 whole-grid chains (N = 48) and FP64 (N = 48
+    with QB_ANYN_FUSED=0).  Run in a child process so the switches do not leak
+    into other tests."""
+    code = r"""
+import os, sys, numpy as np, torch
+sys.path.insert(0, %r); sys.path.insert(0, %r)
+import qbgpu, orc
+def run(N, prec, cells, seed, noisy):
+    q = qbgpu.Quad(N, 2, 2, 6.0, 3.75)
+    Wv = qbgpu.gaussian_mixture_state(N, 6.0, seed=seed, ncells=cells)
+    if noisy:
+        Wv[::2] += 1e-3 * np.random.default_rng(seed).standard_normal(Wv[::2].shape)
+    W = torch.from_numpy(orc.to_fourier(Wv)).cuda()
+    out = []
+    for mb in ("", "1"):
+        os.environ["QB_ANYN_WAVE_MB"] = mb
+        os.environ["QB_ANYN_SLICE_MB"] = mb
+        ws = qbgpu.Workspace(N, precision=prec)
+        out.append([x.cpu().numpy() for x in qbgpu.collision_operators(ws, q, W)])
+        forms = ws.i3_forms()
+    os.environ["QB_ANYN_WAVE_MB"] = os.environ["QB_ANYN_SLICE_MB"] = ""
+    for x, y in zip(*out):
+        assert np.array_equal(x, y), (N, prec)
+    return forms
+assert run(96, 32, 5, 3, True) == (2, 5)
+assert run(48, 32, 5, 4, True) == (2, 5)
+os.environ["QB_ANYN_FUSED"] = "0"
+assert run(48, 64, 3, 5, False) == (0, 0)
+print("ok")
+""" % (os.path.join(ROOT, "inhom-quantum-boltzmann-fourier-c_b200"), os.path.join(ROOT, "oracle"))
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr

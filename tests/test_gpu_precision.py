@@ -96,10 +96,12 @@ def test_fp32_n64_real_form_and_guard():
         assert rel_l2(cd[sl], ref_cd) <= C_TOL
 
 
-@pytest.mark.parametrize("N,J,M", [(32, 4, 3), (64, 4, 3)])
+@pytest.mark.parametrize("N,J,M", [(32, 4, 3), (64, 4, 3), (48, 4, 3), (96, 2, 2), (128, 2, 2)])
 def test_fp32_real_form_guard_routes_non_hermitian_states(N, J, M):
     """The real form of the FP32 I3 sums (N = 32: k_i3pr, N = 64:
-    k_i3_full128r) holds only for Fourier states of real velocity-space
+    k_i3_full128r; N = 48 the whole-grid chains of the any-N engine, N = 96
+    and 128 its three-pass chains, all with two chains packed in one complex
+    transform) holds only for Fourier states of real velocity-space
     components (Hermitian, W(-k) = conj W(k)) without Nyquist content.  Two
     smooth cells take it; two cells with an anti-Hermitian part (a complex
     perturbation kept off the Nyquist row and column, so that only the

@@ -1068,7 +1068,15 @@ template <class C> struct AnyRhs {
 	AnyRhs(Workspace &w, const QuadSet &qs, int nc, cudaStream_t st) : ws(w), q(qs), N(w.N), P(2 * w.N), ncells(nc), s(st) {
 		PP = (long)P * P;
 		pl = with_tw(make_plan(P, ws.anyn_plan));
-		nl1 = pick_lines(P, ws.anyn_lines > 0 ? ws.anyn_lines : std::max(1, 2048 / P), 1, sizeof(C));
+		// lines per tile: the workspace's knob, else QB_ANYN_LINES (read per
+		// call, for comparisons), else tiles of about 4096 (FP32) or 2048 (FP64)
+		// elements.  The FP32 passes keep 4 CTAs an SM, and 16 lines of 192 or
+		// 256 give their radix-16 stages 192 or 256 butterflies a CTA instead of
+		// 96 or 128: 1.3x at N = 96 and 1.24x at N = 128 over 8 lines; the FP64
+		// passes (2 CTAs an SM) were slower with 16.
+		const int env_lines = (int)env_mb("QB_ANYN_LINES");
+		const int def_lines = std::max(1, (sizeof(C) == 8 ? 4096 : 2048) / P);
+		nl1 = pick_lines(P, ws.anyn_lines > 0 ? ws.anyn_lines : env_lines > 0 ? env_lines : def_lines, 1, sizeof(C));
 	}
 	Plan with_tw(Plan p) const {
 		p.twd = ws.anyn_tw.as<double2>();

@@ -304,7 +304,10 @@ template <class C> struct PadRowsP {
 	const R *psiA, *psiB;                 // real N x N tables, one per term
 	const C *psiC;                        // complex N x N tables, one per term
 	C *out;
-	const int *kind; int want;            // kind != null: only the cells of kind `want`
+	// kind != null: the cells of kind 0 (real form) take the first nsub_rf
+	// subs with comp_rf / comp2_rf / psel_rf instead
+	const int *kind;
+	int nsub_rf, comp_rf[4], comp2_rf[4], psel_rf[4];
 	Plan pl;
 };
 template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(const PadRowsP<C> p) {
@@ -321,11 +324,14 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 	const long ct = u / p.nsub;
 	const int t = p.t0 + (int)(ct % p.nt);
 	const long cell = ct / p.nt;
-	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	int ps = p.psel[sub], ca = p.comp[sub], cb = p.comp2[sub];
+	if (p.kind != nullptr && p.kind[cell] == 0) {
+		if (sub >= p.nsub_rf) return;
+		ps = p.psel_rf[sub]; ca = p.comp_rf[sub]; cb = p.comp2_rf[sub];
+	}
 	load_tw(T.tw, P, p.pl);
-	const double2 *w = p.W + cell * p.w_cell + (long)p.comp[sub] * NN;
-	const double2 *w2 = p.W + cell * p.w_cell + (long)p.comp2[sub] * NN;
-	const int ps = p.psel[sub];
+	const double2 *w = p.W + cell * p.w_cell + (long)ca * NN;
+	const double2 *w2 = p.W + cell * p.w_cell + (long)cb * NN;
 	batched<C>(nl * P, [&](int i) {
 		const int li = fdiv(i, mgP), k = i - li * P;
 		const int ls = src_idx(l0 + li, N), ks = src_idx(k, N);
@@ -363,7 +369,9 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 // Fourier representation)
 template <class C> struct PlainP {
 	C *g; int L, nl;
-	const int *kind; int want; long gpc;  // kind != null: only the grids of cells of kind `want` (gpc grids a cell)
+	// kind != null: grids [cell][gpc / nsub][nsub]; a cell of kind 0 (real
+	// form) skips the subs from rf_grids on
+	const int *kind; long gpc; int nsub, rf_grids;
 	Plan pl;
 };
 template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThreads) k_any_plain(const PlainP<C> p) {
@@ -374,7 +382,7 @@ template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThread
 	const int bpg = L / nl;
 	const long u = blockIdx.x / bpg;
 	const int x0 = (int)(blockIdx.x % bpg) * nl;
-	if (p.kind != nullptr && p.kind[u / p.gpc] != p.want) return;
+	if (p.kind != nullptr && p.kind[u / p.gpc] == 0 && (int)(u % p.nsub) >= p.rf_grids) return;
 	init_tw(T.tw, L, p.pl);
 	C *g = p.g + u * (long)L * L;
 	batched<C>(nl * L, [&](int i) {
@@ -529,17 +537,21 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 	}
 }
 
-// I3 chain, first rows: unit u = ((cell nt + tt) 4 + j) 4 + i, inverse
-// transform of the rows of W^_i . P_j into Y[u].  Real form (RF, FP32, cells
-// without Nyquist content, where W^ and P are real): u = ((cell nt + tt) 4 + j)
-// 2 + pr, one complex chain of P_j . (W^_2pr + i W^_2pr+1) for the two combos,
-// and Pg holds two grids per (cell, term), P_2s + i P_2s+1.
+// the real form of the I3 sums exists in FP32 only
+template <class C> __host__ __device__ constexpr bool has_rf() { return sizeof(typename CT<C>::R) == 4; }
+
+// I3 chain, first rows: unit u = (cell nt + tt) 16 + c, inverse transform of
+// the rows of the chain input into Y[u].  Complex form: c = 4 j + i, input
+// W^_i . P_j, Pg holds P_0..P_3 per (cell, term).  Real form (kind 0: FP32
+// cells without Nyquist content, where W^ and P are real): c = 2 j + pr < 8,
+// one complex chain of P_j . (W^_2pr + i W^_2pr+1) for two combos, and Pg
+// slots 0, 1 hold P_0 + i P_1, P_2 + i P_3; its units c >= 8 are idle.
 template <class C> struct I3RowsAP {
 	const C *What, *Pg; C *Y; int N, nl, nt;
-	const int *kind; int want;
+	const int *kind;                      // null: every cell complex
 	Plan pl;
 };
-template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
@@ -548,14 +560,15 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
-	constexpr int kCpt = RF ? 8 : 16;             // chains per (cell, term)
-	const int i3 = (int)(u % (kCpt / 4)), j3 = (int)((u / (kCpt / 4)) % 4);
-	const long ct = u / kCpt, cell = ct / p.nt;
-	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	const int c = (int)(u & 15);
+	const long ct = u >> 4, cell = ct / p.nt;
+	const bool rf = has_rf<C>() && p.kind != nullptr && p.kind[cell] == 0;
+	if (rf && c >= 8) return;
 	load_tw(T.tw, P, p.pl);
-	if constexpr (RF) {
-		const C *G0 = p.What + (cell * 4 + 2 * i3) * PP + (long)l0 * P, *G1 = G0 + PP;
-		const C *Pj = p.Pg + (ct * 2 + j3 / 2) * PP + (long)l0 * P;
+	if (rf) {
+		const int pr = c & 1, j3 = c >> 1;
+		const C *G0 = p.What + (cell * 4 + 2 * pr) * PP + (long)l0 * P, *G1 = G0 + PP;
+		const C *Pj = p.Pg + (ct * 4 + (j3 >> 1)) * PP + (long)l0 * P;
 		const bool im = j3 & 1;
 		batched<Two<C>>(nl * P, [&](int i) {
 			Two<C> v;
@@ -568,8 +581,8 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 			T.a[sw(li * T.pitch + k)] = cscale(v.a, pj);
 		});
 	} else {
-		const C *G = p.What + (cell * 4 + i3) * PP + (long)l0 * P;
-		const C *Pj = p.Pg + (ct * 4 + j3) * PP + (long)l0 * P;
+		const C *G = p.What + (cell * 4 + (c & 3)) * PP + (long)l0 * P;
+		const C *Pj = p.Pg + (ct * 4 + (c >> 2)) * PP + (long)l0 * P;
 		batched<Two<C>>(nl * P, [&](int i) {
 			Two<C> v;
 			v.a = G[i];
@@ -594,8 +607,7 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 template <class C> struct I3ColsP {
 	using R = typename CT<C>::R;
 	C *Y; const R *psi2T; const int *idx; const double *scale; int N, nl, nt, t0;
-	int cpt;                              // chains per (cell, term): 16, or 8 in the real form (no other value)
-	const int *kind; int want;
+	const int *kind;                      // null: every cell complex; kind 0: units c >= 8 idle
 	Plan pl;
 };
 // FP64: two CTAs an SM (at most 128 registers; the pass waits on global loads)
@@ -609,9 +621,9 @@ template <class C> __global__ void __launch_bounds__(kThreads, sizeof(C) == 16 ?
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
-	const int ct = (int)(p.cpt == 8 ? u >> 3 : u >> 4);            // (cell, term) of the wave: below 2^31
+	const int ct = (int)(u >> 4);                                  // (cell, term) of the wave: below 2^31
 	const int cell = ct / p.nt, t = p.t0 + (ct - cell * p.nt);
-	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	if (p.kind != nullptr && p.kind[cell] == 0 && (u & 15) >= 8) return;
 	load_tw(T.tw, P, p.pl);
 	C *g = p.Y + u * PP;
 	batched<C>(nl * P, [&](int i) {
@@ -641,21 +653,21 @@ template <class C> __global__ void __launch_bounds__(kThreads, sizeof(C) == 16 ?
 	}
 }
 
-// I3 chain, last rows: forward transforms of Y[((cell nt + tt) 4 + j) 4 + i],
+// I3 chain, last rows: forward transforms of Y[(cell nt + tt) 16 + 4 j + i],
 // one tile at a time, and X[cell][j] += sum_i eta_i P_i . row, over the
 // wave's terms and i in order, in registers (one CTA per (cell, j, row block);
 // a thread owns the tile elements tid + e kThreads, e < own_of<C>())
 template <class C> __host__ __device__ constexpr int own_of() { return sizeof(C) == 16 ? 8 : 16; }   // nl P <= own_of<C>() kThreads
 template <class C> struct I3RowsBP {
 	const C *Y, *Pg; C *X; int N, nl, nt;
-	const int *kind; int want;
+	const int *kind;                      // null: every cell complex
 	Plan pl;
 };
-// RF: Y holds the two packed chains of (cell, term, j); X[cell][j] (real) +=
-// eta_2pr P_2pr . Re(row) + eta_2pr+1 P_2pr+1 . Im(row)
-template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
+// RF (kind 0): Y[(cell nt + tt) 16 + 2 j + pr] holds the two packed chains of
+// (cell, term, j); X[cell][j] (real) += eta_2pr P_2pr . Re(row) + eta_2pr+1
+// P_2pr+1 . Im(row)
+template <class C, bool RF> __device__ __forceinline__ void i3_rows_b(const I3RowsBP<C> &p, unsigned char *sm) {
 	using R = typename CT<C>::R;
-	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl, ne = nl * P;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
@@ -665,7 +677,6 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 	const int l0 = (int)(blockIdx.x % bpg) * nl;
 	const long cell = cj / 4;
 	const int j3 = (int)(cj % 4);
-	if (p.kind != nullptr && p.kind[cell] != p.want) return;
 	load_tw(T.tw, P, p.pl);
 	C *X = p.X + cj * PP + (long)l0 * P;
 	constexpr int kOwn = own_of<C>();
@@ -679,7 +690,7 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 		const long ct = cell * p.nt + tt;
 		constexpr int kH = RF ? 2 : 4;
 		for (int h = 0; h < kH; h++) {
-			const C *y = p.Y + ((ct * 4 + j3) * kH + h) * PP + (long)l0 * P;
+			const C *y = p.Y + (ct * 16 + j3 * kH + h) * PP + (long)l0 * P;
 			batched<C>(ne, [&](int i) { return y[i]; }, [&](int i, const C &v) {
 				const int li = fdiv(i, mgP), k = i - li * P;
 				T.a[sw(li * T.pitch + k)] = v;
@@ -687,7 +698,7 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 			__syncthreads();
 			const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 			if constexpr (RF) {
-				const C *Pa = p.Pg + (ct * 2 + h) * PP + (long)l0 * P;      // P_2h + i P_2h+1
+				const C *Pa = p.Pg + (ct * 4 + h) * PP + (long)l0 * P;      // P_2h + i P_2h+1
 				const R e0 = h == 0 ? (R)1 : (R)-1;                          // eta_2h; eta_2h+1 = -1
 #pragma unroll
 				for (int e = 0; e < kOwn; e++) {
@@ -721,6 +732,17 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 		if (i < ne) X[i] = acc[e];
 	}
 }
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
+	extern __shared__ __align__(16) unsigned char sm[];
+	const long cell = blockIdx.x / (4L * (2 * p.N / p.nl));         // blocks (cell 4 + j) bpg + row block
+	if constexpr (has_rf<C>()) {
+		if (p.kind != nullptr && p.kind[cell] == 0) {
+			i3_rows_b<C, true>(p, sm);
+			return;
+		}
+	}
+	i3_rows_b<C, false>(p, sm);
+}
 
 // The I3 chains with the whole P x P grid in shared memory (P = 48 and 96 in
 // FP32, P = 48 in FP64): one CTA per (cell, j, i) runs the wave's terms in
@@ -732,23 +754,21 @@ template <class C> struct I3FusedP {
 	using R = typename CT<C>::R;
 	const C *What, *Pg; C *X; const R *psi2T; const int *idx; const double *scale;
 	int N, nt, t0;
-	const int *kind; int want;
+	const int *kind;                      // null: every cell complex
 	Plan pl;
 };
-// RF: one CTA per (cell, j, pr) runs the packed chain of the combos 2pr, 2pr + 1
-// into the real partial X[cell][j][pr] (partials 2, 3 stay zero)
-template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(const I3FusedP<C> p) {
+// RF (kind 0): the CTA (cell, j, pr), pr < 2, runs the packed chain of the
+// combos 2pr, 2pr + 1 into the real partial X[cell][j][pr] (partials 2, 3 stay
+// zero; the CTAs pr >= 2 are idle)
+template <class C, bool RF> __device__ __forceinline__ void i3_fused(const I3FusedP<C> &p, unsigned char *sm) {
 	using R = typename CT<C>::R;
-	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, PPi = P * P;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, P);
 	const unsigned mgP = magic_div((unsigned)P);
-	constexpr int kPer = RF ? 2 : 4;              // CTAs per (cell, j)
-	const long cji = blockIdx.x;                  // (cell 4 + j) kPer + h
-	const long cell = cji / (4 * kPer);
-	const int j3 = (int)((cji / kPer) % 4), h = (int)(cji % kPer);
-	if (p.kind != nullptr && p.kind[cell] != p.want) return;
+	const long cji = blockIdx.x;                  // (cell 4 + j) 4 + h
+	const long cell = cji / 16;
+	const int j3 = (int)((cji / 4) % 4), h = (int)(cji % 4);
 	load_tw(T.tw, P, p.pl);
 	C *X = p.X + ((cell * 4 + j3) * 4 + h) * PP;
 	const C *G = p.What + (cell * 4 + (RF ? 2 * h : h)) * PP;
@@ -757,7 +777,7 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 		const int t = p.t0 + tt;
 		const R sc = (R)p.scale[t];
 		const R *ps = p.psi2T + (long)p.idx[t] * PP;
-		const C *Pj = p.Pg + (RF ? ct * 2 + j3 / 2 : ct * 4 + j3) * PP;
+		const C *Pj = p.Pg + (ct * 4 + (RF ? j3 / 2 : j3)) * PP;
 		{
 			batched<Two<C>>(PPi, [&](int i) {
 				Two<C> v;
@@ -782,7 +802,7 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 			__syncthreads();
 			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, 1, T.pitch, p.pl, T.tw);     // columns
 			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, T.pitch, 1, p.pl, T.tw);     // rows
-			const C *Pa = p.Pg + (RF ? ct * 2 + h : ct * 4 + h) * PP;
+			const C *Pa = p.Pg + (ct * 4 + h) * PP;
 			const R eta = h == 0 ? (R)1 : (R)-1;
 			batched<Two<C>>(PPi, [&](int i) {
 				Two<C> v;
@@ -805,6 +825,17 @@ template <class C, bool RF> __global__ void __launch_bounds__(kThreads) k_any_i3
 			__syncthreads();
 		}
 	}
+}
+template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_fused(const I3FusedP<C> p) {
+	extern __shared__ __align__(16) unsigned char sm[];
+	const long cell = blockIdx.x / 16;
+	if constexpr (has_rf<C>()) {
+		if (p.kind != nullptr && p.kind[cell] == 0) {
+			if (blockIdx.x % 4 < 2) i3_fused<C, true>(p, sm);
+			return;
+		}
+	}
+	i3_fused<C, false>(p, sm);
 }
 
 // assembly rows: Zcc_j and Zcd_j (the combinations of k_assemble) for unit
@@ -1091,10 +1122,11 @@ template <class C> struct AnyRhs {
 		return e != nullptr ? atof(e) : 0.0;
 	}
 	// the wave's scratch in bytes, within L2: the workspace's knob, else
-	// QB_ANYN_WAVE_MB (read per call), else 32 MB
+	// QB_ANYN_WAVE_MB (read per call), else 64 MB (at N = 48 in FP32, 0.82
+	// against 0.90 ms per cell-evaluation with 32 MB)
 	double wave_budget() const {
 		const double mb = ws.anyn_wave_mb > 0 ? ws.anyn_wave_mb : env_mb("QB_ANYN_WAVE_MB");
-		return (mb > 0 ? mb : 32.0) * 1048576.0;
+		return (mb > 0 ? mb : 64.0) * 1048576.0;
 	}
 	// terms per wave: the wave's scratch of `per_term` grids per cell for nc cells within the budget
 	int wave(int nterms, int per_term, int nc = -1) const {
@@ -1117,11 +1149,12 @@ template <class C> struct AnyRhs {
 		return (ncells + nslices - 1) / nslices;
 	}
 
-	// kind != null: only the grids of the cells of kind `want`, gpc grids a cell
-	void plain(C *g, long ngrids, int dir, bool cols, const int *kind = nullptr, int want = 0, long gpc = 1) {
+	// kind != null: grids [cell][gpc / nsub][nsub], and the cells of kind 0
+	// skip the subs from rf_grids on
+	void plain(C *g, long ngrids, int dir, bool cols, const int *kind = nullptr, long gpc = 1, int nsub = 1, int rf_grids = 1) {
 		PlainP<C> p{};
 		p.g = g; p.L = P; p.nl = nl1; p.pl = pl;
-		p.kind = kind; p.want = want; p.gpc = gpc;
+		p.kind = kind; p.gpc = gpc; p.nsub = nsub; p.rf_grids = rf_grids;
 		const long nb = blocks(ngrids, nl1);
 		const size_t sm = smem(nl1, 1);
 		if (dir < 0) {
@@ -1216,35 +1249,33 @@ template <class C> struct AnyRhs {
 
 	// returns the partials of X per (cell, j).  FP32: the cells of kind 0 (no
 	// Nyquist content, Hermitian state) take the real form, two chains packed
-	// in one complex transform; the others the complex chains.
+	// in one complex transform, the others the complex chains, in the same
+	// launches (the kernels read a cell's kind; the real form leaves half of
+	// its units idle)
 	int i3_sums(const DevI3 &t, const double2 *W) {
 		const int nxp = fused_i3() ? 4 : 1;
 		ws.i3p.ensure(sizeof(C) * ncells * 4 * nxp * PP);
 		QB_CUDA(cudaMemsetAsync(ws.i3p.p, 0, sizeof(C) * ncells * 4 * nxp * PP, s));
+		const int *kind = nullptr;
 		if constexpr (sizeof(typename CT<C>::R) == 4) {
-			if (real_form_enabled()) {
-				const int *kind = i3_form_kinds(ws, ncells, W, s);
-				i3_waves<true>(t, W, nxp, kind, 0);
-				i3_waves<false>(t, W, nxp, kind, 1);
-				return nxp;
-			}
+			if (real_form_enabled()) kind = i3_form_kinds(ws, ncells, W, s);
 		}
-		i3_waves<false>(t, W, nxp, nullptr, 0);
+		i3_waves(t, W, nxp, kind);
 		return nxp;
 	}
 
 	// the I3 chains in waves of terms and, where one term of the batch
-	// overflows the scratch cap, slices of cells; RF: the real form (Pg holds
-	// the packed pairs P_0 + i P_1, P_2 + i P_3, and 8 chains a (cell, term)).
-	// A cell's terms still run in order, so the sums do not depend on the waves.
-	template <bool RF> void i3_waves(const DevI3 &t, const double2 *W, int nxp, const int *kind, int want) {
-		constexpr int kGrids = RF ? 2 : 4, kChains = RF ? 8 : 16;
+	// overflows the scratch cap, slices of cells.  Per (cell, term): 4 grids
+	// of Pg (P_0..P_3, or the packed P_0 + i P_1, P_2 + i P_3 of the real
+	// form) and 16 chains (8 in the real form).  A cell's terms still run in
+	// order, so the sums do not depend on the waves.
+	void i3_waves(const DevI3 &t, const double2 *W, int nxp, const int *kind) {
 		const bool fused = nxp == 4;
-		const int per_term = fused ? kGrids : kGrids + kChains;
+		const int per_term = fused ? 4 : 20;
 		const int cpw = wave_cells(per_term);
 		const int nt = wave(t.nterms, per_term, cpw);
-		ws.wave1.ensure(sizeof(C) * (size_t)cpw * nt * kGrids * PP);                // P_j
-		if (!fused) ws.wave2.ensure(sizeof(C) * (size_t)cpw * nt * kChains * PP);   // chains
+		ws.wave1.ensure(sizeof(C) * (size_t)cpw * nt * 4 * PP);                // P_j
+		if (!fused) ws.wave2.ensure(sizeof(C) * (size_t)cpw * nt * 16 * PP);   // chains
 		C *Pg = ws.wave1.as<C>(), *Y = fused ? nullptr : ws.wave2.as<C>();
 		int nl4 = nl1;                                      // one tile, at most kOwn elements a thread
 		while (nl4 > 1 && (nl4 * P > own_of<C>() * kThreads || P % nl4)) nl4--;
@@ -1256,37 +1287,34 @@ template <class C> struct AnyRhs {
 			const int *kc = kind ? kind + c0 : nullptr;
 			for (int t0 = 0; t0 < t.nterms; t0 += nt) {
 				const int n = std::min(nt, t.nterms - t0);
-				PadRowsP<C> p = pad_params(Wc, n, t0, kGrids, Pg);
-				for (int g = 0; g < kGrids; g++) {
-					p.comp[g] = RF ? 2 * g : g;
-					p.comp2[g] = RF ? 2 * g + 1 : g;
-					p.psel[g] = RF ? 4 : 3;
-				}
+				PadRowsP<C> p = pad_params(Wc, n, t0, 4, Pg);
+				for (int g = 0; g < 4; g++) { p.comp[g] = g; p.comp2[g] = g; p.psel[g] = 3; }
+				p.kind = kc; p.nsub_rf = 2;
+				for (int g = 0; g < 2; g++) { p.comp_rf[g] = 2 * g; p.comp2_rf[g] = 2 * g + 1; p.psel_rf[g] = 4; }
 				p.psiC = Tabs<C>::i3_psi1(t);
-				p.kind = kc; p.want = want;
-				launch(k_any_pad_rows<C>, "any_pad_rows", blocks((long)nc * n * kGrids, nl1), smem(nl1, 1), s, p);
-				plain(Pg, (long)nc * n * kGrids, -1, true, kc, want, (long)n * kGrids);
+				pad_rows(p, nc);
+				plain(Pg, (long)nc * n * 4, -1, true, kc, (long)n * 4, 4, 2);
 				if (fused) {
 					I3FusedP<C> f{};
 					f.What = What; f.Pg = Pg; f.X = X;
 					f.psi2T = Tabs<C>::i3_psi2T(t); f.idx = t.idx.as<int>(); f.scale = t.scale.as<double>();
-					f.N = N; f.nt = n; f.t0 = t0; f.kind = kc; f.want = want;
+					f.N = N; f.nt = n; f.t0 = t0; f.kind = kc;
 					// FP32 default: radix-8 stages (the radix-16 register DFTs push this
 					// kernel to 173 registers, one CTA an SM); FP64 runs one CTA an SM anyway
 					f.pl = (ws.anyn_plan == 0 && sizeof(C) == 8) ? with_tw(make_plan(P, 1)) : pl;
-					launch(k_any_i3_fused<C, RF>, "any_i3_fused", (long)nc * kChains, tile_bytes<C>(P, P), s, f);
+					launch(k_any_i3_fused<C>, "any_i3_fused", (long)nc * 16, tile_bytes<C>(P, P), s, f);
 					continue;
 				}
 				I3RowsAP<C> a{};
-				a.What = What; a.Pg = Pg; a.Y = Y; a.N = N; a.nl = nl1; a.nt = n; a.kind = kc; a.want = want; a.pl = pl;
-				launch(k_any_i3_rows_a<C, RF>, "any_i3_rows_a", blocks((long)nc * n * kChains, nl1), smem(nl1, 1), s, a);
+				a.What = What; a.Pg = Pg; a.Y = Y; a.N = N; a.nl = nl1; a.nt = n; a.kind = kc; a.pl = pl;
+				launch(k_any_i3_rows_a<C>, "any_i3_rows_a", blocks((long)nc * n * 16, nl1), smem(nl1, 1), s, a);
 				I3ColsP<C> c{};
 				c.Y = Y; c.psi2T = Tabs<C>::i3_psi2T(t); c.idx = t.idx.as<int>(); c.scale = t.scale.as<double>();
-				c.N = N; c.nl = nl1; c.nt = n; c.t0 = t0; c.cpt = kChains; c.kind = kc; c.want = want; c.pl = pl;
-				launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)nc * n * kChains, nl1), smem(nl1, 1), s, c);
+				c.N = N; c.nl = nl1; c.nt = n; c.t0 = t0; c.kind = kc; c.pl = pl;
+				launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)nc * n * 16, nl1), smem(nl1, 1), s, c);
 				I3RowsBP<C> b{};
-				b.Y = Y; b.Pg = Pg; b.X = X; b.N = N; b.nl = nl4; b.nt = n; b.kind = kc; b.want = want; b.pl = pl;
-				launch(k_any_i3_rows_b<C, RF>, "any_i3_rows_b", blocks((long)nc * 4, nl4), smem(nl4, 1), s, b);
+				b.Y = Y; b.Pg = Pg; b.X = X; b.N = N; b.nl = nl4; b.nt = n; b.kind = kc; b.pl = pl;
+				launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)nc * 4, nl4), smem(nl4, 1), s, b);
 			}
 		}
 	}

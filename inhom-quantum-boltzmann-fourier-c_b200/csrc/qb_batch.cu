@@ -135,10 +135,12 @@ Sched autotune(qb::Workspace &ws, const qb::Quad &q, int N, int prec, int g, con
 		// the any-N engine: radix schedules (fewest stages, radix 8 first, radix 3
 		// first, radix 4 only), tile heights (lines per tile), wave budgets, and the
 		// global-pass I3 chains against the whole-grid ones
-		const int P = 2 * N, dl = std::max(1, 2048 / P);
+		// (the engine's defaults: tiles of about 4096 elements in FP32, 2048 in
+		// FP64; a 64 MB wave budget)
+		const int P = 2 * N, dl = std::max(1, (prec == 32 ? 4096 : 2048) / P);
 		for (int v : { 1, 2, 3 }) { Sched c; c.plan = v; cand.push_back(c); }
 		for (int nl : { dl / 2, 2 * dl }) if (nl >= 1 && nl <= P) { Sched c; c.lines = nl; cand.push_back(c); }
-		for (float mb : { 12.0f, 96.0f }) { Sched c; c.wave_mb = mb; cand.push_back(c); }
+		for (float mb : { 24.0f, 128.0f }) { Sched c; c.wave_mb = mb; cand.push_back(c); }
 		{ Sched c; c.fused = 0; cand.push_back(c); }
 	} else {
 		cand.resize(5);

@@ -212,6 +212,86 @@ template <int DIR, class C> __device__ C *fft_lines(C *a, C *b, int nl, int ls, 
 	return a;
 }
 
+// The same stages with the data path given by functors, so that a pass
+// reads its first stage straight from global memory and its last stage
+// stores straight to its destination (global memory, or shared memory with a
+// pointwise factor applied) instead of staging whole tiles through shared
+// memory.  ld(line, i) -> C and st(line, i, v) address element i of a line.
+// LF (line-fastest) hands consecutive lines to consecutive threads, the
+// coalesced order for the columns of a row-major grid in global memory;
+// otherwise consecutive threads take consecutive butterflies of a line, the
+// coalesced order for rows.  Shared-memory layouts are the caller's.
+template <int RAD, int DIR, bool LF, class C, class Ld, class St>
+__device__ __forceinline__ void stage_f(int nl, int L, int Ns, const C *tw, const Ld &ld, const St &st) {
+	const int m = L / RAD, tstep = L / (Ns * RAD);
+	const unsigned mg_m = magic_div((unsigned)m), mg_ns = magic_div((unsigned)Ns), mg_nl = magic_div((unsigned)nl);
+	for (int b = threadIdx.x; b < nl * m; b += blockDim.x) {
+		int line, j;
+		if (LF) {
+			j = fdiv(b, mg_nl);
+			line = b - j * nl;
+		} else {
+			line = fdiv(b, mg_m);
+			j = b - line * m;
+		}
+		const int jq = fdiv(j, mg_ns), k = j - jq * Ns;
+		C v[RAD];
+#pragma unroll
+		for (int r = 0; r < RAD; r++) v[r] = ld(line, j + r * m);
+		if (Ns > 1) {
+#pragma unroll
+			for (int r = 1; r < RAD; r++) {
+				C w = tw[r * k * tstep];                        // r k tstep < L
+				if (DIR > 0) w.y = -w.y;
+				v[r] = cmul(v[r], w);
+			}
+		}
+		dft_r<RAD, DIR>(v);
+		const int ob = jq * Ns * RAD + k;
+#pragma unroll
+		for (int r = 0; r < RAD; r++) st(line, ob + freq_of<RAD>(r) * Ns, v[r]);
+	}
+}
+template <int DIR, bool LF, class C, class Ld, class St>
+__device__ __forceinline__ void stage_any(int R, int nl, int L, int Ns, const C *tw, const Ld &ld, const St &st) {
+	if (R == 16) stage_f<16, DIR, LF>(nl, L, Ns, tw, ld, st);
+	else if (R == 12) stage_f<12, DIR, LF>(nl, L, Ns, tw, ld, st);
+	else if (R == 8) stage_f<8, DIR, LF>(nl, L, Ns, tw, ld, st);
+	else if (R == 6) stage_f<6, DIR, LF>(nl, L, Ns, tw, ld, st);
+	else if (R == 4) stage_f<4, DIR, LF>(nl, L, Ns, tw, ld, st);
+	else if (R == 3) stage_f<3, DIR, LF>(nl, L, Ns, tw, ld, st);
+	else stage_f<2, DIR, LF>(nl, L, Ns, tw, ld, st);
+}
+// An FFT of nl lines: the first stage reads through ld0 (mapping LF0), the
+// middle stages ping-pong between the line-contiguous shared buffers a and b
+// (element i of a line at sw(line pitch + i)), the last stage (mapping LF1)
+// stores through st1(line, i, v, free), where `free` is the buffer that the
+// last stage does not read.  The first stage writes a, so ld0 must not read a.
+// A barrier follows every stage but the last; returns `free`.
+template <int DIR, bool LF0, bool LF1, class C, class Ld, class St>
+__device__ C *fft_f(int nl, int pitch, const Plan &pl, const C *tw, C *a, C *b, const Ld &ld0, const St &st1) {
+	int Ns = 1;
+	C *cur = b, *nxt = a;
+	for (int s = 0; s < pl.nst; s++) {
+		const int R = pl.r[s];
+		const bool first = s == 0, last = s == pl.nst - 1;
+		C *const in = cur, *const out = nxt;
+		auto sm_ld = [in, pitch](int line, int i) { return in[sw(line * pitch + i)]; };
+		auto sm_st = [out, pitch](int line, int i, const C &v) { out[sw(line * pitch + i)] = v; };
+		auto st_last = [&st1, out](int line, int i, const C &v) { st1(line, i, v, out); };
+		if (first && last) stage_any<DIR, LF0>(R, nl, pl.L, Ns, tw, ld0, st_last);
+		else if (first) stage_any<DIR, LF0>(R, nl, pl.L, Ns, tw, ld0, sm_st);
+		else if (last) stage_any<DIR, LF1>(R, nl, pl.L, Ns, tw, sm_ld, st_last);
+		else stage_any<DIR, false>(R, nl, pl.L, Ns, tw, sm_ld, sm_st);
+		if (last) return out;
+		__syncthreads();
+		cur = out;
+		nxt = (out == a) ? b : a;
+		Ns *= R;
+	}
+	return nxt;
+}
+
 // the twiddle table tw[m] = exp(-2 pi i m / L), then a CTA barrier
 __device__ __forceinline__ const double2 *plan_tw(const Plan &pl, double2 *) { return pl.twd; }
 __device__ __forceinline__ const float2 *plan_tw(const Plan &pl, float2 *) { return pl.twf; }
@@ -537,6 +617,11 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 	}
 }
 
+// resident CTAs an SM that the column pass of the chains is compiled for: two
+// in FP64 (at most 128 registers); FP32 takes the compiler's choice (76
+// registers, three CTAs, measured ahead of four CTAs with spills at N = 128)
+template <class C> constexpr int pass_ctas() { return sizeof(C) == 16 ? 2 : 0; }
+
 // the real form of the I3 sums exists in FP32 only
 template <class C> __host__ __device__ constexpr bool has_rf() { return sizeof(typename CT<C>::R) == 4; }
 
@@ -610,8 +695,7 @@ template <class C> struct I3ColsP {
 	const int *kind;                      // null: every cell complex; kind 0: units c >= 8 idle
 	Plan pl;
 };
-// FP64: two CTAs an SM (at most 128 registers; the pass waits on global loads)
-template <class C> __global__ void __launch_bounds__(kThreads, sizeof(C) == 16 ? 2 : 0) k_any_i3_cols(const I3ColsP<C> p) {
+template <class C> __global__ void __launch_bounds__(kThreads, pass_ctas<C>()) k_any_i3_cols(const I3ColsP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
@@ -625,32 +709,25 @@ template <class C> __global__ void __launch_bounds__(kThreads, sizeof(C) == 16 ?
 	const int cell = ct / p.nt, t = p.t0 + (ct - cell * p.nt);
 	if (p.kind != nullptr && p.kind[cell] == 0 && (u & 15) >= 8) return;
 	load_tw(T.tw, P, p.pl);
+	// columns k0 + line of the chain grid, element i = row i: the first
+	// transform reads them from global memory (line-fastest, coalesced) and
+	// its last stage applies psi2_t (rows k0.. of the transposed table, read
+	// along a line: J-fastest, coalesced) on the way into shared memory; the
+	// second transform writes them back
 	C *g = p.Y + u * PP;
-	batched<C>(nl * P, [&](int i) {
-		const int l = fdiv(i, mgnl), kk = i - l * nl;
-		return g[(long)l * P + k0 + kk];
-	}, [&](int i, const C &v) {
-		const int l = fdiv(i, mgnl), kk = i - l * nl;
-		T.a[sw(kk * T.pitch + l)] = v;
-	});
-	__syncthreads();
-	C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	const R sc = (R)p.scale[t];
-	const R *ps = p.psi2T + (long)p.idx[t] * PP + (long)k0 * P;       // rows k0.. of the transposed table: contiguous
-	batched<R>(nl * P, [&](int i) { return ps[i]; }, [&](int i, const R &f0) {
-		const int kk = fdiv(i, mgP), l = i - kk * P;                   // table element (k0 + kk, l)
-		const R f = sc * f0;
-		C x = r[sw(kk * T.pitch + l)];
-		x.x *= f;
-		x.y *= f;
-		r[sw(kk * T.pitch + l)] = x;
-	});
+	const R *ps = p.psi2T + (long)p.idx[t] * PP + (long)k0 * P;
+	const int pitch = T.pitch;
+	auto ld0 = [g, P, k0](int line, int i) { return g[(long)i * P + k0 + line]; };
+	auto st_psi = [ps, sc, P, pitch](int line, int i, const C &v, C *out) {
+		out[sw(line * pitch + i)] = cscale(v, sc * ps[line * P + i]);
+	};
+	C *X = fft_f<+1, true, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st_psi);
 	__syncthreads();
-	const C *r2 = fft_lines<-1>(r, r == T.a ? T.b : T.a, nl, T.pitch, 1, p.pl, T.tw);
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int l = fdiv(i, mgnl), kk = i - l * nl;
-		g[(long)l * P + k0 + kk] = r2[sw(kk * T.pitch + l)];
-	}
+	auto ld1 = [X, pitch](int line, int i) { return X[sw(line * pitch + i)]; };
+	auto st_g = [g, P, k0](int line, int i, const C &v, C *) { g[(long)i * P + k0 + line] = v; };
+	fft_f<-1, false, true>(nl, pitch, p.pl, T.tw, X == T.a ? T.b : T.a, X, ld1, st_g);
+	(void)mgP; (void)mgnl;
 }
 
 // I3 chain, last rows: forward transforms of Y[(cell nt + tt) 16 + 4 j + i],
@@ -691,12 +768,11 @@ template <class C, bool RF> __device__ __forceinline__ void i3_rows_b(const I3Ro
 		constexpr int kH = RF ? 2 : 4;
 		for (int h = 0; h < kH; h++) {
 			const C *y = p.Y + (ct * 16 + j3 * kH + h) * PP + (long)l0 * P;
-			batched<C>(ne, [&](int i) { return y[i]; }, [&](int i, const C &v) {
-				const int li = fdiv(i, mgP), k = i - li * P;
-				T.a[sw(li * T.pitch + k)] = v;
-			});
+			const int pitch = T.pitch;
+			auto ld0 = [y, P](int line, int i) { return y[(long)line * P + i]; };
+			auto st1 = [pitch](int line, int i, const C &v, C *out) { out[sw(line * pitch + i)] = v; };
+			const C *r = fft_f<-1, false, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
 			__syncthreads();
-			const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 			if constexpr (RF) {
 				const C *Pa = p.Pg + (ct * 4 + h) * PP + (long)l0 * P;      // P_2h + i P_2h+1
 				const R e0 = h == 0 ? (R)1 : (R)-1;                          // eta_2h; eta_2h+1 = -1

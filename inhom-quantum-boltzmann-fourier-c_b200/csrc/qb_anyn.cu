@@ -409,6 +409,11 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 		if (sub >= p.nsub_rf) return;
 		ps = p.psel_rf[sub]; ca = p.comp_rf[sub]; cb = p.comp2_rf[sub];
 	}
+	if (l0 >= N / 2 && l0 + nl <= 3 * N / 2) {     // every row of the tile in the zero band: its transform is zero
+		C *o = p.out + u * PP + (long)l0 * P;
+		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) o[i] = czero<C>();
+		return;
+	}
 	load_tw(T.tw, P, p.pl);
 	const double2 *w = p.W + cell * p.w_cell + (long)ca * NN;
 	const double2 *w2 = p.W + cell * p.w_cell + (long)cb * NN;

@@ -1320,12 +1320,20 @@ template <class C> struct AnyRhs {
 		}
 	}
 
-	// whole-grid chains when the tile fits (QB_ANYN_FUSED=0 or the knob turns them off)
+	// whole-grid chains (k_any_i3_fused) or the three passes.  The workspace's
+	// knob (0 off, 1 on), else QB_ANYN_FUSED (read per call), else the
+	// default: FP64 takes the whole-grid chains where a grid fits a CTA; FP32
+	// takes the three passes, measured faster at N = 24 (0.216 against 0.316
+	// ms per cell-evaluation) and N = 48 (0.710 against 0.807) once the passes
+	// read and store from their FFT stages
 	bool fused_i3() const {
-		if (ws.anyn_fused == 0) return false;
-		const char *e = getenv("QB_ANYN_FUSED");
-		if (e != nullptr && strcmp(e, "0") == 0) return false;
-		return tile_bytes<C>(P, P) <= kMaxSmem;
+		int on = ws.anyn_fused;
+		if (on < 0) {
+			const char *e = getenv("QB_ANYN_FUSED");
+			if (e != nullptr && (strcmp(e, "0") == 0 || strcmp(e, "1") == 0)) on = e[0] - '0';
+		}
+		if (on < 0) on = sizeof(C) == 16 ? 1 : 0;
+		return on == 1 && tile_bytes<C>(P, P) <= kMaxSmem;
 	}
 
 	// returns the partials of X per (cell, j).  FP32: the cells of kind 0 (no

@@ -76,7 +76,7 @@ struct Sched {
 	float s12 = 1.0f, s3 = 1.0f;
 	int ranges = -1, variant = 0;
 	int plan = 0, lines = 0;          // any-N engine: radix-plan variant, lines per tile (0: default)
-	int fused = 1;                    // any-N engine: whole-grid I3 chains where a grid fits shared memory
+	int fused = -1;                   // any-N engine: whole-grid I3 chains (1), three passes (0), default (-1)
 	float wave_mb = 0.0f;             // any-N engine: wave budget (0: default)
 	double ms = 0.0;
 };
@@ -134,14 +134,15 @@ Sched autotune(qb::Workspace &ws, const qb::Quad &q, int N, int prec, int g, con
 	if (qb::anyn_route(N)) {
 		// the any-N engine: radix schedules (fewest stages, radix 8 first, radix 3
 		// first, radix 4 only), tile heights (lines per tile), wave budgets, and the
-		// global-pass I3 chains against the whole-grid ones
+		// three-pass I3 chains against the whole-grid ones (both forced; the
+		// default picks by precision)
 		// (the engine's defaults: tiles of about 4096 elements in FP32, 2048 in
 		// FP64; a 64 MB wave budget)
 		const int P = 2 * N, dl = std::max(1, (prec == 32 ? 4096 : 2048) / P);
 		for (int v : { 1, 2, 3 }) { Sched c; c.plan = v; cand.push_back(c); }
 		for (int nl : { dl / 2, 2 * dl }) if (nl >= 1 && nl <= P) { Sched c; c.lines = nl; cand.push_back(c); }
 		for (float mb : { 24.0f, 128.0f }) { Sched c; c.wave_mb = mb; cand.push_back(c); }
-		{ Sched c; c.fused = 0; cand.push_back(c); }
+		for (int f : { 0, 1 }) { Sched c; c.fused = f; cand.push_back(c); }
 	} else {
 		cand.resize(5);
 		cand[1].s12 = 0.5f;

@@ -96,7 +96,7 @@ struct Workspace {
 	DevBuf wave1, wave2;                     // any-N engine: per-wave scratch of the quadrature sums, assembly scratch
 	// any-N engine knobs (0: default): radix-plan variant, lines per tile, wave budget in MB
 	int anyn_plan = 0, anyn_lines = 0;
-	int anyn_fused = 1;                      // any-N engine: whole-grid I3 chains where a grid fits shared memory
+	int anyn_fused = -1;                     // any-N engine: whole-grid I3 chains (1), three passes (0), the engine's default (-1)
 	float anyn_wave_mb = 0.0f;
 	DevBuf anyn_tw;                          // any-N engine: roots of unity of the padded grid (double2, then float2)
 	int i3_variant = 0;                      // I3 sums: 0 the FFT kernels, 1 DFT-GEMMs on the tensor cores (FP32 form, N = 16)

@@ -66,6 +66,35 @@ def test_operators_fp32_vs_oracle(mods, N, J, M):
         assert rel_l1(cd[i], o.cd(WF[i])) < 1e-5
 
 
+@pytest.mark.parametrize("fused", ["1", "0"])
+def test_fp32_i3_chain_paths_vs_oracle(mods, fused):
+    """The two I3 chain paths of the FP32 form at N = 24: whole-grid chains
+    (QB_ANYN_FUSED=1, the FP64 default where a grid fits) and three global
+    passes (QB_ANYN_FUSED=0, the FP32 default), each on two smooth cells (real
+    form) and one noisy cell (complex form), within 1e-5 of the oracle."""
+    torch, qbgpu, orc = mods
+    N, J, M = 24, 4, 3
+    ws, q = qbgpu.Workspace(N, precision=32), qbgpu.Quad(N, J, M, L, R)
+    o = orc.Oracle(N, J, M, L, R)
+    Wv = qbgpu.gaussian_mixture_state(N, L, seed=124, ncells=3)
+    Wv[2] += 1e-3 * np.random.default_rng(24).standard_normal(Wv[2].shape)
+    WF = orc.to_fourier(Wv)
+    old = os.environ.get("QB_ANYN_FUSED")
+    os.environ["QB_ANYN_FUSED"] = fused
+    try:
+        cc, cd = qbgpu.collision_operators(ws, q, torch.from_numpy(WF).cuda())
+    finally:
+        if old is None:
+            del os.environ["QB_ANYN_FUSED"]
+        else:
+            os.environ["QB_ANYN_FUSED"] = old
+    assert ws.i3_forms() == (2, 3)          # Nyquist fraction of the smooth cells: 2.3e-7 (bound 1e-6)
+    cc, cd = cc.cpu().numpy(), cd.cpu().numpy()
+    for i in range(3):
+        assert rel_l1(cc[i], o.cc(WF[i])) < 1e-5
+        assert rel_l1(cd[i], o.cd(WF[i])) < 1e-5
+
+
 def test_n128_fp64_collision_step_vs_oracle(mods):
     torch, qbgpu, orc = mods
     N, J, M = 128, 2, 2
@@ -187,8 +216,8 @@ def test_waves_do_not_change_the_sums():
     QB_ANYN_SLICE_MB, read per call) cut the batch into slices of one cell
     and one term a wave; Cc and Cd stay
     bit-identical to the default waves, FP32 real and complex forms (N = 96,
-    three global passes), FP32 whole-grid chains (N = 48) and FP64 (N = 48
-    with QB_ANYN_FUSED=0).  Run in a child process so the switches do not leak
+    three global passes), FP32 whole-grid chains (N = 48, QB_ANYN_FUSED=1) and
+    FP64 (N = 48 with QB_ANYN_FUSED=0).  Run in a child process so the switches do not leak
     into other tests."""
     code = r"""
 import os, sys, numpy as np, torch
@@ -212,6 +241,7 @@ def run(N, prec, cells, seed, noisy):
         assert np.array_equal(x, y), (N, prec)
     return forms
 assert run(96, 32, 5, 3, True) == (2, 5)
+os.environ["QB_ANYN_FUSED"] = "1"
 assert run(48, 32, 5, 4, True) == (2, 5)
 os.environ["QB_ANYN_FUSED"] = "0"
 assert run(48, 64, 3, 5, False) == (0, 0)

@@ -292,6 +292,44 @@ __device__ C *fft_f(int nl, int pitch, const Plan &pl, const C *tw, C *a, C *b, 
 	return nxt;
 }
 
+// fft_f for a plan of exactly two stages R1 R2 known at compile time: the
+// same arithmetic with only its two stage bodies in the kernel (the run-time
+// dispatch of fft_f compiles every radix at every position, and the kernels
+// that hold two transforms then stall on instruction fetch).  R1 = 0: fft_f.
+template <int R1, int R2, int DIR, bool LF0, bool LF1, class C, class Ld, class St>
+__device__ C *fft_fx(int nl, int pitch, const Plan &pl, const C *tw, C *a, C *b, const Ld &ld0, const St &st1) {
+	if constexpr (R1 == 0) {
+		return fft_f<DIR, LF0, LF1>(nl, pitch, pl, tw, a, b, ld0, st1);
+	} else {
+		auto sm_st = [a, pitch](int line, int i, const C &v) { a[sw(line * pitch + i)] = v; };
+		stage_f<R1, DIR, LF0>(nl, R1 * R2, 1, tw, ld0, sm_st);
+		__syncthreads();
+		auto sm_ld = [a, pitch](int line, int i) { return a[sw(line * pitch + i)]; };
+		auto st_last = [&st1, b](int line, int i, const C &v) { st1(line, i, v, b); };
+		stage_f<R2, DIR, LF1>(nl, R1 * R2, R1, tw, sm_ld, st_last);
+		return b;
+	}
+}
+// fft_lines with the two stages of the plan known at compile time (R1 = 0:
+// fft_lines); the result is in a again
+template <int R1, int R2, int DIR, class C> __device__ C *fft_lines_x(C *a, C *b, int nl, int ls, int es, const Plan &pl, const C *tw) {
+	if constexpr (R1 == 0) {
+		return fft_lines<DIR>(a, b, nl, ls, es, pl, tw);
+	} else {
+		stage<R1, DIR>(a, b, nl, ls, es, R1 * R2, 1, tw);
+		__syncthreads();
+		stage<R2, DIR>(b, a, nl, ls, es, R1 * R2, R1, tw);
+		__syncthreads();
+		return a;
+	}
+}
+// the (R1, R2) instantiations a pass kernel has: the default plans of the
+// engine's FP32 and FP64 sizes P = 48, 96, 192, 256 (16 3, 16 6, 16 12, 16 16)
+inline int two_stage_key(const Plan &pl) {
+	if (pl.nst != 2 || pl.r[0] != 16) return 0;
+	return (pl.r[1] == 3 || pl.r[1] == 6 || pl.r[1] == 12 || pl.r[1] == 16) ? pl.r[1] : 0;
+}
+
 // the twiddle table tw[m] = exp(-2 pi i m / L), then a CTA barrier
 __device__ __forceinline__ const double2 *plan_tw(const Plan &pl, double2 *) { return pl.twd; }
 __device__ __forceinline__ const float2 *plan_tw(const Plan &pl, float2 *) { return pl.twf; }
@@ -390,7 +428,7 @@ template <class C> struct PadRowsP {
 	int nsub_rf, comp_rf[4], comp2_rf[4], psel_rf[4];
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(const PadRowsP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(const PadRowsP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int N = p.N, P = 2 * N, nl = p.nl;
@@ -442,7 +480,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_pad_rows(co
 		T.a[sw(li * T.pitch + k)] = v;
 	});
 	__syncthreads();
-	const C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+	const C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	C *o = p.out + u * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int li = fdiv(i, mgP), k = i - li * P;
@@ -459,7 +497,7 @@ template <class C> struct PlainP {
 	const int *kind; long gpc; int nsub, rf_grids;
 	Plan pl;
 };
-template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThreads) k_any_plain(const PlainP<C> p) {
+template <class C, int DIR, bool COLS, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_plain(const PlainP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int L = p.L, nl = p.nl;
 	Tile<C> T(sm, L, nl);
@@ -479,7 +517,7 @@ template <class C, int DIR, bool COLS> __global__ void __launch_bounds__(kThread
 		else { const int li = fdiv(i, mgP), k = i - li * L; T.a[sw(li * T.pitch + k)] = v; }
 	});
 	__syncthreads();
-	const C *r = fft_lines<DIR>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+	const C *r = fft_lines_x<R1, R2, DIR>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
 		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; g[(long)l * L + x0 + kk] = r[sw(kk * T.pitch + l)]; }
 		else { const int li = fdiv(i, mgP), k = i - li * L; g[(long)(x0 + li) * L + k] = r[sw(li * T.pitch + k)]; }
@@ -641,7 +679,7 @@ template <class C> struct I3RowsAP {
 	const int *kind;                      // null: every cell complex
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(const I3RowsAP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
@@ -684,7 +722,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_a(c
 		});
 	}
 	__syncthreads();
-	const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+	const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	C *o = p.Y + u * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int li = fdiv(i, mgP), k = i - li * P;
@@ -700,7 +738,7 @@ template <class C> struct I3ColsP {
 	const int *kind;                      // null: every cell complex; kind 0: units c >= 8 idle
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads, pass_ctas<C>()) k_any_i3_cols(const I3ColsP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, pass_ctas<C>()) k_any_i3_cols(const I3ColsP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
@@ -727,11 +765,11 @@ template <class C> __global__ void __launch_bounds__(kThreads, pass_ctas<C>()) k
 	auto st_psi = [ps, sc, P, pitch](int line, int i, const C &v, C *out) {
 		out[sw(line * pitch + i)] = cscale(v, sc * ps[line * P + i]);
 	};
-	C *X = fft_f<+1, true, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st_psi);
+	C *X = fft_fx<R1, R2, +1, true, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st_psi);
 	__syncthreads();
 	auto ld1 = [X, pitch](int line, int i) { return X[sw(line * pitch + i)]; };
 	auto st_g = [g, P, k0](int line, int i, const C &v, C *) { g[(long)i * P + k0 + line] = v; };
-	fft_f<-1, false, true>(nl, pitch, p.pl, T.tw, X == T.a ? T.b : T.a, X, ld1, st_g);
+	fft_fx<R1, R2, -1, false, true>(nl, pitch, p.pl, T.tw, X == T.a ? T.b : T.a, X, ld1, st_g);
 	(void)mgP; (void)mgnl;
 }
 
@@ -748,7 +786,7 @@ template <class C> struct I3RowsBP {
 // RF (kind 0): Y[(cell nt + tt) 16 + 2 j + pr] holds the two packed chains of
 // (cell, term, j); X[cell][j] (real) += eta_2pr P_2pr . Re(row) + eta_2pr+1
 // P_2pr+1 . Im(row)
-template <class C, bool RF> __device__ __forceinline__ void i3_rows_b(const I3RowsBP<C> &p, unsigned char *sm) {
+template <class C, bool RF, int R1, int R2> __device__ __forceinline__ void i3_rows_b(const I3RowsBP<C> &p, unsigned char *sm) {
 	using R = typename CT<C>::R;
 	const int P = 2 * p.N, nl = p.nl, ne = nl * P;
 	const long PP = (long)P * P;
@@ -776,7 +814,7 @@ template <class C, bool RF> __device__ __forceinline__ void i3_rows_b(const I3Ro
 			const int pitch = T.pitch;
 			auto ld0 = [y, P](int line, int i) { return y[(long)line * P + i]; };
 			auto st1 = [pitch](int line, int i, const C &v, C *out) { out[sw(line * pitch + i)] = v; };
-			const C *r = fft_f<-1, false, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
+			const C *r = fft_fx<R1, R2, -1, false, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
 			__syncthreads();
 			if constexpr (RF) {
 				const C *Pa = p.Pg + (ct * 4 + h) * PP + (long)l0 * P;      // P_2h + i P_2h+1
@@ -813,16 +851,17 @@ template <class C, bool RF> __device__ __forceinline__ void i3_rows_b(const I3Ro
 		if (i < ne) X[i] = acc[e];
 	}
 }
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i3_rows_b(const I3RowsBP<C> p) {
+// two CTAs an SM (at most 128 registers: the accumulators live in registers)
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, 2) k_any_i3_rows_b(const I3RowsBP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const long cell = blockIdx.x / (4L * (2 * p.N / p.nl));         // blocks (cell 4 + j) bpg + row block
 	if constexpr (has_rf<C>()) {
 		if (p.kind != nullptr && p.kind[cell] == 0) {
-			i3_rows_b<C, true>(p, sm);
+			i3_rows_b<C, true, R1, R2>(p, sm);
 			return;
 		}
 	}
-	i3_rows_b<C, false>(p, sm);
+	i3_rows_b<C, false, R1, R2>(p, sm);
 }
 
 // The I3 chains with the whole P x P grid in shared memory (P = 48 and 96 in
@@ -1196,6 +1235,17 @@ template <class C> struct AnyRhs {
 		return p;
 	}
 	size_t smem(int nl, int tiles) const { return tile_bytes<C>(P, nl * tiles); }
+	// runs f on the instantiation of a pass kernel for the plan's two stages
+	// (16 3, 16 6, 16 12, 16 16), else on the run-time-plan one
+	template <class F, class K> void by_plan(const F &f, K k3, K k6, K k12, K k16, K kany) const {
+		switch (two_stage_key(pl)) {
+		case 3: f(k3); break;
+		case 6: f(k6); break;
+		case 12: f(k12); break;
+		case 16: f(k16); break;
+		default: f(kany);
+		}
+	}
 	long blocks(long units, int nl) const { return units * (P / nl); }
 
 	static double env_mb(const char *name) {
@@ -1238,12 +1288,17 @@ template <class C> struct AnyRhs {
 		p.kind = kind; p.gpc = gpc; p.nsub = nsub; p.rf_grids = rf_grids;
 		const long nb = blocks(ngrids, nl1);
 		const size_t sm = smem(nl1, 1);
+		auto go = [&](const char *name) { return [&, name](auto kern) { launch(kern, name, nb, sm, s, p); }; };
 		if (dir < 0) {
-			if (cols) launch(k_any_plain<C, -1, true>, "any_cols", nb, sm, s, p);
-			else launch(k_any_plain<C, -1, false>, "any_rows", nb, sm, s, p);
+			if (cols) by_plan(go("any_cols"), k_any_plain<C, -1, true, 16, 3>, k_any_plain<C, -1, true, 16, 6>, k_any_plain<C, -1, true, 16, 12>,
+			                  k_any_plain<C, -1, true, 16, 16>, k_any_plain<C, -1, true, 0, 0>);
+			else by_plan(go("any_rows"), k_any_plain<C, -1, false, 16, 3>, k_any_plain<C, -1, false, 16, 6>, k_any_plain<C, -1, false, 16, 12>,
+			             k_any_plain<C, -1, false, 16, 16>, k_any_plain<C, -1, false, 0, 0>);
 		} else {
-			if (cols) launch(k_any_plain<C, +1, true>, "any_cols", nb, sm, s, p);
-			else launch(k_any_plain<C, +1, false>, "any_rows", nb, sm, s, p);
+			if (cols) by_plan(go("any_cols"), k_any_plain<C, +1, true, 16, 3>, k_any_plain<C, +1, true, 16, 6>, k_any_plain<C, +1, true, 16, 12>,
+			                  k_any_plain<C, +1, true, 16, 16>, k_any_plain<C, +1, true, 0, 0>);
+			else by_plan(go("any_rows"), k_any_plain<C, +1, false, 16, 3>, k_any_plain<C, +1, false, 16, 6>, k_any_plain<C, +1, false, 16, 12>,
+			             k_any_plain<C, +1, false, 16, 16>, k_any_plain<C, +1, false, 0, 0>);
 		}
 	}
 
@@ -1253,7 +1308,9 @@ template <class C> struct AnyRhs {
 		return p;
 	}
 	void pad_rows(const PadRowsP<C> &p, int nc = -1) {
-		launch(k_any_pad_rows<C>, "any_pad_rows", blocks((long)(nc < 0 ? ncells : nc) * p.nt * p.nsub, nl1), smem(nl1, 1), s, p);
+		by_plan([&](auto kern) { launch(kern, "any_pad_rows", blocks((long)(nc < 0 ? ncells : nc) * p.nt * p.nsub, nl1), smem(nl1, 1), s, p); },
+		        k_any_pad_rows<C, 16, 3>, k_any_pad_rows<C, 16, 6>, k_any_pad_rows<C, 16, 12>, k_any_pad_rows<C, 16, 16>,
+		        k_any_pad_rows<C, 0, 0>);
 	}
 
 	void spectra(const double2 *W) {
@@ -1396,14 +1453,20 @@ template <class C> struct AnyRhs {
 				}
 				I3RowsAP<C> a{};
 				a.What = What; a.Pg = Pg; a.Y = Y; a.N = N; a.nl = nl1; a.nt = n; a.kind = kc; a.pl = pl;
-				launch(k_any_i3_rows_a<C>, "any_i3_rows_a", blocks((long)nc * n * 16, nl1), smem(nl1, 1), s, a);
+				by_plan([&](auto kern) { launch(kern, "any_i3_rows_a", blocks((long)nc * n * 16, nl1), smem(nl1, 1), s, a); },
+				        k_any_i3_rows_a<C, 16, 3>, k_any_i3_rows_a<C, 16, 6>, k_any_i3_rows_a<C, 16, 12>, k_any_i3_rows_a<C, 16, 16>,
+				        k_any_i3_rows_a<C, 0, 0>);
 				I3ColsP<C> c{};
 				c.Y = Y; c.psi2T = Tabs<C>::i3_psi2T(t); c.idx = t.idx.as<int>(); c.scale = t.scale.as<double>();
 				c.N = N; c.nl = nl1; c.nt = n; c.t0 = t0; c.kind = kc; c.pl = pl;
-				launch(k_any_i3_cols<C>, "any_i3_cols", blocks((long)nc * n * 16, nl1), smem(nl1, 1), s, c);
+				by_plan([&](auto kern) { launch(kern, "any_i3_cols", blocks((long)nc * n * 16, nl1), smem(nl1, 1), s, c); },
+				        k_any_i3_cols<C, 16, 3>, k_any_i3_cols<C, 16, 6>, k_any_i3_cols<C, 16, 12>, k_any_i3_cols<C, 16, 16>,
+				        k_any_i3_cols<C, 0, 0>);
 				I3RowsBP<C> b{};
 				b.Y = Y; b.Pg = Pg; b.X = X; b.N = N; b.nl = nl4; b.nt = n; b.kind = kc; b.pl = pl;
-				launch(k_any_i3_rows_b<C>, "any_i3_rows_b", blocks((long)nc * 4, nl4), smem(nl4, 1), s, b);
+				by_plan([&](auto kern) { launch(kern, "any_i3_rows_b", blocks((long)nc * 4, nl4), smem(nl4, 1), s, b); },
+				        k_any_i3_rows_b<C, 16, 3>, k_any_i3_rows_b<C, 16, 6>, k_any_i3_rows_b<C, 16, 12>,
+				        k_any_i3_rows_b<C, 16, 16>, k_any_i3_rows_b<C, 0, 0>);
 			}
 		}
 	}
@@ -1510,11 +1573,11 @@ void repr_passes(int N, int ngrids, double2 *a, int dir, cudaStream_t s) {
 	const size_t sm = tile_bytes<double2>(N, p.nl);
 	const long nb = (long)ngrids * (N / p.nl);
 	if (dir < 0) {
-		launch(k_any_plain<double2, -1, false>, "any_rows", nb, sm, s, p);
-		launch(k_any_plain<double2, -1, true>, "any_cols", nb, sm, s, p);
+		launch(k_any_plain<double2, -1, false, 0, 0>, "any_rows", nb, sm, s, p);
+		launch(k_any_plain<double2, -1, true, 0, 0>, "any_cols", nb, sm, s, p);
 	} else {
-		launch(k_any_plain<double2, +1, false>, "any_rows", nb, sm, s, p);
-		launch(k_any_plain<double2, +1, true>, "any_cols", nb, sm, s, p);
+		launch(k_any_plain<double2, +1, false, 0, 0>, "any_rows", nb, sm, s, p);
+		launch(k_any_plain<double2, +1, true, 0, 0>, "any_cols", nb, sm, s, p);
 	}
 }
 }  // namespace

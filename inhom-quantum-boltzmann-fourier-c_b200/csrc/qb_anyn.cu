@@ -531,7 +531,7 @@ template <class C> struct I1ColsP {
 	double fa, fb;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(const I1ColsP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(const I1ColsP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
@@ -553,7 +553,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(con
 		T.a[sw(kk * T.pitch + l)] = v;
 	});
 	__syncthreads();
-	C *r = fft_lines<-1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+	C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	const R fa = (R)p.fa, fb = (R)p.fb;
 	batched<C>(nl * P, [&](int i) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
@@ -564,7 +564,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_cols(con
 		r[sw(kk * T.pitch + l)] = cmul(f, r[sw(kk * T.pitch + l)]);
 	});
 	__syncthreads();
-	const C *r2 = fft_lines<+1>(r, r == T.a ? T.b : T.a, nl, T.pitch, 1, p.pl, T.tw);
+	const C *r2 = fft_lines_x<R1, R2, +1>(r, r == T.a ? T.b : T.a, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		g[(long)l * P + k0 + kk] = r2[sw(kk * T.pitch + l)];
@@ -578,7 +578,7 @@ template <class C> struct I1RowsP {
 	const C *g; C *S; const R *phi; int N, nl, nt, t0, nsub;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(const I1RowsP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(const I1RowsP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
@@ -599,7 +599,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i1_rows(con
 			T.a[sw(li * T.pitch + k)] = v;
 		});
 		__syncthreads();
-		const C *r = fft_lines<+1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+		const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 		const R *phi = p.phi + (long)(p.t0 + tt) * PP + (long)l0 * P;
 		batched<Two<C>>(nl * P, [&](int i) {
 			Two<C> v;
@@ -625,7 +625,7 @@ template <class C> struct I2ColsP {
 	const C *g; C *Q; int N, nl, nt;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(const I2ColsP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(const I2ColsP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
@@ -648,7 +648,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_i2_cols(con
 			T.a[sw((h * nl + kk) * T.pitch + l)] = v;
 		});
 		__syncthreads();
-		const C *r = fft_lines<-1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
+		const C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
 		batched<C>(nl * P, [&](int i) {
 			const int l = fdiv(i, mgnl), kk = i - l * nl;
 			return Q[(long)l * P + k0 + kk];
@@ -970,7 +970,7 @@ template <class C> struct AsmP {
 	const double2 *base, *wcur; const double *B; double dtc; double2 *out;
 	Plan pl;
 };
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(const AsmP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(const AsmP<C> p) {
 	using R = typename CT<C>::R;
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int P = 2 * p.N, nl = p.nl;
@@ -1029,7 +1029,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 		T.a[sw((nl + li) * T.pitch + k)] = zd;
 	}
 	__syncthreads();
-	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
+	const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
 	C *z = p.Z + cj * 2 * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
 		const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, li = fdiv(rem, mgP), k = rem - li * P;
@@ -1039,7 +1039,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_rows(co
 
 // assembly columns: inverse column transforms of Zcc_j, Zcd_j, Extract, and
 // the outputs (mode 0: Cc = s1 Zcc, Cd = Zcd; mode 1: base + dtc (Cc + Cd + CB))
-template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(const AsmP<C> p) {
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(const AsmP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const int N = p.N, P = 2 * N, nl = p.nl;
 	const long PP = (long)P * P, NN = (long)N * N;
@@ -1057,7 +1057,7 @@ template <class C> __global__ void __launch_bounds__(kThreads) k_any_asm_cols(co
 		T.a[sw((h * nl + kk) * T.pitch + l)] = z[h * PP + (long)l * P + k0 + kk];
 	}
 	__syncthreads();
-	const C *r = fft_lines<+1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
+	const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		const int ls = src_idx(l, N), ks = src_idx(k0 + kk, N);
@@ -1341,11 +1341,13 @@ template <class C> struct AnyRhs {
 				I1ColsP<C> c{};
 				c.g = G; c.What = ws.What.as<C>() + (long)c0 * 4 * PP; c.N = N; c.nl = nl1; c.nt = n; c.nsub = ntask; c.fcomp = 0;
 				c.fa = cc ? -4.0 : 2.0; c.fb = cc ? 2.0 : -1.0; c.pl = pl;
-				launch(k_any_i1_cols<C>, "any_i1_cols", blocks((long)nc * n * ntask, nl1), smem(nl1, 1), s, c);
+				by_plan([&](auto kern) { launch(kern, "any_i1_cols", blocks((long)nc * n * ntask, nl1), smem(nl1, 1), s, c); },
+		        k_any_i1_cols<C, 16, 3>, k_any_i1_cols<C, 16, 6>, k_any_i1_cols<C, 16, 12>, k_any_i1_cols<C, 16, 16>, k_any_i1_cols<C, 0, 0>);
 				I1RowsP<C> r{};
 				r.g = G; r.S = Sbuf.as<C>() + (long)c0 * ntask * PP; r.phi = Tabs<C>::i1_phi(t); r.N = N; r.nl = nl1; r.nt = n; r.t0 = t0;
 				r.nsub = ntask; r.pl = pl;
-				launch(k_any_i1_rows<C>, "any_i1_rows", blocks((long)nc * ntask, nl1), smem(nl1, 1), s, r);
+				by_plan([&](auto kern) { launch(kern, "any_i1_rows", blocks((long)nc * ntask, nl1), smem(nl1, 1), s, r); },
+		        k_any_i1_rows<C, 16, 3>, k_any_i1_rows<C, 16, 6>, k_any_i1_rows<C, 16, 12>, k_any_i1_rows<C, 16, 16>, k_any_i1_rows<C, 0, 0>);
 			}
 		}
 		FSbuf.ensure(sizeof(C) * ncells * ntask * PP);
@@ -1372,24 +1374,25 @@ template <class C> struct AnyRhs {
 				pad_rows(p, nc);
 				I2ColsP<C> c{};
 				c.g = G; c.Q = ws.i2p.as<C>() + (long)c0 * 4 * PP; c.N = N; c.nl = nl2; c.nt = n; c.pl = pl;
-				launch(k_any_i2_cols<C>, "any_i2_cols", blocks((long)nc * 4, nl2), smem(nl2, 2), s, c);
+				by_plan([&](auto kern) { launch(kern, "any_i2_cols", blocks((long)nc * 4, nl2), smem(nl2, 2), s, c); },
+		        k_any_i2_cols<C, 16, 3>, k_any_i2_cols<C, 16, 6>, k_any_i2_cols<C, 16, 12>, k_any_i2_cols<C, 16, 16>, k_any_i2_cols<C, 0, 0>);
 			}
 		}
 	}
 
-	// whole-grid chains (k_any_i3_fused) or the three passes.  The workspace's
-	// knob (0 off, 1 on), else QB_ANYN_FUSED (read per call), else the
-	// default: FP64 takes the whole-grid chains where a grid fits a CTA; FP32
-	// takes the three passes, measured faster at N = 24 (0.216 against 0.316
-	// ms per cell-evaluation) and N = 48 (0.710 against 0.807) once the passes
-	// read and store from their FFT stages
+	// whole-grid chains (k_any_i3_fused, where a grid fits a CTA) or the three
+	// passes.  The workspace's knob (0 off, 1 on), else QB_ANYN_FUSED (read per
+	// call), else the three passes: measured faster in FP32 at N = 24 (0.216
+	// against 0.316 ms per cell-evaluation) and N = 48 (0.710 against 0.807)
+	// once the passes read and store from their FFT stages, and faster still
+	// with their plans compiled in
 	bool fused_i3() const {
 		int on = ws.anyn_fused;
 		if (on < 0) {
 			const char *e = getenv("QB_ANYN_FUSED");
 			if (e != nullptr && (strcmp(e, "0") == 0 || strcmp(e, "1") == 0)) on = e[0] - '0';
 		}
-		if (on < 0) on = sizeof(C) == 16 ? 1 : 0;
+		if (on < 0) on = 0;
 		return on == 1 && tile_bytes<C>(P, P) <= kMaxSmem;
 	}
 
@@ -1494,8 +1497,10 @@ template <class C> struct AnyRhs {
 		a.nl = nl2;
 		ws.wave1.ensure(sizeof(C) * (size_t)ncells * 8 * PP);
 		a.Z = ws.wave1.as<C>();
-		launch(k_any_asm_rows<C>, "any_asm_rows", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, a);
-		launch(k_any_asm_cols<C>, "any_asm_cols", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, a);
+		by_plan([&](auto kern) { launch(kern, "any_asm_rows", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, a); },
+		        k_any_asm_rows<C, 16, 3>, k_any_asm_rows<C, 16, 6>, k_any_asm_rows<C, 16, 12>, k_any_asm_rows<C, 16, 16>, k_any_asm_rows<C, 0, 0>);
+		by_plan([&](auto kern) { launch(kern, "any_asm_cols", blocks((long)ncells * 4, nl2), smem(nl2, 2), s, a); },
+		        k_any_asm_cols<C, 16, 3>, k_any_asm_cols<C, 16, 6>, k_any_asm_cols<C, 16, 12>, k_any_asm_cols<C, 16, 16>, k_any_asm_cols<C, 0, 0>);
 	}
 };
 

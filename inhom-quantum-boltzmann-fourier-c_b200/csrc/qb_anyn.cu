@@ -154,9 +154,15 @@ template <int RAD> __host__ __device__ constexpr int freq_of(int s) {
 // length Ns done): butterfly j of a line reads x[j + r L/RAD], twiddles by
 // w^(r (j mod Ns)) with w = exp(DIR 2 pi i / (Ns RAD)), and writes its outputs
 // to (j / Ns) Ns RAD + (j mod Ns) + r Ns.  tw[m] = exp(-2 pi i m / L).
-// shared-memory slot of tile element i: one pad element every 16 spreads the
-// strided accesses of the Stockham stages over the banks
-__device__ __forceinline__ int sw(int i) { return i + (i >> 4); }
+// shared-memory slot of tile element (row, col) in rows of `pitch` slots: one
+// pad slot after every 16 columns of a row, and rows of L + L/16 + 3 slots
+// (tile_pitch).  Among the layouts of this form, and the global pad-every-16
+// and XOR forms, this one gave the fewest shared-memory wavefronts in a
+// count of every access of the passes (8-byte elements, half-warps) at
+// P = 48, 96, 192 and 256: 1.25-1.5 per ideal at P = 192 and 1.0 at P = 256,
+// against about 1.95 and 1.75 for a global pad every 16 over rows of L + 1.
+__host__ __device__ __forceinline__ int tile_pitch(int L) { return L + (L >> 4) + 3; }
+__device__ __forceinline__ int tat(int row, int col, int pitch) { return row * pitch + col + (col >> 4); }
 
 // x / d for x, d < 2^16 as a high multiply by floor(2^32 / d) + 1: the error
 // x (d - 2^32 mod d) / (d 2^32) stays below 1/d, so the quotient is exact;
@@ -171,10 +177,11 @@ __device__ __forceinline__ void stage(const C *in, C *out, int nl, int ls, int e
 	for (int b = threadIdx.x; b < nl * m; b += blockDim.x) {
 		const int line = fdiv(b, mg_m), j = b - line * m;
 		const int jq = fdiv(j, mg_ns), k = j - jq * Ns;
-		const int base = line * ls + j * es;
+		// lines are the tile's rows (es = 1, row pitch ls) or its columns (ls = 1, row pitch es)
+		auto at = [ls, es, line](int e) { return es == 1 ? tat(line, e, ls) : tat(e, line, es); };
 		C v[RAD];
 #pragma unroll
-		for (int r = 0; r < RAD; r++) v[r] = in[sw(base + r * m * es)];
+		for (int r = 0; r < RAD; r++) v[r] = in[at(j + r * m)];
 		if (Ns > 1) {
 #pragma unroll
 			for (int r = 1; r < RAD; r++) {
@@ -184,9 +191,9 @@ __device__ __forceinline__ void stage(const C *in, C *out, int nl, int ls, int e
 			}
 		}
 		dft_r<RAD, DIR>(v);
-		const int ob = line * ls + (jq * Ns * RAD + k) * es;
+		const int ob = jq * Ns * RAD + k;
 #pragma unroll
-		for (int r = 0; r < RAD; r++) out[sw(ob + freq_of<RAD>(r) * Ns * es)] = v[r];
+		for (int r = 0; r < RAD; r++) out[at(ob + freq_of<RAD>(r) * Ns)] = v[r];
 	}
 }
 
@@ -264,7 +271,7 @@ __device__ __forceinline__ void stage_any(int R, int nl, int L, int Ns, const C 
 }
 // An FFT of nl lines: the first stage reads through ld0 (mapping LF0), the
 // middle stages ping-pong between the line-contiguous shared buffers a and b
-// (element i of a line at sw(line pitch + i)), the last stage (mapping LF1)
+// (element i of a line at tat(line, i, pitch)), the last stage (mapping LF1)
 // stores through st1(line, i, v, free), where `free` is the buffer that the
 // last stage does not read.  The first stage writes a, so ld0 must not read a.
 // A barrier follows every stage but the last; returns `free`.
@@ -276,8 +283,8 @@ __device__ C *fft_f(int nl, int pitch, const Plan &pl, const C *tw, C *a, C *b, 
 		const int R = pl.r[s];
 		const bool first = s == 0, last = s == pl.nst - 1;
 		C *const in = cur, *const out = nxt;
-		auto sm_ld = [in, pitch](int line, int i) { return in[sw(line * pitch + i)]; };
-		auto sm_st = [out, pitch](int line, int i, const C &v) { out[sw(line * pitch + i)] = v; };
+		auto sm_ld = [in, pitch](int line, int i) { return in[tat(line, i, pitch)]; };
+		auto sm_st = [out, pitch](int line, int i, const C &v) { out[tat(line, i, pitch)] = v; };
 		auto st_last = [&st1, out](int line, int i, const C &v) { st1(line, i, v, out); };
 		if (first && last) stage_any<DIR, LF0>(R, nl, pl.L, Ns, tw, ld0, st_last);
 		else if (first) stage_any<DIR, LF0>(R, nl, pl.L, Ns, tw, ld0, sm_st);
@@ -301,10 +308,10 @@ __device__ C *fft_fx(int nl, int pitch, const Plan &pl, const C *tw, C *a, C *b,
 	if constexpr (R1 == 0) {
 		return fft_f<DIR, LF0, LF1>(nl, pitch, pl, tw, a, b, ld0, st1);
 	} else {
-		auto sm_st = [a, pitch](int line, int i, const C &v) { a[sw(line * pitch + i)] = v; };
+		auto sm_st = [a, pitch](int line, int i, const C &v) { a[tat(line, i, pitch)] = v; };
 		stage_f<R1, DIR, LF0>(nl, R1 * R2, 1, tw, ld0, sm_st);
 		__syncthreads();
-		auto sm_ld = [a, pitch](int line, int i) { return a[sw(line * pitch + i)]; };
+		auto sm_ld = [a, pitch](int line, int i) { return a[tat(line, i, pitch)]; };
 		auto st_last = [&st1, b](int line, int i, const C &v) { st1(line, i, v, b); };
 		stage_f<R2, DIR, LF1>(nl, R1 * R2, R1, tw, sm_ld, st_last);
 		return b;
@@ -369,22 +376,22 @@ __global__ void k_any_build_tw(int L, double2 *twd, float2 *twf) {
 	}
 }
 
-// shared-memory layout of a pass: the twiddles, then two buffers of nl lines
+// shared-memory layout of a pass: the twiddles, then two buffers of nl rows
+// (element (row, col) of a buffer at at(row, col))
 template <class C> struct Tile {
 	C *tw, *a, *b;
 	int pitch;
 	__device__ Tile(unsigned char *sm, int L, int nl) {
-		pitch = L + 1;
+		pitch = tile_pitch(L);
 		tw = reinterpret_cast<C *>(sm);
 		a = tw + L;
-		const int n = nl * pitch;
-		b = a + n + (n >> 4) + 1;
+		b = a + nl * pitch;
 	}
+	__device__ __forceinline__ int at(int row, int col) const { return tat(row, col, pitch); }
 };
-// the twiddles and two buffers of nl lines of pitch L + 1, with the pads of sw()
+// the twiddles and two buffers of nl rows of tile_pitch(L) slots
 template <class C> size_t tile_bytes(int L, int nl) {
-	const size_t n = (size_t)nl * (L + 1);
-	return sizeof(C) * ((size_t)L + 2 * (n + (n >> 4) + 1));
+	return sizeof(C) * ((size_t)L + 2 * (size_t)nl * tile_pitch(L));
 }
 
 // ---------------------------------------------------------------------------
@@ -477,14 +484,14 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		return v;
 	}, [&](int i, const C &v) {
 		const int li = fdiv(i, mgP), k = i - li * P;
-		T.a[sw(li * T.pitch + k)] = v;
+		T.a[T.at(li, k)] = v;
 	});
 	__syncthreads();
 	const C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	C *o = p.out + u * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int li = fdiv(i, mgP), k = i - li * P;
-		o[(long)li * P + k] = r[sw(li * T.pitch + k)];
+		o[(long)li * P + k] = r[T.at(li, k)];
 	}
 }
 
@@ -513,14 +520,14 @@ template <class C, int DIR, bool COLS, int R1, int R2> __global__ void __launch_
 		const int li = fdiv(i, mgP), k = i - li * L;
 		return g[(long)(x0 + li) * L + k];
 	}, [&](int i, const C &v) {
-		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; T.a[sw(kk * T.pitch + l)] = v; }
-		else { const int li = fdiv(i, mgP), k = i - li * L; T.a[sw(li * T.pitch + k)] = v; }
+		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; T.a[T.at(kk, l)] = v; }
+		else { const int li = fdiv(i, mgP), k = i - li * L; T.a[T.at(li, k)] = v; }
 	});
 	__syncthreads();
 	const C *r = fft_lines_x<R1, R2, DIR>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; g[(long)l * L + x0 + kk] = r[sw(kk * T.pitch + l)]; }
-		else { const int li = fdiv(i, mgP), k = i - li * L; g[(long)(x0 + li) * L + k] = r[sw(li * T.pitch + k)]; }
+		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; g[(long)l * L + x0 + kk] = r[T.at(kk, l)]; }
+		else { const int li = fdiv(i, mgP), k = i - li * L; g[(long)(x0 + li) * L + k] = r[T.at(li, k)]; }
 	}
 }
 
@@ -550,7 +557,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		return g[(long)l * P + k0 + kk];
 	}, [&](int i, const C &v) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
-		T.a[sw(kk * T.pitch + l)] = v;
+		T.a[T.at(kk, l)] = v;
 	});
 	__syncthreads();
 	C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
@@ -561,13 +568,13 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 	}, [&](int i, const C &w) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		C f; f.x = fa * w.x + fb; f.y = fa * w.y;
-		r[sw(kk * T.pitch + l)] = cmul(f, r[sw(kk * T.pitch + l)]);
+		r[T.at(kk, l)] = cmul(f, r[T.at(kk, l)]);
 	});
 	__syncthreads();
 	const C *r2 = fft_lines_x<R1, R2, +1>(r, r == T.a ? T.b : T.a, nl, T.pitch, 1, p.pl, T.tw);
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
-		g[(long)l * P + k0 + kk] = r2[sw(kk * T.pitch + l)];
+		g[(long)l * P + k0 + kk] = r2[T.at(kk, l)];
 	}
 }
 
@@ -596,7 +603,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		const C *g = p.g + ((cell * p.nt + tt) * p.nsub + sub) * PP + (long)l0 * P;
 		batched<C>(nl * P, [&](int i) { return g[i]; }, [&](int i, const C &v) {
 			const int li = fdiv(i, mgP), k = i - li * P;
-			T.a[sw(li * T.pitch + k)] = v;
+			T.a[T.at(li, k)] = v;
 		});
 		__syncthreads();
 		const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
@@ -609,7 +616,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		}, [&](int i, const Two<C> &v) {
 			const int li = fdiv(i, mgP), k = i - li * P;
 			const R f = v.b.x;
-			const C x = r[sw(li * T.pitch + k)];
+			const C x = r[T.at(li, k)];
 			C s = v.a;
 			s.x += f * x.x;
 			s.y += f * x.y;
@@ -645,7 +652,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 			return ga[h * PP + (long)l * P + k0 + kk];
 		}, [&](int i, const C &v) {
 			const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
-			T.a[sw((h * nl + kk) * T.pitch + l)] = v;
+			T.a[T.at(h * nl + kk, l)] = v;
 		});
 		__syncthreads();
 		const C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
@@ -654,7 +661,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 			return Q[(long)l * P + k0 + kk];
 		}, [&](int i, const C &q) {
 			const int l = fdiv(i, mgnl), kk = i - l * nl;
-			Q[(long)l * P + k0 + kk] = cfma(r[sw(kk * T.pitch + l)], r[sw((nl + kk) * T.pitch + l)], q);
+			Q[(long)l * P + k0 + kk] = cfma(r[T.at(kk, l)], r[T.at(nl + kk, l)], q);
 		});
 		__syncthreads();
 	}
@@ -706,7 +713,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		}, [&](int i, const Two<C> &v) {
 			const int li = fdiv(i, mgP), k = i - li * P;
 			const typename CT<C>::R pj = im ? v.b.y : v.b.x;
-			T.a[sw(li * T.pitch + k)] = cscale(v.a, pj);
+			T.a[T.at(li, k)] = cscale(v.a, pj);
 		});
 	} else {
 		const C *G = p.What + (cell * 4 + (c & 3)) * PP + (long)l0 * P;
@@ -718,7 +725,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 			return v;
 		}, [&](int i, const Two<C> &v) {
 			const int li = fdiv(i, mgP), k = i - li * P;
-			T.a[sw(li * T.pitch + k)] = cmul(v.a, v.b);
+			T.a[T.at(li, k)] = cmul(v.a, v.b);
 		});
 	}
 	__syncthreads();
@@ -726,7 +733,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 	C *o = p.Y + u * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
 		const int li = fdiv(i, mgP), k = i - li * P;
-		o[(long)li * P + k] = r[sw(li * T.pitch + k)];
+		o[(long)li * P + k] = r[T.at(li, k)];
 	}
 }
 
@@ -763,11 +770,11 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, p
 	const int pitch = T.pitch;
 	auto ld0 = [g, P, k0](int line, int i) { return g[(long)i * P + k0 + line]; };
 	auto st_psi = [ps, sc, P, pitch](int line, int i, const C &v, C *out) {
-		out[sw(line * pitch + i)] = cscale(v, sc * ps[line * P + i]);
+		out[tat(line, i, pitch)] = cscale(v, sc * ps[line * P + i]);
 	};
 	C *X = fft_fx<R1, R2, +1, true, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st_psi);
 	__syncthreads();
-	auto ld1 = [X, pitch](int line, int i) { return X[sw(line * pitch + i)]; };
+	auto ld1 = [X, pitch](int line, int i) { return X[tat(line, i, pitch)]; };
 	auto st_g = [g, P, k0](int line, int i, const C &v, C *) { g[(long)i * P + k0 + line] = v; };
 	fft_fx<R1, R2, -1, false, true>(nl, pitch, p.pl, T.tw, X == T.a ? T.b : T.a, X, ld1, st_g);
 	(void)mgP; (void)mgnl;
@@ -813,7 +820,7 @@ template <class C, bool RF, int R1, int R2> __device__ __forceinline__ void i3_r
 			const C *y = p.Y + (ct * 16 + j3 * kH + h) * PP + (long)l0 * P;
 			const int pitch = T.pitch;
 			auto ld0 = [y, P](int line, int i) { return y[(long)line * P + i]; };
-			auto st1 = [pitch](int line, int i, const C &v, C *out) { out[sw(line * pitch + i)] = v; };
+			auto st1 = [pitch](int line, int i, const C &v, C *out) { out[tat(line, i, pitch)] = v; };
 			const C *r = fft_fx<R1, R2, -1, false, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
 			__syncthreads();
 			if constexpr (RF) {
@@ -824,7 +831,7 @@ template <class C, bool RF, int R1, int R2> __device__ __forceinline__ void i3_r
 					const int i = threadIdx.x + e * kThreads;
 					if (i < ne) {
 						const int li = fdiv(i, mgP), k = i - li * P;
-						const C pa = Pa[i], y = r[sw(li * T.pitch + k)];
+						const C pa = Pa[i], y = r[T.at(li, k)];
 						acc[e].x += e0 * (pa.x * y.x) - pa.y * y.y;
 					}
 				}
@@ -836,7 +843,7 @@ template <class C, bool RF, int R1, int R2> __device__ __forceinline__ void i3_r
 					const int i = threadIdx.x + e * kThreads;
 					if (i < ne) {
 						const int li = fdiv(i, mgP), k = i - li * P;
-						const C v = cmul(Pa[i], r[sw(li * T.pitch + k)]);
+						const C v = cmul(Pa[i], r[T.at(li, k)]);
 						acc[e].x += eta * v.x;
 						acc[e].y += eta * v.y;
 					}
@@ -906,7 +913,7 @@ template <class C, bool RF> __device__ __forceinline__ void i3_fused(const I3Fus
 				return v;
 			}, [&](int i, const Two<C> &v) {
 				const int l = fdiv(i, mgP), k = i - l * P;
-				T.a[sw(l * T.pitch + k)] = RF ? cscale(v.a, (j3 & 1) ? v.b.y : v.b.x) : cmul(v.a, v.b);
+				T.a[T.at(l, k)] = RF ? cscale(v.a, (j3 & 1) ? v.b.y : v.b.x) : cmul(v.a, v.b);
 			});
 			__syncthreads();
 			C *r = fft_lines<+1>(T.a, T.b, P, T.pitch, 1, p.pl, T.tw);               // rows
@@ -914,10 +921,10 @@ template <class C, bool RF> __device__ __forceinline__ void i3_fused(const I3Fus
 			batched<R>(PPi, [&](int i) { return ps[i]; }, [&](int i, const R &f0) {
 				const int k = fdiv(i, mgP), l = i - k * P;                   // transposed table: element (l, k)
 				const R f = sc * f0;
-				C x = r[sw(l * T.pitch + k)];
+				C x = r[T.at(l, k)];
 				x.x *= f;
 				x.y *= f;
-				r[sw(l * T.pitch + k)] = x;
+				r[T.at(l, k)] = x;
 			});
 			__syncthreads();
 			r = fft_lines<-1>(r, r == T.a ? T.b : T.a, P, 1, T.pitch, p.pl, T.tw);     // columns
@@ -932,7 +939,7 @@ template <class C, bool RF> __device__ __forceinline__ void i3_fused(const I3Fus
 			}, [&](int i, const Two<C> &v) {
 				const int l = fdiv(i, mgP), k = i - l * P;
 				C x = v.b;
-				const C y0 = r[sw(l * T.pitch + k)];
+				const C y0 = r[T.at(l, k)];
 				if (RF) {                                  // eta_2h P_2h Re + eta_2h+1 P_2h+1 Im (eta_2h+1 = -1)
 					x.x += eta * (v.a.x * y0.x) - v.a.y * y0.y;
 				} else {
@@ -1025,15 +1032,15 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 			zd.x += s1 * v.x;
 			zd.y += s1 * v.y;
 		}
-		T.a[sw(li * T.pitch + k)] = zc;
-		T.a[sw((nl + li) * T.pitch + k)] = zd;
+		T.a[T.at(li, k)] = zc;
+		T.a[T.at(nl + li, k)] = zd;
 	}
 	__syncthreads();
 	const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
 	C *z = p.Z + cj * 2 * PP + (long)l0 * P;
 	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
 		const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, li = fdiv(rem, mgP), k = rem - li * P;
-		z[h * PP + (long)li * P + k] = r[sw((h * nl + li) * T.pitch + k)];
+		z[h * PP + (long)li * P + k] = r[T.at(h * nl + li, k)];
 	}
 }
 
@@ -1054,7 +1061,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 	const C *z = p.Z + cj * 2 * PP;
 	for (int i = threadIdx.x; i < 2 * nl * P; i += blockDim.x) {
 		const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
-		T.a[sw((h * nl + kk) * T.pitch + l)] = z[h * PP + (long)l * P + k0 + kk];
+		T.a[T.at(h * nl + kk, l)] = z[h * PP + (long)l * P + k0 + kk];
 	}
 	__syncthreads();
 	const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, 2 * nl, T.pitch, 1, p.pl, T.tw);
@@ -1062,7 +1069,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		const int ls = src_idx(l, N), ks = src_idx(k0 + kk, N);
 		if (ls < 0 || ks < 0) continue;
-		const C zc = r[sw(kk * T.pitch + l)], zd = r[sw((nl + kk) * T.pitch + l)];
+		const C zc = r[T.at(kk, l)], zd = r[T.at(nl + kk, l)];
 		const double2 cc = make_double2(p.s1 * (double)zc.x, p.s1 * (double)zc.y);
 		const double2 cd = make_double2((double)zd.x, (double)zd.y);
 		const long q = (long)ls * N + ks, o = cj * NN + q;
@@ -1160,8 +1167,7 @@ Plan make_plan(int L, int variant) {
 int pick_lines(int L, int want, int tiles, size_t elem) {
 	for (int nl = want; nl >= 1; nl--) {
 		if (L % nl) continue;
-		const size_t n = (size_t)tiles * nl * (L + 1);
-		if (elem * ((size_t)L + 2 * (n + (n >> 4) + 1)) <= kMaxSmem) return nl;
+		if (elem * ((size_t)L + 2 * (size_t)tiles * nl * tile_pitch(L)) <= kMaxSmem) return nl;
 	}
 	return 1;
 }

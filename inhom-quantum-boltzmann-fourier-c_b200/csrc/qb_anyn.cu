@@ -785,6 +785,20 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, p
 // wave's terms and i in order, in registers (one CTA per (cell, j, row block);
 // a thread owns the tile elements tid + e kThreads, e < own_of<C>())
 template <class C> __host__ __device__ constexpr int own_of() { return sizeof(C) == 16 ? 8 : 16; }   // nl P <= own_of<C>() kThreads
+// the same for a compiled plan R1 R2 (P = R1 R2): FP32 tiles of 16 lines of
+// 192 and 32 of 96 need 12 values a thread, 48 lines of 48 need 9; fewer
+// accumulators leave the registers for three CTAs an SM
+template <class C, int R1, int R2> __host__ __device__ constexpr int own_for() {
+	return (sizeof(C) == 16 || R1 == 0) ? own_of<C>() : (R1 * R2 == 192 || R1 * R2 == 96) ? 12 : R1 * R2 == 48 ? 9 : 16;
+}
+inline int own_for_plan(const Plan &pl, bool fp64) {
+	if (fp64) return 8;
+	switch (two_stage_key(pl)) {
+	case 12: case 6: return 12;
+	case 3: return 9;
+	default: return 16;
+	}
+}
 template <class C> struct I3RowsBP {
 	const C *Y, *Pg; C *X; int N, nl, nt;
 	const int *kind;                      // null: every cell complex
@@ -806,7 +820,7 @@ template <class C, bool RF, int R1, int R2> __device__ __forceinline__ void i3_r
 	const int j3 = (int)(cj % 4);
 	load_tw(T.tw, P, p.pl);
 	C *X = p.X + cj * PP + (long)l0 * P;
-	constexpr int kOwn = own_of<C>();
+	constexpr int kOwn = own_for<C, R1, R2>();
 	C acc[kOwn];
 #pragma unroll
 	for (int e = 0; e < kOwn; e++) {
@@ -858,8 +872,11 @@ template <class C, bool RF, int R1, int R2> __device__ __forceinline__ void i3_r
 		if (i < ne) X[i] = acc[e];
 	}
 }
-// two CTAs an SM (at most 128 registers: the accumulators live in registers)
-template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, 2) k_any_i3_rows_b(const I3RowsBP<C> p) {
+// two CTAs an SM (at most 128 registers: the accumulators live in
+// registers); three (85) in FP32 where a thread holds 12 or fewer of them
+// (FP64 stays at two: 1.5x slower at three)
+template <class C, int R1, int R2> constexpr int rows_b_ctas() { return sizeof(C) == 8 && own_for<C, R1, R2>() <= 12 ? 3 : 2; }
+template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, rows_b_ctas<C, R1, R2>()) k_any_i3_rows_b(const I3RowsBP<C> p) {
 	extern __shared__ __align__(16) unsigned char sm[];
 	const long cell = blockIdx.x / (4L * (2 * p.N / p.nl));         // blocks (cell 4 + j) bpg + row block
 	if constexpr (has_rf<C>()) {
@@ -1433,7 +1450,8 @@ template <class C> struct AnyRhs {
 		if (!fused) ws.wave2.ensure(sizeof(C) * (size_t)cpw * nt * 16 * PP);   // chains
 		C *Pg = ws.wave1.as<C>(), *Y = fused ? nullptr : ws.wave2.as<C>();
 		int nl4 = nl1;                                      // one tile, at most kOwn elements a thread
-		while (nl4 > 1 && (nl4 * P > own_of<C>() * kThreads || P % nl4)) nl4--;
+		const int own = own_for_plan(pl, sizeof(C) == 16);
+		while (nl4 > 1 && (nl4 * P > own * kThreads || P % nl4)) nl4--;
 		for (int c0 = 0; c0 < ncells; c0 += cpw) {
 			const int nc = std::min(cpw, ncells - c0);
 			const double2 *Wc = W + (long)c0 * 4 * N * N;

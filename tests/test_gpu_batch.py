@@ -85,3 +85,29 @@ def test_batch_graph_replay_and_tuned_schedules(monkeypatch):
     tuned = [s for s in qbgpu.batch_schedules() if s["J"] == J and s["M"] == M and s["rk4"] == 1]
     assert {(s["N"], s["instances"]) for s in tuned} >= {(8, 2), (16, 2), (32, 1)}
     assert all(s["step_ms"] > 0 for s in tuned)
+
+
+def test_fp32_any_n_batch_graph_replay_and_fp64_bound(monkeypatch):
+    """the any-N sizes of the configuration (N = 24, 48, 96, 128) in the FP32
+    form: a 7-step batch call replays its two-step CUDA graphs (the per-cell
+    choice between the real and the complex form of the I3 sums is made on
+    the device inside the graph) bit for bit like direct launches, and stays
+    within the 1e-5 bound of the FP64 batch"""
+    sizes = [24, 96, 48, 128, 24]
+    Wf = [orc.to_fourier(qbgpu.gaussian_mixture_state(n, L, seed=700 + i, ncells=1))[0] for i, n in enumerate(sizes)]
+    B = np.random.default_rng(27).standard_normal((len(sizes), 3)) * 0.1
+    dt, steps = 0.01, 7
+    graphed = [torch.from_numpy(w.copy()).cuda() for w in Wf]
+    qbgpu.homogeneous_batch(graphed, dt, steps, B=B, rk4=True, J=J, M=M, L=L, R=R, precision=32)
+    fp64 = [torch.from_numpy(w.copy()).cuda() for w in Wf]
+    qbgpu.homogeneous_batch(fp64, dt, steps, B=B, rk4=True, J=J, M=M, L=L, R=R, precision=64)
+    monkeypatch.setenv("QB_CUDA_GRAPHS", "0")
+    direct = [torch.from_numpy(w.copy()).cuda() for w in Wf]
+    qbgpu.homogeneous_batch(direct, dt, steps, B=B, rk4=True, J=J, M=M, L=L, R=R, precision=32)
+    torch.cuda.synchronize()
+    for a, b in zip(graphed, direct):
+        assert torch.equal(a, b)
+    for i, n in enumerate(sizes):
+        a, b = graphed[i].cpu().numpy(), fp64[i].cpu().numpy()
+        e = float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+        assert 0 < e <= 1e-5, (n, e)

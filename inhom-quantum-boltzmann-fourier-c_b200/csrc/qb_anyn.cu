@@ -154,6 +154,9 @@ template <int RAD> __host__ __device__ constexpr int freq_of(int s) {
 // length Ns done): butterfly j of a line reads x[j + r L/RAD], twiddles by
 // w^(r (j mod Ns)) with w = exp(DIR 2 pi i / (Ns RAD)), and writes its outputs
 // to (j / Ns) Ns RAD + (j mod Ns) + r Ns.  tw[m] = exp(-2 pi i m / L).
+// row l of a padded P = 2N grid lies in the zero band of the padding
+__device__ __forceinline__ bool in_zero_band(int l, int N) { return l >= N / 2 && l < 3 * N / 2; }
+
 // shared-memory slot of tile element (row, col) in rows of `pitch` slots: one
 // pad slot after every 16 columns of a row, and rows of L + L/16 + 3 slots
 // (tile_pitch).  Among the layouts of this form, and the global pad-every-16
@@ -454,11 +457,10 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		if (sub >= p.nsub_rf) return;
 		ps = p.psel_rf[sub]; ca = p.comp_rf[sub]; cb = p.comp2_rf[sub];
 	}
-	if (l0 >= N / 2 && l0 + nl <= 3 * N / 2) {     // every row of the tile in the zero band: its transform is zero
-		C *o = p.out + u * PP + (long)l0 * P;
-		for (int i = threadIdx.x; i < nl * P; i += blockDim.x) o[i] = czero<C>();
-		return;
-	}
+	// every row of the tile in the zero band: its transform is zero, and the
+	// column passes that read this output (k_any_plain with zband, the I1 and
+	// I2 column passes) take those rows as zero without reading them
+	if (l0 >= N / 2 && l0 + nl <= 3 * N / 2) return;
 	load_tw(T.tw, P, p.pl);
 	const double2 *w = p.W + cell * p.w_cell + (long)ca * NN;
 	const double2 *w2 = p.W + cell * p.w_cell + (long)cb * NN;
@@ -502,6 +504,7 @@ template <class C> struct PlainP {
 	// kind != null: grids [cell][gpc / nsub][nsub]; a cell of kind 0 (real
 	// form) skips the subs from rf_grids on
 	const int *kind; long gpc; int nsub, rf_grids;
+	int zband;                            // N > 0: the grids come from k_any_pad_rows, rows in its zero band read as zero (columns only)
 	Plan pl;
 };
 template <class C, int DIR, bool COLS, int R1, int R2> __global__ void __launch_bounds__(kThreads) k_any_plain(const PlainP<C> p) {
@@ -516,7 +519,10 @@ template <class C, int DIR, bool COLS, int R1, int R2> __global__ void __launch_
 	init_tw(T.tw, L, p.pl);
 	C *g = p.g + u * (long)L * L;
 	batched<C>(nl * L, [&](int i) {
-		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; return g[(long)l * L + x0 + kk]; }
+		if (COLS) {
+			const int l = fdiv(i, mgnl), kk = i - l * nl;
+			return (p.zband > 0 && in_zero_band(l, p.zband)) ? czero<C>() : g[(long)l * L + x0 + kk];
+		}
 		const int li = fdiv(i, mgP), k = i - li * L;
 		return g[(long)(x0 + li) * L + k];
 	}, [&](int i, const C &v) {
@@ -552,9 +558,9 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 	const long cell = u / ((long)p.nsub * p.nt);
 	C *g = p.g + u * PP;
 	const C *F = p.What + (cell * 4 + p.fcomp) * PP;
-	batched<C>(nl * P, [&](int i) {
+	batched<C>(nl * P, [&](int i) {             // rows in the zero band of k_any_pad_rows read as zero
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
-		return g[(long)l * P + k0 + kk];
+		return in_zero_band(l, p.N) ? czero<C>() : g[(long)l * P + k0 + kk];
 	}, [&](int i, const C &v) {
 		const int l = fdiv(i, mgnl), kk = i - l * nl;
 		T.a[T.at(kk, l)] = v;
@@ -649,7 +655,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		const C *ga = p.g + ((cell * p.nt + tt) * 8 + 2 * ii) * PP;
 		batched<C>(2 * nl * P, [&](int i) {
 			const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
-			return ga[h * PP + (long)l * P + k0 + kk];
+			return in_zero_band(l, p.N) ? czero<C>() : ga[h * PP + (long)l * P + k0 + kk];   // zero band of k_any_pad_rows
 		}, [&](int i, const C &v) {
 			const int h = i >= nl * P ? 1 : 0, rem = i - h * nl * P, l = fdiv(rem, mgnl), kk = rem - l * nl;
 			T.a[T.at(h * nl + kk, l)] = v;
@@ -1305,10 +1311,13 @@ template <class C> struct AnyRhs {
 
 	// kind != null: grids [cell][gpc / nsub][nsub], and the cells of kind 0
 	// skip the subs from rf_grids on
-	void plain(C *g, long ngrids, int dir, bool cols, const int *kind = nullptr, long gpc = 1, int nsub = 1, int rf_grids = 1) {
+	// zband: the grids come from k_any_pad_rows (column passes only)
+	void plain(C *g, long ngrids, int dir, bool cols, const int *kind = nullptr, long gpc = 1, int nsub = 1, int rf_grids = 1,
+	           bool zband = false) {
 		PlainP<C> p{};
 		p.g = g; p.L = P; p.nl = nl1; p.pl = pl;
 		p.kind = kind; p.gpc = gpc; p.nsub = nsub; p.rf_grids = rf_grids;
+		p.zband = (zband && cols) ? N : 0;
 		const long nb = blocks(ngrids, nl1);
 		const size_t sm = smem(nl1, 1);
 		auto go = [&](const char *name) { return [&, name](auto kern) { launch(kern, name, nb, sm, s, p); }; };
@@ -1341,7 +1350,7 @@ template <class C> struct AnyRhs {
 		PadRowsP<C> p = pad_params(W, 1, 0, 4, ws.What.as<C>());
 		for (int c = 0; c < 4; c++) { p.comp[c] = c; p.psel[c] = 0; }
 		pad_rows(p);
-		plain(ws.What.as<C>(), 4L * ncells, -1, true);
+		plain(ws.What.as<C>(), 4L * ncells, -1, true, nullptr, 1, 1, 1, true);
 	}
 
 	// I1-type sums into S [cell][ntask] and their forward transforms into FS
@@ -1466,7 +1475,7 @@ template <class C> struct AnyRhs {
 				for (int g = 0; g < 2; g++) { p.comp_rf[g] = 2 * g; p.comp2_rf[g] = 2 * g + 1; p.psel_rf[g] = 4; }
 				p.psiC = Tabs<C>::i3_psi1(t);
 				pad_rows(p, nc);
-				plain(Pg, (long)nc * n * 4, -1, true, kc, (long)n * 4, 4, 2);
+				plain(Pg, (long)nc * n * 4, -1, true, kc, (long)n * 4, 4, 2, true);
 				if (fused) {
 					I3FusedP<C> f{};
 					f.What = What; f.Pg = Pg; f.X = X;

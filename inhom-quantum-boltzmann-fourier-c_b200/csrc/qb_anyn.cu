@@ -757,7 +757,6 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, p
 	const int P = 2 * p.N, nl = p.nl;
 	const long PP = (long)P * P;
 	Tile<C> T(sm, P, nl);
-	const unsigned mgP = magic_div((unsigned)P), mgnl = magic_div((unsigned)nl);
 	const int bpg = P / nl;
 	const long u = blockIdx.x / bpg;
 	const int k0 = (int)(blockIdx.x % bpg) * nl;
@@ -783,7 +782,6 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads, p
 	auto ld1 = [X, pitch](int line, int i) { return X[tat(line, i, pitch)]; };
 	auto st_g = [g, P, k0](int line, int i, const C &v, C *) { g[(long)i * P + k0 + line] = v; };
 	fft_fx<R1, R2, -1, false, true>(nl, pitch, p.pl, T.tw, X == T.a ? T.b : T.a, X, ld1, st_g);
-	(void)mgP; (void)mgnl;
 }
 
 // I3 chain, last rows: forward transforms of Y[(cell nt + tt) 16 + 4 j + i],

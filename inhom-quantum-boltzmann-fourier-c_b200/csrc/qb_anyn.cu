@@ -486,15 +486,16 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		return v;
 	}, [&](int i, const C &v) {
 		const int li = fdiv(i, mgP), k = i - li * P;
-		T.a[T.at(li, k)] = v;
+		T.b[T.at(li, k)] = v;
 	});
 	__syncthreads();
-	const C *r = fft_lines_x<R1, R2, -1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+	// staged in b; the last stage stores the rows to global memory
 	C *o = p.out + u * PP + (long)l0 * P;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = fdiv(i, mgP), k = i - li * P;
-		o[(long)li * P + k] = r[T.at(li, k)];
-	}
+	const int pitch = T.pitch;
+	const C *sb = T.b;
+	auto ld0 = [sb, pitch](int line, int i) { return sb[tat(line, i, pitch)]; };
+	auto st1 = [o, P](int line, int i, const C &v, C *) { o[(long)line * P + i] = v; };
+	fft_fx<R1, R2, -1, false, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
 }
 
 // in-place row or column transforms of L x L grids g[u] (spectra, FS, the
@@ -526,15 +527,19 @@ template <class C, int DIR, bool COLS, int R1, int R2> __global__ void __launch_
 		const int li = fdiv(i, mgP), k = i - li * L;
 		return g[(long)(x0 + li) * L + k];
 	}, [&](int i, const C &v) {
-		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; T.a[T.at(kk, l)] = v; }
-		else { const int li = fdiv(i, mgP), k = i - li * L; T.a[T.at(li, k)] = v; }
+		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; T.b[T.at(kk, l)] = v; }
+		else { const int li = fdiv(i, mgP), k = i - li * L; T.b[T.at(li, k)] = v; }
 	});
 	__syncthreads();
-	const C *r = fft_lines_x<R1, R2, DIR>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
-	for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-		if (COLS) { const int l = fdiv(i, mgnl), kk = i - l * nl; g[(long)l * L + x0 + kk] = r[T.at(kk, l)]; }
-		else { const int li = fdiv(i, mgP), k = i - li * L; g[(long)(x0 + li) * L + k] = r[T.at(li, k)]; }
-	}
+	// staged in b; the last stage stores to global memory in the coalesced order
+	const int pitch = T.pitch;
+	const C *sb = T.b;
+	auto ld0 = [sb, pitch](int line, int i) { return sb[tat(line, i, pitch)]; };
+	auto st1 = [g, L, x0](int line, int i, const C &v, C *) {
+		if (COLS) g[(long)i * L + x0 + line] = v;
+		else g[(long)(x0 + line) * L + i] = v;
+	};
+	fft_fx<R1, R2, DIR, false, COLS>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
 }
 
 // I1 / I4 columns of unit u = (cell nt + tt) nsub + sub: forward transform,
@@ -719,7 +724,7 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 		}, [&](int i, const Two<C> &v) {
 			const int li = fdiv(i, mgP), k = i - li * P;
 			const typename CT<C>::R pj = im ? v.b.y : v.b.x;
-			T.a[T.at(li, k)] = cscale(v.a, pj);
+			T.b[T.at(li, k)] = cscale(v.a, pj);
 		});
 	} else {
 		const C *G = p.What + (cell * 4 + (c & 3)) * PP + (long)l0 * P;
@@ -731,16 +736,17 @@ template <class C, int R1, int R2> __global__ void __launch_bounds__(kThreads) k
 			return v;
 		}, [&](int i, const Two<C> &v) {
 			const int li = fdiv(i, mgP), k = i - li * P;
-			T.a[T.at(li, k)] = cmul(v.a, v.b);
+			T.b[T.at(li, k)] = cmul(v.a, v.b);
 		});
 	}
 	__syncthreads();
-	const C *r = fft_lines_x<R1, R2, +1>(T.a, T.b, nl, T.pitch, 1, p.pl, T.tw);
+	// staged in b; the last stage stores the rows to global memory
 	C *o = p.Y + u * PP + (long)l0 * P;
-	for (int i = threadIdx.x; i < nl * P; i += blockDim.x) {
-		const int li = fdiv(i, mgP), k = i - li * P;
-		o[(long)li * P + k] = r[T.at(li, k)];
-	}
+	const int pitch = T.pitch;
+	const C *sb = T.b;
+	auto ld0 = [sb, pitch](int line, int i) { return sb[tat(line, i, pitch)]; };
+	auto st1 = [o, P](int line, int i, const C &v, C *) { o[(long)line * P + i] = v; };
+	fft_fx<R1, R2, +1, false, false>(nl, pitch, p.pl, T.tw, T.a, T.b, ld0, st1);
 }
 
 // I3 chain, columns of Y[u]: inverse transform, times psi2_t (element (l, k)
